@@ -1,0 +1,313 @@
+"""Benchmark: shot solves/s of the batched eikonal solve on 201x201x101 nodes.
+
+Workload (one step): the config-2 batch -- 64 shots on a jittered 8x8 surface grid over a
+201x201x101 model at 12.5 m (three dipping layers + eight +-10 % anomalies), each on a
+brick-aligned window covering 60-100 % of the lateral extent, all solved by one persistent
+launch; 2,500 surface receivers (50x50) sampled per shot.  Synthetic seeded data.
+
+  value  shots/s with the model resident in HBM (CUDA events on the library's stream)
+  e2e    shots/s through the C ABI with host buffers: pinned velocity upload (16.3 MB) +
+         solve + receiver-times download every step
+  roofline  dominant kernel (k_fim_solve): algorithmic bytes = brick activations x 64
+         nodes x 12 B (slowness + traveltime in + traveltime out) / its event time
+  cpu_baseline  the reference's own Accurate_FSM (compiled unmodified into oracle/_ref)
+         on a bounded sample of the same shots and windows, all host threads
+
+``--impl reference`` times the reference's CPU eikonal path (Accurate_FSM) the same way.
+Multi-GPU (torchrun): shots are independent, each rank solves its own 64-shot batch (weak
+scaling, no data-path collective); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "shot solves/s on 201x201x101, learned-warm vs plain FIM, at 1e-4 rel err"
+UNIT = "shots/s"
+BYTES_PER_NODE_ACT = 12  # slowness read + traveltime read + traveltime write (float32)
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.stop = threading.Event()
+        self.th = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.th.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 5 + i and s[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def workload(rank):
+    from seismic_tomography_3d_b200 import workloads as wl
+
+    return wl.config2(seed=2 + 1000 * rank)
+
+
+def cpu_reference_sample(sv, max_shots=None, budget_s=20.0):
+    """The reference Accurate_FSM (oracle/_ref) on the host cores over the batch's own
+    shots and windows.  Returns (shots/s, threads, sample description)."""
+    import oracle
+
+    nthreads = os.cpu_count() or 1
+    nshots = len(sv.shots) if max_shots is None else min(max_shots, len(sv.shots))
+    # windows differ per shot: group shots by window so each group is one cropped model
+    t_start = time.perf_counter()
+    done = 0
+    solve_s = 0.0
+    groups = {}
+    for i in range(nshots):
+        key = tuple(int(v) for v in sv.windows[i]) if sv.windows is not None else (0, sv.nx, 0, sv.ny)
+        groups.setdefault(key, []).append(i)
+    # one shot per window here: run windows in parallel by packing them into threads
+    import concurrent.futures as cf
+
+    def run_one(key_idx):
+        (x0, x1, y0, y1), idx = key_idx
+        vel = np.ascontiguousarray(sv.velocity[y0:y1, x0:x1, :])
+        shots = sv.shots[idx].copy()
+        shots[:, 0] -= np.float32(x0) * np.float32(sv.h)
+        shots[:, 1] -= np.float32(y0) * np.float32(sv.h)
+        _, secs = oracle.ref_solve(oracle.REF_FSM, vel, sv.h, shots, nthreads=1, want_T=False)
+        return len(idx), float(np.sum(secs))
+
+    items = list(groups.items())
+    with oracle.quiet_stdout():
+        with cf.ThreadPoolExecutor(max_workers=nthreads) as ex:
+            futs = []
+            for it in items:
+                futs.append(ex.submit(run_one, it))
+            for f in futs:
+                n, s = f.result()
+                done += n
+                solve_s += s
+                if time.perf_counter() - t_start > budget_s:
+                    break
+            for f in futs:
+                f.cancel()
+    wall = time.perf_counter() - t_start
+    desc = (f"reference Accurate_FSM (NGB 2014 FSM, oracle/_ref, g++ -O3) on {done} of the batch's shots "
+            f"(own windows), {nthreads} host threads, {wall:.1f} s wall")
+    return done / wall, nthreads, desc
+
+
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return 0
+    sv = workload(0)
+    per_step = []
+    desc = ""
+    threads = os.cpu_count() or 1
+    sample = min(len(sv.shots), max(8, 2 * threads))
+    for i in range(args.warmup + args.steps):
+        rate, threads, desc = cpu_reference_sample(sv, max_shots=sample, budget_s=60.0)
+        if i >= args.warmup:
+            per_step.append(rate)
+    value = float(statistics.median(per_step))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sample / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded config-2 model, shots, windows)",
+            "config": {"workload": "config2: 64 shots, 201x201x101 @12.5 m, windows 60-100 %",
+                       "sample_shots_per_step": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    import seismic_tomography_3d_b200 as tomo
+
+    rank, world, local = rank_info()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    sv = workload(rank)
+    ns = len(sv.shots)
+    ctx = tomo.Context(sv.nx, sv.ny, sv.nz, sv.h, device=local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    vel_pinned = torch.from_numpy(sv.velocity.copy()).pin_memory()
+    ctx.set_velocity(sv.velocity)
+
+    def step_resident():
+        _, st = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=False)
+        return st
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step_resident()
+    # ---- value: model resident ---------------------------------------------------------
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            stats.append(step_resident())
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * ns / (ms_max / 1000.0)
+
+    # ---- e2e: host buffers through the C ABI ---------------------------------------------
+    nrec = len(sv.receivers)
+    t_out = np.empty((ns, nrec), np.float32)
+    lib = ctx.lib
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        tomo_rc = lib.tomo_set_velocity(ctx.h, vel_pinned.data_ptr())
+        assert tomo_rc == 0
+        t_out, _ = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=True)
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * ns / (e2e_ms / 1000.0)
+
+    # ---- roofline of the dominant kernel -----------------------------------------------
+    act = statistics.mean(s["activations"] for s in stats)
+    kern_ms = statistics.mean(s["solve_ms"] for s in stats)
+    alg_bytes = act * stats[0]["nodes_per_brick"] * BYTES_PER_NODE_ACT
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (kern_ms / 1000.0) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "k_fim_solve_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded config-2 model, shots, windows, receivers)",
+            "config": {"workload": "config2: 64 shots/GPU, 201x201x101 @12.5 m, brick-aligned windows "
+                                   "60-100 % lateral, 2500 receivers, plain FIM (JW operator)",
+                       "shots_per_gpu": ns, "grid": [sv.nx, sv.ny, sv.nz], "h_m": sv.h,
+                       "l2": "traveltime pool 1.1 GB > 126 MB L2 (inputs larger than L2)",
+                       "parallelism": f"shot-sharded x{world}"},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": int(sv.velocity.nbytes),
+                    "d2h_bytes_per_step": int(t_out.nbytes) if t_out is not None else 0},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_fim_solve", "kernel_ms": kern_ms,
+                         "alg_bytes_per_launch": alg_bytes, "activations_per_launch": act},
+            "clocks": clk.summary(),
+            "gpu_launches": 3 * args.steps,
+            "solver": {"rounds": stats[-1]["rounds"], "activations": stats[-1]["activations"],
+                       "inner_iterations": stats[-1]["inner_iterations"]}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, desc = cpu_reference_sample(sv, max_shots=min(ns, max(8, 2 * (os.cpu_count() or 1))),
+                                                 budget_s=25.0)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

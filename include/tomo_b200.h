@@ -1,0 +1,135 @@
+/*
+ * tomo_b200 -- B200-native (sm_100a) hot path of 3D first-arrival traveltime tomography:
+ * batched eikonal solve -> ray tracing into a sparse Frechet matrix -> CGLS -> model
+ * update.  Plain C ABI: opaque context, plain pointers and sizes, int status codes.
+ *
+ * Conventions
+ *  - Volumes are float32, z fastest, then x, then y: idx = z + x*nz + y*nx*nz, exactly
+ *    the reference layout (src/eikonal/block_FIM/block_FIM.cpp:17, files written by
+ *    numpy as (nz,nx,ny) Fortran order, src/utils/py_codes/functions.py:23-25).
+ *  - Positions are metres from the model origin; shot i / receiver r order is the
+ *    caller's (the reference's Geometry x/y/z arrays, src/geometry/geometry.hpp:21-24).
+ *  - Every call returns TOMO_OK (0) or a negative TOMO_ERR_*; tomo_last_error(ctx) gives
+ *    a message.  Nothing crosses the ABI as an exception and nothing calls exit().
+ *  - Host buffers belong to the caller and are only read/written during the call.
+ *    Device memory belongs to the context.  One host thread per context at a time.
+ *  - All device work of a context runs on one CUDA stream (its own, or the one given to
+ *    tomo_ctx_create_on_stream); calls return after that work completes.
+ */
+#ifndef TOMO_B200_H
+#define TOMO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TOMO_OK                 0
+#define TOMO_ERR_INVALID_ARG   -1  /* bad sizes, pointers, positions outside the model */
+#define TOMO_ERR_OOM           -2  /* device allocation failed                          */
+#define TOMO_ERR_CUDA          -3  /* CUDA runtime error (message has the detail)       */
+#define TOMO_ERR_NOT_CONVERGED -4  /* eikonal round cap reached before the fixed point  */
+#define TOMO_ERR_TIMEOUT       -5  /* a device-side wait hit its iteration limit        */
+#define TOMO_ERR_STATE         -6  /* call order (no model / no solve / no Jacobian)    */
+#define TOMO_ERR_IO            -7  /* file could not be opened / short read             */
+#define TOMO_ERR_NO_DEVICE     -8  /* no CUDA device, or not sm_100                      */
+#define TOMO_ERR_CAPACITY      -9  /* a fixed device capacity was exceeded              */
+
+typedef struct tomo_ctx tomo_ctx;
+
+/* Model grid: x_samples, y_samples, z_samples and x/y/z_spacing of parameters.txt
+ * (run/parameters.txt:5-11). */
+typedef struct {
+    int nx, ny, nz;
+    float dx, dy, dz;
+} tomo_grid;
+
+typedef struct {
+    float x, y, z;
+} tomo_point;
+
+/* Lateral solve window of one shot: nodes [x0,x1) x [y0,y1), full depth.  x0, y0 must be
+ * multiples of 4; x1 (y1) must be a multiple of 4 or equal nx (ny).  Each windowed solve
+ * equals the reference solve on the model cropped to that window. */
+typedef struct {
+    int x0, x1, y0, y1;
+} tomo_window;
+
+/* Local Godunov operator of the eikonal solve. */
+#define TOMO_OP_JW  0  /* Jeong & Whitaker 2008 first-order update, isotropic h = dx, single
+                          node source seed: Block_FIM (src/eikonal/block_FIM/cuda_kernel.cu:217-248) */
+
+typedef struct {
+    int op;          /* TOMO_OP_*                                                     */
+    int max_inner;   /* cap of in-brick iterations per activation (0: default 16)     */
+    int max_rounds;  /* cap of outer rounds (0: default 1<<20)                        */
+    int brick;       /* brick shape id (0: tuned default); see tomo_eik_brick_shapes  */
+    int block_warps; /* warps per CTA of the persistent kernel (0: default)           */
+} tomo_eik_opts;
+
+typedef struct {
+    long long rounds;            /* outer rounds of the persistent solve                  */
+    long long activations;       /* brick activations (sum over shots)                    */
+    long long inner_iterations;  /* sum over activations of in-brick iterations           */
+    long long nodes_per_brick;   /* nodes of one brick                                    */
+    float setup_ms;              /* device time of the pool reset + seeding kernels       */
+    float solve_ms;              /* device time of the persistent solve kernel             */
+    float total_ms;              /* device time of the whole call incl. copies             */
+} tomo_eik_stats;
+
+/* ---------------------------------------------------------------- context ---------- */
+/* Replaces Eikonal::set_parameters + prepare_volumes (src/eikonal/eikonal.hpp:48-49) for
+ * the device side: binds device `device` (must be sm_100) and records the grid. */
+int tomo_ctx_create(const tomo_grid *grid, int device, tomo_ctx **out);
+/* Same, but all device work is enqueued on the caller's stream (a cudaStream_t). */
+int tomo_ctx_create_on_stream(const tomo_grid *grid, int device, void *stream, tomo_ctx **out);
+/* Replaces Eikonal::destroy_volumes (eikonal.hpp:57). */
+int tomo_ctx_destroy(tomo_ctx *ctx);
+const char *tomo_last_error(const tomo_ctx *ctx);
+const char *tomo_status_string(int status);
+/* The cudaStream_t the context enqueues on. */
+void *tomo_ctx_stream(tomo_ctx *ctx);
+
+/* --------------------------------------------------------------- the model --------- */
+/* Velocity model (m/s), host, nz*nx*ny; slowness = 1/v as Eikonal::set_parameters does
+ * (block_FIM.cpp:85-91). */
+int tomo_set_velocity(tomo_ctx *ctx, const float *velocity);
+/* Slowness model (s/m), host, nz*nx*ny. */
+int tomo_set_slowness(tomo_ctx *ctx, const float *slowness);
+/* Copies the current slowness (after model updates) to the host. */
+int tomo_get_slowness(tomo_ctx *ctx, float *slowness_out);
+
+/* ------------------------------------------------------------ eikonal solve --------- */
+/* Solves nshots first-arrival traveltime fields in ONE persistent launch.
+ * Replaces the per-shot loop of Eikonal::eikonal_equation + write_first_arrival
+ * (src/eikonal/eikonal_main.cpp:31-39, src/tomography/least_squares/least_squares.cpp:172-183;
+ * device part: block_FIM_solver, src/eikonal/block_FIM/cuda_kernel.cu:17-215).
+ *   shots      nshots source positions (metres)
+ *   windows    NULL (full model) or nshots windows
+ *   receivers  nrec receiver positions (may be NULL if nrec == 0)
+ *   t_recv     host nshots*nrec (row-major shot, receiver) receiver times by trilinear
+ *              interpolation (block_FIM.cpp:228-262); NULL keeps them on the device only
+ *   opts/stats may be NULL.
+ * Traveltime fields stay on the device for tomo_eik_volume / tomo_raytrace. */
+int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows,
+                   int nrec, const tomo_point *receivers, float *t_recv,
+                   const tomo_eik_opts *opts, tomo_eik_stats *stats);
+
+/* Copies the traveltime field of shot `shot` of the last solve to the host, cropped to
+ * its window: wz*wx*wy floats (z fastest) -- Eikonal::travel_time after
+ * eikonal_equation (block_FIM.cpp:59-69, 371-401). */
+int tomo_eik_volume(tomo_ctx *ctx, int shot, float *t_out);
+
+/* Window extents of shot `shot` of the last solve (nodes). */
+int tomo_eik_window(tomo_ctx *ctx, int shot, tomo_window *out);
+
+/* Brick shapes the solver supports: writes up to `cap` triples (bx,by,bz) of nodes and
+ * returns how many there are. */
+int tomo_eik_brick_shapes(int *xyz_triples, int cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TOMO_B200_H */

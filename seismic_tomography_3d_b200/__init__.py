@@ -1,0 +1,203 @@
+"""seismic_tomography_3d_b200 -- Python view of the libtomo_b200 C ABI.
+
+The product is the shared library ``_lib/libtomo_b200.so`` (CUDA kernels for sm_100a plus
+the C ABI declared in ``include/tomo_b200.h``).  This module only binds it with ctypes for
+tests, benchmarks and scripting; every call goes straight through the C ABI.  There is no
+CPU fallback: without the library or an sm_100 GPU the calls raise.
+
+Array convention: a volume is a numpy array of shape (ny, nx, nz) in C order, which is
+exactly the reference's z-fastest layout ``idx = z + x*nz + y*nx*nz``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "_lib", "libtomo_b200.so")
+INCLUDE_DIR = os.path.join(os.path.dirname(_PKG), "include")
+
+TOMO_OK = 0
+ERRORS = {
+    -1: "TOMO_ERR_INVALID_ARG", -2: "TOMO_ERR_OOM", -3: "TOMO_ERR_CUDA", -4: "TOMO_ERR_NOT_CONVERGED",
+    -5: "TOMO_ERR_TIMEOUT", -6: "TOMO_ERR_STATE", -7: "TOMO_ERR_IO", -8: "TOMO_ERR_NO_DEVICE",
+    -9: "TOMO_ERR_CAPACITY",
+}
+
+
+class TomoError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{ERRORS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("dx", ctypes.c_float), ("dy", ctypes.c_float), ("dz", ctypes.c_float)]
+
+
+class Point(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_float), ("y", ctypes.c_float), ("z", ctypes.c_float)]
+
+
+class Window(ctypes.Structure):
+    _fields_ = [("x0", ctypes.c_int), ("x1", ctypes.c_int), ("y0", ctypes.c_int), ("y1", ctypes.c_int)]
+
+
+class EikOpts(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_int), ("max_inner", ctypes.c_int), ("max_rounds", ctypes.c_int),
+                ("brick", ctypes.c_int), ("block_warps", ctypes.c_int)]
+
+
+class EikStats(ctypes.Structure):
+    _fields_ = [("rounds", ctypes.c_longlong), ("activations", ctypes.c_longlong),
+                ("inner_iterations", ctypes.c_longlong), ("nodes_per_brick", ctypes.c_longlong),
+                ("setup_ms", ctypes.c_float), ("solve_ms", ctypes.c_float), ("total_ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libtomo_b200.so (raises if it has not been built: no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libtomo_b200.so not built ({path}); run "
+                           "`python -m seismic_tomography_3d_b200.build`")
+    lib = ctypes.CDLL(path)
+    P, I, F, V = ctypes.POINTER, ctypes.c_int, ctypes.c_float, ctypes.c_void_p
+    lib.tomo_ctx_create.argtypes = [P(Grid), I, P(V)]
+    lib.tomo_ctx_create_on_stream.argtypes = [P(Grid), I, V, P(V)]
+    lib.tomo_ctx_destroy.argtypes = [V]
+    lib.tomo_last_error.argtypes = [V]
+    lib.tomo_last_error.restype = ctypes.c_char_p
+    lib.tomo_status_string.argtypes = [I]
+    lib.tomo_status_string.restype = ctypes.c_char_p
+    lib.tomo_ctx_stream.argtypes = [V]
+    lib.tomo_ctx_stream.restype = V
+    lib.tomo_set_velocity.argtypes = [V, V]
+    lib.tomo_set_slowness.argtypes = [V, V]
+    lib.tomo_get_slowness.argtypes = [V, V]
+    lib.tomo_eik_solve.argtypes = [V, I, P(Point), P(Window), I, P(Point), V, P(EikOpts), P(EikStats)]
+    lib.tomo_eik_volume.argtypes = [V, I, V]
+    lib.tomo_eik_window.argtypes = [V, I, P(Window)]
+    lib.tomo_eik_brick_shapes.argtypes = [P(I), I]
+    _bind_tomography(lib)
+    _lib = lib
+    return lib
+
+
+def _bind_tomography(lib):
+    """Bindings of the tomography half of the ABI (filled in as it grows)."""
+
+
+def _points(a):
+    a = np.asarray(a, np.float32).reshape(-1, 3)
+    arr = (Point * max(len(a), 1))()
+    for i, (x, y, z) in enumerate(a):
+        arr[i].x, arr[i].y, arr[i].z = float(x), float(y), float(z)
+    return arr, len(a)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Context:
+    """One device context (tomo_ctx) over a model grid."""
+
+    def __init__(self, nx, ny, nz, dx, dy=None, dz=None, device=0, stream=None):
+        self.lib = load_library()
+        self.grid = Grid(nx, ny, nz, dx, dy if dy is not None else dx, dz if dz is not None else dx)
+        self.shape = (ny, nx, nz)
+        h = ctypes.c_void_p()
+        if stream is None:
+            rc = self.lib.tomo_ctx_create(ctypes.byref(self.grid), device, ctypes.byref(h))
+        else:
+            rc = self.lib.tomo_ctx_create_on_stream(ctypes.byref(self.grid), device, ctypes.c_void_p(stream),
+                                                    ctypes.byref(h))
+        if rc != TOMO_OK:
+            raise TomoError(rc, self.lib.tomo_status_string(rc).decode())
+        self.h = h
+
+    # -- plumbing ---------------------------------------------------------------------
+    def _check(self, rc):
+        if rc != TOMO_OK:
+            raise TomoError(rc, self.lib.tomo_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tomo_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream(self):
+        return self.lib.tomo_ctx_stream(self.h)
+
+    # -- model --------------------------------------------------------------------------
+    def set_velocity(self, v):
+        v = _f32(v)
+        assert v.shape == self.shape, (v.shape, self.shape)
+        self._check(self.lib.tomo_set_velocity(self.h, v.ctypes.data))
+
+    def set_slowness(self, s):
+        s = _f32(s)
+        assert s.shape == self.shape
+        self._check(self.lib.tomo_set_slowness(self.h, s.ctypes.data))
+
+    def get_slowness(self):
+        out = np.empty(self.shape, np.float32)
+        self._check(self.lib.tomo_get_slowness(self.h, out.ctypes.data))
+        return out
+
+    # -- eikonal ------------------------------------------------------------------------
+    def eik_solve(self, shots, windows=None, receivers=None, want_recv=True, max_inner=0, max_rounds=0,
+                  block_warps=0, op=0):
+        """Batched solve.  shots (n,3) metres; windows (n,4) [x0,x1,y0,y1] nodes or None;
+        receivers (m,3).  Returns (t_recv (n,m) float32 or None, stats dict)."""
+        sp, ns = _points(shots)
+        wp = None
+        if windows is not None:
+            w = np.asarray(windows, np.int32).reshape(-1, 4)
+            wp = (Window * len(w))(*[Window(*map(int, row)) for row in w])
+        nr = 0
+        rp = None
+        if receivers is not None and len(receivers):
+            rp, nr = _points(receivers)
+        out = np.empty((ns, nr), np.float32) if (want_recv and nr) else None
+        opts = EikOpts(op, max_inner, max_rounds, 0, block_warps)
+        st = EikStats()
+        self._check(self.lib.tomo_eik_solve(self.h, ns, sp, wp, nr, rp,
+                                            out.ctypes.data if out is not None else None,
+                                            ctypes.byref(opts), ctypes.byref(st)))
+        return out, st.as_dict()
+
+    def eik_window(self, shot):
+        w = Window()
+        self._check(self.lib.tomo_eik_window(self.h, shot, ctypes.byref(w)))
+        return (w.x0, w.x1, w.y0, w.y1)
+
+    def eik_volume(self, shot):
+        x0, x1, y0, y1 = self.eik_window(shot)
+        out = np.empty((y1 - y0, x1 - x0, self.grid.nz), np.float32)
+        self._check(self.lib.tomo_eik_volume(self.h, shot, out.ctypes.data))
+        return out

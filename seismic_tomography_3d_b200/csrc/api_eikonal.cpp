@@ -1,0 +1,390 @@
+// C ABI: context, model and batched eikonal solve (include/tomo_b200.h).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "common.cuh"
+#include "context.hpp"
+
+using tomo::ShotDesc;
+
+namespace {
+
+constexpr int kDefaultMaxInner = 16;
+constexpr int kDefaultMaxRounds = 1 << 20;
+constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~ seconds of polling, then error
+
+int fail(tomo_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(tomo_ctx *c, cudaError_t e, const char *where)
+{
+    const int code = (e == cudaErrorMemoryAllocation) ? TOMO_ERR_OOM : TOMO_ERR_CUDA;
+    return fail(c, code, std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);   \
+    } while (0)
+
+int pad4(int n) { return n + (tomo::kBrick - n % tomo::kBrick) % tomo::kBrick; }
+
+int upload_model(tomo_ctx *ctx, const float *host, bool is_velocity)
+{
+    const size_t n = (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz;
+    CK(ctx->slow.ensure(n));
+    if (is_velocity) {
+        CK(ctx->scratch_v.ensure(n));
+        CK(cudaMemcpyAsync(ctx->scratch_v.ptr, host, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        CK(tomo::velocity_to_slowness(ctx->scratch_v.ptr, ctx->slow.ptr, n, ctx->stream));
+    } else {
+        CK(cudaMemcpyAsync(ctx->slow.ptr, host, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CK(ctx->S.ensure((size_t)ctx->nxx * ctx->nyy * ctx->nzz));
+    CK(tomo::fim_brick_model(ctx->slow.ptr, ctx->S.ptr, ctx->g.nx, ctx->g.ny, ctx->g.nz, ctx->nxx, ctx->nyy,
+                             ctx->nzz, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->have_model = true;
+    return TOMO_OK;
+}
+
+}  // namespace
+
+namespace tomo {
+// Re-brick the device model after it changed on the device (model update).
+int rebrick_model(tomo_ctx *ctx)
+{
+    CK(fim_brick_model(ctx->slow.ptr, ctx->S.ptr, ctx->g.nx, ctx->g.ny, ctx->g.nz, ctx->nxx, ctx->nyy, ctx->nzz,
+                       ctx->stream));
+    return TOMO_OK;
+}
+}  // namespace tomo
+
+extern "C" {
+
+const char *tomo_status_string(int s)
+{
+    switch (s) {
+    case TOMO_OK: return "ok";
+    case TOMO_ERR_INVALID_ARG: return "invalid argument";
+    case TOMO_ERR_OOM: return "out of device memory";
+    case TOMO_ERR_CUDA: return "CUDA error";
+    case TOMO_ERR_NOT_CONVERGED: return "eikonal solve did not converge within the round cap";
+    case TOMO_ERR_TIMEOUT: return "device-side wait timed out";
+    case TOMO_ERR_STATE: return "call order (missing model, solve or Jacobian)";
+    case TOMO_ERR_IO: return "file could not be opened";
+    case TOMO_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    case TOMO_ERR_CAPACITY: return "device capacity exceeded";
+    default: return "unknown status";
+    }
+}
+
+int tomo_ctx_create_on_stream(const tomo_grid *grid, int device, void *stream, tomo_ctx **out)
+{
+    if (!out) return TOMO_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (!grid || grid->nx < 2 || grid->ny < 2 || grid->nz < 2 || !(grid->dx > 0) || !(grid->dy > 0) ||
+        !(grid->dz > 0))
+        return TOMO_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return TOMO_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) return TOMO_ERR_NO_DEVICE;
+    if (!prop.cooperativeLaunch) return TOMO_ERR_NO_DEVICE;
+    tomo_ctx *ctx = new (std::nothrow) tomo_ctx();
+    if (!ctx) return TOMO_ERR_OOM;
+    ctx->g = *grid;
+    ctx->device = device;
+    ctx->nxx = pad4(grid->nx);
+    ctx->nyy = pad4(grid->ny);
+    ctx->nzz = pad4(grid->nz);
+    ctx->gbx = ctx->nxx / tomo::kBrick;
+    ctx->gby = ctx->nyy / tomo::kBrick;
+    ctx->gbz = ctx->nzz / tomo::kBrick;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) {
+        if (stream) {
+            ctx->stream = static_cast<cudaStream_t>(stream);
+        } else {
+            e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+            ctx->own_stream = (e == cudaSuccess);
+        }
+    }
+    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&ctx->pinned_ctrl), 64 * sizeof(unsigned));
+    if (e == cudaSuccess) e = ctx->ctrl.ensure(tomo::kCtrlWords);
+    if (e == cudaSuccess) e = ctx->stats.ensure(4);
+    if (e != cudaSuccess) {
+        tomo_ctx_destroy(ctx);
+        return e == cudaErrorMemoryAllocation ? TOMO_ERR_OOM : TOMO_ERR_CUDA;
+    }
+    *out = ctx;
+    return TOMO_OK;
+}
+
+int tomo_ctx_create(const tomo_grid *grid, int device, tomo_ctx **out)
+{
+    return tomo_ctx_create_on_stream(grid, device, nullptr, out);
+}
+
+void tomo_release_tomography(tomo_ctx *ctx);  // api_tomography.cpp
+
+int tomo_ctx_destroy(tomo_ctx *ctx)
+{
+    if (!ctx) return TOMO_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    tomo_release_tomography(ctx);
+    ctx->slow.release();
+    ctx->S.release();
+    ctx->scratch_v.release();
+    ctx->T.release();
+    ctx->qflag.release();
+    ctx->lists.release();
+    ctx->ctrl.release();
+    ctx->stats.release();
+    ctx->shots_d.release();
+    ctx->rec.release();
+    ctx->t_recv.release();
+    for (auto &ev : ctx->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->pinned_ctrl) cudaFreeHost(ctx->pinned_ctrl);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return TOMO_OK;
+}
+
+const char *tomo_last_error(const tomo_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void *tomo_ctx_stream(tomo_ctx *ctx) { return ctx ? static_cast<void *>(ctx->stream) : nullptr; }
+
+int tomo_set_velocity(tomo_ctx *ctx, const float *velocity)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (!velocity) return fail(ctx, TOMO_ERR_INVALID_ARG, "velocity is NULL");
+    CK(cudaSetDevice(ctx->device));
+    return upload_model(ctx, velocity, true);
+}
+
+int tomo_set_slowness(tomo_ctx *ctx, const float *slowness)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (!slowness) return fail(ctx, TOMO_ERR_INVALID_ARG, "slowness is NULL");
+    CK(cudaSetDevice(ctx->device));
+    return upload_model(ctx, slowness, false);
+}
+
+int tomo_get_slowness(tomo_ctx *ctx, float *out)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (!out) return fail(ctx, TOMO_ERR_INVALID_ARG, "output is NULL");
+    if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set");
+    CK(cudaSetDevice(ctx->device));
+    const size_t n = (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz;
+    CK(cudaMemcpyAsync(out, ctx->slow.ptr, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TOMO_OK;
+}
+
+int tomo_eik_brick_shapes(int *xyz, int cap)
+{
+    if (xyz && cap >= 1) {
+        xyz[0] = xyz[1] = xyz[2] = tomo::kBrick;
+    }
+    return 1;
+}
+
+int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows, int nrec,
+                   const tomo_point *receivers, float *t_recv, const tomo_eik_opts *opts,
+                   tomo_eik_stats *stats)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (nshots < 1 || !shots) return fail(ctx, TOMO_ERR_INVALID_ARG, "nshots must be >= 1 with shot positions");
+    if (nrec < 0 || (nrec > 0 && !receivers)) return fail(ctx, TOMO_ERR_INVALID_ARG, "bad receivers");
+    if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
+    if (opts && opts->op != TOMO_OP_JW) return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown eikonal operator");
+    const tomo_grid &g = ctx->g;
+    const int max_inner = (opts && opts->max_inner > 0) ? opts->max_inner : kDefaultMaxInner;
+    const int max_rounds = (opts && opts->max_rounds > 0) ? opts->max_rounds : kDefaultMaxRounds;
+    const int block_warps = (opts && opts->block_warps > 0) ? opts->block_warps : 8;
+    CK(cudaSetDevice(ctx->device));
+
+    // ---- per-shot descriptors --------------------------------------------------------
+    std::vector<ShotDesc> sd((size_t)nshots);
+    long long t_total = 0;
+    unsigned long long q_total = 0;
+    int max_bricks = 1;
+    for (int s = 0; s < nshots; s++) {
+        tomo_window w{0, g.nx, 0, g.ny};
+        if (windows) w = windows[s];
+        if (w.x0 < 0 || w.y0 < 0 || w.x1 > g.nx || w.y1 > g.ny || w.x1 - w.x0 < 2 || w.y1 - w.y0 < 2 ||
+            w.x0 % tomo::kBrick || w.y0 % tomo::kBrick || (w.x1 % tomo::kBrick && w.x1 != g.nx) ||
+            (w.y1 % tomo::kBrick && w.y1 != g.ny))
+            return fail(ctx, TOMO_ERR_INVALID_ARG,
+                        "window " + std::to_string(s) + ": origin must be a multiple of 4 and the end a "
+                        "multiple of 4 or the model edge");
+        ShotDesc &d = sd[(size_t)s];
+        d.wx0 = w.x0;
+        d.wy0 = w.y0;
+        d.wnx = w.x1 - w.x0;
+        d.wny = w.y1 - w.y0;
+        d.nbx = pad4(d.wnx) / tomo::kBrick;
+        d.nby = pad4(d.wny) / tomo::kBrick;
+        d.nbz = ctx->gbz;
+        // Source seed in window coordinates (Block_FIM::apply_source_time, block_FIM.cpp:305-317).
+        const float sx = shots[s].x - (float)w.x0 * g.dx;
+        const float sy = shots[s].y - (float)w.y0 * g.dy;
+        const float sz = shots[s].z;
+        if (!(sx >= 0.f) || !(sy >= 0.f) || !(sz >= 0.f))
+            return fail(ctx, TOMO_ERR_INVALID_ARG, "shot " + std::to_string(s) + " outside its window");
+        const int sidx = (int)(sx / g.dx), sidy = (int)(sy / g.dy), sidz = (int)(sz / g.dz);
+        if (sidx >= d.wnx || sidy >= d.wny || sidz >= g.nz)
+            return fail(ctx, TOMO_ERR_INVALID_ARG, "shot " + std::to_string(s) + " outside its window");
+        const float ex = (float)(sidx * g.dx) - sx, ey = (float)(sidy * g.dy) - sy, ez = (float)(sidz * g.dz) - sz;
+        d.src_dist = std::sqrt(std::pow(ex, 2.0f) + std::pow(ey, 2.0f) + std::pow(ez, 2.0f));
+        d.src_brick = (sidz >> 2) + d.nbz * ((sidx >> 2) + d.nbx * (sidy >> 2));
+        d.src_node = (sidz & 3) + 4 * (sidx & 3) + 16 * (sidy & 3);
+        const long long nb = (long long)d.nbx * d.nby * d.nbz;
+        d.t_off = t_total;
+        d.qbase = q_total;
+        t_total += nb * tomo::kBrickNodes;
+        q_total += (unsigned long long)nb;
+        if (nb > max_bricks) max_bricks = (int)nb;
+    }
+    unsigned local_bits = 1;
+    while ((1ll << local_bits) < max_bricks) local_bits++;
+    if (local_bits + 1 >= 32 || ((unsigned long long)nshots << local_bits) >= (1ull << 32))
+        return fail(ctx, TOMO_ERR_CAPACITY, "too many shots x bricks for one batch; split the batch");
+    for (int r = 0; r < nrec; r++) {
+        const tomo_point &p = receivers[r];
+        if (!(p.x >= 0.f) || !(p.y >= 0.f) || !(p.z >= 0.f) || p.x > (g.nx - 1) * g.dx || p.y > (g.ny - 1) * g.dy ||
+            p.z > (g.nz - 1) * g.dz)
+            return fail(ctx, TOMO_ERR_INVALID_ARG, "receiver " + std::to_string(r) + " outside the model");
+    }
+
+    // ---- buffers ----------------------------------------------------------------------
+    CK(ctx->T.ensure((size_t)t_total));
+    CK(ctx->qflag.ensure((size_t)q_total));
+    CK(ctx->lists.ensure((size_t)q_total * 3));
+    CK(ctx->shots_d.ensure((size_t)nshots));
+    if (nrec > 0) {
+        CK(ctx->rec.ensure((size_t)nrec * 3));
+        CK(ctx->t_recv.ensure((size_t)nshots * nrec));
+        std::vector<float> rh((size_t)nrec * 3);
+        for (int r = 0; r < nrec; r++) {
+            rh[(size_t)r] = receivers[r].x;
+            rh[(size_t)nrec + r] = receivers[r].y;
+            rh[(size_t)2 * nrec + r] = receivers[r].z;
+        }
+        CK(cudaMemcpyAsync(ctx->rec.ptr, rh.data(), rh.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CK(cudaMemcpyAsync(ctx->shots_d.ptr, sd.data(), sd.size() * sizeof(ShotDesc), cudaMemcpyHostToDevice,
+                       ctx->stream));
+
+    // ---- launch -----------------------------------------------------------------------
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    CK(tomo::fim_init(ctx->T.ptr, (size_t)t_total, ctx->qflag.ptr, (size_t)q_total, ctx->ctrl.ptr, ctx->stats.ptr,
+                      ctx->stream));
+    CK(tomo::fim_seed(ctx->shots_d.ptr, nshots, ctx->S.ptr, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
+                      ctx->lists.ptr, local_bits, ctx->ctrl.ptr, ctx->stream));
+    tomo::FimLaunch p{};
+    p.S = ctx->S.ptr;
+    p.T = ctx->T.ptr;
+    p.shots = ctx->shots_d.ptr;
+    p.nshots = nshots;
+    p.qflag = ctx->qflag.ptr;
+    p.lists = ctx->lists.ptr;
+    p.list_cap = (unsigned)q_total;
+    p.ctrl = ctx->ctrl.ptr;
+    p.stats = ctx->stats.ptr;
+    p.gbx = ctx->gbx;
+    p.gbz = ctx->gbz;
+    p.h = g.dx;  // isotropic spacing h = dx (block_FIM.cpp:173)
+    p.max_inner = max_inner;
+    p.max_rounds = max_rounds;
+    p.local_bits = local_bits;
+    p.spin_limit = kSpinLimit;
+    p.nrec = nrec;
+    p.rx = nrec ? ctx->rec.ptr : nullptr;
+    p.ry = nrec ? ctx->rec.ptr + nrec : nullptr;
+    p.rz = nrec ? ctx->rec.ptr + 2 * nrec : nullptr;
+    p.t_recv = nrec ? ctx->t_recv.ptr : nullptr;
+    p.dx = g.dx;
+    p.dy = g.dy;
+    p.dz = g.dz;
+    p.nz = g.nz;
+    int grid = 0;
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    CK(tomo::fim_solve(p, block_warps, &grid, ctx->stream));
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    CK(cudaMemcpyAsync(ctx->pinned_ctrl, ctx->ctrl.ptr, tomo::kCtrlWords * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(ctx->pinned_ctrl + tomo::kCtrlWords, ctx->stats.ptr, 2 * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    if (t_recv && nrec > 0)
+        CK(cudaMemcpyAsync(t_recv, ctx->t_recv.ptr, (size_t)nshots * nrec * sizeof(float), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+
+    ctx->shots_h = sd;
+    ctx->shot_pos.assign(shots, shots + nshots);
+    ctx->rec_h.assign(receivers, receivers + nrec);
+    ctx->nshots = nshots;
+    ctx->nrec = nrec;
+    const unsigned derr = ctx->pinned_ctrl[tomo::kErr];
+    ctx->have_solve = (derr == tomo::kDevOk);
+    if (stats) {
+        unsigned long long st[2];
+        std::memcpy(st, ctx->pinned_ctrl + tomo::kCtrlWords, sizeof(st));
+        stats->rounds = ctx->pinned_ctrl[tomo::kRounds];
+        stats->activations = (long long)st[0];
+        stats->inner_iterations = (long long)st[1];
+        stats->nodes_per_brick = tomo::kBrickNodes;
+        cudaEventElapsedTime(&stats->setup_ms, ctx->ev[0], ctx->ev[3]);
+        cudaEventElapsedTime(&stats->solve_ms, ctx->ev[3], ctx->ev[1]);
+        cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[2]);
+    }
+    if (derr == tomo::kDevRoundCap)
+        return fail(ctx, TOMO_ERR_NOT_CONVERGED, "eikonal solve hit the round cap (" + std::to_string(max_rounds) + ")");
+    if (derr != tomo::kDevOk) return fail(ctx, TOMO_ERR_TIMEOUT, "eikonal solve: device barrier wait timed out");
+    return TOMO_OK;
+}
+
+int tomo_eik_window(tomo_ctx *ctx, int shot, tomo_window *out)
+{
+    if (!ctx || !out) return TOMO_ERR_INVALID_ARG;
+    if (!ctx->have_solve) return fail(ctx, TOMO_ERR_STATE, "no eikonal solve");
+    if (shot < 0 || shot >= ctx->nshots) return fail(ctx, TOMO_ERR_INVALID_ARG, "shot index out of range");
+    const ShotDesc &d = ctx->shots_h[(size_t)shot];
+    *out = tomo_window{d.wx0, d.wx0 + d.wnx, d.wy0, d.wy0 + d.wny};
+    return TOMO_OK;
+}
+
+int tomo_eik_volume(tomo_ctx *ctx, int shot, float *t_out)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (!t_out) return fail(ctx, TOMO_ERR_INVALID_ARG, "output is NULL");
+    if (!ctx->have_solve) return fail(ctx, TOMO_ERR_STATE, "no eikonal solve");
+    if (shot < 0 || shot >= ctx->nshots) return fail(ctx, TOMO_ERR_INVALID_ARG, "shot index out of range");
+    CK(cudaSetDevice(ctx->device));
+    const ShotDesc &d = ctx->shots_h[(size_t)shot];
+    const size_t n = (size_t)ctx->g.nz * d.wnx * d.wny;
+    CK(ctx->scratch_v.ensure(n));
+    CK(tomo::fim_unbrick(ctx->T.ptr, ctx->shots_d.ptr, shot, ctx->g.nz, ctx->scratch_v.ptr, ctx->stream));
+    CK(cudaMemcpyAsync(t_out, ctx->scratch_v.ptr, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TOMO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,415 @@
+// Batched persistent fast-iterative eikonal solver for sm_100a.
+//
+// Replaces Block_FIM (src/eikonal/block_FIM/block_FIM.cpp, cuda_kernel.cu) with a design
+// of its own:
+//  * All shots of a batch are solved by ONE cooperative launch.  Work items are
+//    (shot, 4x4x4 brick) pairs; one warp owns one brick, so the in-brick relaxation is
+//    synchronised with __syncwarp/__any_sync only (warp-vote convergence).
+//  * The active list lives on the device (3 rotating lists + a per-brick "queued for
+//    round" word updated with atomicMax), so there are no host round trips, no per-shot
+//    allocations and no re-bricking on the host.
+//  * A brick re-queues a neighbour only when a value on the shared face dropped, and
+//    itself when its in-brick iteration cap was hit.  Updates are monotone (min), so this
+//    chaotic relaxation converges to the same fixed point as Block_FIM's schedule.
+//  * Slowness is read from one brick-major copy of the model shared by all shots; each
+//    shot's window is a brick-aligned sub-grid of it.
+#include "common.cuh"
+#include "fim.cuh"
+
+namespace tomo {
+
+// -------------------------------------------------------------------------------------
+// Local update.  First-order Godunov upwind solution of |grad T| = s on a cubic grid of
+// spacing h given the smaller neighbour of each axis (a, b, c): the largest root that is
+// causal (exceeds every neighbour it uses), trying 1, 2 then 3 neighbours in ascending
+// order -- the Jeong & Whitaker (2008) update of get_time_eikonal
+// (src/eikonal/block_FIM/cuda_kernel.cu:217-248), written in symmetric form.
+// -------------------------------------------------------------------------------------
+__device__ __forceinline__ float godunov_jw(float a, float b, float c, float h, float s)
+{
+    const float lo = fminf(a, b), hi = fmaxf(a, b);
+    const float u0 = fminf(lo, c);
+    const float mid = fmaxf(lo, c);
+    const float u1 = fminf(mid, hi), u2 = fmaxf(mid, hi);
+    if (!(u0 < kInf)) return kInf;
+    const float hs = h * s;
+    float t = u0 + hs;
+    if (t > u1) {
+        const float d01 = u1 - u0;
+        const float t2 = 0.5f * ((u0 + u1) + sqrtf(2.0f * hs * hs - d01 * d01));
+        if (t2 > u1) t = t2;
+        if (t > u2) {
+            const float sum = u0 + u1 + u2;
+            const float d12 = u2 - u1, d02 = u2 - u0;
+            const float disc = 3.0f * hs * hs - (d01 * d01 + d12 * d12 + d02 * d02);
+            const float t3 = (sum + sqrtf(disc)) * (1.0f / 3.0f);
+            if (t3 > u2) t = t3;
+        }
+    }
+    return t;
+}
+
+// Tile of one warp: (4+2)^3 nodes, the brick plus a one-node face halo.
+constexpr int kTile = kBrick + 2;
+constexpr int kTileNodes = kTile * kTile * kTile;
+
+__device__ __forceinline__ int tile_idx(int z, int x, int y)
+{
+    return (z + 1) + kTile * ((x + 1) + kTile * (y + 1));
+}
+
+// Lane masks of the brick faces for the two node sets of a lane (node = lane and
+// lane + 32; node = z + 4x + 16y).
+constexpr unsigned kMaskZm = 0x11111111u;  // z == 0
+constexpr unsigned kMaskZp = 0x88888888u;  // z == 3
+constexpr unsigned kMaskXm = 0x000F000Fu;  // x == 0
+constexpr unsigned kMaskXp = 0xF000F000u;  // x == 3
+constexpr unsigned kMaskY0 = 0x0000FFFFu;  // y == 0 (first node set)
+constexpr unsigned kMaskY3 = 0xFFFF0000u;  // y == 3 (second node set)
+
+__device__ __forceinline__ float brick_T(const float *T, const ShotDesc &d, int x, int y, int z)
+{
+    const long long b = (z >> 2) + (long long)d.nbz * ((x >> 2) + (long long)d.nbx * (y >> 2));
+    return __ldcg(T + d.t_off + b * kBrickNodes + (z & 3) + 4 * (x & 3) + 16 * (y & 3));
+}
+
+struct WarpStats {
+    unsigned long long act, inner;
+};
+
+// One activation of one brick by one warp.
+__device__ __forceinline__ void process_brick(const FimLaunch &p, unsigned item, unsigned round,
+                                              float *tile, WarpStats &ws)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned s = item >> p.local_bits;
+    const unsigned b = item & ((1u << p.local_bits) - 1u);
+    const ShotDesc &d = p.shots[s];
+    const int nbz = d.nbz, nbx = d.nbx, nby = d.nby;
+    const int bz = (int)(b % (unsigned)nbz);
+    const unsigned tq = b / (unsigned)nbz;
+    const int bx = (int)(tq % (unsigned)nbx);
+    const int by = (int)(tq / (unsigned)nbx);
+
+    const long long gb = bz + (long long)p.gbz * ((bx + (d.wx0 >> 2)) + (long long)p.gbx * (by + (d.wy0 >> 2)));
+    const float *Sb = p.S + gb * kBrickNodes;
+    float *Tb = p.T + d.t_off + (long long)b * kBrickNodes;
+
+    // Own nodes: n0 = lane (y in {0,1}), n1 = lane + 32 (y in {2,3}).
+    const float s0 = __ldg(Sb + lane), s1 = __ldg(Sb + 32 + lane);
+    const float i0 = __ldcg(Tb + lane), i1 = __ldcg(Tb + 32 + lane);
+
+    // Face halo: 6 faces x 16 nodes, three per lane.  Missing neighbours (grid edge) are
+    // INF; the reference's "halo = self" at the edge cannot lower a node either.
+    float hv[3];
+    int ht[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const int k = lane + 32 * q;
+        const int f = k >> 4, j = k & 15, u = j & 3, v = j >> 2;
+        long long nb = -1;
+        int node = 0, tz = 0, tx = 0, ty = 0;
+        switch (f) {
+        case 0: if (bz > 0) nb = (long long)b - 1;                      node = 3 + 4 * u + 16 * v; tz = -1; tx = u; ty = v; break;
+        case 1: if (bz < nbz - 1) nb = (long long)b + 1;                node = 0 + 4 * u + 16 * v; tz = 4;  tx = u; ty = v; break;
+        case 2: if (bx > 0) nb = (long long)b - nbz;                    node = u + 12 + 16 * v;    tz = u;  tx = -1; ty = v; break;
+        case 3: if (bx < nbx - 1) nb = (long long)b + nbz;              node = u + 0 + 16 * v;     tz = u;  tx = 4;  ty = v; break;
+        case 4: if (by > 0) nb = (long long)b - (long long)nbz * nbx;   node = u + 4 * v + 48;     tz = u;  tx = v;  ty = -1; break;
+        default: if (by < nby - 1) nb = (long long)b + (long long)nbz * nbx; node = u + 4 * v;     tz = u;  tx = v;  ty = 4; break;
+        }
+        hv[q] = nb >= 0 ? __ldcg(p.T + d.t_off + nb * kBrickNodes + node) : kInf;
+        ht[q] = tile_idx(tz, tx, ty);
+    }
+
+    const int z0 = lane & 3, x0 = (lane >> 2) & 3, y0 = lane >> 4;
+    const int ti0 = tile_idx(z0, x0, y0);
+    const int ti1 = ti0 + 2 * kTile * kTile;
+
+    float c0 = i0, c1 = i1;
+    tile[ti0] = c0;
+    tile[ti1] = c1;
+#pragma unroll
+    for (int q = 0; q < 3; q++) tile[ht[q]] = hv[q];
+    __syncwarp();
+
+    const float h = p.h;
+    bool more = true;
+    int it = 0;
+    for (; it < p.max_inner; ++it) {
+        const float a0 = fminf(tile[ti0 - kTile], tile[ti0 + kTile]);
+        const float b0 = fminf(tile[ti0 - kTile * kTile], tile[ti0 + kTile * kTile]);
+        const float g0 = fminf(tile[ti0 - 1], tile[ti0 + 1]);
+        const float a1 = fminf(tile[ti1 - kTile], tile[ti1 + kTile]);
+        const float b1 = fminf(tile[ti1 - kTile * kTile], tile[ti1 + kTile * kTile]);
+        const float g1 = fminf(tile[ti1 - 1], tile[ti1 + 1]);
+        const float n0 = fminf(c0, godunov_jw(a0, b0, g0, h, s0));
+        const float n1 = fminf(c1, godunov_jw(a1, b1, g1, h, s1));
+        const bool ch = (n0 < c0) | (n1 < c1);
+        __syncwarp();
+        tile[ti0] = n0;
+        tile[ti1] = n1;
+        c0 = n0;
+        c1 = n1;
+        __syncwarp();
+        if (!__any_sync(kFull, ch)) {
+            more = false;
+            ++it;
+            break;
+        }
+    }
+    ws.act += 1;
+    ws.inner += (unsigned long long)it;
+
+    const unsigned m0 = __ballot_sync(kFull, c0 < i0);
+    const unsigned m1 = __ballot_sync(kFull, c1 < i1);
+    const unsigned mm = m0 | m1;
+    if (mm) {
+        __stcg(Tb + lane, c0);
+        __stcg(Tb + 32 + lane, c1);
+    }
+
+    // Queue the neighbours across changed faces, and this brick if it hit the cap.
+    bool want = false;
+    long long tgt = -1;
+    if (lane < 6) {
+        bool chg = false;
+        switch (lane) {
+        case 0: chg = (mm & kMaskZm) && bz > 0;        tgt = (long long)b - 1; break;
+        case 1: chg = (mm & kMaskZp) && bz < nbz - 1;  tgt = (long long)b + 1; break;
+        case 2: chg = (mm & kMaskXm) && bx > 0;        tgt = (long long)b - nbz; break;
+        case 3: chg = (mm & kMaskXp) && bx < nbx - 1;  tgt = (long long)b + nbz; break;
+        case 4: chg = (m0 & kMaskY0) && by > 0;        tgt = (long long)b - (long long)nbz * nbx; break;
+        default: chg = (m1 & kMaskY3) && by < nby - 1; tgt = (long long)b + (long long)nbz * nbx; break;
+        }
+        want = chg;
+    } else if (lane == 6) {
+        want = more;
+        tgt = b;
+    }
+    const unsigned tag = round + 2u;  // "queued for round+1", offset by one so 0 = never
+    if (want) {
+        const unsigned old = atomicMax(p.qflag + d.qbase + (unsigned long long)tgt, tag);
+        want = old < tag;
+    }
+    const unsigned wm = __ballot_sync(kFull, want);
+    if (wm) {
+        const int leader = __ffs(wm) - 1;
+        const unsigned nxt = (round + 1u) % 3u;
+        unsigned base = 0;
+        if (lane == leader) base = atomicAdd(p.ctrl + kCnt0 + nxt, (unsigned)__popc(wm));
+        base = __shfl_sync(kFull, base, leader);
+        if (want) {
+            const unsigned slot = base + __popc(wm & ((1u << lane) - 1u));
+            p.lists[(size_t)nxt * p.list_cap + slot] = (s << p.local_bits) | (unsigned)tgt;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_fim_solve(FimLaunch p)
+{
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x >> 5;
+    float *tile = smem + warp * kTileNodes;
+    const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
+    const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    WarpStats ws{0ull, 0ull};
+
+    unsigned round = 0;
+    bool ok = true;
+    for (;;) {
+        const unsigned cur = round % 3u;
+        const unsigned n = ld_volatile(p.ctrl + kCnt0 + cur);
+        if (n == 0u) break;
+        if ((int)round >= p.max_rounds) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(p.ctrl + kErr, 0u, (unsigned)kDevRoundCap);
+            ok = false;
+            break;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kCnt0 + (round + 2u) % 3u] = 0u;
+        const unsigned *list = p.lists + (size_t)cur * p.list_cap;
+        for (unsigned i = gwarp; i < n; i += nwarps) process_brick(p, __ldcg(list + i), round, tile, ws);
+        if (!grid_barrier(p.ctrl, p.spin_limit)) { ok = false; break; }
+        ++round;
+    }
+    if ((threadIdx.x & 31) == 0 && ws.act) {
+        atomicAdd(p.stats + 0, ws.act);
+        atomicAdd(p.stats + 1, ws.inner);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kRounds] = round;
+    if (!ok || p.nrec == 0) return;
+
+    // Receiver sampling (Block_FIM::write_first_arrival, block_FIM.cpp:228-262): trilinear
+    // from the floor node of the window-cropped field, with the reference's flattened
+    // index arithmetic (an offset past a column wraps into the next; past the end: 0).
+    const long long total = (long long)p.nshots * p.nrec;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(e / p.nrec), r = (int)(e % p.nrec);
+        const ShotDesc &d = p.shots[s];
+        const float dx = p.dx, dy = p.dy, dz = p.dz;
+        const float x = fsub(p.rx[r], fmul((float)d.wx0, dx));
+        const float y = fsub(p.ry[r], fmul((float)d.wy0, dy));
+        const float z = p.rz[r];
+        if (x < 0.0f || y < 0.0f || x > fmul((float)(d.wnx - 1), dx) || y > fmul((float)(d.wny - 1), dy)) {
+            p.t_recv[e] = kInf;  // receiver outside this shot's window: no traveltime
+            continue;
+        }
+        const float fx = floorf(fdiv(x, dx)), fy = floorf(fdiv(y, dy)), fz = floorf(fdiv(z, dz));
+        const float x0 = fmul(fx, dx), y0 = fmul(fy, dy), z0 = fmul(fz, dz);
+        const float x1 = fadd(fmul(fx, dx), dx), y1 = fadd(fmul(fy, dy), dy), z1 = fadd(fmul(fz, dz), dz);
+        const long long nz = p.nz, wnx = d.wnx, n = nz * wnx * d.wny;
+        const long long id = (long long)(int)fdiv(z, dz) + (long long)(int)fdiv(x, dx) * nz +
+                             (long long)(int)fdiv(y, dy) * wnx * nz;
+        const long long offs[8] = {0, 1, nz, 1 + nz, wnx * nz, 1 + wnx * nz, nz + wnx * nz, 1 + nz + wnx * nz};
+        float c[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const long long f = id + offs[q];
+            if (f >= 0 && f < n) {
+                const int zz = (int)(f % nz);
+                const long long rest = f / nz;
+                const int xx = (int)(rest % wnx), yy = (int)(rest / wnx);
+                c[q] = brick_T(p.T, d, xx, yy, zz);
+            } else {
+                c[q] = 0.0f;
+            }
+        }
+        p.t_recv[e] = trilinear_ref(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], x0, x1, y0, y1,
+                                    z0, z1, x, y, z);
+    }
+}
+
+// -------------------------------------------------------------------------------------
+// Set-up kernels
+// -------------------------------------------------------------------------------------
+__global__ void k_velocity_to_slowness(const float *v, float *s, size_t n)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        s[i] = __fdiv_rn(1.0f, v[i]);
+}
+
+// Pad to the brick multiple by edge replication (Block_FIM::expand_model,
+// block_FIM.cpp:8-57, is a clamp of the index) and store brick-major.
+__global__ void k_brick_model(const float *slow, float *S, int nx, int ny, int nz, int nxx, int nyy, int nzz)
+{
+    const int gbz = nzz / kBrick, gbx = nxx / kBrick;
+    const size_t total = (size_t)nxx * nyy * nzz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t brick = i / kBrickNodes;
+        const int node = (int)(i % kBrickNodes);
+        const int bz = (int)(brick % gbz);
+        const size_t t = brick / gbz;
+        const int bx = (int)(t % gbx), by = (int)(t / gbx);
+        const int z = bz * kBrick + (node & 3), x = bx * kBrick + ((node >> 2) & 3), y = by * kBrick + (node >> 4);
+        const int zc = min(z, nz - 1), xc = min(x, nx - 1), yc = min(y, ny - 1);
+        S[i] = slow[zc + (size_t)xc * nz + (size_t)yc * nx * nz];
+    }
+}
+
+__global__ void k_fim_init(float4 *T4, size_t n4, unsigned *qflag, size_t nq, unsigned *ctrl,
+                           unsigned long long *stats)
+{
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const float4 inf4 = make_float4(kInf, kInf, kInf, kInf);
+    for (size_t i = t; i < n4; i += stride) __stcg(T4 + i, inf4);
+    for (size_t i = t; i < nq; i += stride) qflag[i] = 0u;
+    if (t < kCtrlWords) ctrl[t] = 0u;
+    if (t < 2) stats[t] = 0ull;
+}
+
+__global__ void k_fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
+                           unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nshots) {
+        const ShotDesc d = shots[s];
+        // Seed value S(seed node) * distance (block_FIM.cpp:315-317); S read from the
+        // brick-major model at the window's brick.
+        const int bz = d.src_brick % d.nbz, t = d.src_brick / d.nbz;
+        const int bx = t % d.nbx, by = t / d.nbx;
+        const long long gb = bz + (long long)gbz * ((bx + (d.wx0 >> 2)) + (long long)gbx * (by + (d.wy0 >> 2)));
+        T[d.t_off + (long long)d.src_brick * kBrickNodes + d.src_node] = __fmul_rn(S[gb * kBrickNodes + d.src_node], d.src_dist);
+        qflag[d.qbase + d.src_brick] = 1u;
+        lists[s] = ((unsigned)s << local_bits) | (unsigned)d.src_brick;
+    }
+    if (s == 0) ctrl[kCnt0] = (unsigned)nshots;
+}
+
+__global__ void k_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out)
+{
+    const ShotDesc d = shots[shot];
+    const size_t total = (size_t)nz * d.wnx * d.wny;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int z = (int)(i % nz);
+        const size_t r = i / nz;
+        const int x = (int)(r % d.wnx), y = (int)(r / d.wnx);
+        out[i] = brick_T(T, d, x, y, z);
+    }
+}
+
+// -------------------------------------------------------------------------------------
+// Launchers
+// -------------------------------------------------------------------------------------
+static int grid_for(size_t n, int threads)
+{
+    size_t g = (n + threads - 1) / threads;
+    if (g > 148u * 32u) g = 148u * 32u;
+    return g < 1 ? 1 : (int)g;
+}
+
+cudaError_t velocity_to_slowness(const float *v, float *s, size_t n, cudaStream_t st)
+{
+    k_velocity_to_slowness<<<grid_for(n, 256), 256, 0, st>>>(v, s, n);
+    return cudaGetLastError();
+}
+
+cudaError_t fim_brick_model(const float *slow, float *S, int nx, int ny, int nz, int nxx, int nyy,
+                            int nzz, cudaStream_t st)
+{
+    k_brick_model<<<grid_for((size_t)nxx * nyy * nzz, 256), 256, 0, st>>>(slow, S, nx, ny, nz, nxx, nyy, nzz);
+    return cudaGetLastError();
+}
+
+cudaError_t fim_init(float *T, size_t t_count, unsigned *qflag, size_t q_count, unsigned *ctrl,
+                     unsigned long long *stats, cudaStream_t st)
+{
+    k_fim_init<<<grid_for(t_count / 4, 256), 256, 0, st>>>(reinterpret_cast<float4 *>(T), t_count / 4,
+                                                            qflag, q_count, ctrl, stats);
+    return cudaGetLastError();
+}
+
+cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
+                     unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st)
+{
+    k_fim_seed<<<(nshots + 127) / 128, 128, 0, st>>>(shots, nshots, S, gbx, gbz, T, qflag, lists, local_bits, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t fim_solve(const FimLaunch &p, int block_warps, int *grid_out, cudaStream_t st)
+{
+    if (block_warps < 1 || block_warps > 8) block_warps = 8;
+    const int threads = 32 * block_warps;
+    const size_t smem = (size_t)block_warps * kTileNodes * sizeof(float);
+    int dev = 0, nsm = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fim_solve, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const int grid = nsm * per_sm;
+    if (grid_out) *grid_out = grid;
+    FimLaunch pp = p;
+    void *args[] = {&pp};
+    return cudaLaunchCooperativeKernel((const void *)k_fim_solve, dim3(grid), dim3(threads), args, smem, st);
+}
+
+cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out, cudaStream_t st)
+{
+    k_unbrick<<<148 * 8, 256, 0, st>>>(T, shots, shot, nz, out);
+    return cudaGetLastError();
+}
+
+}  // namespace tomo

@@ -1,0 +1,171 @@
+"""Parity of the batched persistent FIM (through the C ABI) against the CPU oracle.
+
+The oracle is the FP64 fixed point of the reference Block_FIM operator
+(src/eikonal/block_FIM/cuda_kernel.cu:217-248) with Block_FIM's padding and single-node
+source seed (src/eikonal/block_FIM/block_FIM.cpp:142-157, 305-317).  Tolerance: 1e-4
+relative traveltime error on nodes with T >= 2h/v_max (the error target of the task); the
+measured error is ~1e-6 (FP32 rounding only).  Receiver sampling is checked bit-exact.
+"""
+import numpy as np
+import pytest
+
+from seismic_tomography_3d_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-4
+
+
+def rel_err(T, Tref, h, vmax):
+    m = Tref >= 2.0 * h / vmax
+    return float(np.max(np.abs(T[m] - Tref[m]) / Tref[m])) if m.any() else 0.0
+
+
+def solve_oracle(oracle_mod, v, h, shot, window=None):
+    s = (1.0 / v).astype(np.float32)
+    sx, sy, sz = map(float, shot)
+    if window is not None:
+        x0, x1, y0, y1 = window
+        s = s[y0:y1, x0:x1, :]
+        sx -= np.float32(x0) * np.float32(h)
+        sy -= np.float32(y0) * np.float32(h)
+    T, _ = oracle_mod.fim_jw(s, h, (sx, sy, sz))
+    return T
+
+
+@pytest.mark.parametrize("dims", [(13, 11, 9), (16, 16, 16), (21, 17, 10), (33, 29, 18)])
+def test_single_shot_matches_oracle(tomo, oracle_mod, dims):
+    nx, ny, nz = dims
+    sv = wl.small(sum(dims), nx, ny, nz, nshots=1)
+    with tomo.Context(nx, ny, nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(sv.shots)
+        T = ctx.eik_volume(0)
+    Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, sv.shots[0])
+    assert T.shape == Tref.shape
+    assert rel_err(T, Tref, sv.h, sv.velocity.max()) < REL_TOL
+
+
+def test_constant_velocity_corner_and_interior(tomo, oracle_mod):
+    nx, ny, nz, h = 24, 20, 12, 10.0
+    v = np.full((ny, nx, nz), 2000.0, np.float32)
+    shots = np.array([[0, 0, 0], [110.0, 90.0, 40.0], [230.0, 190.0, 110.0]], np.float32)
+    with tomo.Context(nx, ny, nz, h) as ctx:
+        ctx.set_velocity(v)
+        ctx.eik_solve(shots)
+        for i, sh in enumerate(shots):
+            T = ctx.eik_volume(i)
+            Tref = solve_oracle(oracle_mod, v, h, sh)
+            assert rel_err(T, Tref, h, 2000.0) < REL_TOL
+            # the axis through the source is exactly |x - xs| * s (1D operator)
+            ix, iy, iz = (int(round(c / h)) for c in sh)
+            line = T[iy, :, iz].astype(np.float64)
+            exact = np.abs(np.arange(nx) * h - sh[0]) / 2000.0
+            assert np.max(np.abs(line - exact)) < 1e-5
+
+
+def test_off_node_source(tomo, oracle_mod):
+    nx, ny, nz, h = 18, 18, 10, 20.0
+    sv = wl.small(7, nx, ny, nz, h=h)
+    shot = np.array([[101.3, 77.7, 13.1]], np.float32)
+    with tomo.Context(nx, ny, nz, h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(shot)
+        T = ctx.eik_volume(0)
+    Tref = solve_oracle(oracle_mod, sv.velocity, h, shot[0])
+    assert rel_err(T, Tref, h, sv.velocity.max()) < REL_TOL
+
+
+def test_batched_windows_match_cropped_oracle(tomo, oracle_mod):
+    nx, ny, nz = 37, 30, 14
+    sv = wl.small(11, nx, ny, nz, nshots=6, windows=True)
+    with tomo.Context(nx, ny, nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(sv.shots, windows=sv.windows)
+        for i in range(len(sv.shots)):
+            assert ctx.eik_window(i) == tuple(sv.windows[i])
+            T = ctx.eik_volume(i)
+            Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, sv.shots[i], sv.windows[i])
+            assert T.shape == Tref.shape
+            assert rel_err(T, Tref, sv.h, sv.velocity.max()) < REL_TOL
+
+
+def test_batch_equals_single_solves(tomo):
+    nx, ny, nz = 29, 26, 13
+    sv = wl.small(5, nx, ny, nz, nshots=5)
+    with tomo.Context(nx, ny, nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(sv.shots)
+        batch = [ctx.eik_volume(i) for i in range(len(sv.shots))]
+        for i in range(len(sv.shots)):
+            ctx.eik_solve(sv.shots[i:i + 1])
+            one = ctx.eik_volume(0)
+            assert rel_err(batch[i], one, sv.h, sv.velocity.max()) < 1e-5
+
+
+def test_receivers_bit_exact_vs_oracle_trilinear(tomo, oracle_mod):
+    nx, ny, nz = 25, 23, 11
+    sv = wl.small(3, nx, ny, nz, nshots=2, nrec=40)
+    rec = sv.receivers.copy()
+    rng = np.random.default_rng(0)
+    rec[:20, 0] += rng.uniform(0, sv.h, 20).astype(np.float32)  # off-node receivers
+    rec[:20, 1] += rng.uniform(0, sv.h, 20).astype(np.float32)
+    rec[:, 0] = np.minimum(rec[:, 0], (nx - 1) * sv.h)
+    rec[:, 1] = np.minimum(rec[:, 1], (ny - 1) * sv.h)
+    rec[:10, 2] = rng.uniform(0, (nz - 1) * sv.h, 10).astype(np.float32)
+    rec[-1] = ((nx - 1) * sv.h, (ny - 1) * sv.h, (nz - 1) * sv.h)  # last node: the reference's wrap case
+    with tomo.Context(nx, ny, nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        t_recv, _ = ctx.eik_solve(sv.shots, receivers=rec)
+        for i in range(len(sv.shots)):
+            T = ctx.eik_volume(i)
+            ref = oracle_mod.first_arrival(T, sv.h, rec[:, 0], rec[:, 1], rec[:, 2])
+            np.testing.assert_array_equal(t_recv[i], ref)
+
+
+def test_repeat_runs_agree(tomo):
+    nx, ny, nz = 40, 36, 20
+    sv = wl.small(9, nx, ny, nz, nshots=4)
+    with tomo.Context(nx, ny, nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(sv.shots)
+        a = [ctx.eik_volume(i) for i in range(4)]
+        ctx.eik_solve(sv.shots)
+        b = [ctx.eik_volume(i) for i in range(4)]
+    for x, y in zip(a, b):
+        assert rel_err(x, y, sv.h, sv.velocity.max()) < 1e-5
+
+
+def test_errors_are_status_codes(tomo):
+    nx, ny, nz, h = 12, 12, 8, 10.0
+    v = np.full((ny, nx, nz), 1500.0, np.float32)
+    with tomo.Context(nx, ny, nz, h) as ctx:
+        with pytest.raises(tomo.TomoError) as e:
+            ctx.eik_solve([[5.0, 5.0, 0.0]])  # no model yet
+        assert e.value.status == -6
+        ctx.set_velocity(v)
+        with pytest.raises(tomo.TomoError) as e:
+            ctx.eik_solve([[500.0, 5.0, 0.0]])  # outside
+        assert e.value.status == -1
+        with pytest.raises(tomo.TomoError) as e:
+            ctx.eik_solve([[5.0, 5.0, 0.0]], windows=[[1, 12, 0, 12]])  # unaligned window
+        assert e.value.status == -1
+        with pytest.raises(tomo.TomoError) as e:
+            ctx.eik_solve([[50.0, 50.0, 0.0]], max_rounds=2)  # round cap
+        assert e.value.status == -4
+        t, st = ctx.eik_solve([[50.0, 50.0, 0.0]])  # context still usable
+        assert st["rounds"] > 2
+
+
+@pytest.mark.slow
+def test_config1_full_size(tomo, oracle_mod):
+    sv = wl.config1()
+    with tomo.Context(sv.nx, sv.ny, sv.nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        t_recv, st = ctx.eik_solve(sv.shots, receivers=sv.receivers)
+        T = ctx.eik_volume(0)
+    Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, sv.shots[0])
+    assert rel_err(T, Tref, sv.h, sv.velocity.max()) < REL_TOL
+    ref_recv = oracle_mod.first_arrival(Tref.astype(np.float32), sv.h, *sv.receivers.T)
+    m = ref_recv >= 2 * sv.h / sv.velocity.max()
+    assert np.max(np.abs(t_recv[0][m] - ref_recv[m]) / ref_recv[m]) < REL_TOL
