@@ -97,10 +97,15 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def workload(rank):
+def workload(rank, shots=None):
+    import dataclasses
+
     from seismic_tomography_3d_b200 import workloads as wl
 
-    return wl.config2(seed=2 + 1000 * rank)
+    sv = wl.config2(seed=2 + 1000 * rank)
+    if shots:  # a smaller batch of the same workload (profiling captures)
+        sv = dataclasses.replace(sv, shots=sv.shots[:shots], windows=sv.windows[:shots])
+    return sv
 
 
 def cpu_reference_sample(sv, max_shots=None, budget_s=20.0):
@@ -192,7 +197,7 @@ def run_ours(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     torch.cuda.set_device(local)
-    sv = workload(rank)
+    sv = workload(rank, args.shots)
     ns = len(sv.shots)
     ctx = tomo.Context(sv.nx, sv.ny, sv.nz, sv.h, device=local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
@@ -303,6 +308,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shots", type=int, default=0, help="first N shots of the batch only (profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -67,6 +67,10 @@ typedef struct {
     int max_rounds;  /* cap of outer rounds (0: default 1<<20)                        */
     int brick;       /* brick shape id (0: tuned default); see tomo_eik_brick_shapes  */
     int block_warps; /* warps per CTA of the persistent kernel (0: default)           */
+    int occupancy;   /* CTAs per SM the kernel is compiled for, 1..4 (0: default 4)   */
+    float change_tol;/* a face value must drop by more than this (s) to re-queue the
+                        neighbour brick.  0: default 1e-6 s, the reference's EPS
+                        (cuda_kernel.cuh:8); < 0: any drop (exact FP32 fixed point) */
 } tomo_eik_opts;
 
 typedef struct {
@@ -128,6 +132,84 @@ int tomo_eik_window(tomo_ctx *ctx, int shot, tomo_window *out);
 /* Brick shapes the solver supports: writes up to `cap` triples (bx,by,bz) of nodes and
  * returns how many there are. */
 int tomo_eik_brick_shapes(int *xyz_triples, int cap);
+
+/* ------------------------------------------------- ray tracing and the Jacobian ------- */
+typedef struct {
+    float dx, dy, dz;       /* inversion cell size: dx_tomo, dy_tomo, dz_tomo (parameters.txt)  */
+    int tk_order;           /* Tikhonov order (tk_order)                                         */
+    float tk_param;         /* lambda (tk_param)                                                 */
+    int max_ray_steps;      /* step cap per ray (0: 20 x the grid diagonal in ray steps)         */
+    int max_cells_per_ray;  /* distinct cells one ray may cross (0: 1024)                        */
+    int illumination;       /* 1: accumulate the illumination volume (least_squares.cpp:234)     */
+} tomo_jacobian_opts;
+
+typedef struct {
+    int nx, ny, nz;               /* inversion grid (least_squares.cpp:124-126)            */
+    long long rows, cols;         /* N = n_data + n_model - tk_order, M = n_model          */
+    long long nnz_rays, nnz;      /* non-zeros of G, of A = [G ; lambda L]                 */
+    long long rays, rays_ok, rays_stalled, rays_capped, rays_nonfinite, rays_outside, rays_overflow;
+    long long ray_steps;          /* total marching steps                                  */
+    float ms;                     /* device time of ray tracing + matrix assembly          */
+} tomo_jacobian_stats;
+
+/* Traces one ray per (shot, receiver) of the last tomo_eik_solve back through its
+ * traveltime field and assembles the sparse Frechet matrix G and the Tikhonov rows on the
+ * device: Least_squares::ray_tracing + tk_reg_matrix + the COO assembly of optimization
+ * (src/tomography/least_squares/least_squares.cpp:192-280, 358-422, 321-347).  Row
+ * ray + shot*nrec, column = inversion cell, value = run-length path length.  Rays the
+ * reference would trace forever (stalled next to the source, zero gradient, step cap) are
+ * cut and counted in the stats. */
+int tomo_build_jacobian(tomo_ctx *ctx, const tomo_jacobian_opts *opts, tomo_jacobian_stats *stats);
+/* Copies A = [G ; lambda L] in CSR to the host: row_ptr (rows+1), cols/vals (nnz). */
+int tomo_jacobian_copy(tomo_ctx *ctx, int *row_ptr, int *cols, float *vals);
+/* Per-ray status (nshots*nrec): 0 ok, 1 stalled at the source, 2 step cap, 3 zero
+ * gradient, 4 outside the grid/window, 5 too many cells. */
+int tomo_ray_status(tomo_ctx *ctx, int *status);
+/* Illumination volume (nz*nx*ny) of the last tomo_build_jacobian with illumination = 1. */
+int tomo_illumination(tomo_ctx *ctx, float *out);
+
+/* ------------------------------------------------------------- inversion ----------- */
+/* Observed picks, nshots*nrec (row-major shot, receiver): Least_squares::import_obs_data
+ * (least_squares.cpp:144-161). */
+int tomo_set_observed(tomo_ctx *ctx, const float *dobs);
+/* ||dobs - dcal||_2 in FP64 with dcal the receiver times of the last solve:
+ * Least_squares::converged (least_squares.cpp:301-319). */
+int tomo_data_residual(tomo_ctx *ctx, double *norm);
+
+typedef struct {
+    int iterations;     /* iterations run                                      */
+    double rnorm0;      /* ||B||                                               */
+    double rnorm;       /* ||B - A x|| after the last iteration                */
+    float ms;           /* device time                                         */
+} tomo_cgls_stats;
+
+/* CGLS on A x = [dobs - dcal ; 0]: Least_squares::optimization + sparse_cgls
+ * (least_squares.cpp:321-356, 424-496), FP32 vectors, FP64 inner products and step
+ * lengths, one persistent launch.  x_out (host, M floats) and history (host, ||B - A x||
+ * per iteration) may be NULL; the solution stays on the device for tomo_model_update. */
+int tomo_cgls(tomo_ctx *ctx, int iterations, float *x_out, double *history, tomo_cgls_stats *stats);
+
+typedef struct {
+    int smooth;                /* smooth (parameters.txt)                          */
+    int filter_samples;        /* filter_samples (odd)                             */
+    float standard_deviation;  /* standard_deviation                               */
+    int use_reference_masks;   /* 1 (default behaviour): the reference's hard-coded
+                                  interior masks (least_squares.cpp:520, 559);
+                                  0: no mask                                      */
+} tomo_update_opts;
+
+/* Least_squares::model_update (least_squares.cpp:498-570): trilinear coarse-to-fine of the
+ * CGLS solution, optional Gaussian smoothing (src/utils/smoothing/gaussian.cpp:5-73),
+ * slowness += dm, velocity = 1/slowness.  The device model is updated in place (as the
+ * reference updates Eikonal::slowness); velocity_out (host nz*nx*ny) may be NULL. */
+int tomo_model_update(tomo_ctx *ctx, const tomo_update_opts *opts, float *velocity_out);
+
+/* The reference's GPU CGLS entry point, sparse_cgls_gpu (src/utils/cgls/cgls.cuh:47):
+ * host COO (iA, jA, vA; rows need not be sorted), host B and x, N rows, M columns, NIT
+ * iterations, stop when ||A'(B - A x)|| < TOL.  Self-contained (own device buffers);
+ * returns a status instead of printing. */
+int tomo_sparse_cgls_gpu(const int *iA, const int *jA, const float *vA, const float *B, float *x, int N, int M,
+                         int NNZ, int NIT, float TOL);
 
 #ifdef __cplusplus
 }

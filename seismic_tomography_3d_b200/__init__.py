@@ -48,7 +48,8 @@ class Window(ctypes.Structure):
 
 class EikOpts(ctypes.Structure):
     _fields_ = [("op", ctypes.c_int), ("max_inner", ctypes.c_int), ("max_rounds", ctypes.c_int),
-                ("brick", ctypes.c_int), ("block_warps", ctypes.c_int)]
+                ("brick", ctypes.c_int), ("block_warps", ctypes.c_int), ("occupancy", ctypes.c_int),
+                ("change_tol", ctypes.c_float)]
 
 
 class EikStats(ctypes.Structure):
@@ -94,8 +95,62 @@ def load_library(path: str = LIB_PATH):
     return lib
 
 
+class JacobianOpts(ctypes.Structure):
+    _fields_ = [("dx", ctypes.c_float), ("dy", ctypes.c_float), ("dz", ctypes.c_float),
+                ("tk_order", ctypes.c_int), ("tk_param", ctypes.c_float), ("max_ray_steps", ctypes.c_int),
+                ("max_cells_per_ray", ctypes.c_int), ("illumination", ctypes.c_int)]
+
+
+class JacobianStats(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int)] + [
+        (n, ctypes.c_longlong) for n in ("rows", "cols", "nnz_rays", "nnz", "rays", "rays_ok", "rays_stalled",
+                                         "rays_capped", "rays_nonfinite", "rays_outside", "rays_overflow",
+                                         "ray_steps")] + [("ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class CglsStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("rnorm0", ctypes.c_double), ("rnorm", ctypes.c_double),
+                ("ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class UpdateOpts(ctypes.Structure):
+    _fields_ = [("smooth", ctypes.c_int), ("filter_samples", ctypes.c_int),
+                ("standard_deviation", ctypes.c_float), ("use_reference_masks", ctypes.c_int)]
+
+
 def _bind_tomography(lib):
-    """Bindings of the tomography half of the ABI (filled in as it grows)."""
+    """Bindings of the tomography half of the ABI."""
+    P, I, V = ctypes.POINTER, ctypes.c_int, ctypes.c_void_p
+    lib.tomo_build_jacobian.argtypes = [V, P(JacobianOpts), P(JacobianStats)]
+    lib.tomo_jacobian_copy.argtypes = [V, V, V, V]
+    lib.tomo_ray_status.argtypes = [V, V]
+    lib.tomo_illumination.argtypes = [V, V]
+    lib.tomo_set_observed.argtypes = [V, V]
+    lib.tomo_data_residual.argtypes = [V, P(ctypes.c_double)]
+    lib.tomo_cgls.argtypes = [V, I, V, V, P(CglsStats)]
+    lib.tomo_model_update.argtypes = [V, P(UpdateOpts), V]
+    lib.tomo_sparse_cgls_gpu.argtypes = [V, V, V, V, V, I, I, I, I, ctypes.c_float]
+
+
+def sparse_cgls_gpu(iA, jA, vA, B, N, M, nit, tol=0.0):
+    """The reference's sparse_cgls_gpu entry point (src/utils/cgls/cgls.cuh:47)."""
+    lib = load_library()
+    iA = np.ascontiguousarray(iA, np.int32)
+    jA = np.ascontiguousarray(jA, np.int32)
+    vA = np.ascontiguousarray(vA, np.float32)
+    B = np.ascontiguousarray(B, np.float32)
+    x = np.zeros(M, np.float32)
+    rc = lib.tomo_sparse_cgls_gpu(iA.ctypes.data, jA.ctypes.data, vA.ctypes.data, B.ctypes.data, x.ctypes.data,
+                                  N, M, len(vA), nit, tol)
+    if rc != TOMO_OK:
+        raise TomoError(rc, lib.tomo_status_string(rc).decode())
+    return x
 
 
 def _points(a):
@@ -171,7 +226,7 @@ class Context:
 
     # -- eikonal ------------------------------------------------------------------------
     def eik_solve(self, shots, windows=None, receivers=None, want_recv=True, max_inner=0, max_rounds=0,
-                  block_warps=0, op=0):
+                  block_warps=0, op=0, occupancy=0, change_tol=0.0):
         """Batched solve.  shots (n,3) metres; windows (n,4) [x0,x1,y0,y1] nodes or None;
         receivers (m,3).  Returns (t_recv (n,m) float32 or None, stats dict)."""
         sp, ns = _points(shots)
@@ -184,7 +239,7 @@ class Context:
         if receivers is not None and len(receivers):
             rp, nr = _points(receivers)
         out = np.empty((ns, nr), np.float32) if (want_recv and nr) else None
-        opts = EikOpts(op, max_inner, max_rounds, 0, block_warps)
+        opts = EikOpts(op, max_inner, max_rounds, 0, block_warps, occupancy, change_tol)
         st = EikStats()
         self._check(self.lib.tomo_eik_solve(self.h, ns, sp, wp, nr, rp,
                                             out.ctypes.data if out is not None else None,
@@ -195,6 +250,59 @@ class Context:
         w = Window()
         self._check(self.lib.tomo_eik_window(self.h, shot, ctypes.byref(w)))
         return (w.x0, w.x1, w.y0, w.y1)
+
+    # -- tomography ---------------------------------------------------------------------
+    def build_jacobian(self, d_tomo, tk_order=2, tk_param=0.1, max_ray_steps=0, max_cells_per_ray=0,
+                       illumination=False):
+        o = JacobianOpts(*map(float, d_tomo), tk_order, tk_param, max_ray_steps, max_cells_per_ray,
+                         int(illumination))
+        st = JacobianStats()
+        self._check(self.lib.tomo_build_jacobian(self.h, ctypes.byref(o), ctypes.byref(st)))
+        self.jac = st.as_dict()
+        return self.jac
+
+    def jacobian(self):
+        """A = [G ; lambda L] as CSR (row_ptr, cols, vals)."""
+        j = self.jac
+        rp = np.empty(j["rows"] + 1, np.int32)
+        cols = np.empty(j["nnz"], np.int32)
+        vals = np.empty(j["nnz"], np.float32)
+        self._check(self.lib.tomo_jacobian_copy(self.h, rp.ctypes.data, cols.ctypes.data, vals.ctypes.data))
+        return rp, cols, vals
+
+    def ray_status(self):
+        out = np.empty(self.jac["rays"], np.int32)
+        self._check(self.lib.tomo_ray_status(self.h, out.ctypes.data))
+        return out
+
+    def illumination(self):
+        out = np.empty(self.shape, np.float32)
+        self._check(self.lib.tomo_illumination(self.h, out.ctypes.data))
+        return out
+
+    def set_observed(self, dobs):
+        d = _f32(dobs)
+        self._check(self.lib.tomo_set_observed(self.h, d.ctypes.data))
+
+    def data_residual(self):
+        v = ctypes.c_double()
+        self._check(self.lib.tomo_data_residual(self.h, ctypes.byref(v)))
+        return v.value
+
+    def cgls(self, iterations=30, want_x=True):
+        x = np.empty(self.jac["cols"], np.float32) if want_x else None
+        hist = np.empty(max(iterations, 1), np.float64)
+        st = CglsStats()
+        self._check(self.lib.tomo_cgls(self.h, iterations, x.ctypes.data if x is not None else None,
+                                       hist.ctypes.data, ctypes.byref(st)))
+        return x, hist[:iterations], st.as_dict()
+
+    def model_update(self, smooth=True, filter_samples=5, standard_deviation=2.0, reference_masks=True,
+                     want_velocity=True):
+        o = UpdateOpts(int(smooth), filter_samples, standard_deviation, int(reference_masks))
+        v = np.empty(self.shape, np.float32) if want_velocity else None
+        self._check(self.lib.tomo_model_update(self.h, ctypes.byref(o), v.ctypes.data if v is not None else None))
+        return v
 
     def eik_volume(self, shot):
         x0, x1, y0, y1 = self.eik_window(shot)

@@ -13,6 +13,7 @@ using tomo::ShotDesc;
 namespace {
 
 constexpr int kDefaultMaxInner = 16;
+constexpr float kDefaultChangeTol = 1e-6f;
 constexpr int kDefaultMaxRounds = 1 << 20;
 constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~ seconds of polling, then error
 
@@ -217,6 +218,11 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     const int max_inner = (opts && opts->max_inner > 0) ? opts->max_inner : kDefaultMaxInner;
     const int max_rounds = (opts && opts->max_rounds > 0) ? opts->max_rounds : kDefaultMaxRounds;
     const int block_warps = (opts && opts->block_warps > 0) ? opts->block_warps : 8;
+    const int occupancy = (opts && opts->occupancy > 0) ? opts->occupancy : 4;
+    // Default: the reference's convergence threshold EPS = 1e-6 s (cuda_kernel.cuh:8).
+    float change_tol = kDefaultChangeTol;
+    if (opts && opts->change_tol > 0.f) change_tol = opts->change_tol;
+    if (opts && opts->change_tol < 0.f) change_tol = 0.f;
     CK(cudaSetDevice(ctx->device));
 
     // ---- per-shot descriptors --------------------------------------------------------
@@ -311,6 +317,7 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     p.gbz = ctx->gbz;
     p.h = g.dx;  // isotropic spacing h = dx (block_FIM.cpp:173)
     p.max_inner = max_inner;
+    p.change_tol = change_tol;
     p.max_rounds = max_rounds;
     p.local_bits = local_bits;
     p.spin_limit = kSpinLimit;
@@ -325,7 +332,7 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     p.nz = g.nz;
     int grid = 0;
     CK(cudaEventRecord(ctx->ev[3], ctx->stream));
-    CK(tomo::fim_solve(p, block_warps, &grid, ctx->stream));
+    CK(tomo::fim_solve(p, block_warps, occupancy, &grid, ctx->stream));
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     CK(cudaMemcpyAsync(ctx->pinned_ctrl, ctx->ctrl.ptr, tomo::kCtrlWords * sizeof(unsigned), cudaMemcpyDeviceToHost,
                        ctx->stream));

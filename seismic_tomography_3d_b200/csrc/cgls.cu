@@ -1,0 +1,162 @@
+// CGLS for the Tikhonov-regularised tomography system A x = B on the device (sm_100a).
+//
+// Same recurrence as Least_squares::sparse_cgls (src/tomography/least_squares/
+// least_squares.cpp:424-496) -- s = B, r = A's, p = r, q = A p, then per iteration
+// a = r'r/q'q, x += a p, s -= a q, r = A's, b = r'r/r'r_old, p = r + b p, q = A p --
+// with FP32 vectors and the matrix in CSR (A) and CSR of the transpose (A', so both
+// products are gathers, no atomics), and FP64 for every inner product, the step lengths
+// and the row sums.  One cooperative persistent launch runs all iterations; the four
+// grid-wide dependencies per iteration are software grid barriers with bounded waits.
+// Reductions are deterministic: fixed row-to-thread mapping, fixed-order block and grid
+// sums computed identically by every block.
+#include "common.cuh"
+#include "cgls.cuh"
+
+namespace tomo {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+// Block-wide FP64 sum in a fixed order; result valid in every thread.
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int i = 0; i < kWarps; i++) t += sh[i];
+    return t;
+}
+
+// Sum of the per-block partials (same order in every block).
+__device__ __forceinline__ double grid_sum(const double *partials, int nb, double *sh)
+{
+    double v = 0.0;
+    if (threadIdx.x < 32) {
+        for (int i = threadIdx.x; i < nb; i += 32) v += partials[i];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+        if (threadIdx.x == 0) sh[kWarps] = v;
+    }
+    __syncthreads();
+    v = sh[kWarps];
+    __syncthreads();
+    return v;
+}
+
+// y = M x for a CSR matrix with `G` lanes per row (FP64 row sums, FP32 output); returns
+// this thread's share of y'y.
+template <int G>
+__device__ __forceinline__ double spmv(const int *ptr, const int *idx, const float *val, const float *x, float *y,
+                                       int nrows)
+{
+    const int lane = threadIdx.x & 31;
+    const int sub = lane % G;
+    const long long gthread = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long groups = (long long)gridDim.x * blockDim.x / G;
+    const long long iters = (nrows + groups - 1) / groups;  // warp-uniform trip count
+    double local = 0.0;
+    for (long long it = 0; it < iters; it++) {
+        const long long row = gthread / G + it * groups;
+        double acc = 0.0;
+        if (row < nrows) {
+            const int b = __ldg(ptr + row), e = __ldg(ptr + row + 1);
+            for (int k = b + sub; k < e; k += G) acc += (double)__ldg(val + k) * (double)__ldg(x + __ldg(idx + k));
+        }
+        for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o, G);
+        if (row < nrows && sub == 0) {
+            const float yr = (float)acc;
+            y[row] = yr;
+            local += (double)yr * (double)yr;
+        }
+    }
+    return local;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads) k_cgls(CglsLaunch p)
+{
+    __shared__ double sh[kWarps + 1];
+    const int nb = gridDim.x;
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nth = (long long)gridDim.x * blockDim.x;
+    double *pa = p.partials, *pb = p.partials + nb, *pc = p.partials + 2 * nb;
+
+    // s = B, x = 0
+    for (long long i = tid; i < p.N; i += nth) p.s[i] = p.B[i];
+    for (long long i = tid; i < p.M; i += nth) p.x[i] = 0.0f;
+    if (!grid_barrier(p.ctrl, p.spin_limit)) return;
+    // r = A' s
+    double v = block_sum(spmv<32>(p.t_ptr, p.t_idx, p.t_val, p.s, p.r, p.M), sh);
+    if (threadIdx.x == 0) pa[blockIdx.x] = v;
+    if (!grid_barrier(p.ctrl, p.spin_limit)) return;
+    // p = r, q = A r (= A p)
+    for (long long i = tid; i < p.M; i += nth) p.p[i] = p.r[i];
+    v = block_sum(spmv<8>(p.a_ptr, p.a_idx, p.a_val, p.r, p.q, p.N), sh);
+    if (threadIdx.x == 0) pb[blockIdx.x] = v;
+    if (!grid_barrier(p.ctrl, p.spin_limit)) return;
+    double rTr = grid_sum(pa, nb, sh);
+    double qTq = grid_sum(pb, nb, sh);
+
+    for (int it = 0; it < p.nit; it++) {
+        const double a = rTr / qTq;
+        double ss = 0.0;
+        for (long long i = tid; i < p.M; i += nth) p.x[i] = (float)((double)p.x[i] + a * (double)p.p[i]);
+        for (long long i = tid; i < p.N; i += nth) {
+            const float si = (float)((double)p.s[i] - a * (double)p.q[i]);
+            p.s[i] = si;
+            ss += (double)si * (double)si;
+        }
+        v = block_sum(ss, sh);
+        if (threadIdx.x == 0) pc[blockIdx.x] = v;
+        if (!grid_barrier(p.ctrl, p.spin_limit)) return;
+        if (p.hist) {
+            const double sn = grid_sum(pc, nb, sh);
+            if (blockIdx.x == 0 && threadIdx.x == 0) p.hist[it] = sqrt(sn);
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kRounds] = (unsigned)(it + 1);
+        // sparse_cgls_gpu's exit test on the r of this iteration (src/utils/cgls/cgls.cu:102)
+        if (p.tol > 0.0 && sqrt(rTr) < p.tol) break;
+        // r = A' s
+        v = block_sum(spmv<32>(p.t_ptr, p.t_idx, p.t_val, p.s, p.r, p.M), sh);
+        if (threadIdx.x == 0) pa[blockIdx.x] = v;
+        if (!grid_barrier(p.ctrl, p.spin_limit)) return;
+        const double rTr_new = grid_sum(pa, nb, sh);
+        const double b = rTr_new / rTr;
+        rTr = rTr_new;
+        for (long long i = tid; i < p.M; i += nth) p.p[i] = (float)((double)p.r[i] + b * (double)p.p[i]);
+        if (!grid_barrier(p.ctrl, p.spin_limit)) return;
+        // q = A p
+        v = block_sum(spmv<8>(p.a_ptr, p.a_idx, p.a_val, p.p, p.q, p.N), sh);
+        if (threadIdx.x == 0) pb[blockIdx.x] = v;
+        if (!grid_barrier(p.ctrl, p.spin_limit)) return;
+        qTq = grid_sum(pb, nb, sh);
+    }
+}
+
+cudaError_t cgls_grid(int *grid)
+{
+    int dev = 0, nsm = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgls, kThreads, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    *grid = nsm * (per_sm < 4 ? per_sm : 4);
+    return cudaSuccess;
+}
+
+cudaError_t cgls_run(const CglsLaunch &p, int grid, cudaStream_t st)
+{
+    CglsLaunch pp = p;
+    void *args[] = {&pp};
+    return cudaLaunchCooperativeKernel((const void *)k_cgls, dim3(grid), dim3(kThreads), args, 0, st);
+}
+
+}  // namespace tomo

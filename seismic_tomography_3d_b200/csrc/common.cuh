@@ -23,6 +23,7 @@ enum CtrlSlot : int {
     kBarCount = 3, kBarGen = 4,       // grid barrier
     kErr = 5,                         // DevErr
     kRounds = 6,                      // rounds run (written by block 0)
+    kCur0 = 7, kCur1 = 8, kCur2 = 9,  // per-round fetch cursors (3-way rotation)
     kCtrlWords = 16,
 };
 

@@ -67,4 +67,26 @@ struct tomo_ctx {
 
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     unsigned *pinned_ctrl = nullptr;  // kCtrlWords + stats
+
+    // ---- tomography (api_tomography.cpp) -----------------------------------------------
+    // ray tracing scratch
+    tomo::DevBuf<uint2> runs;
+    tomo::DevBuf<int> nuniq, ray_status, ray_steps;
+    tomo::DevBuf<float> final_dist, spos, tk_coef, illum;
+    // A = [G ; lambda L] in CSR and its transpose
+    tomo::DevBuf<int> a_ptr, a_idx, t_ptr, t_idx;
+    tomo::DevBuf<float> a_val, t_val;
+    tomo::DevBuf<int> sort_keys, sort_keys_out, sort_pos, sort_pos_out, rows_of;
+    tomo::DevBuf<unsigned char> cub_temp;
+    int n_data = 0, n_model = 0, n_rows = 0, tk_order = 0;
+    int nxt = 0, nyt = 0, nzt = 0;
+    float dxt = 0, dyt = 0, dzt = 0;
+    long long nnz_g = 0, nnz = 0;
+    bool have_jacobian = false, have_illum = false;
+    // CGLS and model update
+    tomo::DevBuf<float> dobs, rhs, x, cg_s, cg_r, cg_p, cg_q;
+    tomo::DevBuf<double> partials, hist, norm2;
+    tomo::DevBuf<unsigned> cg_ctrl;
+    tomo::DevBuf<float> dm, dm_smooth, vel_out, gauss_kernel;
+    bool have_dobs = false, have_x = false;
 };

@@ -160,10 +160,11 @@ __device__ __forceinline__ void process_brick(const FimLaunch &p, unsigned item,
     ws.act += 1;
     ws.inner += (unsigned long long)it;
 
-    const unsigned m0 = __ballot_sync(kFull, c0 < i0);
-    const unsigned m1 = __ballot_sync(kFull, c1 < i1);
+    const bool any_drop = __any_sync(kFull, (c0 < i0) | (c1 < i1));
+    const unsigned m0 = __ballot_sync(kFull, c0 < i0 - p.change_tol);
+    const unsigned m1 = __ballot_sync(kFull, c1 < i1 - p.change_tol);
     const unsigned mm = m0 | m1;
-    if (mm) {
+    if (any_drop) {
         __stcg(Tb + lane, c0);
         __stcg(Tb + 32 + lane, c1);
     }
@@ -205,13 +206,12 @@ __device__ __forceinline__ void process_brick(const FimLaunch &p, unsigned item,
     }
 }
 
-__global__ void __launch_bounds__(256) k_fim_solve(FimLaunch p)
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
 {
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5;
     float *tile = smem + warp * kTileNodes;
-    const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
-    const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     WarpStats ws{0ull, 0ull};
 
     unsigned round = 0;
@@ -225,9 +225,20 @@ __global__ void __launch_bounds__(256) k_fim_solve(FimLaunch p)
             ok = false;
             break;
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kCnt0 + (round + 2u) % 3u] = 0u;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            p.ctrl[kCnt0 + (round + 2u) % 3u] = 0u;
+            p.ctrl[kCur0 + (round + 2u) % 3u] = 0u;
+        }
+        // Items are fetched one at a time from the round's cursor, so warps that draw
+        // cheap bricks take more of them and the round ends together.
         const unsigned *list = p.lists + (size_t)cur * p.list_cap;
-        for (unsigned i = gwarp; i < n; i += nwarps) process_brick(p, __ldcg(list + i), round, tile, ws);
+        for (;;) {
+            unsigned i = 0;
+            if ((threadIdx.x & 31) == 0) i = atomicAdd(p.ctrl + kCur0 + cur, 1u);
+            i = __shfl_sync(kFull, i, 0);
+            if (i >= n) break;
+            process_brick(p, __ldcg(list + i), round, tile, ws);
+        }
         if (!grid_barrier(p.ctrl, p.spin_limit)) { ok = false; break; }
         ++round;
     }
@@ -386,9 +397,9 @@ cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx,
     return cudaGetLastError();
 }
 
-cudaError_t fim_solve(const FimLaunch &p, int block_warps, int *grid_out, cudaStream_t st)
+template <int MINB>
+static cudaError_t launch_solve(const FimLaunch &p, int block_warps, int *grid_out, cudaStream_t st)
 {
-    if (block_warps < 1 || block_warps > 8) block_warps = 8;
     const int threads = 32 * block_warps;
     const size_t smem = (size_t)block_warps * kTileNodes * sizeof(float);
     int dev = 0, nsm = 0, per_sm = 0;
@@ -396,14 +407,25 @@ cudaError_t fim_solve(const FimLaunch &p, int block_warps, int *grid_out, cudaSt
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fim_solve, threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fim_solve<MINB>, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int grid = nsm * per_sm;
     if (grid_out) *grid_out = grid;
     FimLaunch pp = p;
     void *args[] = {&pp};
-    return cudaLaunchCooperativeKernel((const void *)k_fim_solve, dim3(grid), dim3(threads), args, smem, st);
+    return cudaLaunchCooperativeKernel((const void *)k_fim_solve<MINB>, dim3(grid), dim3(threads), args, smem, st);
+}
+
+cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, int *grid_out, cudaStream_t st)
+{
+    if (block_warps < 1 || block_warps > 8) block_warps = 8;
+    switch (occupancy) {
+    case 1: return launch_solve<1>(p, block_warps, grid_out, st);
+    case 2: return launch_solve<2>(p, block_warps, grid_out, st);
+    case 4: return launch_solve<4>(p, block_warps, grid_out, st);
+    default: return launch_solve<3>(p, block_warps, grid_out, st);
+    }
 }
 
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out, cudaStream_t st)

@@ -35,6 +35,7 @@ struct FimLaunch {
     int gbx, gbz;         // global brick grid (x, z) for S addressing
     float h;              // grid spacing of the update (dx, as the reference)
     int max_inner, max_rounds;
+    float change_tol;     // face drops <= this do not re-queue the neighbour
     unsigned local_bits;  // item = shot << local_bits | local brick
     unsigned long long spin_limit;
     // receivers
@@ -52,7 +53,7 @@ cudaError_t fim_init(float *T, size_t t_count, unsigned *qflag, size_t q_count, 
                      unsigned long long *stats, cudaStream_t st);
 cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
                      unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st);
-cudaError_t fim_solve(const FimLaunch &p, int block_warps, int *grid_out, cudaStream_t st);
+cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, int *grid_out, cudaStream_t st);
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out,
                         cudaStream_t st);
 cudaError_t velocity_to_slowness(const float *v, float *s, size_t n, cudaStream_t st);

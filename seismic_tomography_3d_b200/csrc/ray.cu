@@ -1,0 +1,268 @@
+// Ray tracing through the device-resident traveltime fields into the sparse Frechet
+// matrix G, the Tikhonov rows and the transposed matrix (sm_100a).
+//
+// One thread marches one ray (rows are independent, as in the reference's per-receiver
+// loop, src/tomography/least_squares/least_squares.cpp:205-279).  The FP32 arithmetic of
+// the march, the binning and the run-length values is restated operation for operation
+// with round-to-nearest intrinsics, so with the same traveltime field the Jacobian is
+// bit-identical to the reference's COO (iG, jG, vG).  Cells are run-length encoded while
+// marching (a ray re-enters a cell rarely), then sorted per ray, which is the reference's
+// std::sort + run-length pass without materialising one index per step.
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+#include "ray.cuh"
+
+namespace tomo {
+
+namespace {
+
+// Traveltime of window-local node (z, x, y) of shot d (brick-major pool).
+__device__ __forceinline__ float t_node(const float *T, const ShotDesc &d, int x, int y, int z)
+{
+    const long long b = (z >> 2) + (long long)d.nbz * ((x >> 2) + (long long)d.nbx * (y >> 2));
+    return __ldg(T + d.t_off + b * kBrickNodes + (z & 3) + 4 * (x & 3) + 16 * (y & 3));
+}
+
+// expand_fdm (least_squares.cpp:11-67) adds a replicated one-node halo: expanded index
+// (i, j, k) reads the cropped node (i-1, j-1, k-1) clamped into the field.  Beyond the
+// halo (undefined in the reference) the clamp continues.
+__device__ __forceinline__ float t_exp(const float *T, const ShotDesc &d, int nz, int i, int j, int k)
+{
+    const int z = min(max(i - 1, 0), nz - 1);
+    const int x = min(max(j - 1, 0), d.wnx - 1);
+    const int y = min(max(k - 1, 0), d.wny - 1);
+    return t_node(T, d, x, y, z);
+}
+
+__device__ __forceinline__ int trunc_div(float a, float b) { return (int)fdiv(a, b); }
+
+}  // namespace
+
+__global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
+{
+    const long long nrays = (long long)p.nshots * p.nrec;
+    const float rayStep = fmul(0.2f, p.dz);  // least_squares.cpp:203
+    for (long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x; ray < nrays;
+         ray += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(ray / p.nrec), r = (int)(ray % p.nrec);
+        const ShotDesc &d = p.shots[s];
+        const float ox = fmul((float)d.wx0, p.dx), oy = fmul((float)d.wy0, p.dy);
+        const float sxg = p.spos[s], syg = p.spos[p.nshots + s], sz = p.spos[2 * p.nshots + s];
+        const float sx = fsub(sxg, ox), sy = fsub(syg, oy);
+        // source cell (least_squares.cpp:197-201) and source floor node (stall guard)
+        const int sId = trunc_div(sz, p.dzt) + trunc_div(sxg, p.dxt) * p.nzt + trunc_div(syg, p.dyt) * p.nxt * p.nzt;
+        const int snz = trunc_div(sz, p.dz), snx = trunc_div(sx, p.dx), sny = trunc_div(sy, p.dy);
+
+        float zi = p.rz[r], xi = fsub(p.rx[r], ox), yi = fsub(p.ry[r], oy);
+        uint2 *runs = p.runs + ray * (long long)p.cap_runs;
+        int nr = 0, L = 0, st = kRayCapped;
+        bool overflow = false;
+        unsigned cur = 0xffffffffu, cnt = 0;
+        if (xi < 0.0f || yi < 0.0f || xi > fmul((float)(d.wnx - 1), p.dx) || yi > fmul((float)(d.wny - 1), p.dy)) {
+            st = kRayOutside;  // receiver outside this shot's window
+            L = p.max_steps;   // skip the march
+        }
+        const float two_dz = fmul(2.0f, p.dz), two_dx = fmul(2.0f, p.dx), two_dy = fmul(2.0f, p.dy);
+        while (L < p.max_steps) {
+            const int i = trunc_div(zi, p.dz) + 1, j = trunc_div(xi, p.dx) + 1, k = trunc_div(yi, p.dy) + 1;
+            const float dTz = fdiv(fsub(t_exp(p.T, d, p.nz, i + 1, j, k), t_exp(p.T, d, p.nz, i - 1, j, k)), two_dz);
+            const float dTx = fdiv(fsub(t_exp(p.T, d, p.nz, i, j + 1, k), t_exp(p.T, d, p.nz, i, j - 1, k)), two_dx);
+            const float dTy = fdiv(fsub(t_exp(p.T, d, p.nz, i, j, k + 1), t_exp(p.T, d, p.nz, i, j, k - 1)), two_dy);
+            const float norm = __fsqrt_rn(fadd(fadd(fmul(dTx, dTx), fmul(dTy, dTy)), fmul(dTz, dTz)));
+            zi = fsub(zi, fdiv(fmul(rayStep, dTz), norm));
+            xi = fsub(xi, fdiv(fmul(rayStep, dTx), norm));
+            yi = fsub(yi, fdiv(fmul(rayStep, dTy), norm));
+            if (!isfinite(zi) || !isfinite(xi) || !isfinite(yi)) {
+                st = kRayNonFinite;
+                break;
+            }
+            const int im = trunc_div(zi, p.dzt), jm = trunc_div(fadd(xi, ox), p.dxt), km = trunc_div(fadd(yi, oy), p.dyt);
+            if (im < 0 || im >= p.nzt || jm < 0 || jm >= p.nxt || km < 0 || km >= p.nyt) {
+                st = kRayOutside;
+                break;
+            }
+            const unsigned cell = (unsigned)(im + jm * p.nzt + km * p.nxt * p.nzt);
+            ++L;
+            if (cell == cur) {
+                ++cnt;
+            } else {
+                if (cnt) {
+                    if (nr < p.cap_runs) runs[nr++] = make_uint2(cur, cnt);
+                    else overflow = true;
+                }
+                cur = cell;
+                cnt = 1;
+            }
+            if (p.illum) {  // expanded (i,j,k) with cropped strides (least_squares.cpp:234)
+                const long long li = i + (long long)j * p.nz + (long long)k * p.model_nx * p.nz;
+                if (li >= 0 && li < (long long)p.nz * p.model_nx * p.model_ny) atomicAdd(p.illum + li, rayStep);
+            }
+            if ((int)cell == sId) {
+                st = kRayOk;
+                break;
+            }
+            if (trunc_div(zi, p.dz) == snz && trunc_div(xi, p.dx) == snx && trunc_div(yi, p.dy) == sny) {
+                st = kRayStalled;
+                break;
+            }
+        }
+        if (cnt) {
+            if (nr < p.cap_runs) runs[nr++] = make_uint2(cur, cnt);
+            else overflow = true;
+        }
+        // sort the runs by cell and merge repeated cells (std::sort + run-length, :241-263)
+        for (int a = 1; a < nr; a++) {
+            const uint2 key = runs[a];
+            int b = a - 1;
+            while (b >= 0 && runs[b].x > key.x) {
+                runs[b + 1] = runs[b];
+                --b;
+            }
+            runs[b + 1] = key;
+        }
+        int w = 0;
+        for (int a = 0; a < nr; a++) {
+            const uint2 e = runs[a];
+            if (w > 0 && runs[w - 1].x == e.x) runs[w - 1].y += e.y;
+            else runs[w++] = e;
+        }
+        if (overflow) {
+            st = kRayOverflow;
+            w = 0;
+        }
+        p.nuniq[ray] = w;
+        p.status[ray] = st;
+        p.steps[ray] = L;
+        const float ez = fsub(zi, sz), ex = fsub(xi, sx), ey = fsub(yi, sy);
+        p.final_dist[ray] = __fsqrt_rn(fadd(fadd(fmul(ez, ez), fmul(ex, ex)), fmul(ey, ey)));
+    }
+}
+
+// Values of the run-length entries: the reference accumulates rayStep once per step by
+// repeated FP32 addition, starting from rayStep; the first (smallest) cell gets one extra
+// step and the source cell gets the final distance to the source (:243-276).
+__global__ void __launch_bounds__(128) k_ray_emit(RayLaunch p, const int *row_ptr, int *cols, float *vals)
+{
+    const long long nrays = (long long)p.nshots * p.nrec;
+    const float rayStep = fmul(0.2f, p.dz);
+    for (long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x; ray < nrays;
+         ray += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(ray / p.nrec);
+        const float sxg = p.spos[s], syg = p.spos[p.nshots + s], sz = p.spos[2 * p.nshots + s];
+        const int sId = trunc_div(sz, p.dzt) + trunc_div(sxg, p.dxt) * p.nzt + trunc_div(syg, p.dyt) * p.nxt * p.nzt;
+        const uint2 *runs = p.runs + ray * (long long)p.cap_runs;
+        const int n = p.nuniq[ray];
+        const int base = row_ptr[ray];
+        const float fd = p.final_dist[ray];
+        for (int k = 0; k < n; k++) {
+            const uint2 e = runs[k];
+            float v = rayStep;
+            const unsigned adds = (k == 0) ? e.y : e.y - 1u;
+            for (unsigned t = 0; t < adds; t++) v = fadd(v, rayStep);
+            cols[base + k] = (int)e.x;
+            vals[base + k] = ((int)e.x == sId) ? fd : v;
+        }
+    }
+}
+
+// Least_squares::tk_reg_matrix (:358-422): row n_data + t holds lambda*df[k] at column t+k.
+__global__ void k_tk_rows(int n_data_rows, long long nnz_g, int n_model, int tk_order, const float *coef, int *row_ptr,
+                          int *cols, float *vals)
+{
+    const int e = tk_order + 1;
+    const int nL = n_model - tk_order;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t <= nL; t += gridDim.x * blockDim.x) {
+        row_ptr[n_data_rows + t] = (int)(nnz_g + (long long)e * t);
+        if (t < nL)
+            for (int k = 0; k < e; k++) {
+                cols[nnz_g + (long long)e * t + k] = t + k;
+                vals[nnz_g + (long long)e * t + k] = coef[k];
+            }
+    }
+}
+
+__global__ void k_transpose_prepare(const int *row_ptr, const int *cols, int nrows, int *keys, int *pos, int *rows_of)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x)
+        for (int k = row_ptr[r]; k < row_ptr[r + 1]; k++) {
+            keys[k] = cols[k];
+            pos[k] = k;
+            rows_of[k] = r;
+        }
+}
+
+__global__ void k_transpose_finish(const int *sorted_pos, const int *rows_of, const float *vals, long long nnz, int ncols,
+                                   const int *sorted_keys, int *t_ptr, int *t_rows, float *t_vals)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nnz; k += (long long)gridDim.x * blockDim.x) {
+        const int src = sorted_pos[k];
+        t_rows[k] = rows_of[src];
+        t_vals[k] = vals[src];
+        const int c = sorted_keys[k];
+        const int prev = (k == 0) ? -1 : sorted_keys[k - 1];
+        for (int q = prev + 1; q <= c; q++) t_ptr[q] = (int)k;
+        if (k == nnz - 1)
+            for (int q = c + 1; q <= ncols; q++) t_ptr[q] = (int)nnz;
+    }
+    if (nnz == 0 && blockIdx.x == 0)
+        for (int q = threadIdx.x; q <= ncols; q += blockDim.x) t_ptr[q] = 0;
+}
+
+static int grid_for(long long n, int threads)
+{
+    long long g = (n + threads - 1) / threads;
+    if (g > 148LL * 32) g = 148LL * 32;
+    return g < 1 ? 1 : (int)g;
+}
+
+cudaError_t ray_march(const RayLaunch &p, cudaStream_t st)
+{
+    k_ray_march<<<grid_for((long long)p.nshots * p.nrec, 128), 128, 0, st>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t ray_emit(const RayLaunch &p, const int *row_ptr, int *cols, float *vals, cudaStream_t st)
+{
+    k_ray_emit<<<grid_for((long long)p.nshots * p.nrec, 128), 128, 0, st>>>(p, row_ptr, cols, vals);
+    return cudaGetLastError();
+}
+
+cudaError_t tk_rows(int n_data_rows, long long nnz_g, int n_model, int tk_order, const float *coef, int *row_ptr,
+                    int *cols, float *vals, cudaStream_t st)
+{
+    k_tk_rows<<<grid_for(n_model + 1, 256), 256, 0, st>>>(n_data_rows, nnz_g, n_model, tk_order, coef, row_ptr, cols,
+                                                          vals);
+    return cudaGetLastError();
+}
+
+cudaError_t csr_transpose_prepare(const int *row_ptr, const int *cols, int nrows, long long nnz, int *keys, int *pos,
+                                  int *rows_of, cudaStream_t st)
+{
+    (void)nnz;
+    k_transpose_prepare<<<grid_for(nrows, 256), 256, 0, st>>>(row_ptr, cols, nrows, keys, pos, rows_of);
+    return cudaGetLastError();
+}
+
+cudaError_t csr_transpose_finish(const int *sorted_pos, const int *rows_of, const float *vals, long long nnz, int ncols,
+                                 const int *sorted_keys, int *t_ptr, int *t_rows, float *t_vals, cudaStream_t st)
+{
+    k_transpose_finish<<<grid_for(nnz > 0 ? nnz : 1, 256), 256, 0, st>>>(sorted_pos, rows_of, vals, nnz, ncols,
+                                                                        sorted_keys, t_ptr, t_rows, t_vals);
+    return cudaGetLastError();
+}
+
+// CUB device primitives (scan, stable radix sort) used for the CSR set-up.
+cudaError_t scan_exclusive(const int *in, int *out, int n, void *temp, size_t *temp_bytes, cudaStream_t st)
+{
+    return cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, in, out, n, st);
+}
+
+cudaError_t sort_pairs(const int *keys_in, int *keys_out, const int *vals_in, int *vals_out, long long n, int key_bits,
+                       void *temp, size_t *temp_bytes, cudaStream_t st)
+{
+    return cub::DeviceRadixSort::SortPairs(temp, *temp_bytes, keys_in, keys_out, vals_in, vals_out, (int)n, 0, key_bits,
+                                           st);
+}
+
+}  // namespace tomo

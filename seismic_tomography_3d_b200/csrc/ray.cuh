@@ -1,0 +1,56 @@
+// Ray tracing through the device-resident traveltime fields into the sparse Frechet
+// matrix, Tikhonov rows, transpose, CGLS and model update: shared declarations.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fim.cuh"
+
+namespace tomo {
+
+// Ray status (same codes as the CPU oracle).
+enum RayStatus : int {
+    kRayOk = 0,        // reached the source cell (reference stop rule)
+    kRayStalled = 1,   // entered the source node box outside the source cell
+    kRayCapped = 2,    // step cap
+    kRayNonFinite = 3, // zero gradient -> NaN position
+    kRayOutside = 4,   // left the inversion grid / receiver outside the window
+    kRayOverflow = 5,  // more distinct cells than the per-ray capacity
+};
+
+struct RayLaunch {
+    const float *T;
+    const ShotDesc *shots;
+    int nshots;
+    const float *spos;    // 3*nshots: x | y | z (metres)
+    const float *rx, *ry, *rz;
+    int nrec;
+    int nz;               // model nz
+    float dx, dy, dz;
+    float dxt, dyt, dzt;  // inversion cell size
+    int nxt, nyt, nzt;    // inversion grid
+    int max_steps;
+    int cap_runs;         // per-ray capacity of distinct cells
+    uint2 *runs;          // nrays*cap_runs (cell, count), sorted by cell on exit
+    int *nuniq;           // per ray: distinct cells
+    int *status, *steps;
+    float *final_dist;
+    float *illum;         // nz*nx*ny of the model or nullptr (full windows only)
+    int model_nx, model_ny;
+};
+
+cudaError_t ray_march(const RayLaunch &p, cudaStream_t st);
+cudaError_t ray_emit(const RayLaunch &p, const int *row_ptr, int *cols, float *vals, cudaStream_t st);
+cudaError_t tk_rows(int n_data_rows, long long nnz_g, int n_model, int tk_order, const float *coef, int *row_ptr,
+                    int *cols, float *vals, cudaStream_t st);
+cudaError_t csr_transpose_prepare(const int *row_ptr, const int *cols, int nrows, long long nnz, int *keys,
+                                  int *pos, int *rows_of, cudaStream_t st);
+// CUB device-wide primitives (temp == nullptr queries *temp_bytes).
+cudaError_t scan_exclusive(const int *in, int *out, int n, void *temp, size_t *temp_bytes, cudaStream_t st);
+cudaError_t sort_pairs(const int *keys_in, int *keys_out, const int *vals_in, int *vals_out, long long n, int key_bits,
+                       void *temp, size_t *temp_bytes, cudaStream_t st);
+cudaError_t csr_transpose_finish(const int *sorted_pos, const int *rows_of, const float *vals, long long nnz, int ncols,
+                                 const int *sorted_keys, int *t_ptr, int *t_rows, float *t_vals, cudaStream_t st);
+
+}  // namespace tomo

@@ -61,12 +61,12 @@ def make_cpu():
     make_tomo()
 
 
-def make_gpu():
+def make_gpu(out_dir=HERE):
     data = {}
     for seed, v, h, shots in eik_models():
         T, _ = oracle.ref_solve(oracle.REF_BLOCK_FIM, v, h, shots)
         data[f"fim_{seed}"] = T
-    np.savez_compressed(os.path.join(HERE, "block_fim_ref.npz"), **data)
+    np.savez_compressed(os.path.join(out_dir, "block_fim_ref.npz"), **data)
 
 
 # --------------------------------------------------------------------------------------
@@ -189,8 +189,9 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--cpu", action="store_true")
     ap.add_argument("--gpu", action="store_true")
+    ap.add_argument("--out", default=HERE, help="output folder of the GPU fixtures")
     a = ap.parse_args()
     if a.cpu:
         make_cpu()
     if a.gpu:
-        make_gpu()
+        make_gpu(a.out)

@@ -1,0 +1,226 @@
+"""Ray tracing, Jacobian, CGLS and model update on the device vs the CPU oracle.
+
+The oracle restatement of these steps reproduces the reference tomography.exe bit for bit
+(tests/test_oracle_cpu.py).  Here the device path is fed the SAME traveltime fields (the
+device's own, copied back) so that:
+  * the Jacobian (columns, run-length values, ray status, illumination) is bit-identical;
+  * the CGLS solution (FP32 vectors, FP64 reductions) matches the FP64 oracle CGLS to a
+    relative L2 error below 1e-4;
+  * the model update (trilinear + Gaussian + masks) is bit-identical given the same x;
+  * a full iteration recovers the same model as the oracle pipeline within 0.5 % RMS.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import make_golden as mg  # noqa: E402
+
+from seismic_tomography_3d_b200 import workloads as wl  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+MAX_STEPS = 6000
+
+
+def n_tomo(nx, ny, nz, h, d):
+    return [int(np.float32((n - 1) * np.float32(h)) / np.float32(dd)) + 1 for n, dd in zip((nx, ny, nz), d)]
+
+
+def oracle_G(oracle_mod, vols, h, shots, rec, d, nt, illum=False):
+    rows, cols, vals, status = [], [], [], []
+    il = None
+    nrec = len(rec)
+    for i, sh in enumerate(shots):
+        rt = oracle_mod.raytrace(vols[i], h, sh, *rec.T, d, nt, max_steps=MAX_STEPS, illum=illum)
+        status.append(rt["status"])
+        if illum:
+            il = rt["illum"] if il is None else il + rt["illum"]
+        rp = rt["row_ptr"]
+        for r in range(nrec):
+            for k in range(rp[r], rp[r + 1]):
+                rows.append(i * nrec + r)
+                cols.append(rt["cols"][k])
+                vals.append(rt["vals"][k])
+    return np.array(rows, np.int64), np.array(cols, np.int32), np.array(vals, np.float32), np.concatenate(status), il
+
+
+def csr_to_coo(rp):
+    return np.repeat(np.arange(len(rp) - 1), np.diff(rp))
+
+
+@pytest.fixture(scope="module")
+def small_survey():
+    g = np.load(os.path.join(HERE, "golden", "tomo_ref.npz"))
+    t = mg.TOMO
+    return dict(nx=t["nx"], ny=t["ny"], nz=t["nz"], h=t["h"], true_v=g["true_v"], start_v=g["start_v"],
+                shots=g["shots"], nodes=g["nodes"], d=(100.0, 100.0, 100.0))
+
+
+def _solve(tomo, sv, v, shots, rec):
+    ctx = tomo.Context(sv["nx"], sv["ny"], sv["nz"], sv["h"])
+    ctx.set_velocity(v)
+    dcal, _ = ctx.eik_solve(shots, receivers=rec)
+    vols = [ctx.eik_volume(i) for i in range(len(shots))]
+    return ctx, dcal, vols
+
+
+def test_jacobian_bit_exact(tomo, oracle_mod, small_survey):
+    sv = small_survey
+    ctx, dcal, vols = _solve(tomo, sv, sv["start_v"], sv["shots"], sv["nodes"])
+    with ctx:
+        st = ctx.build_jacobian(sv["d"], tk_order=2, tk_param=0.5, max_ray_steps=MAX_STEPS, illumination=True)
+        rp, cols, vals = ctx.jacobian()
+        status = ctx.ray_status()
+        illum = ctx.illumination()
+    nt = n_tomo(sv["nx"], sv["ny"], sv["nz"], sv["h"], sv["d"])
+    assert (st["nx"], st["ny"], st["nz"]) == tuple(nt)
+    r_o, c_o, v_o, s_o, il_o = oracle_G(oracle_mod, vols, sv["h"], sv["shots"], sv["nodes"], sv["d"], nt, illum=True)
+    ng = st["nnz_rays"]
+    assert ng == len(c_o)
+    np.testing.assert_array_equal(csr_to_coo(rp)[:ng], r_o)
+    np.testing.assert_array_equal(cols[:ng], c_o)
+    np.testing.assert_array_equal(vals[:ng], v_o)
+    np.testing.assert_array_equal(status, s_o)
+    np.testing.assert_array_equal(illum, il_o)
+    # Tikhonov rows: lambda * [1, -2, 1] on consecutive flattened cells
+    M = nt[0] * nt[1] * nt[2]
+    nd = len(sv["shots"]) * len(sv["nodes"])
+    assert st["rows"] == nd + M - 2 and st["cols"] == M
+    L = vals[ng:].reshape(-1, 3)
+    np.testing.assert_array_equal(L, np.tile(np.float32(0.5) * np.array([1, -2, 1], np.float32), (M - 2, 1)))
+    np.testing.assert_array_equal(cols[ng:].reshape(-1, 3), np.arange(M - 2)[:, None] + np.arange(3)[None, :])
+
+
+def test_jacobian_stall_rule_matches_oracle(tomo, oracle_mod):
+    """51 m cells on a 12.5 m grid: cell faces split some source-node boxes, so reference
+    rays would loop forever next to the source.  Both sides cut them by the same rule."""
+    nx, ny, nz, h = 49, 45, 21, 12.5
+    rng = np.random.default_rng(3)
+    v = (wl.gradient_model(nx, ny, nz, h, 1500.0, 1.0) * wl._anomalies(rng, nx, ny, nz, h, 2, sigma=60.0)).astype(np.float32)
+    shots = np.array([[12 * h, 10 * h, 0.0], [33 * h, 31 * h, 0.0], [41 * h, 8 * h, 0.0]], np.float32)
+    rec = wl.regular_receivers(9, 2 * h, 42 * h)
+    d = (51.0, 51.0, 52.0)
+    with tomo.Context(nx, ny, nz, h) as ctx:
+        ctx.set_velocity(v)
+        ctx.eik_solve(shots, receivers=rec)
+        vols = [ctx.eik_volume(i) for i in range(len(shots))]
+        st = ctx.build_jacobian(d, tk_order=2, tk_param=0.1, max_ray_steps=MAX_STEPS)
+        rp, cols, vals = ctx.jacobian()
+        status = ctx.ray_status()
+    nt = n_tomo(nx, ny, nz, h, d)
+    r_o, c_o, v_o, s_o, _ = oracle_G(oracle_mod, vols, h, shots, rec, d, nt)
+    np.testing.assert_array_equal(status, s_o)
+    ng = st["nnz_rays"]
+    np.testing.assert_array_equal(cols[:ng], c_o)
+    np.testing.assert_array_equal(vals[:ng], v_o)
+    assert st["rays_ok"] + st["rays_stalled"] == st["rays"]
+
+
+def _coo(rp, cols, vals):
+    return csr_to_coo(rp).astype(np.int32), cols, vals
+
+
+def test_cgls_matches_fp64_oracle_and_update_bit_exact(tomo, oracle_mod, small_survey):
+    sv = small_survey
+    # observed picks from the true model with the device solver (+ noise)
+    with tomo.Context(sv["nx"], sv["ny"], sv["nz"], sv["h"]) as c0:
+        c0.set_velocity(sv["true_v"])
+        dobs, _ = c0.eik_solve(sv["shots"], receivers=sv["nodes"])
+    dobs = dobs + np.random.default_rng(1).normal(0, 1e-3, dobs.shape).astype(np.float32)
+    ctx, dcal, vols = _solve(tomo, sv, sv["start_v"], sv["shots"], sv["nodes"])
+    with ctx:
+        ctx.set_observed(dobs)
+        res = ctx.data_residual()
+        assert np.isclose(res, np.sqrt(np.sum((dobs.astype(np.float64) - dcal) ** 2)), rtol=1e-12)
+        jst = ctx.build_jacobian(sv["d"], tk_order=2, tk_param=0.5, max_ray_steps=MAX_STEPS)
+        rp, cols, vals = ctx.jacobian()
+        x, hist, cst = ctx.cgls(30)
+        vel = ctx.model_update(smooth=True, filter_samples=5, standard_deviation=2.0)
+        s_after = ctx.get_slowness()
+    N, M = len(rp) - 1, jst["cols"]
+    iA, jA, vA = _coo(rp, cols, vals)
+    B = np.zeros(N, np.float32)
+    B[:dobs.size] = (dobs - dcal).ravel()
+    x64, h64 = oracle_mod.cgls_f64(N, M, iA, jA, vA, B, 30)
+    assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-4
+    np.testing.assert_allclose(hist, h64, rtol=1e-5)
+    assert np.all(np.diff(hist) <= 1e-12 * hist[0])
+    assert cst["iterations"] == 30
+    # model update, same x -> bit-identical velocity and slowness
+    nt = n_tomo(sv["nx"], sv["ny"], sv["nz"], sv["h"], sv["d"])
+    start_s = (np.float32(1.0) / sv["start_v"]).astype(np.float32)
+    s_o, vel_o = oracle_mod.model_update(start_s, sv["h"], sv["d"], nt, x, True, 5, 2.0)
+    np.testing.assert_array_equal(vel, vel_o)
+    np.testing.assert_array_equal(s_after, s_o)
+
+
+def test_model_update_options(tomo, oracle_mod, small_survey):
+    sv = small_survey
+    ctx, dcal, _ = _solve(tomo, sv, sv["start_v"], sv["shots"], sv["nodes"])
+    with ctx:
+        ctx.set_observed(dcal + np.float32(1e-3))
+        ctx.build_jacobian(sv["d"], tk_order=1, tk_param=0.2, max_ray_steps=MAX_STEPS)
+        x, _, _ = ctx.cgls(10)
+        vel = ctx.model_update(smooth=False)
+    nt = n_tomo(sv["nx"], sv["ny"], sv["nz"], sv["h"], sv["d"])
+    start_s = (np.float32(1.0) / sv["start_v"]).astype(np.float32)
+    _, vel_o = oracle_mod.model_update(start_s, sv["h"], sv["d"], nt, x, False, 5, 2.0)
+    np.testing.assert_array_equal(vel, vel_o)
+
+
+def test_sparse_cgls_gpu_entry_point(tomo, oracle_mod):
+    rng = np.random.default_rng(5)
+    N, M, nnz = 900, 300, 6000
+    iA = rng.integers(0, N, nnz).astype(np.int32)
+    jA = rng.integers(0, M, nnz).astype(np.int32)
+    vA = rng.uniform(0.1, 2.0, nnz).astype(np.float32)
+    B = rng.standard_normal(N).astype(np.float32)
+    x = tomo.sparse_cgls_gpu(iA, jA, vA, B, N, M, 25)
+    x64, _ = oracle_mod.cgls_f64(N, M, iA, jA, vA, B, 25)
+    assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-4
+    # TOL exit: a huge tolerance stops after the first update (x = a0 * A'B)
+    x1 = tomo.sparse_cgls_gpu(iA, jA, vA, B, N, M, 25, tol=1e30)
+    x1o, _ = oracle_mod.cgls_f64(N, M, iA, jA, vA, B, 1)
+    assert np.linalg.norm(x1 - x1o) / np.linalg.norm(x1o) < 1e-5
+    with pytest.raises(tomo.TomoError):
+        tomo.sparse_cgls_gpu(iA, jA + M, vA, B, N, M, 5)  # column out of range
+
+
+def test_full_iteration_recovered_model(tomo, oracle_mod, small_survey):
+    """Device iteration vs the oracle pipeline on the device traveltimes: recovered
+    velocity models agree within 0.5 % RMS; in practice ~1e-7."""
+    sv = small_survey
+    with tomo.Context(sv["nx"], sv["ny"], sv["nz"], sv["h"]) as c0:
+        c0.set_velocity(sv["true_v"])
+        dobs, _ = c0.eik_solve(sv["shots"], receivers=sv["nodes"])
+    ctx, dcal, vols = _solve(tomo, sv, sv["start_v"], sv["shots"], sv["nodes"])
+    with ctx:
+        ctx.set_observed(dobs)
+        ctx.build_jacobian(sv["d"], tk_order=2, tk_param=0.5, max_ray_steps=MAX_STEPS)
+        rp, cols, vals = ctx.jacobian()
+        ctx.cgls(30, want_x=False)
+        vel = ctx.model_update()
+    nt = n_tomo(sv["nx"], sv["ny"], sv["nz"], sv["h"], sv["d"])
+    r_o, c_o, v_o, _, _ = oracle_G(oracle_mod, vols, sv["h"], sv["shots"], sv["nodes"], sv["d"], nt)
+    M = nt[0] * nt[1] * nt[2]
+    nd = dobs.size
+    df = oracle_mod.tk_coeffs(2)
+    tr = np.repeat(np.arange(M - 2), 3) + nd
+    tc = (np.arange(M - 2)[:, None] + np.arange(3)[None, :]).ravel()
+    tv = np.tile(np.float32(0.5) * df.astype(np.float32), M - 2)
+    iA = np.concatenate([r_o, tr]).astype(np.int32)
+    jA = np.concatenate([c_o, tc]).astype(np.int32)
+    vA = np.concatenate([v_o, tv]).astype(np.float32)
+    B = np.zeros(nd + M - 2, np.float32)
+    B[:nd] = (dobs - dcal).ravel()
+    x64, _ = oracle_mod.cgls_f64(nd + M - 2, M, iA, jA, vA, B, 30)
+    start_s = (np.float32(1.0) / sv["start_v"]).astype(np.float32)
+    _, vel_o = oracle_mod.model_update(start_s, sv["h"], sv["d"], nt, x64.astype(np.float32), True, 5, 2.0)
+    rms = np.sqrt(np.mean(((vel - vel_o) / vel_o) ** 2))
+    assert rms < 5e-3
+    assert np.count_nonzero(vel != sv["start_v"]) > 1000
