@@ -169,9 +169,20 @@ int tomo_ray_status(tomo_ctx *ctx, int *status);
 int tomo_illumination(tomo_ctx *ctx, float *out);
 
 /* ------------------------------------------------------------- inversion ----------- */
-/* Observed picks, nshots*nrec (row-major shot, receiver): Least_squares::import_obs_data
- * (least_squares.cpp:144-161). */
-int tomo_set_observed(tomo_ctx *ctx, const float *dobs);
+/* Observed picks, n = nshots*nrec (row-major shot, receiver): Least_squares::import_obs_data
+ * (least_squares.cpp:144-161).  n must match the survey of the solve they are used with. */
+int tomo_set_observed(tomo_ctx *ctx, const float *dobs, int n);
+
+/* ------------------------------------------------- parameters.txt helpers --------- */
+/* catch_parameter (src/utils/file_manager/file_manager.cpp:74-120) with its quirks: writes
+ * the value of `key` in the parameter file to out (NUL-terminated, at most cap bytes) and
+ * returns its length, or TOMO_ERR_INVALID_ARG if it does not fit. */
+int tomo_catch_parameter(const char *key, const char *parameter_file, char *out, int cap);
+/* Builds the "shots" or "nodes" geometry of a parameter file like Regular/Circular
+ * set_geometry (src/geometry/regular/regular.cpp:29-56, circular/circular.cpp:5-30), incl.
+ * writing its xyz text file; type 0 regular, 1 circular.  Writes up to cap points (x,y,z)
+ * and returns the number of points, or a negative status. */
+int tomo_geometry(const char *parameter_file, const char *name, int type, float *xyz, int cap);
 /* ||dobs - dcal||_2 in FP64 with dcal the receiver times of the last solve:
  * Least_squares::converged (least_squares.cpp:301-319). */
 int tomo_data_residual(tomo_ctx *ctx, double *norm);
@@ -184,8 +195,9 @@ typedef struct {
 } tomo_cgls_stats;
 
 /* CGLS on A x = [dobs - dcal ; 0]: Least_squares::optimization + sparse_cgls
- * (least_squares.cpp:321-356, 424-496), FP32 vectors, FP64 inner products and step
- * lengths, one persistent launch.  x_out (host, M floats) and history (host, ||B - A x||
+ * (least_squares.cpp:321-356, 424-496).  FP32 matrix; FP64 vectors, row sums, inner
+ * products and step lengths (FP32 vectors drift ~10 % from the FP64 iterates after 30
+ * iterations on these ill-conditioned systems); one persistent launch.  x_out (host, M floats) and history (host, ||B - A x||
  * per iteration) may be NULL; the solution stays on the device for tomo_model_update. */
 int tomo_cgls(tomo_ctx *ctx, int iterations, float *x_out, double *history, tomo_cgls_stats *stats);
 

@@ -250,3 +250,24 @@ def ref_solve(kind, velocity, h, shots, nthreads=1, want_T=True):
 
 def ref_tomography_exe():
     return os.path.join(_REF, "tomography.exe")
+
+
+def ref_catch_parameter(key, param_file):
+    """The reference's own catch_parameter (src/utils/file_manager/file_manager.cpp:74-120)."""
+    lib = _load_ref()
+    lib.ref_catch_parameter.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
+    buf = ctypes.create_string_buffer(4096)
+    n = lib.ref_catch_parameter(key.encode(), param_file.encode(), buf, len(buf))
+    if n < 0:
+        raise ValueError("value too long")
+    return buf.raw[:n].decode("latin-1")
+
+
+def ref_geometry(param_file, name, gtype, cap=100000):
+    """The reference's own Regular (0) / Circular (1) set_geometry; returns (n, 3) float32."""
+    lib = _load_ref()
+    lib.ref_geometry.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+    out = np.zeros((cap, 3), np.float32)
+    with quiet_stdout():
+        n = lib.ref_geometry(param_file.encode(), name.encode(), gtype, out.ctypes.data, cap)
+    return out[:n].copy()

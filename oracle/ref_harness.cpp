@@ -132,6 +132,28 @@ int ref_eikonal_solve(int type, const char *workdir, int nx, int ny, int nz, flo
     return err.load();
 }
 
+// The reference's own catch_parameter (src/utils/file_manager/file_manager.cpp:74-120).
+int ref_catch_parameter(const char *key, const char *file, char *out, int cap)
+{
+    const std::string v = catch_parameter(key, file);
+    if ((int)v.size() + 1 > cap) return -1;
+    std::memcpy(out, v.c_str(), v.size() + 1);
+    return (int)v.size();
+}
+
+// The reference's own Regular / Circular set_geometry (src/geometry/).
+int ref_geometry(const char *file, const char *name, int type, float *xyz, int cap)
+{
+    Geometry *g = type == 0 ? static_cast<Geometry *>(new Regular()) : static_cast<Geometry *>(new Circular());
+    g->set_geometry(file, name);
+    for (int i = 0; i < g->all && i < cap; i++) {
+        xyz[3 * i] = g->x[i];
+        xyz[3 * i + 1] = g->y[i];
+        xyz[3 * i + 2] = g->z[i];
+    }
+    return g->all;
+}
+
 int ref_has_block_fim(void)
 {
 #ifdef REF_WITH_FIM

@@ -131,7 +131,9 @@ def _bind_tomography(lib):
     lib.tomo_jacobian_copy.argtypes = [V, V, V, V]
     lib.tomo_ray_status.argtypes = [V, V]
     lib.tomo_illumination.argtypes = [V, V]
-    lib.tomo_set_observed.argtypes = [V, V]
+    lib.tomo_set_observed.argtypes = [V, V, I]
+    lib.tomo_catch_parameter.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, I]
+    lib.tomo_geometry.argtypes = [ctypes.c_char_p, ctypes.c_char_p, I, V, I]
     lib.tomo_data_residual.argtypes = [V, P(ctypes.c_double)]
     lib.tomo_cgls.argtypes = [V, I, V, V, P(CglsStats)]
     lib.tomo_model_update.argtypes = [V, P(UpdateOpts), V]
@@ -282,7 +284,7 @@ class Context:
 
     def set_observed(self, dobs):
         d = _f32(dobs)
-        self._check(self.lib.tomo_set_observed(self.h, d.ctypes.data))
+        self._check(self.lib.tomo_set_observed(self.h, d.ctypes.data, d.size))
 
     def data_residual(self):
         v = ctypes.c_double()

@@ -15,6 +15,7 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
+HOST = os.path.join(PKG, "host")
 OBJ = os.path.join(PKG, "_build")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libtomo_b200.so")
@@ -59,14 +60,23 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         if _stale(obj, [src] + hdrs) or ptxas_info:
             extra = ["-Xptxas", "-v"] if ptxas_info else []
             _run([NVCC] + NVCC_FLAGS + extra + ["-c", src, "-o", obj], verbose)
-    for src in sorted(glob.glob(os.path.join(CSRC, "*.cpp"))):
+    host_hdrs = hdrs + glob.glob(os.path.join(HOST, "*.hpp"))
+    for src in sorted(glob.glob(os.path.join(CSRC, "*.cpp")) + glob.glob(os.path.join(HOST, "*.cpp"))):
         obj = os.path.join(OBJ, os.path.basename(src) + ".o")
         objs.append(obj)
-        if _stale(obj, [src] + hdrs):
+        if _stale(obj, [src] + host_hdrs):
             _run([CXX] + CXX_FLAGS + ["-c", src, "-o", obj], verbose)
     if _stale(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"],
-             verbose)
+        # -Bsymbolic: calls inside the library bind to its own definitions even when another
+        # library in the process exports the same C++ names (e.g. the reference's own
+        # catch_parameter when both are loaded for a parity test)
+        _run([NVCC] + ARCH + ["-shared", "-Xlinker", "-Bsymbolic", "-o", LIB] + objs
+             + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"], verbose)
+    # drop-in executables (the reference's eikonal.exe / tomography.exe flows)
+    for src in sorted(glob.glob(os.path.join(HOST, "apps", "*_main.cpp"))):
+        exe = os.path.join(LIBDIR, os.path.basename(src)[:-len("_main.cpp")])
+        if _stale(exe, [src, LIB] + host_hdrs):
+            _run([CXX] + CXX_FLAGS + [src, "-o", exe, "-L" + LIBDIR, "-ltomo_b200", "-Wl,-rpath,$ORIGIN"], verbose)
     return LIB
 
 

@@ -126,7 +126,7 @@ void tomo_release_tomography(tomo_ctx *ctx)
                     &ctx->rows_of})
         b->release();
     for (auto *b : {&ctx->final_dist, &ctx->spos, &ctx->tk_coef, &ctx->illum, &ctx->a_val, &ctx->t_val, &ctx->dobs,
-                    &ctx->rhs, &ctx->x, &ctx->cg_s, &ctx->cg_r, &ctx->cg_p, &ctx->cg_q, &ctx->dm, &ctx->dm_smooth,
+                    &ctx->rhs, &ctx->x, &ctx->dm, &ctx->dm_smooth,
                     &ctx->vel_out, &ctx->gauss_kernel})
         b->release();
     ctx->runs.release();
@@ -135,6 +135,7 @@ void tomo_release_tomography(tomo_ctx *ctx)
     ctx->hist.release();
     ctx->norm2.release();
     ctx->cg_ctrl.release();
+    for (auto *b : {&ctx->cg_x, &ctx->cg_s, &ctx->cg_r, &ctx->cg_p, &ctx->cg_q}) b->release();
 }
 
 int tomo_build_jacobian(tomo_ctx *ctx, const tomo_jacobian_opts *opts, tomo_jacobian_stats *stats)
@@ -329,16 +330,15 @@ int tomo_illumination(tomo_ctx *ctx, float *out)
     return TOMO_OK;
 }
 
-int tomo_set_observed(tomo_ctx *ctx, const float *dobs)
+int tomo_set_observed(tomo_ctx *ctx, const float *dobs, int n)
 {
     if (!ctx) return TOMO_ERR_INVALID_ARG;
-    if (!dobs) return fail(ctx, TOMO_ERR_INVALID_ARG, "NULL dobs");
-    if (!ctx->have_solve || ctx->nrec < 1) return fail(ctx, TOMO_ERR_STATE, "solve the survey first (sets n_data)");
+    if (!dobs || n < 1) return fail(ctx, TOMO_ERR_INVALID_ARG, "NULL dobs or n < 1");
     CK(cudaSetDevice(ctx->device));
-    const size_t n = (size_t)ctx->nshots * ctx->nrec;
-    CK(ctx->dobs.ensure(n));
-    CK(cudaMemcpyAsync(ctx->dobs.ptr, dobs, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx->dobs.ensure((size_t)n));
+    CK(cudaMemcpyAsync(ctx->dobs.ptr, dobs, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    ctx->n_dobs = n;
     ctx->have_dobs = true;
     return TOMO_OK;
 }
@@ -348,6 +348,8 @@ int tomo_data_residual(tomo_ctx *ctx, double *norm)
     if (!ctx) return TOMO_ERR_INVALID_ARG;
     if (!norm) return fail(ctx, TOMO_ERR_INVALID_ARG, "NULL output");
     if (!ctx->have_dobs || !ctx->have_solve) return fail(ctx, TOMO_ERR_STATE, "need observed data and a solve");
+    if (ctx->n_dobs != ctx->nshots * ctx->nrec)
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "observed data size does not match nshots*nrec of the solve");
     CK(cudaSetDevice(ctx->device));
     const int n = ctx->nshots * ctx->nrec;
     CK(ctx->norm2.ensure(1));
@@ -366,7 +368,8 @@ namespace {
 // Runs the CGLS kernel on prepared device buffers.
 template <class Ctx>
 int run_cgls(Ctx *ctx, int N, int M, const int *a_ptr, const int *a_idx, const float *a_val, const int *t_ptr,
-             const int *t_idx, const float *t_val, const float *B, float *x, float *s, float *r, float *p, float *q,
+             const int *t_idx, const float *t_val, const float *B, double *x, double *s, double *r, double *p, double *q,
+             float *x32,
              tomo::DevBuf<double> &partials, double *hist, tomo::DevBuf<unsigned> &ctrl, int nit, double tol,
              cudaStream_t st, int *iters_run)
 {
@@ -386,6 +389,7 @@ int run_cgls(Ctx *ctx, int N, int M, const int *a_ptr, const int *a_idx, const f
     cl.t_val = t_val;
     cl.B = B;
     cl.x = x;
+    cl.x32 = x32;
     cl.s = s;
     cl.r = r;
     cl.p = p;
@@ -429,10 +433,13 @@ int tomo_cgls(tomo_ctx *ctx, int iterations, float *x_out, double *history, tomo
     if (iterations < 0) return fail(ctx, TOMO_ERR_INVALID_ARG, "iterations < 0");
     if (!ctx->have_jacobian) return fail(ctx, TOMO_ERR_STATE, "no Jacobian (tomo_build_jacobian)");
     if (!ctx->have_dobs) return fail(ctx, TOMO_ERR_STATE, "no observed data (tomo_set_observed)");
+    if (ctx->n_dobs != ctx->n_data)
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "observed data size does not match the Jacobian's rays");
     CK(cudaSetDevice(ctx->device));
     const int N = ctx->n_rows, M = ctx->n_model, nd = ctx->n_data;
     CK(ctx->rhs.ensure((size_t)N));
     CK(ctx->x.ensure((size_t)M));
+    CK(ctx->cg_x.ensure((size_t)M));
     CK(ctx->cg_s.ensure((size_t)N));
     CK(ctx->cg_q.ensure((size_t)N));
     CK(ctx->cg_r.ensure((size_t)M));
@@ -444,8 +451,8 @@ int tomo_cgls(tomo_ctx *ctx, int iterations, float *x_out, double *history, tomo
     CK(tomo::data_residual(ctx->dobs.ptr, ctx->t_recv.ptr, ctx->rhs.ptr, nd, N, ctx->norm2.ptr, ctx->stream));
     int iters = 0;
     int rc = run_cgls(ctx, N, M, ctx->a_ptr.ptr, ctx->a_idx.ptr, ctx->a_val.ptr, ctx->t_ptr.ptr, ctx->t_idx.ptr,
-                      ctx->t_val.ptr, ctx->rhs.ptr, ctx->x.ptr, ctx->cg_s.ptr, ctx->cg_r.ptr, ctx->cg_p.ptr,
-                      ctx->cg_q.ptr, ctx->partials, ctx->hist.ptr, ctx->cg_ctrl, iterations, 0.0, ctx->stream, &iters);
+                      ctx->t_val.ptr, ctx->rhs.ptr, ctx->cg_x.ptr, ctx->cg_s.ptr, ctx->cg_r.ptr, ctx->cg_p.ptr,
+                      ctx->cg_q.ptr, ctx->x.ptr, ctx->partials, ctx->hist.ptr, ctx->cg_ctrl, iterations, 0.0, ctx->stream, &iters);
     if (rc != TOMO_OK) return rc;
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     std::vector<double> h((size_t)(iterations > 0 ? iterations : 1), 0.0);
@@ -530,7 +537,8 @@ int tomo_sparse_cgls_gpu(const int *iA, const int *jA, const float *vA, const fl
     Plain pl;
     Plain *ctx = &pl;
     tomo::DevBuf<int> a_ptr, a_idx, t_ptr, t_idx, k0, k1, p0, p1, rows_of;
-    tomo::DevBuf<float> a_val, t_val, dB, dx_, s, r, p, q;
+    tomo::DevBuf<float> a_val, t_val, dB, dx_;
+    tomo::DevBuf<double> x64, s, r, p, q;
     tomo::DevBuf<double> partials;
     tomo::DevBuf<unsigned> ctrl;
     tomo::DevBuf<unsigned char> temp;
@@ -538,7 +546,8 @@ int tomo_sparse_cgls_gpu(const int *iA, const int *jA, const float *vA, const fl
     int rc = TOMO_OK;
     auto cleanup = [&]() {
         for (auto *b : {&a_ptr, &a_idx, &t_ptr, &t_idx, &k0, &k1, &p0, &p1, &rows_of}) b->release();
-        for (auto *b : {&a_val, &t_val, &dB, &dx_, &s, &r, &p, &q}) b->release();
+        for (auto *b : {&a_val, &t_val, &dB, &dx_}) b->release();
+        for (auto *b : {&x64, &s, &r, &p, &q}) b->release();
         partials.release();
         ctrl.release();
         temp.release();
@@ -551,6 +560,7 @@ int tomo_sparse_cgls_gpu(const int *iA, const int *jA, const float *vA, const fl
         CK(a_val.ensure((size_t)NNZ));
         CK(dB.ensure((size_t)N));
         CK(dx_.ensure((size_t)M));
+        CK(x64.ensure((size_t)M));
         CK(s.ensure((size_t)N));
         CK(q.ensure((size_t)N));
         CK(r.ensure((size_t)M));
@@ -562,8 +572,8 @@ int tomo_sparse_cgls_gpu(const int *iA, const int *jA, const float *vA, const fl
         int r2 = build_transpose(ctx, a_ptr.ptr, a_idx.ptr, a_val.ptr, N, M, NNZ, t_ptr, t_idx, t_val, k0, k1, p0, p1,
                                  rows_of, temp, st);
         if (r2 != TOMO_OK) return r2;
-        r2 = run_cgls(ctx, N, M, a_ptr.ptr, a_idx.ptr, a_val.ptr, t_ptr.ptr, t_idx.ptr, t_val.ptr, dB.ptr, dx_.ptr,
-                      s.ptr, r.ptr, p.ptr, q.ptr, partials, nullptr, ctrl, NIT, (double)TOL, st, nullptr);
+        r2 = run_cgls(ctx, N, M, a_ptr.ptr, a_idx.ptr, a_val.ptr, t_ptr.ptr, t_idx.ptr, t_val.ptr, dB.ptr, x64.ptr,
+                      s.ptr, r.ptr, p.ptr, q.ptr, dx_.ptr, partials, nullptr, ctrl, NIT, (double)TOL, st, nullptr);
         if (r2 != TOMO_OK) return r2;
         CK(cudaMemcpyAsync(x, dx_.ptr, (size_t)M * sizeof(float), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));

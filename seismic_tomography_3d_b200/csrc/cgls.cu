@@ -3,7 +3,7 @@
 // Same recurrence as Least_squares::sparse_cgls (src/tomography/least_squares/
 // least_squares.cpp:424-496) -- s = B, r = A's, p = r, q = A p, then per iteration
 // a = r'r/q'q, x += a p, s -= a q, r = A's, b = r'r/r'r_old, p = r + b p, q = A p --
-// with FP32 vectors and the matrix in CSR (A) and CSR of the transpose (A', so both
+// with the FP32 matrix in CSR (A) and CSR of the transpose (A', so both
 // products are gathers, no atomics), and FP64 for every inner product, the step lengths
 // and the row sums.  One cooperative persistent launch runs all iterations; the four
 // grid-wide dependencies per iteration are software grid barriers with bounded waits.
@@ -37,7 +37,7 @@ __device__ __forceinline__ double grid_sum(const double *partials, int nb, doubl
 {
     double v = 0.0;
     if (threadIdx.x < 32) {
-        for (int i = threadIdx.x; i < nb; i += 32) v += partials[i];
+        for (int i = threadIdx.x; i < nb; i += 32) v += __ldcg(partials + i);
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
         if (threadIdx.x == 0) sh[kWarps] = v;
     }
@@ -47,10 +47,10 @@ __device__ __forceinline__ double grid_sum(const double *partials, int nb, doubl
     return v;
 }
 
-// y = M x for a CSR matrix with `G` lanes per row (FP64 row sums, FP32 output); returns
-// this thread's share of y'y.
+// y = M x for a CSR matrix with `G` lanes per row: FP32 matrix values, FP64 vectors and
+// row sums.  Returns this thread's share of y'y.
 template <int G>
-__device__ __forceinline__ double spmv(const int *ptr, const int *idx, const float *val, const float *x, float *y,
+__device__ __forceinline__ double spmv(const int *ptr, const int *idx, const float *val, const double *x, double *y,
                                        int nrows)
 {
     const int lane = threadIdx.x & 31;
@@ -64,13 +64,12 @@ __device__ __forceinline__ double spmv(const int *ptr, const int *idx, const flo
         double acc = 0.0;
         if (row < nrows) {
             const int b = __ldg(ptr + row), e = __ldg(ptr + row + 1);
-            for (int k = b + sub; k < e; k += G) acc += (double)__ldg(val + k) * (double)__ldg(x + __ldg(idx + k));
+            for (int k = b + sub; k < e; k += G) acc += (double)__ldg(val + k) * __ldcg(x + __ldg(idx + k));
         }
         for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o, G);
         if (row < nrows && sub == 0) {
-            const float yr = (float)acc;
-            y[row] = yr;
-            local += (double)yr * (double)yr;
+            y[row] = acc;
+            local += acc * acc;
         }
     }
     return local;
@@ -87,8 +86,8 @@ __global__ void __launch_bounds__(kThreads) k_cgls(CglsLaunch p)
     double *pa = p.partials, *pb = p.partials + nb, *pc = p.partials + 2 * nb;
 
     // s = B, x = 0
-    for (long long i = tid; i < p.N; i += nth) p.s[i] = p.B[i];
-    for (long long i = tid; i < p.M; i += nth) p.x[i] = 0.0f;
+    for (long long i = tid; i < p.N; i += nth) p.s[i] = (double)p.B[i];
+    for (long long i = tid; i < p.M; i += nth) p.x[i] = 0.0;
     if (!grid_barrier(p.ctrl, p.spin_limit)) return;
     // r = A' s
     double v = block_sum(spmv<32>(p.t_ptr, p.t_idx, p.t_val, p.s, p.r, p.M), sh);
@@ -105,11 +104,11 @@ __global__ void __launch_bounds__(kThreads) k_cgls(CglsLaunch p)
     for (int it = 0; it < p.nit; it++) {
         const double a = rTr / qTq;
         double ss = 0.0;
-        for (long long i = tid; i < p.M; i += nth) p.x[i] = (float)((double)p.x[i] + a * (double)p.p[i]);
+        for (long long i = tid; i < p.M; i += nth) p.x[i] += a * __ldcg(p.p + i);
         for (long long i = tid; i < p.N; i += nth) {
-            const float si = (float)((double)p.s[i] - a * (double)p.q[i]);
+            const double si = __ldcg(p.s + i) - a * __ldcg(p.q + i);
             p.s[i] = si;
-            ss += (double)si * (double)si;
+            ss += si * si;
         }
         v = block_sum(ss, sh);
         if (threadIdx.x == 0) pc[blockIdx.x] = v;
@@ -128,7 +127,7 @@ __global__ void __launch_bounds__(kThreads) k_cgls(CglsLaunch p)
         const double rTr_new = grid_sum(pa, nb, sh);
         const double b = rTr_new / rTr;
         rTr = rTr_new;
-        for (long long i = tid; i < p.M; i += nth) p.p[i] = (float)((double)p.r[i] + b * (double)p.p[i]);
+        for (long long i = tid; i < p.M; i += nth) p.p[i] = __ldcg(p.r + i) + b * __ldcg(p.p + i);
         if (!grid_barrier(p.ctrl, p.spin_limit)) return;
         // q = A p
         v = block_sum(spmv<8>(p.a_ptr, p.a_idx, p.a_val, p.p, p.q, p.N), sh);
@@ -136,6 +135,8 @@ __global__ void __launch_bounds__(kThreads) k_cgls(CglsLaunch p)
         if (!grid_barrier(p.ctrl, p.spin_limit)) return;
         qTq = grid_sum(pb, nb, sh);
     }
+    // the model update consumes the solution in FP32, as the reference's xdm
+    for (long long i = tid; i < p.M; i += nth) p.x32[i] = (float)p.x[i];
 }
 
 cudaError_t cgls_grid(int *grid)

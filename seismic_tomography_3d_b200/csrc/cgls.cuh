@@ -10,7 +10,8 @@ struct CglsLaunch {
     const int *a_ptr, *a_idx; const float *a_val;           // A in CSR
     const int *t_ptr, *t_idx; const float *t_val;           // A' in CSR
     const float *B;                                         // right-hand side (N)
-    float *x, *s, *r, *p, *q;                               // M, N, M, M, N
+    double *x, *s, *r, *p, *q;                              // M, N, M, M, N (FP64 vectors)
+    float *x32;                                             // solution rounded to FP32 (M)
     double *partials;                                       // 3 * gridDim.x
     double *hist;                                           // ||s|| per iteration (nit) or nullptr
     unsigned *ctrl;                                         // kCtrlWords (barrier, error, iterations run)

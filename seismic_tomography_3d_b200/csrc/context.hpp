@@ -84,9 +84,11 @@ struct tomo_ctx {
     long long nnz_g = 0, nnz = 0;
     bool have_jacobian = false, have_illum = false;
     // CGLS and model update
-    tomo::DevBuf<float> dobs, rhs, x, cg_s, cg_r, cg_p, cg_q;
+    tomo::DevBuf<float> dobs, rhs, x;                 // x: CGLS solution in FP32
+    tomo::DevBuf<double> cg_x, cg_s, cg_r, cg_p, cg_q;  // CGLS vectors (FP64)
     tomo::DevBuf<double> partials, hist, norm2;
     tomo::DevBuf<unsigned> cg_ctrl;
     tomo::DevBuf<float> dm, dm_smooth, vel_out, gauss_kernel;
     bool have_dobs = false, have_x = false;
+    int n_dobs = 0;
 };
