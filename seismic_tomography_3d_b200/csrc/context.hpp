@@ -55,6 +55,7 @@ struct tomo_ctx {
     // last eikonal solve
     tomo::DevBuf<float> T;
     tomo::DevBuf<unsigned> qflag, lists, ctrl;
+    tomo::DevBuf<unsigned> key, minkey, smin_bits;  // band-ordered scheduling
     tomo::DevBuf<unsigned long long> stats;
     tomo::DevBuf<tomo::ShotDesc> shots_d;
     std::vector<tomo::ShotDesc> shots_h;

@@ -25,6 +25,16 @@ namespace tomo {
 // order -- the Jeong & Whitaker (2008) update of get_time_eikonal
 // (src/eikonal/block_FIM/cuda_kernel.cu:217-248), written in symmetric form.
 // -------------------------------------------------------------------------------------
+// Square root to ~1 ulp (sqrt.approx): the candidates it feeds are compared and min-ed,
+// never accumulated, so the rounding stays at the 1e-7 level of the FP32 fixed point.
+__device__ __forceinline__ float sqrt_fast(float v)
+{
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(v));
+    return r;
+}
+
+template <bool kFastSqrt>
 __device__ __forceinline__ float godunov_jw(float a, float b, float c, float h, float s)
 {
     const float lo = fminf(a, b), hi = fmaxf(a, b);
@@ -36,13 +46,14 @@ __device__ __forceinline__ float godunov_jw(float a, float b, float c, float h, 
     float t = u0 + hs;
     if (t > u1) {
         const float d01 = u1 - u0;
-        const float t2 = 0.5f * ((u0 + u1) + sqrtf(2.0f * hs * hs - d01 * d01));
+        const float q2 = 2.0f * hs * hs - d01 * d01;
+        const float t2 = 0.5f * ((u0 + u1) + (kFastSqrt ? sqrt_fast(q2) : sqrtf(q2)));
         if (t2 > u1) t = t2;
         if (t > u2) {
             const float sum = u0 + u1 + u2;
             const float d12 = u2 - u1, d02 = u2 - u0;
             const float disc = 3.0f * hs * hs - (d01 * d01 + d12 * d12 + d02 * d02);
-            const float t3 = (sum + sqrtf(disc)) * (1.0f / 3.0f);
+            const float t3 = (sum + (kFastSqrt ? sqrt_fast(disc) : sqrtf(disc))) * (1.0f / 3.0f);
             if (t3 > u2) t = t3;
         }
     }
@@ -77,7 +88,22 @@ struct WarpStats {
     unsigned long long act, inner;
 };
 
+constexpr unsigned kInfBits = 0x49742400u;  // __float_as_uint(1e6f)
+
+// Appends `item` to the work list of round+1 unless it is queued there already.
+__device__ __forceinline__ void requeue_one(const FimLaunch &p, const ShotDesc &d, unsigned b, unsigned item,
+                                            unsigned round)
+{
+    const unsigned tag = round + 2u;
+    if (atomicMax(p.qflag + d.qbase + b, tag) < tag) {
+        const unsigned nxt = (round + 1u) % 3u;
+        const unsigned slot = atomicAdd(p.ctrl + kCnt0 + nxt, 1u);
+        p.lists[(size_t)nxt * p.list_cap + slot] = item;
+    }
+}
+
 // One activation of one brick by one warp.
+template <bool kFastSqrt>
 __device__ __forceinline__ void process_brick(const FimLaunch &p, unsigned item, unsigned round,
                                               float *tile, WarpStats &ws)
 {
@@ -85,6 +111,28 @@ __device__ __forceinline__ void process_brick(const FimLaunch &p, unsigned item,
     const unsigned s = item >> p.local_bits;
     const unsigned b = item & ((1u << p.local_bits) - 1u);
     const ShotDesc &d = p.shots[s];
+
+    if (p.band > 0.0f) {
+        unsigned kb = 0;
+        if (lane == 0) kb = __ldcg(p.key + d.qbase + b);
+        kb = __shfl_sync(kFull, kb, 0);
+        // Nothing pending: the push that queued it happened before this brick's last
+        // relaxation started, which already read the pushed values.
+        if (kb == kInfBits) return;
+        const float thr = __uint_as_float(__ldcg(p.minkey + (round % 3u) * p.nshots + s)) + p.band;
+        if (__uint_as_float(kb) > thr) {  // ahead of the front: keep it for a later round
+            if (lane == 0) {
+                requeue_one(p, d, b, item, round);
+                atomicMin(p.minkey + ((round + 1u) % 3u) * p.nshots + s, kb);
+            }
+            return;
+        }
+        if (lane == 0) {
+            atomicExch(p.key + d.qbase + b, kInfBits);
+            __threadfence();
+        }
+        __syncwarp();
+    }
     const int nbz = d.nbz, nbx = d.nbx, nby = d.nby;
     const int bz = (int)(b % (unsigned)nbz);
     const unsigned tq = b / (unsigned)nbz;
@@ -142,9 +190,9 @@ __device__ __forceinline__ void process_brick(const FimLaunch &p, unsigned item,
         const float a1 = fminf(tile[ti1 - kTile], tile[ti1 + kTile]);
         const float b1 = fminf(tile[ti1 - kTile * kTile], tile[ti1 + kTile * kTile]);
         const float g1 = fminf(tile[ti1 - 1], tile[ti1 + 1]);
-        const float n0 = fminf(c0, godunov_jw(a0, b0, g0, h, s0));
-        const float n1 = fminf(c1, godunov_jw(a1, b1, g1, h, s1));
-        const bool ch = (n0 < c0) | (n1 < c1);
+        const float n0 = fminf(c0, godunov_jw<kFastSqrt>(a0, b0, g0, h, s0));
+        const float n1 = fminf(c1, godunov_jw<kFastSqrt>(a1, b1, g1, h, s1));
+        const bool ch = (n0 < c0 - p.inner_tol) | (n1 < c1 - p.inner_tol);
         __syncwarp();
         tile[ti0] = n0;
         tile[ti1] = n1;
@@ -187,6 +235,16 @@ __device__ __forceinline__ void process_brick(const FimLaunch &p, unsigned item,
         want = more;
         tgt = b;
     }
+    unsigned kbits = 0;
+    if (p.band > 0.0f) {  // key of the pushes: this brick's smallest traveltime
+        float bm = fminf(c0, c1);
+        for (int o = 16; o > 0; o >>= 1) bm = fminf(bm, __shfl_xor_sync(kFull, bm, o));
+        kbits = __float_as_uint(bm);
+        if (want) {
+            atomicMin(p.key + d.qbase + (unsigned long long)tgt, kbits);
+            atomicMin(p.minkey + ((round + 1u) % 3u) * p.nshots + s, kbits);
+        }
+    }
     const unsigned tag = round + 2u;  // "queued for round+1", offset by one so 0 = never
     if (want) {
         const unsigned old = atomicMax(p.qflag + d.qbase + (unsigned long long)tgt, tag);
@@ -206,7 +264,7 @@ __device__ __forceinline__ void process_brick(const FimLaunch &p, unsigned item,
     }
 }
 
-template <int MINB>
+template <int MINB, bool kFastSqrt>
 __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
 {
     extern __shared__ float smem[];
@@ -229,6 +287,9 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
             p.ctrl[kCnt0 + (round + 2u) % 3u] = 0u;
             p.ctrl[kCur0 + (round + 2u) % 3u] = 0u;
         }
+        if (p.band > 0.0f && blockIdx.x == 0)
+            for (int s = threadIdx.x; s < p.nshots; s += blockDim.x)
+                p.minkey[((round + 2u) % 3u) * p.nshots + s] = kInfBits;
         // Items are fetched one at a time from the round's cursor, so warps that draw
         // cheap bricks take more of them and the round ends together.
         const unsigned *list = p.lists + (size_t)cur * p.list_cap;
@@ -237,7 +298,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
             if ((threadIdx.x & 31) == 0) i = atomicAdd(p.ctrl + kCur0 + cur, 1u);
             i = __shfl_sync(kFull, i, 0);
             if (i >= n) break;
-            process_brick(p, __ldcg(list + i), round, tile, ws);
+            process_brick<kFastSqrt>(p, __ldcg(list + i), round, tile, ws);
         }
         if (!grid_barrier(p.ctrl, p.spin_limit)) { ok = false; break; }
         ++round;
@@ -318,19 +379,24 @@ __global__ void k_brick_model(const float *slow, float *S, int nx, int ny, int n
 }
 
 __global__ void k_fim_init(float4 *T4, size_t n4, unsigned *qflag, size_t nq, unsigned *ctrl,
-                           unsigned long long *stats)
+                           unsigned long long *stats, unsigned *key, unsigned *minkey, int nshots)
 {
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     const float4 inf4 = make_float4(kInf, kInf, kInf, kInf);
     for (size_t i = t; i < n4; i += stride) __stcg(T4 + i, inf4);
     for (size_t i = t; i < nq; i += stride) qflag[i] = 0u;
+    if (key) {
+        for (size_t i = t; i < nq; i += stride) key[i] = kInfBits;
+        for (size_t i = t; i < (size_t)3 * nshots; i += stride) minkey[i] = kInfBits;
+    }
     if (t < kCtrlWords) ctrl[t] = 0u;
     if (t < 2) stats[t] = 0ull;
 }
 
 __global__ void k_fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
-                           unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl)
+                           unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, unsigned *key,
+                           unsigned *minkey)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < nshots) {
@@ -343,6 +409,10 @@ __global__ void k_fim_seed(const ShotDesc *shots, int nshots, const float *S, in
         T[d.t_off + (long long)d.src_brick * kBrickNodes + d.src_node] = __fmul_rn(S[gb * kBrickNodes + d.src_node], d.src_dist);
         qflag[d.qbase + d.src_brick] = 1u;
         lists[s] = ((unsigned)s << local_bits) | (unsigned)d.src_brick;
+        if (key) {
+            key[d.qbase + d.src_brick] = 0u;  // +0.0f
+            minkey[s] = 0u;
+        }
     }
     if (s == 0) ctrl[kCnt0] = (unsigned)nshots;
 }
@@ -369,6 +439,23 @@ static int grid_for(size_t n, int threads)
     return g < 1 ? 1 : (int)g;
 }
 
+__global__ void k_slowness_min(const float *s, size_t n, unsigned *out)
+{
+    float m = kInf;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        m = fminf(m, s[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(kFull, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMin(out, __float_as_uint(m));
+}
+
+// Smallest (positive) slowness of the model as float bits in *out_bits (which must hold
+// +INF bits or a larger value on entry).
+cudaError_t slowness_min(const float *s, size_t n, unsigned *out_bits, cudaStream_t st)
+{
+    k_slowness_min<<<grid_for(n, 256), 256, 0, st>>>(s, n, out_bits);
+    return cudaGetLastError();
+}
+
 cudaError_t velocity_to_slowness(const float *v, float *s, size_t n, cudaStream_t st)
 {
     k_velocity_to_slowness<<<grid_for(n, 256), 256, 0, st>>>(v, s, n);
@@ -383,21 +470,23 @@ cudaError_t fim_brick_model(const float *slow, float *S, int nx, int ny, int nz,
 }
 
 cudaError_t fim_init(float *T, size_t t_count, unsigned *qflag, size_t q_count, unsigned *ctrl,
-                     unsigned long long *stats, cudaStream_t st)
+                     unsigned long long *stats, unsigned *key, unsigned *minkey, int nshots, cudaStream_t st)
 {
     k_fim_init<<<grid_for(t_count / 4, 256), 256, 0, st>>>(reinterpret_cast<float4 *>(T), t_count / 4,
-                                                            qflag, q_count, ctrl, stats);
+                                                            qflag, q_count, ctrl, stats, key, minkey, nshots);
     return cudaGetLastError();
 }
 
 cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
-                     unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st)
+                     unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, unsigned *key,
+                     unsigned *minkey, cudaStream_t st)
 {
-    k_fim_seed<<<(nshots + 127) / 128, 128, 0, st>>>(shots, nshots, S, gbx, gbz, T, qflag, lists, local_bits, ctrl);
+    k_fim_seed<<<(nshots + 127) / 128, 128, 0, st>>>(shots, nshots, S, gbx, gbz, T, qflag, lists, local_bits, ctrl,
+                                                     key, minkey);
     return cudaGetLastError();
 }
 
-template <int MINB>
+template <int MINB, bool kFastSqrt>
 static cudaError_t launch_solve(const FimLaunch &p, int block_warps, int *grid_out, cudaStream_t st)
 {
     const int threads = 32 * block_warps;
@@ -407,25 +496,34 @@ static cudaError_t launch_solve(const FimLaunch &p, int block_warps, int *grid_o
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fim_solve<MINB>, threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fim_solve<MINB, kFastSqrt>, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int grid = nsm * per_sm;
     if (grid_out) *grid_out = grid;
     FimLaunch pp = p;
     void *args[] = {&pp};
-    return cudaLaunchCooperativeKernel((const void *)k_fim_solve<MINB>, dim3(grid), dim3(threads), args, smem, st);
+    return cudaLaunchCooperativeKernel((const void *)k_fim_solve<MINB, kFastSqrt>, dim3(grid), dim3(threads), args,
+                                       smem, st);
 }
 
-cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, int *grid_out, cudaStream_t st)
+template <bool kFastSqrt>
+static cudaError_t solve_occ(const FimLaunch &p, int block_warps, int occupancy, int *grid_out, cudaStream_t st)
+{
+    switch (occupancy) {
+    case 1: return launch_solve<1, kFastSqrt>(p, block_warps, grid_out, st);
+    case 2: return launch_solve<2, kFastSqrt>(p, block_warps, grid_out, st);
+    case 3: return launch_solve<3, kFastSqrt>(p, block_warps, grid_out, st);
+    default: return launch_solve<4, kFastSqrt>(p, block_warps, grid_out, st);
+    }
+}
+
+cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, bool ieee_sqrt, int *grid_out,
+                      cudaStream_t st)
 {
     if (block_warps < 1 || block_warps > 8) block_warps = 8;
-    switch (occupancy) {
-    case 1: return launch_solve<1>(p, block_warps, grid_out, st);
-    case 2: return launch_solve<2>(p, block_warps, grid_out, st);
-    case 4: return launch_solve<4>(p, block_warps, grid_out, st);
-    default: return launch_solve<3>(p, block_warps, grid_out, st);
-    }
+    return ieee_sqrt ? solve_occ<false>(p, block_warps, occupancy, grid_out, st)
+                     : solve_occ<true>(p, block_warps, occupancy, grid_out, st);
 }
 
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out, cudaStream_t st)

@@ -45,6 +45,7 @@ void Eikonal_B200::set_parameters()
     nodes = make(nodes_type);
     shots->set_geometry(parameters, "shots");
     nodes->set_geometry(parameters, "nodes");
+    geometry_ready = true;
 
     reciprocity = str2bool(catch_parameter("reciprocity", parameters));
     if (reciprocity) {
@@ -134,7 +135,25 @@ void Eikonal_B200::write_first_arrival()
 
 void Eikonal_B200::destroy_volumes() { batch_ready = false; }
 
+Eikonal_B200::Eikonal_B200()
+{
+    slowness = travel_time = first_arrival = nullptr;
+    shots = nodes = nullptr;
+    shot_id = total_shots = total_nodes = 0;
+}
+
 Eikonal_B200::~Eikonal_B200()
 {
     if (ctx) tomo_ctx_destroy(ctx);
+    delete[] slowness;
+    delete[] travel_time;
+    delete[] first_arrival;
+    if (geometry_ready)  // coordinate arrays exist (swapped, never shared, under reciprocity)
+        for (Geometry *g : {shots, nodes}) {
+            delete[] g->x;
+            delete[] g->y;
+            delete[] g->z;
+        }
+    delete shots;
+    delete nodes;
 }

@@ -26,6 +26,7 @@ class Eikonal_B200 : public Eikonal {
 protected:
     tomo_ctx *ctx = nullptr;
     bool batch_ready = false;
+    bool geometry_ready = false;
     std::vector<float> recv_times;  // total_shots x total_nodes, trilinear receiver times
 
     void expand_model() {}  // padding to whole bricks happens on the device
@@ -43,6 +44,7 @@ public:
     void write_first_arrival();
 
     void destroy_volumes();
+    Eikonal_B200();
     ~Eikonal_B200();
 
     // for the device-resident tomography

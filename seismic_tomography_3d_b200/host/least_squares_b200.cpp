@@ -166,6 +166,15 @@ void Least_squares_B200::export_convergency()
     for (float r : residuo) f << r << "\n";
 }
 
+Least_squares_B200::Least_squares_B200()
+{
+    // the interface's raw pointers start out empty so that an exception thrown by
+    // set_parameters() leaves a destructible object
+    dm = dobs = dcal = nullptr;
+    eikonal = nullptr;
+    iteration = 0;
+}
+
 Least_squares_B200::~Least_squares_B200()
 {
     delete b200;

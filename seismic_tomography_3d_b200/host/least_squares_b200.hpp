@@ -45,6 +45,7 @@ public:
     void model_update();
 
     void export_convergency();
+    Least_squares_B200();
     ~Least_squares_B200();
 };
 
