@@ -76,7 +76,7 @@ typedef struct {
                         band x (time to cross one brick at the fastest velocity) of its
                         shot's smallest pending key.  0: default; < 0: off            */
     float inner_tol; /* in-brick relaxation stops when no node drops by more than this
-                        (s).  0: default (= change_tol); < 0: exact                  */
+                        (s).  <= 0: exact (default)                                  */
     int ieee_sqrt;   /* 1: IEEE sqrtf in the local update; 0 (default): sqrt.approx  */
 } tomo_eik_opts;
 

@@ -345,7 +345,10 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     p.h = g.dx;  // isotropic spacing h = dx (block_FIM.cpp:173)
     p.max_inner = max_inner;
     p.change_tol = change_tol;
-    p.inner_tol = change_tol;
+    // Default: exact in-brick convergence.  Stopping the in-brick relaxation at the face
+    // tolerance is 13 % faster on config 2 but raises the error vs the exact fixed point
+    // from ~1e-6 to ~2e-5 relative, too close to the 1e-4 budget on larger grids.
+    p.inner_tol = 0.f;
     if (opts && opts->inner_tol > 0.f) p.inner_tol = opts->inner_tol;
     if (opts && opts->inner_tol < 0.f) p.inner_tol = 0.f;
     p.max_rounds = max_rounds;
