@@ -301,6 +301,66 @@ def run_ours(args):
     return 0
 
 
+def run_tomography(args):
+    """Config 3: one full tomography iteration on the device (64 shots x 2,500 receivers,
+    201x201x101 at 12.5 m, 50x50x25 cells, Tikhonov order 2, lambda 0.1, 30 CGLS
+    iterations).  Prints its own JSON line (not the headline metric)."""
+    import torch
+
+    import seismic_tomography_3d_b200 as tomo
+    from seismic_tomography_3d_b200 import workloads as wl
+
+    sv, start, inv = wl.config3()
+    rng = np.random.default_rng(3)
+    ctx = tomo.Context(sv.nx, sv.ny, sv.nz, sv.h)
+    ctx.set_velocity(sv.velocity)
+    dobs, _ = ctx.eik_solve(sv.shots, receivers=sv.receivers)
+    dobs = (dobs + rng.normal(0.0, inv["pick_noise"], dobs.shape)).astype(np.float32)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    timings = {k: [] for k in ("eikonal", "jacobian", "cgls", "update", "total")}
+    last = {}
+    for it in range(args.warmup + args.steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        ev[0].record(stream)
+        ctx.set_velocity(start)
+        _, est = ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False)
+        ev[1].record(stream)
+        jst = ctx.build_jacobian(inv["d_tomo"], inv["tk_order"], inv["tk_param"])
+        ev[2].record(stream)
+        ctx.set_observed(dobs)
+        _, hist, cst = ctx.cgls(inv["cg_iterations"], want_x=False)
+        ev[3].record(stream)
+        ctx.model_update(inv["smooth"], inv["filter_samples"], inv["standard_deviation"], want_velocity=False)
+        ev[4].record(stream)
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            for k, (a, b) in zip(("eikonal", "jacobian", "cgls", "update"), zip(ev[:4], ev[1:])):
+                timings[k].append(a.elapsed_time(b))
+            timings["total"].append(ev[0].elapsed_time(ev[4]))
+        last = dict(eik=est, jac=jst, cgls=cst, hist=hist)
+    med = {k: statistics.median(v) for k, v in timings.items()}
+    j, c = last["jac"], last["cgls"]
+    N, M, nnz = j["rows"], j["cols"], j["nnz"]
+    cg_bytes = 16 * nnz + 4 * (N + M) + 8 * (5 * N + 8 * M)  # per CGLS iteration, see DESIGN.md
+    cg_ms_it = c["ms"] / max(c["iterations"], 1)
+    peak, peak_kind = peaks()
+    line = {"metric": "tomography iteration time (config 3)", "value": med["total"], "unit": "ms",
+            "higher_is_better": False, "steps": args.steps, "warmup": args.warmup,
+            "breakdown_ms": med, "shots_per_s_eikonal": len(sv.shots) / (med["eikonal"] / 1000.0),
+            "jacobian": {k: j[k] for k in ("rows", "cols", "nnz_rays", "nnz", "rays", "rays_ok", "rays_stalled",
+                                           "rays_capped", "rays_nonfinite", "rays_outside", "ray_steps")},
+            "ray_steps_per_s": j["ray_steps"] / (med["jacobian"] / 1000.0),
+            "cgls": {"iterations": c["iterations"], "ms_per_iteration": cg_ms_it, "rnorm0": c["rnorm0"],
+                     "rnorm": c["rnorm"],
+                     "roofline": {"bound": "hbm", "achieved": cg_bytes / (cg_ms_it / 1000.0) / 1e9, "peak": peak,
+                                  "unit": "GB/s", "frac": cg_bytes / (cg_ms_it / 1000.0) / 1e9 / peak,
+                                  "peak_kind": peak_kind, "alg_bytes_per_iteration": cg_bytes}},
+            "data": "synthetic (seeded config-3 model, 64 shots x 2500 receivers, picks + N(0, 2 ms))"}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -309,7 +369,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shots", type=int, default=0, help="first N shots of the batch only (profiling)")
+    ap.add_argument("--tomography", action="store_true",
+                    help="time one config-3 tomography iteration instead (separate JSON line)")
     args = ap.parse_args()
+    if args.tomography:
+        return run_tomography(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

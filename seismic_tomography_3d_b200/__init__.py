@@ -157,11 +157,15 @@ def sparse_cgls_gpu(iA, jA, vA, B, N, M, nit, tol=0.0):
 
 
 def _points(a):
-    a = np.asarray(a, np.float32).reshape(-1, 3)
-    arr = (Point * max(len(a), 1))()
-    for i, (x, y, z) in enumerate(a):
-        arr[i].x, arr[i].y, arr[i].z = float(x), float(y), float(z)
-    return arr, len(a)
+    """(n, 3) float32 array viewed as tomo_point[n] without copying (tomo_point is three
+    packed floats).  Returns (pointer, n, owner) -- keep `owner` alive during the call."""
+    a = np.ascontiguousarray(np.asarray(a, np.float32).reshape(-1, 3))
+    return a.ctypes.data_as(ctypes.POINTER(Point)), len(a), a
+
+
+def _windows(w):
+    w = np.ascontiguousarray(np.asarray(w, np.int32).reshape(-1, 4))
+    return w.ctypes.data_as(ctypes.POINTER(Window)), w
 
 
 def _f32(a):
@@ -232,15 +236,14 @@ class Context:
                   block_warps=0, op=0, occupancy=0, change_tol=0.0, band=0.0, inner_tol=0.0, ieee_sqrt=0):
         """Batched solve.  shots (n,3) metres; windows (n,4) [x0,x1,y0,y1] nodes or None;
         receivers (m,3).  Returns (t_recv (n,m) float32 or None, stats dict)."""
-        sp, ns = _points(shots)
-        wp = None
+        sp, ns, _s = _points(shots)
+        wp = _w = None
         if windows is not None:
-            w = np.asarray(windows, np.int32).reshape(-1, 4)
-            wp = (Window * len(w))(*[Window(*map(int, row)) for row in w])
+            wp, _w = _windows(windows)
         nr = 0
-        rp = None
+        rp = _r = None
         if receivers is not None and len(receivers):
-            rp, nr = _points(receivers)
+            rp, nr, _r = _points(receivers)
         out = np.empty((ns, nr), np.float32) if (want_recv and nr) else None
         opts = EikOpts(op, max_inner, max_rounds, 0, block_warps, occupancy, change_tol, band, inner_tol, ieee_sqrt)
         st = EikStats()
