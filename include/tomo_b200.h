@@ -98,6 +98,8 @@ int tomo_ctx_create(const tomo_grid *grid, int device, tomo_ctx **out);
 int tomo_ctx_create_on_stream(const tomo_grid *grid, int device, void *stream, tomo_ctx **out);
 /* Replaces Eikonal::destroy_volumes (eikonal.hpp:57). */
 int tomo_ctx_destroy(tomo_ctx *ctx);
+/* Message of the last failed call on ctx; with ctx == NULL, of the last failed
+ * context-free call (tomo_eik_solve_static) on this host thread. */
 const char *tomo_last_error(const tomo_ctx *ctx);
 const char *tomo_status_string(int status);
 /* The cudaStream_t the context enqueues on. */
@@ -139,6 +141,25 @@ int tomo_eik_window(tomo_ctx *ctx, int shot, tomo_window *out);
 /* Brick shapes the solver supports: writes up to `cap` triples (bx,by,bz) of nodes and
  * returns how many there are. */
 int tomo_eik_brick_shapes(int *xyz_triples, int cap);
+
+/* Allocation-free single-shot solve, for callers that cannot call cudaMalloc (their
+ * application already owns the GPU's memory through its own pool, or must stay within
+ * a fixed device-memory budget).  No counterpart in the reference: it has no library
+ * boundary, and its Block_FIM allocates and frees device memory for every shot.
+ *   slowness  device pointer, nz*nx*ny floats (z fastest), read only
+ *   t_out     device pointer, nz*nx*ny floats: the traveltime field, as tomo_eik_volume
+ *   stream    cudaStream_t the work is enqueued on (NULL: default stream); the call
+ *             returns after that work completes
+ * Same operator, seed and tolerances as tomo_eik_solve.  The solver's working memory is a
+ * fixed device array inside the library (about 34.6 MB, reserved on each GPU where the
+ * library's code is loaded, until the process exits), so the grid is limited to
+ * 4,194,304 nodes after padding each axis to a multiple of 4; larger grids return
+ * TOMO_ERR_CAPACITY.  All calls on a device share that array: calls whose GPU work
+ * overlaps race and must not be issued.  The first call on a device looks up the array's
+ * address with that device current; make it before any stream capture.  Errors:
+ * tomo_last_error(NULL). */
+int tomo_eik_solve_static(const float *slowness, int nx, int ny, int nz, float dx, float dy, float dz, float sx,
+                          float sy, float sz, float *t_out, void *stream);
 
 /* ------------------------------------------------- ray tracing and the Jacobian ------- */
 typedef struct {

@@ -12,6 +12,7 @@ using tomo::ShotDesc;
 
 namespace tomo {
 int rebrick_model(tomo_ctx *ctx);
+const char *static_error_text();  // fim_static.cu
 }
 
 namespace {
@@ -178,7 +179,7 @@ int tomo_ctx_destroy(tomo_ctx *ctx)
     return TOMO_OK;
 }
 
-const char *tomo_last_error(const tomo_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+const char *tomo_last_error(const tomo_ctx *ctx) { return ctx ? ctx->err.c_str() : tomo::static_error_text(); }
 
 void *tomo_ctx_stream(tomo_ctx *ctx) { return ctx ? static_cast<void *>(ctx->stream) : nullptr; }
 
