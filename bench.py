@@ -259,14 +259,15 @@ def run_ours(args):
     alg_bytes = act * stats[0]["nodes_per_brick"] * BYTES_PER_NODE_ACT
     peak, peak_kind = peaks()
     achieved = alg_bytes / (kern_ms / 1000.0) / 1e9
+    # DRAM bytes per brick activation from the committed ncu summary (one capture of a
+    # 16-shot launch of the same workload), scaled to this launch's activations
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "k_fim_solve_traffic.json")
+    tpath = os.path.join(ROOT, "profiles", "k_fim_solve_config2.md")
     if os.path.exists(tpath):
-        try:
-            with open(tpath) as f:
-                traffic = json.load(f).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
+        with open(tpath) as f:
+            for ln in f:
+                if ln.startswith("dram_bytes_per_activation:"):
+                    traffic = float(ln.split(":")[1]) * act
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",

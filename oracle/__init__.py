@@ -54,6 +54,9 @@ def _load():
         lib.oracle_fim_jw.argtypes = [c_int, c_int, c_int, c_float, c_float, c_float, _f32p,
                                       c_float, c_float, c_float, _f64p, c_int, c_double]
         lib.oracle_fim_jw.restype = c_int
+        lib.oracle_fsm_ngb.argtypes = [c_int, c_int, c_int, c_float, c_float, c_float, _f32p,
+                                       c_float, c_float, c_float, _f32p, c_int]
+        lib.oracle_fsm_ngb.restype = c_int
         lib.oracle_first_arrival.argtypes = [c_int, c_int, c_int, c_float, c_float, c_float, _f32p,
                                              c_int, _f32p, _f32p, _f32p, _f32p]
         lib.oracle_first_arrival.restype = None
@@ -98,6 +101,19 @@ def fim_jw(slowness, h, src, max_passes=200, tol=1e-10):
     if rc < 0:
         raise ValueError(f"oracle_fim_jw failed ({rc})")
     return out, rc
+
+
+def fsm_ngb(slowness, h, src, extra_full_sweeps=0):
+    """Noble-Gesret-Belayouni FSM restated (FP32).  extra_full_sweeps=0 reproduces the
+    reference's 16 sweeps; -1 sweeps on to the fixed point.  Returns (T, extra passes)."""
+    lib = _load()
+    s = _vol(slowness)
+    ny, nx, nz = s.shape
+    dx, dy, dz = (h, h, h) if np.isscalar(h) else h
+    out = np.empty_like(s)
+    extra = lib.oracle_fsm_ngb(nx, ny, nz, dx, dy, dz, s.ravel(), src[0], src[1], src[2], out.ravel(),
+                               extra_full_sweeps)
+    return out, extra
 
 
 def first_arrival(T, h, rx, ry, rz):

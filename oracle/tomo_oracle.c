@@ -124,6 +124,179 @@ int oracle_fim_jw(int nx, int ny, int nz, float dx, float dy, float dz,
 }
 
 /* ------------------------------------------------------------------------------------
+ * Noble-Gesret-Belayouni fast sweeping (src/eikonal/accurate_FSM/accurate_FSM.cpp),
+ * FP32, same operation order as inner_sweep (:159-265).  Grid with a one-node replicated
+ * halo (nzz = nz+2, ...).  Neighbour reads use the reference's flattened index, so a read
+ * one past a column edge lands in the next column exactly as there; past the array end
+ * (undefined in the reference) it reads 1e6.
+ * ---------------------------------------------------------------------------------- */
+typedef struct {
+    int nxx, nyy, nzz;
+    long n;
+    float dx, dy, dz, dz2i, dx2i, dy2i, dz2dx2, dz2dy2, dx2dy2, dsum;
+    float *S, *T;
+} Ngb;
+
+static inline float ngb_t(const Ngb *g, long idx) { return (idx >= 0 && idx < g->n) ? g->T[idx] : 1e6f; }
+#define NS(ii, jj, kk) (g->S[(ii) + (long)(jj) * g->nzz + (long)(kk) * g->nxx * g->nzz])
+static inline float fmin2(float a, float b) { return a < b ? a : b; }   /* std::min(a, b) */
+static inline float fmax2(float a, float b) { return a < b ? b : a; }   /* std::max(a, b) */
+
+static int ngb_sweep_point(Ngb *g, int i, int j, int k, int sgntz, int sgntx, int sgnty)
+{
+    const int nxx = g->nxx, nyy = g->nyy, nzz = g->nzz;
+    const long sx = nzz, sy = (long)nxx * nzz;
+    const int sgnvz = sgntz == 1, sgnvx = sgntx == 1, sgnvy = sgnty == 1;
+    const int i1 = i - sgnvz, j1 = j - sgnvx, k1 = k - sgnvy;
+    const float tv = ngb_t(g, (i - sgntz) + j * sx + k * sy);
+    const float te = ngb_t(g, i + (j - sgntx) * sx + k * sy);
+    const float tn = ngb_t(g, i + j * sx + (k - sgnty) * sy);
+    const float tev = ngb_t(g, (i - sgntz) + (j - sgntx) * sx + k * sy);
+    const float ten = ngb_t(g, i + (j - sgntx) * sx + (k - sgnty) * sy);
+    const float tnv = ngb_t(g, (i - sgntz) + j * sx + (k - sgnty) * sy);
+    const float tnve = ngb_t(g, (i - sgntz) + (j - sgntx) * sx + (k - sgnty) * sy);
+    const long ijk = i + j * sx + k * sy;
+    const int jm = imax(j - 1, 1), jp = imin(j, nxx - 1), km = imax(k - 1, 1), kp = imin(k, nyy - 1);
+    const int im = imax(i - 1, 1), ip = imin(i, nzz - 1);
+    float t1D1 = tv + g->dz * fmin2(NS(i1, jm, km), fmin2(NS(i1, jm, kp), fmin2(NS(i1, jp, km), NS(i1, jp, kp))));
+    float t1D2 = te + g->dx * fmin2(NS(im, j1, km), fmin2(NS(ip, j1, km), fmin2(NS(im, j1, kp), NS(ip, j1, kp))));
+    float t1D3 = tn + g->dy * fmin2(NS(im, jm, k1), fmin2(NS(im, jp, k1), fmin2(NS(ip, jm, k1), NS(ip, jp, k1))));
+    const float t1D = fmin2(t1D1, fmin2(t1D2, t1D3));
+    float t2D1 = 1e6f, t2D2 = 1e6f, t2D3 = 1e6f, ta, tb, tc, Sref;
+    const float dz2i = g->dz2i, dx2i = g->dx2i, dy2i = g->dy2i;
+    Sref = fmin2(NS(i1, j1, km), NS(i1, j1, kp));
+    if ((tv < te + g->dx * Sref) && (te < tv + g->dz * Sref)) {
+        ta = tev + te - tv;
+        tb = tev - te + tv;
+        t2D1 = ((tb * dz2i + ta * dx2i) + sqrtf(4.0f * Sref * Sref * (dz2i + dx2i) - dz2i * dx2i * (ta - tb) * (ta - tb))) / (dz2i + dx2i);
+    }
+    Sref = fmin2(NS(i1, jm, k1), NS(i1, jp, k1));
+    if ((tv < tn + g->dy * Sref) && (tn < tv + g->dz * Sref)) {
+        ta = tv - tn + tnv;
+        tb = tn - tv + tnv;
+        t2D2 = ((ta * dz2i + tb * dy2i) + sqrtf(4.0f * Sref * Sref * (dz2i + dy2i) - dz2i * dy2i * (ta - tb) * (ta - tb))) / (dz2i + dy2i);
+    }
+    Sref = fmin2(NS(im, j1, k1), NS(ip, j1, k1));
+    if ((te < tn + g->dy * Sref) && (tn < te + g->dx * Sref)) {
+        ta = te - tn + ten;
+        tb = tn - te + ten;
+        t2D3 = ((ta * dx2i + tb * dy2i) + sqrtf(4.0f * Sref * Sref * (dx2i + dy2i) - dx2i * dy2i * (ta - tb) * (ta - tb))) / (dx2i + dy2i);
+    }
+    const float t2D = fmin2(t2D1, fmin2(t2D2, t2D3));
+    float t3D = 1e6f;
+    Sref = NS(i1, j1, k1);
+    ta = te - 0.5f * tn + 0.5f * ten - 0.5f * tv + 0.5f * tev - tnv + tnve;
+    tb = tv - 0.5f * tn + 0.5f * tnv - 0.5f * te + 0.5f * tev - ten + tnve;
+    tc = tn - 0.5f * te + 0.5f * ten - 0.5f * tv + 0.5f * tnv - tev + tnve;
+    if (fmin2(t1D, t2D) > fmax2(tv, fmax2(te, tn))) {
+        const float t2 = 9.0f * Sref * Sref * g->dsum;
+        const float t3 = g->dz2dx2 * (ta - tb) * (ta - tb) + g->dz2dy2 * (tb - tc) * (tb - tc) + g->dx2dy2 * (ta - tc) * (ta - tc);
+        if (t2 >= t3) {
+            const float t1 = tb * dz2i + ta * dx2i + tc * dy2i;
+            t3D = (t1 + sqrtf(t2 - t3)) / g->dsum;
+        }
+    }
+    const float nv = fmin2(g->T[ijk], fmin2(t1D, fmin2(t2D, t3D)));
+    const int changed = nv != g->T[ijk];
+    g->T[ijk] = nv;
+    return changed;
+}
+
+/* One sweep over a box of loop ranges (k outer, j, i inner), each given as first/last. */
+static int ngb_sweep(Ngb *g, int sgntz, int sgntx, int sgnty, int i0, int i1, int j0, int j1, int k0, int k1)
+{
+    int changed = 0;
+    const int di = i1 >= i0 ? 1 : -1, dj = j1 >= j0 ? 1 : -1, dk = k1 >= k0 ? 1 : -1;
+    for (int k = k0; dk > 0 ? k <= k1 : k >= k1; k += dk)
+        for (int j = j0; dj > 0 ? j <= j1 : j >= j1; j += dj)
+            for (int i = i0; di > 0 ? i <= i1 : i >= i1; i += di) changed |= ngb_sweep_point(g, i, j, k, sgntz, sgntx, sgnty);
+    return changed;
+}
+
+int oracle_fsm_ngb(int nx, int ny, int nz, float dx, float dy, float dz, const float *slowness,
+                   float sx, float sy, float sz, float *T_out, int extra_full_sweeps)
+{
+    Ngb G, *g = &G;
+    g->nxx = nx + 2;
+    g->nyy = ny + 2;
+    g->nzz = nz + 2;
+    const int nxx = g->nxx, nyy = g->nyy, nzz = g->nzz;
+    g->n = (long)nxx * nyy * nzz;
+    g->S = (float *)malloc(sizeof(float) * g->n);
+    g->T = (float *)malloc(sizeof(float) * g->n);
+    /* expand_model (:8-60): replicate one node around (clamp) */
+    for (int k = 0; k < nyy; k++)
+        for (int j = 0; j < nxx; j++)
+            for (int i = 0; i < nzz; i++)
+                g->S[i + (long)j * nzz + (long)k * nxx * nzz] =
+                    slowness[imin(imax(i - 1, 0), nz - 1) + (long)imin(imax(j - 1, 0), nx - 1) * nz +
+                             (long)imin(imax(k - 1, 0), ny - 1) * nx * nz];
+    const int nb = 1;
+    const int sidx = (int)(sx / dx) + nb, sidy = (int)(sy / dy) + nb, sidz = (int)(sz / dz) + nb;
+    const long sId = sidz + (long)sidx * nzz + (long)sidy * nxx * nzz;
+    for (long q = 0; q < g->n; q++) g->T[q] = 1e6f;
+    /* the source node and its 26 neighbours: analytic time with the source slowness
+     * (:596-630).  As in the reference, the nodes at (z+1, x-1) and (z-1, x+1) receive each
+     * other's distance (:608-609); identical for a source on a node. */
+    for (int oy = -1; oy <= 1; oy++)
+        for (int ox = -1; ox <= 1; ox++)
+            for (int oz = -1; oz <= 1; oz++) {
+                int fx = ox, fz = oz;
+                if (oy == 0 && oz * ox == -1) {
+                    fx = -ox;
+                    fz = -oz;
+                }
+                g->T[sId + oz + (long)ox * nzz + (long)oy * nxx * nzz] =
+                    g->S[sId] * sqrtf(powf(((sidx - nb) + fx) * dx - sx, 2.0f) + powf(((sidy - nb) + oy) * dy - sy, 2.0f) +
+                                      powf(((sidz - nb) + fz) * dz - sz, 2.0f));
+            }
+    g->dx = dx;
+    g->dy = dy;
+    g->dz = dz;
+    g->dz2i = 1.0f / (dz * dz);
+    g->dx2i = 1.0f / (dx * dx);
+    g->dy2i = 1.0f / (dy * dy);
+    g->dz2dx2 = g->dz2i * g->dx2i;
+    g->dz2dy2 = g->dz2i * g->dy2i;
+    g->dx2dy2 = g->dx2i * g->dy2i;
+    g->dsum = g->dz2i + g->dx2i + g->dy2i;
+    /* init_sweep (:267-388): 8 sweeps anchored at the source */
+    const int zA = imax(1, sidz), xA = imax(1, sidx), yA = imax(1, sidy);
+    ngb_sweep(g, 1, 1, 1, zA, nzz - 1, xA, nxx - 1, yA, nyy - 1);
+    ngb_sweep(g, -1, 1, 1, sidz + 1, 0, xA, nxx - 1, yA, nyy - 1);
+    ngb_sweep(g, 1, 1, -1, zA, nzz - 1, xA, nxx - 1, sidy + 1, 0);
+    ngb_sweep(g, -1, 1, -1, sidz + 1, 0, xA, nxx - 1, sidy + 1, 0);
+    ngb_sweep(g, 1, -1, 1, zA, nzz - 1, sidx + 1, 0, yA, nyy - 1);
+    ngb_sweep(g, -1, -1, 1, sidz + 1, 0, sidx + 1, 0, yA, nyy - 1);
+    ngb_sweep(g, 1, -1, -1, zA, nzz - 1, sidx + 1, 0, sidy + 1, 0);
+    ngb_sweep(g, -1, -1, -1, sidz + 1, 0, sidx + 1, 0, sidy + 1, 0);
+    /* full_sweep (:390-511) once, then optional extra passes to the fixed point */
+    int pass = -1, extra = 0;
+    for (;;) {
+        int ch = 0;
+        ch |= ngb_sweep(g, 1, 1, 1, 1, nzz - 1, 1, nxx - 1, 1, nyy - 1);
+        ch |= ngb_sweep(g, -1, 1, 1, nzz - 2, 0, 1, nxx - 1, 1, nyy - 1);
+        ch |= ngb_sweep(g, 1, 1, -1, 1, nzz - 1, 1, nxx - 1, nyy - 2, 0);
+        ch |= ngb_sweep(g, -1, 1, -1, nzz - 2, 0, 1, nxx - 1, nyy - 2, 0);
+        ch |= ngb_sweep(g, 1, -1, 1, 1, nzz - 1, nxx - 2, 0, 1, nyy - 1);
+        ch |= ngb_sweep(g, -1, -1, 1, nzz - 2, 0, nxx - 2, 0, 1, nyy - 1);
+        ch |= ngb_sweep(g, 1, -1, -1, 1, nzz - 1, nxx - 2, 0, nyy - 2, 0);
+        ch |= ngb_sweep(g, -1, -1, -1, nzz - 2, 0, nxx - 2, 0, nyy - 2, 0);
+        pass++;
+        if (pass > 0) extra++;
+        if (extra_full_sweeps == 0 || (extra_full_sweeps > 0 && extra >= extra_full_sweeps) || (pass > 0 && !ch)) break;
+    }
+    /* reduce_model (:62-72) */
+    for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++)
+            for (int z = 0; z < nz; z++)
+                T_out[z + (long)x * nz + (long)y * nx * nz] = g->T[(z + 1) + (long)(x + 1) * nzz + (long)(y + 1) * nxx * nzz];
+    free(g->S);
+    free(g->T);
+    return extra;
+}
+
+/* ------------------------------------------------------------------------------------
  * trilinear (src/utils/interpolation/trilinear.cpp:3-20), FP32 reference order.
  * ---------------------------------------------------------------------------------- */
 static float tri32(float c000, float c001, float c100, float c101, float c010, float c011,

@@ -31,6 +31,14 @@ int oracle_fim_jw(int nx, int ny, int nz, float dx, float dy, float dz,
                   const float *slowness, float sx, float sy, float sz,
                   double *T_out, int max_passes, double tol);
 
+/* Noble-Gesret-Belayouni fast sweeping (Accurate_FSM, src/eikonal/accurate_FSM/
+ * accurate_FSM.cpp:159-650) restated in FP32 with the reference's operation order.
+ * extra_full_sweeps = 0 reproduces the reference (8 source-anchored + 8 full sweeps);
+ * > 0 runs that many more full 8-octant passes, or until nothing changes (< 0: no limit).
+ * T_out: nz*nx*ny floats (cropped).  Returns the number of extra passes run. */
+int oracle_fsm_ngb(int nx, int ny, int nz, float dx, float dy, float dz, const float *slowness,
+                   float sx, float sy, float sz, float *T_out, int extra_full_sweeps);
+
 /* Trilinear receiver sampling of a cropped traveltime volume (Block_FIM/Accurate_FSM
  * write_first_arrival), FP32 with the reference's operation order. */
 void oracle_first_arrival(int nx, int ny, int nz, float dx, float dy, float dz,
