@@ -60,6 +60,10 @@ typedef struct {
 /* Local Godunov operator of the eikonal solve. */
 #define TOMO_OP_JW  0  /* Jeong & Whitaker 2008 first-order update, isotropic h = dx, single
                           node source seed: Block_FIM (src/eikonal/block_FIM/cuda_kernel.cu:217-248) */
+#define TOMO_OP_NGB 1  /* Noble, Gesret & Belayouni 2014 operator with dx, dy, dz and the 27-node
+                          seed, run as the reference's 8 source-anchored + 8 full sweeps:
+                          Accurate_FSM (src/eikonal/accurate_FSM/accurate_FSM.cpp:159-650),
+                          reproduced bit for bit */
 
 typedef struct {
     int op;          /* TOMO_OP_*                                                     */
@@ -78,6 +82,8 @@ typedef struct {
     float inner_tol; /* in-brick relaxation stops when no node drops by more than this
                         (s).  <= 0: exact (default)                                  */
     int ieee_sqrt;   /* 1: IEEE sqrtf in the local update; 0 (default): sqrt.approx  */
+    int sweep_groups;/* TOMO_OP_NGB: independent block groups sweeping their own shots
+                        (0: default)                                                  */
 } tomo_eik_opts;
 
 typedef struct {

@@ -26,6 +26,8 @@ CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                      "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
+# Sources that restate a reference FP32 computation bit for bit: no FMA contraction.
+NO_FMA_SOURCES = {"fsm.cu"}
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function",
              "-I" + os.path.join(CUDA, "include"), "-I" + os.path.join(ROOT, "include")]
 
@@ -59,6 +61,8 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         objs.append(obj)
         if _stale(obj, [src] + hdrs) or ptxas_info:
             extra = ["-Xptxas", "-v"] if ptxas_info else []
+            if os.path.basename(src) in NO_FMA_SOURCES:
+                extra += ["-fmad=false"]
             _run([NVCC] + NVCC_FLAGS + extra + ["-c", src, "-o", obj], verbose)
     host_hdrs = hdrs + glob.glob(os.path.join(HOST, "*.hpp"))
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cpp")) + glob.glob(os.path.join(HOST, "*.cpp"))):

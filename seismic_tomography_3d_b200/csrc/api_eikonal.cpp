@@ -7,6 +7,7 @@
 
 #include "common.cuh"
 #include "context.hpp"
+#include "fsm.cuh"
 
 using tomo::ShotDesc;
 
@@ -60,6 +61,87 @@ int upload_model(tomo_ctx *ctx, const float *host, bool is_velocity)
     if (rc != TOMO_OK) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->have_model = true;
+    return TOMO_OK;
+}
+
+// TOMO_OP_NGB: the reference's Accurate_FSM sweeps for every shot (csrc/fsm.cu), written
+// into the brick-major pool described by sd, then the receivers.
+int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point *shots, int nshots, int nrec,
+               int groups)
+{
+    const tomo_grid &g = ctx->g;
+    std::vector<tomo::FsmShot> fs((size_t)nshots);
+    long long total = 0;
+    for (int s = 0; s < nshots; s++) {
+        tomo::FsmShot &f = fs[(size_t)s];
+        const ShotDesc &d = sd[(size_t)s];
+        f.wx0 = d.wx0;
+        f.wy0 = d.wy0;
+        f.wnx = d.wnx;
+        f.wny = d.wny;
+        const float sx = shots[s].x - (float)d.wx0 * g.dx, sy = shots[s].y - (float)d.wy0 * g.dy, sz = shots[s].z;
+        const int nb = 1;
+        f.sidx = (int)(sx / g.dx) + nb;
+        f.sidy = (int)(sy / g.dy) + nb;
+        f.sidz = (int)(sz / g.dz) + nb;
+        // the 27 seeded nodes (accurate_FSM.cpp:596-630), including the reference's swap of
+        // the (z+1, x-1) and (z-1, x+1) distances (:608-609)
+        for (int oy = -1; oy <= 1; oy++)
+            for (int ox = -1; ox <= 1; ox++)
+                for (int oz = -1; oz <= 1; oz++) {
+                    int fx = ox, fz = oz;
+                    if (oy == 0 && oz * ox == -1) {
+                        fx = -ox;
+                        fz = -oz;
+                    }
+                    f.seed_dist[(oz + 1) + 3 * (ox + 1) + 9 * (oy + 1)] =
+                        sqrtf(powf(((f.sidx - nb) + fx) * g.dx - sx, 2.0f) + powf(((f.sidy - nb) + oy) * g.dy - sy, 2.0f) +
+                              powf(((f.sidz - nb) + fz) * g.dz - sz, 2.0f));
+                }
+        f.t_off = total;
+        total += (long long)(g.nz + 2) * (d.wnx + 2) * (d.wny + 2);
+    }
+    int ngroups = groups > 0 ? groups : 1;
+    if (ngroups > nshots) ngroups = nshots;
+    CK(ctx->fsm_T.ensure((size_t)total));
+    CK(ctx->fsm_shots.ensure((size_t)nshots));
+    CK(ctx->fsm_bar.ensure((size_t)2 * ngroups));
+    CK(cudaMemcpyAsync(ctx->fsm_shots.ptr, fs.data(), fs.size() * sizeof(tomo::FsmShot), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaMemsetAsync(ctx->fsm_bar.ptr, 0, 2 * ngroups * sizeof(unsigned), ctx->stream));
+    CK(cudaMemsetAsync(ctx->ctrl.ptr, 0, tomo::kCtrlWords * sizeof(unsigned), ctx->stream));
+    CK(cudaMemsetAsync(ctx->stats.ptr, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    tomo::FsmLaunch p{};
+    p.slow = ctx->slow.ptr;
+    p.nx = g.nx;
+    p.ny = g.ny;
+    p.nz = g.nz;
+    p.dx = g.dx;
+    p.dy = g.dy;
+    p.dz = g.dz;
+    // Accurate_FSM::eikonal_equation (accurate_FSM.cpp:632-644), FP32 on the host
+    p.dz2i = 1.0f / (g.dz * g.dz);
+    p.dx2i = 1.0f / (g.dx * g.dx);
+    p.dy2i = 1.0f / (g.dy * g.dy);
+    p.dz2dx2 = p.dz2i * p.dx2i;
+    p.dz2dy2 = p.dz2i * p.dy2i;
+    p.dx2dy2 = p.dx2i * p.dy2i;
+    p.dsum = p.dz2i + p.dx2i + p.dy2i;
+    p.T = ctx->fsm_T.ptr;
+    p.shots = ctx->fsm_shots.ptr;
+    p.nshots = nshots;
+    p.ngroups = ngroups;
+    p.bar = ctx->fsm_bar.ptr;
+    p.err = ctx->ctrl.ptr + tomo::kErr;
+    p.spin_limit = kSpinLimit;
+    p.Tb = ctx->T.ptr;
+    p.desc = ctx->shots_d.ptr;
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    int grid = 0;
+    CK(tomo::fsm_solve(p, &grid, ctx->stream));
+    if (nrec > 0)
+        CK(tomo::receivers_sample(ctx->T.ptr, ctx->shots_d.ptr, nshots, ctx->rec.ptr, ctx->rec.ptr + nrec,
+                                  ctx->rec.ptr + 2 * nrec, nrec, g.dx, g.dy, g.dz, g.nz, ctx->t_recv.ptr, ctx->stream));
     return TOMO_OK;
 }
 
@@ -227,7 +309,8 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     if (nshots < 1 || !shots) return fail(ctx, TOMO_ERR_INVALID_ARG, "nshots must be >= 1 with shot positions");
     if (nrec < 0 || (nrec > 0 && !receivers)) return fail(ctx, TOMO_ERR_INVALID_ARG, "bad receivers");
     if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
-    if (opts && opts->op != TOMO_OP_JW) return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown eikonal operator");
+    if (opts && opts->op != TOMO_OP_JW && opts->op != TOMO_OP_NGB)
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown eikonal operator");
     const tomo_grid &g = ctx->g;
     const int max_inner = (opts && opts->max_inner > 0) ? opts->max_inner : kDefaultMaxInner;
     const int max_rounds = (opts && opts->max_rounds > 0) ? opts->max_rounds : kDefaultMaxRounds;
@@ -320,6 +403,11 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
 
     // ---- launch -----------------------------------------------------------------------
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    const bool ngb = opts && opts->op == TOMO_OP_NGB;
+    if (ngb) {
+        const int rc = launch_ngb(ctx, sd, shots, nshots, nrec, opts ? opts->sweep_groups : 0);
+        if (rc != TOMO_OK) return rc;
+    } else {
     unsigned *key = nullptr, *minkey = nullptr;
     if (band_s > 0.f) {
         CK(ctx->key.ensure((size_t)q_total));
@@ -370,6 +458,7 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     int grid = 0;
     CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     CK(tomo::fim_solve(p, block_warps, occupancy, opts && opts->ieee_sqrt, &grid, ctx->stream));
+    }
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     CK(cudaMemcpyAsync(ctx->pinned_ctrl, ctx->ctrl.ptr, tomo::kCtrlWords * sizeof(unsigned), cudaMemcpyDeviceToHost,
                        ctx->stream));

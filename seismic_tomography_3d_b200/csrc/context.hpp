@@ -8,6 +8,7 @@
 
 #include "../../include/tomo_b200.h"
 #include "fim.cuh"
+#include "fsm.cuh"
 
 namespace tomo {
 
@@ -56,6 +57,9 @@ struct tomo_ctx {
     tomo::DevBuf<float> T;
     tomo::DevBuf<unsigned> qflag, lists, ctrl;
     tomo::DevBuf<unsigned> key, minkey, smin_bits;  // band-ordered scheduling
+    tomo::DevBuf<float> fsm_T;                      // TOMO_OP_NGB sweep grids (with halo)
+    tomo::DevBuf<tomo::FsmShot> fsm_shots;
+    tomo::DevBuf<unsigned> fsm_bar;
     tomo::DevBuf<unsigned long long> stats;
     tomo::DevBuf<tomo::ShotDesc> shots_d;
     std::vector<tomo::ShotDesc> shots_h;

@@ -84,6 +84,50 @@ __device__ __forceinline__ float brick_T(const float *T, const ShotDesc &d, int 
     return __ldcg(T + d.t_off + b * kBrickNodes + (z & 3) + 4 * (x & 3) + 16 * (y & 3));
 }
 
+// Receiver sampling (Block_FIM::write_first_arrival, block_FIM.cpp:228-262): trilinear
+// from the floor node of the window-cropped field, with the reference's flattened index
+// arithmetic (an offset past a column wraps into the next; past the end: 0).  Grid-stride
+// over (shot, receiver); receivers outside a shot's window get kInf.
+__device__ void sample_receivers(const float *T, const ShotDesc *shots, int nshots, const float *rx,
+                                 const float *ry, const float *rz, int nrec, float dx, float dy, float dz,
+                                 int nz_, float *t_recv)
+{
+    const long long total = (long long)nshots * nrec;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(e / nrec), r = (int)(e % nrec);
+        const ShotDesc &d = shots[s];
+        const float x = fsub(rx[r], fmul((float)d.wx0, dx));
+        const float y = fsub(ry[r], fmul((float)d.wy0, dy));
+        const float z = rz[r];
+        if (x < 0.0f || y < 0.0f || x > fmul((float)(d.wnx - 1), dx) || y > fmul((float)(d.wny - 1), dy)) {
+            t_recv[e] = kInf;
+            continue;
+        }
+        const float fx = floorf(fdiv(x, dx)), fy = floorf(fdiv(y, dy)), fz = floorf(fdiv(z, dz));
+        const float x0 = fmul(fx, dx), y0 = fmul(fy, dy), z0 = fmul(fz, dz);
+        const float x1 = fadd(fmul(fx, dx), dx), y1 = fadd(fmul(fy, dy), dy), z1 = fadd(fmul(fz, dz), dz);
+        const long long nz = nz_, wnx = d.wnx, n = nz * wnx * d.wny;
+        const long long id = (long long)(int)fdiv(z, dz) + (long long)(int)fdiv(x, dx) * nz +
+                             (long long)(int)fdiv(y, dy) * wnx * nz;
+        const long long offs[8] = {0, 1, nz, 1 + nz, wnx * nz, 1 + wnx * nz, nz + wnx * nz, 1 + nz + wnx * nz};
+        float c[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const long long f = id + offs[q];
+            if (f >= 0 && f < n) {
+                const int zz = (int)(f % nz);
+                const long long rest = f / nz;
+                const int xx = (int)(rest % wnx), yy = (int)(rest / wnx);
+                c[q] = brick_T(T, d, xx, yy, zz);
+            } else {
+                c[q] = 0.0f;
+            }
+        }
+        t_recv[e] = trilinear_ref(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], x0, x1, y0, y1, z0, z1, x, y, z);
+    }
+}
+
 struct WarpStats {
     unsigned long long act, inner;
 };
@@ -310,45 +354,23 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
     if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kRounds] = round;
     if (!ok || p.nrec == 0) return;
 
-    // Receiver sampling (Block_FIM::write_first_arrival, block_FIM.cpp:228-262): trilinear
-    // from the floor node of the window-cropped field, with the reference's flattened
-    // index arithmetic (an offset past a column wraps into the next; past the end: 0).
-    const long long total = (long long)p.nshots * p.nrec;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int s = (int)(e / p.nrec), r = (int)(e % p.nrec);
-        const ShotDesc &d = p.shots[s];
-        const float dx = p.dx, dy = p.dy, dz = p.dz;
-        const float x = fsub(p.rx[r], fmul((float)d.wx0, dx));
-        const float y = fsub(p.ry[r], fmul((float)d.wy0, dy));
-        const float z = p.rz[r];
-        if (x < 0.0f || y < 0.0f || x > fmul((float)(d.wnx - 1), dx) || y > fmul((float)(d.wny - 1), dy)) {
-            p.t_recv[e] = kInf;  // receiver outside this shot's window: no traveltime
-            continue;
-        }
-        const float fx = floorf(fdiv(x, dx)), fy = floorf(fdiv(y, dy)), fz = floorf(fdiv(z, dz));
-        const float x0 = fmul(fx, dx), y0 = fmul(fy, dy), z0 = fmul(fz, dz);
-        const float x1 = fadd(fmul(fx, dx), dx), y1 = fadd(fmul(fy, dy), dy), z1 = fadd(fmul(fz, dz), dz);
-        const long long nz = p.nz, wnx = d.wnx, n = nz * wnx * d.wny;
-        const long long id = (long long)(int)fdiv(z, dz) + (long long)(int)fdiv(x, dx) * nz +
-                             (long long)(int)fdiv(y, dy) * wnx * nz;
-        const long long offs[8] = {0, 1, nz, 1 + nz, wnx * nz, 1 + wnx * nz, nz + wnx * nz, 1 + nz + wnx * nz};
-        float c[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-            const long long f = id + offs[q];
-            if (f >= 0 && f < n) {
-                const int zz = (int)(f % nz);
-                const long long rest = f / nz;
-                const int xx = (int)(rest % wnx), yy = (int)(rest / wnx);
-                c[q] = brick_T(p.T, d, xx, yy, zz);
-            } else {
-                c[q] = 0.0f;
-            }
-        }
-        p.t_recv[e] = trilinear_ref(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], x0, x1, y0, y1,
-                                    z0, z1, x, y, z);
-    }
+    sample_receivers(p.T, p.shots, p.nshots, p.rx, p.ry, p.rz, p.nrec, p.dx, p.dy, p.dz, p.nz, p.t_recv);
+}
+
+__global__ void k_receivers(const float *T, const ShotDesc *shots, int nshots, const float *rx, const float *ry,
+                            const float *rz, int nrec, float dx, float dy, float dz, int nz, float *t_recv)
+{
+    sample_receivers(T, shots, nshots, rx, ry, rz, nrec, dx, dy, dz, nz, t_recv);
+}
+
+cudaError_t receivers_sample(const float *T, const ShotDesc *shots, int nshots, const float *rx, const float *ry,
+                             const float *rz, int nrec, float dx, float dy, float dz, int nz, float *t_recv,
+                             cudaStream_t st)
+{
+    const long long n = (long long)nshots * nrec;
+    const int grid = (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
+    k_receivers<<<grid > 0 ? grid : 1, 256, 0, st>>>(T, shots, nshots, rx, ry, rz, nrec, dx, dy, dz, nz, t_recv);
+    return cudaGetLastError();
 }
 
 // -------------------------------------------------------------------------------------
