@@ -269,6 +269,22 @@ def run_ours(args):
                 if ln.startswith("dram_bytes_per_activation:"):
                     traffic = float(ln.split(":")[1]) * act
 
+    # ---- the NGB operator: the reference's own Accurate_FSM sweeps, bit-exact ------------
+    ngb_steps = max(1, min(args.steps, 5))
+    ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=False, op=1)
+    barrier()
+    n0, n1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0.record(stream)
+    for _ in range(ngb_steps):
+        ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=False, op=1)
+    n1.record(stream)
+    barrier()
+    ngb_ms = n0.elapsed_time(n1) / ngb_steps
+    if dist is not None:
+        t = torch.tensor([ngb_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ngb_ms = float(t.item())
+
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
@@ -288,7 +304,11 @@ def run_ours(args):
             "clocks": clk.summary(),
             "gpu_launches": 3 * args.steps,
             "solver": {"rounds": stats[-1]["rounds"], "activations": stats[-1]["activations"],
-                       "inner_iterations": stats[-1]["inner_iterations"]}}
+                       "inner_iterations": stats[-1]["inner_iterations"]},
+            "ngb_fsm": {"value": world * ns / (ngb_ms / 1000.0), "unit": UNIT, "ms_per_step": ngb_ms,
+                        "steps": ngb_steps,
+                        "what": "TOMO_OP_NGB: the reference Accurate_FSM's 8+8 sweeps on the same batch, "
+                                "bit-exact with the reference CPU solver (the cpu_baseline's algorithm)"}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, desc = cpu_reference_sample(sv, max_shots=min(ns, max(8, 2 * (os.cpu_count() or 1))),
                                                  budget_s=25.0)

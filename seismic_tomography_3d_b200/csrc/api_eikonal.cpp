@@ -101,7 +101,7 @@ int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point 
         f.t_off = total;
         total += (long long)(g.nz + 2) * (d.wnx + 2) * (d.wny + 2);
     }
-    int ngroups = groups > 0 ? groups : 1;
+    int ngroups = groups > 0 ? groups : 4;  // 4 groups: fastest of 1..16 on the 64-shot batch
     if (ngroups > nshots) ngroups = nshots;
     CK(ctx->fsm_T.ensure((size_t)total));
     CK(ctx->fsm_shots.ensure((size_t)nshots));

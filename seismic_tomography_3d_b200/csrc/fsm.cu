@@ -179,7 +179,7 @@ __device__ float ngb_update(const FsmLaunch &p, const ShotGrid &g, int i, int j,
 
 }  // namespace
 
-__global__ void __launch_bounds__(256) k_fsm_sweeps(FsmLaunch p)
+__global__ void __launch_bounds__(256, 3) k_fsm_sweeps(FsmLaunch p)
 {
     const int G = p.ngroups;
     const int grp = blockIdx.x % G;

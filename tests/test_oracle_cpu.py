@@ -115,6 +115,32 @@ def test_fsm_golden_reproduces(oracle_mod):
         np.testing.assert_array_equal(T, g[f"fsm_{seed}"])
 
 
+def test_fsm_restatement_bit_exact(oracle_mod):
+    """The oracle's FP32 restatement of Accurate_FSM (incl. the reference's swapped seed
+    distances at (z+1, x-1) / (z-1, x+1)) reproduces the reference's volumes exactly."""
+    g = np.load(os.path.join(GOLD, "eik_ref.npz"))
+    for seed, nx, ny, nz, h, shots in mg.EIK_CASES:
+        s = (np.float32(1.0) / g[f"v_{seed}"]).astype(np.float32)
+        for i, sh in enumerate(g[f"shots_{seed}"]):
+            T, _ = oracle_mod.fsm_ngb(s, h, tuple(map(float, sh)), 0)
+            np.testing.assert_array_equal(T, g[f"fsm_{seed}"][i])
+
+
+def test_fsm_sixteen_sweeps_not_always_converged(oracle_mod):
+    """On a layered model the reference's fixed 8+8 sweeps stop short of the NGB fixed
+    point (head waves need more passes): the reason the device NGB solver reproduces the
+    sweeps instead of iterating to the fixed point."""
+    from seismic_tomography_3d_b200 import workloads as wl
+
+    sv = wl.small(7, 41, 37, 29, h=25.0, layered=True)
+    s = (np.float32(1.0) / sv.velocity).astype(np.float32)
+    src = (float(sv.shots[0][0]), float(sv.shots[0][1]), 0.0)
+    T16, _ = oracle_mod.fsm_ngb(s, sv.h, src, 0)
+    Tfp, extra = oracle_mod.fsm_ngb(s, sv.h, src, -1)
+    assert extra >= 1
+    assert np.all(Tfp <= T16)
+
+
 def test_jw_oracle_vs_reference_solvers(oracle_mod):
     g = np.load(os.path.join(GOLD, "eik_ref.npz"))
     fim = None
