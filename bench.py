@@ -53,29 +53,63 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event reasons sampled during the timed region (read only).
 
+    Reads NVML directly every 10 ms (the GPU is found by its PCI bus id, so the index
+    stays right under CUDA_VISIBLE_DEVICES); falls back to polling nvidia-smi."""
+
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device):
         self.device = device
-        self.samples = []
+        self.samples = []  # (sm_mhz, sm_max_mhz, set of reason names)
         self.stop = threading.Event()
-        self.th = threading.Thread(target=self._run, daemon=True)
+        self.nvml = None
+        try:
+            import pynvml
+            import torch
 
-    def _run(self):
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(device)
+            bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            self.nvml = pynvml
+        except Exception:
+            self.nvml = None
+        self.th = threading.Thread(target=self._run_nvml if self.nvml else self._run_smi, daemon=True)
+
+    def _run_nvml(self):
+        n = self.nvml
+        bits = {"hw_slowdown": n.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": n.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": n.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": n.nvmlClocksEventReasonSwPowerCap}
+        while not self.stop.is_set():
+            try:
+                sm = n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM)
+                mx = n.nvmlDeviceGetMaxClockInfo(self.handle, n.NVML_CLOCK_SM)
+                r = n.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                self.samples.append((float(sm), float(mx), {k for k, v in bits.items() if r & v}))
+            except Exception:
+                pass
+            self.stop.wait(0.01)
+
+    def _run_smi(self):
         while not self.stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True,
                                      timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([c.strip() for c in out.split(",")])
+                c = [x.strip() for x in out.split(",")]
+                if len(c) >= 9 and c[1].replace(".", "").isdigit():
+                    self.samples.append((float(c[1]), float(c[2]),
+                                         {self.REASONS[i] for i in range(4) if c[5 + i].lower() == "active"}))
             except Exception:
                 pass
-            self.stop.wait(0.2)
+            self.stop.wait(0.05)
 
     def __enter__(self):
         self.th.start()
@@ -88,13 +122,10 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4)
-                          if len(s) > 5 + i and s[5 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
+                "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": sorted(set().union(*(s[2] for s in self.samples))),
+                "samples": len(self.samples), "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 def workload(rank, shots=None):

@@ -75,10 +75,6 @@ typedef struct {
     float change_tol;/* a face value must drop by more than this (s) to re-queue the
                         neighbour brick.  0: default 1e-6 s, the reference's EPS
                         (cuda_kernel.cuh:8); < 0: any drop (exact FP32 fixed point) */
-    float band;      /* band-ordered scheduling: a queued brick is relaxed only once its
-                        key (the smallest time of the bricks that queued it) is within
-                        band x (time to cross one brick at the fastest velocity) of its
-                        shot's smallest pending key.  0: default; < 0: off            */
     float inner_tol; /* in-brick relaxation stops when no node drops by more than this
                         (s).  <= 0: exact (default)                                  */
     int ieee_sqrt;   /* 1: IEEE sqrtf in the local update; 0 (default): sqrt.approx  */

@@ -49,7 +49,7 @@ class Window(ctypes.Structure):
 class EikOpts(ctypes.Structure):
     _fields_ = [("op", ctypes.c_int), ("max_inner", ctypes.c_int), ("max_rounds", ctypes.c_int),
                 ("brick", ctypes.c_int), ("block_warps", ctypes.c_int), ("occupancy", ctypes.c_int),
-                ("change_tol", ctypes.c_float), ("band", ctypes.c_float), ("inner_tol", ctypes.c_float),
+                ("change_tol", ctypes.c_float), ("inner_tol", ctypes.c_float),
                 ("ieee_sqrt", ctypes.c_int), ("sweep_groups", ctypes.c_int)]
 
 
@@ -233,7 +233,7 @@ class Context:
 
     # -- eikonal ------------------------------------------------------------------------
     def eik_solve(self, shots, windows=None, receivers=None, want_recv=True, max_inner=0, max_rounds=0,
-                  block_warps=0, op=0, occupancy=0, change_tol=0.0, band=0.0, inner_tol=0.0, ieee_sqrt=0,
+                  block_warps=0, op=0, occupancy=0, change_tol=0.0, inner_tol=0.0, ieee_sqrt=0,
                   sweep_groups=0):
         """Batched solve.  shots (n,3) metres; windows (n,4) [x0,x1,y0,y1] nodes or None;
         receivers (m,3).  Returns (t_recv (n,m) float32 or None, stats dict)."""
@@ -246,7 +246,7 @@ class Context:
         if receivers is not None and len(receivers):
             rp, nr, _r = _points(receivers)
         out = np.empty((ns, nr), np.float32) if (want_recv and nr) else None
-        opts = EikOpts(op, max_inner, max_rounds, 0, block_warps, occupancy, change_tol, band, inner_tol, ieee_sqrt,
+        opts = EikOpts(op, max_inner, max_rounds, 0, block_warps, occupancy, change_tol, inner_tol, ieee_sqrt,
                        sweep_groups)
         st = EikStats()
         self._check(self.lib.tomo_eik_solve(self.h, ns, sp, wp, nr, rp,

@@ -20,8 +20,6 @@ namespace {
 
 constexpr int kDefaultMaxInner = 16;
 constexpr float kDefaultChangeTol = 1e-6f;
-constexpr float kDefaultBand = 0.0f;  // off until tuned
-constexpr int kSminWord = 48;         // pinned_ctrl slot of the smallest slowness (float bits)
 constexpr int kDefaultMaxRounds = 1 << 20;
 constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~ seconds of polling, then error
 
@@ -148,17 +146,10 @@ int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point 
 }  // namespace
 
 namespace tomo {
-// Bricks the device model (after an upload or a model update) and refreshes its smallest
-// slowness, read back into pinned memory by the caller's next stream synchronisation.
+// Bricks the device model (after an upload or a model update).
 int rebrick_model(tomo_ctx *ctx)
 {
     CK(fim_brick_model(ctx->slow.ptr, ctx->S.ptr, ctx->g.nx, ctx->g.ny, ctx->g.nz, ctx->nxx, ctx->nyy, ctx->nzz,
-                       ctx->stream));
-    CK(ctx->smin_bits.ensure(1));
-    const unsigned inf_bits = 0x7f800000u;
-    CK(cudaMemcpyAsync(ctx->smin_bits.ptr, &inf_bits, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
-    CK(slowness_min(ctx->slow.ptr, (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz, ctx->smin_bits.ptr, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->pinned_ctrl + kSminWord, ctx->smin_bits.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost,
                        ctx->stream));
     return TOMO_OK;
 }
@@ -320,13 +311,6 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     float change_tol = kDefaultChangeTol;
     if (opts && opts->change_tol > 0.f) change_tol = opts->change_tol;
     if (opts && opts->change_tol < 0.f) change_tol = 0.f;
-    // band width in seconds: units of the time to cross one brick at the fastest velocity
-    float band_units = kDefaultBand;
-    if (opts && opts->band > 0.f) band_units = opts->band;
-    if (opts && opts->band < 0.f) band_units = 0.f;
-    float smin = 0.f;
-    std::memcpy(&smin, ctx->pinned_ctrl + kSminWord, sizeof(float));
-    const float band_s = (band_units > 0.f && smin > 0.f && smin < 1e30f) ? band_units * tomo::kBrick * g.dx * smin : 0.f;
     CK(cudaSetDevice(ctx->device));
 
     // ---- per-shot descriptors --------------------------------------------------------
@@ -408,17 +392,10 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
         const int rc = launch_ngb(ctx, sd, shots, nshots, nrec, opts ? opts->sweep_groups : 0);
         if (rc != TOMO_OK) return rc;
     } else {
-    unsigned *key = nullptr, *minkey = nullptr;
-    if (band_s > 0.f) {
-        CK(ctx->key.ensure((size_t)q_total));
-        CK(ctx->minkey.ensure((size_t)nshots * 3));
-        key = ctx->key.ptr;
-        minkey = ctx->minkey.ptr;
-    }
     CK(tomo::fim_init(ctx->T.ptr, (size_t)t_total, ctx->qflag.ptr, (size_t)q_total, ctx->ctrl.ptr, ctx->stats.ptr,
-                      key, minkey, nshots, ctx->stream));
+                      ctx->stream));
     CK(tomo::fim_seed(ctx->shots_d.ptr, nshots, ctx->S.ptr, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
-                      ctx->lists.ptr, local_bits, ctx->ctrl.ptr, key, minkey, ctx->stream));
+                      ctx->lists.ptr, local_bits, ctx->ctrl.ptr, ctx->stream));
     tomo::FimLaunch p{};
     p.S = ctx->S.ptr;
     p.T = ctx->T.ptr;
@@ -443,9 +420,6 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     p.max_rounds = max_rounds;
     p.local_bits = local_bits;
     p.spin_limit = kSpinLimit;
-    p.key = key;
-    p.minkey = minkey;
-    p.band = band_s;
     p.nrec = nrec;
     p.rx = nrec ? ctx->rec.ptr : nullptr;
     p.ry = nrec ? ctx->rec.ptr + nrec : nullptr;

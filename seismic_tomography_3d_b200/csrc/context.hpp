@@ -56,7 +56,6 @@ struct tomo_ctx {
     // last eikonal solve
     tomo::DevBuf<float> T;
     tomo::DevBuf<unsigned> qflag, lists, ctrl;
-    tomo::DevBuf<unsigned> key, minkey, smin_bits;  // band-ordered scheduling
     tomo::DevBuf<float> fsm_T;                      // TOMO_OP_NGB sweep grids (with halo)
     tomo::DevBuf<tomo::FsmShot> fsm_shots;
     tomo::DevBuf<unsigned> fsm_bar;

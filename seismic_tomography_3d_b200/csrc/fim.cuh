@@ -39,12 +39,6 @@ struct FimLaunch {
     float inner_tol;      // in-brick iterations stop when no node drops by more than this
     unsigned local_bits;  // item = shot << local_bits | local brick
     unsigned long long spin_limit;
-    // band-ordered scheduling (band > 0): a queued brick carries the smallest traveltime
-    // of the bricks that queued it (float bits; +INF bits = nothing pending) and is only
-    // relaxed once that key is within `band` seconds of its shot's smallest pending key.
-    unsigned *key;        // per (shot, brick)
-    unsigned *minkey;     // 3 x nshots, per-round minimum pending key of each shot
-    float band;
     // receivers
     int nrec;
     const float *rx, *ry, *rz;
@@ -57,11 +51,9 @@ struct FimLaunch {
 cudaError_t fim_brick_model(const float *slow, float *S, int nx, int ny, int nz, int nxx, int nyy,
                             int nzz, cudaStream_t st);
 cudaError_t fim_init(float *T, size_t t_count, unsigned *qflag, size_t q_count, unsigned *ctrl,
-                     unsigned long long *stats, unsigned *key, unsigned *minkey, int nshots, cudaStream_t st);
+                     unsigned long long *stats, cudaStream_t st);
 cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
-                     unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, unsigned *key,
-                     unsigned *minkey, cudaStream_t st);
-cudaError_t slowness_min(const float *s, size_t n, unsigned *out_bits, cudaStream_t st);
+                     unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st);
 cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, bool ieee_sqrt, int *grid_out,
                       cudaStream_t st);
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out,

@@ -140,8 +140,8 @@ extern "C" int tomo_eik_solve_static(const float *slowness, int nx, int ny, int 
     CKS(cudaGetLastError());
     CKS(fim_brick_model(slowness, S, nx, ny, nz, pad4(nx), pad4(ny), pad4(nz), st));
     // everything the solve reads is re-initialised: traveltimes, queue flags, control words
-    CKS(fim_init(T, (size_t)nbricks * kBrickNodes, qflag, (size_t)nbricks, ctrl, stats, nullptr, nullptr, 1, st));
-    CKS(fim_seed(desc, 1, S, d.nbx, d.nbz, T, qflag, lists, local_bits, ctrl, nullptr, nullptr, st));
+    CKS(fim_init(T, (size_t)nbricks * kBrickNodes, qflag, (size_t)nbricks, ctrl, stats, st));
+    CKS(fim_seed(desc, 1, S, d.nbx, d.nbz, T, qflag, lists, local_bits, ctrl, st));
     FimLaunch p{};
     p.S = S;
     p.T = T;
