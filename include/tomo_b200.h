@@ -140,6 +140,38 @@ int tomo_eik_volume(tomo_ctx *ctx, int shot, float *t_out);
 /* Window extents of shot `shot` of the last solve (nodes). */
 int tomo_eik_window(tomo_ctx *ctx, int shot, tomo_window *out);
 
+/* All traveltime fields of the last solve, device to device: shot s's window volume
+ * (nz*wx*wy floats, z fastest) at offset sum_{r<s} nz*wx_r*wy_r of the DEVICE array dst. */
+int tomo_eik_volumes(tomo_ctx *ctx, float *dst);
+
+typedef struct {
+    long long violations;              /* nodes below the update of their final neighbours   */
+    int shots_fallback;                /* shots solved again from INF (plain FIM)            */
+    long long rounds_seeded;           /* outer rounds of the warm-started launch            */
+    long long activations_seeded;      /* brick activations of the warm-started launch       */
+    long long inner_iterations_seeded; /* in-brick iterations of the warm-started launch     */
+    float seeded_ms;                   /* device time of the warm-started launch             */
+    float verify_ms;                   /* device time of the check                           */
+    float fallback_ms;                 /* device time of the fallback solves (0 if none)     */
+} tomo_seed_stats;
+
+/* Warm-started batch solve: tomo_eik_solve (JW operator), but every window node starts at
+ * ceiling x (1 + inflate) instead of INF, so that only updates that beat the ceiling
+ * propagate.  No counterpart in the reference (its solvers always start from INF).
+ *   ceiling  DEVICE array, all shots' window volumes back to back as tomo_eik_volumes
+ *            writes them: predicted traveltimes (s).  Entries <= 0 or non-finite: no
+ *            ceiling at that node.
+ *   inflate  in [0, 1): margin that makes the prediction an upper bound
+ * A ceiling below the true time would stay in the result, so every shot is checked after
+ * the solve: a node (source node excepted) whose time is below the local update of its
+ * final neighbours can only hold a ceiling value; such shots are solved again from INF
+ * within the call (the plain solver is the fallback).  stats counts both launches;
+ * seed_stats (may be NULL) splits them. */
+int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows,
+                          int nrec, const tomo_point *receivers, float *t_recv, const float *ceiling,
+                          float inflate, const tomo_eik_opts *opts, tomo_eik_stats *stats,
+                          tomo_seed_stats *seed_stats);
+
 /* Brick shapes the solver supports: writes up to `cap` triples (bx,by,bz) of nodes and
  * returns how many there are. */
 int tomo_eik_brick_shapes(int *xyz_triples, int cap);

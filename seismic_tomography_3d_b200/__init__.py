@@ -62,6 +62,16 @@ class EikStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class SeedStats(ctypes.Structure):
+    _fields_ = [("violations", ctypes.c_longlong), ("shots_fallback", ctypes.c_int),
+                ("rounds_seeded", ctypes.c_longlong), ("activations_seeded", ctypes.c_longlong),
+                ("inner_iterations_seeded", ctypes.c_longlong), ("seeded_ms", ctypes.c_float),
+                ("verify_ms", ctypes.c_float), ("fallback_ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -91,6 +101,9 @@ def load_library(path: str = LIB_PATH):
     lib.tomo_eik_volume.argtypes = [V, I, V]
     lib.tomo_eik_window.argtypes = [V, I, P(Window)]
     lib.tomo_eik_brick_shapes.argtypes = [P(I), I]
+    lib.tomo_eik_volumes.argtypes = [V, V]
+    lib.tomo_eik_solve_seeded.argtypes = [V, I, P(Point), P(Window), I, P(Point), V, V, F, P(EikOpts),
+                                          P(EikStats), P(SeedStats)]
     _bind_tomography(lib)
     _lib = lib
     return lib
@@ -253,6 +266,40 @@ class Context:
                                             out.ctypes.data if out is not None else None,
                                             ctypes.byref(opts), ctypes.byref(st)))
         return out, st.as_dict()
+
+    def eik_solve_seeded(self, shots, ceiling_ptr, inflate=0.02, windows=None, receivers=None, want_recv=True,
+                         max_inner=0, max_rounds=0, block_warps=0, occupancy=0, change_tol=0.0, inner_tol=0.0,
+                         ieee_sqrt=0):
+        """Warm-started batched solve (tomo_eik_solve_seeded).  ceiling_ptr: device address
+        of all shots' predicted window volumes back to back (see volume_sizes).  Returns
+        (t_recv or None, stats dict, seed-stats dict)."""
+        sp, ns, _s = _points(shots)
+        wp = _w = None
+        if windows is not None:
+            wp, _w = _windows(windows)
+        nr = 0
+        rp = _r = None
+        if receivers is not None and len(receivers):
+            rp, nr, _r = _points(receivers)
+        out = np.empty((ns, nr), np.float32) if (want_recv and nr) else None
+        opts = EikOpts(0, max_inner, max_rounds, 0, block_warps, occupancy, change_tol, inner_tol, ieee_sqrt, 0)
+        st, ss = EikStats(), SeedStats()
+        self._check(self.lib.tomo_eik_solve_seeded(self.h, ns, sp, wp, nr, rp,
+                                                   out.ctypes.data if out is not None else None,
+                                                   ctypes.c_void_p(ceiling_ptr), float(inflate), ctypes.byref(opts),
+                                                   ctypes.byref(st), ctypes.byref(ss)))
+        return out, st.as_dict(), ss.as_dict()
+
+    def volume_sizes(self, nshots, windows=None):
+        """Floats of each shot's window volume (nz*wx*wy) in the back-to-back layout."""
+        if windows is None:
+            return [self.grid.nz * self.grid.nx * self.grid.ny] * nshots
+        w = np.asarray(windows).reshape(-1, 4)
+        return [int(self.grid.nz * (x1 - x0) * (y1 - y0)) for x0, x1, y0, y1 in w]
+
+    def eik_volumes_to(self, dst_ptr):
+        """All window volumes of the last solve into the device array at dst_ptr."""
+        self._check(self.lib.tomo_eik_volumes(self.h, ctypes.c_void_p(dst_ptr)))
 
     def eik_window(self, shot):
         w = Window()

@@ -22,6 +22,10 @@ constexpr int kDefaultMaxInner = 16;
 constexpr float kDefaultChangeTol = 1e-6f;
 constexpr int kDefaultMaxRounds = 1 << 20;
 constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~ seconds of polling, then error
+// Warm-start check: a node more than this (relative, ~3 ulp) below the update of its final
+// neighbours flags its shot.  Along a path of n nodes the tolerated deficit adds up to at
+// most n x 2e-7 relative (6e-5 over 300 nodes), inside the 1e-4 traveltime budget.
+constexpr float kVerifyRelTol = 2e-7f;
 
 int fail(tomo_ctx *c, int code, const std::string &msg)
 {
@@ -208,7 +212,7 @@ int tomo_ctx_create_on_stream(const tomo_grid *grid, int device, void *stream, t
             ctx->own_stream = (e == cudaSuccess);
         }
     }
-    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
+    for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&ctx->pinned_ctrl), 64 * sizeof(unsigned));
     if (e == cudaSuccess) e = ctx->ctrl.ensure(tomo::kCtrlWords);
     if (e == cudaSuccess) e = ctx->stats.ensure(4);
@@ -242,6 +246,11 @@ int tomo_ctx_destroy(tomo_ctx *ctx)
     ctx->ctrl.release();
     ctx->stats.release();
     ctx->shots_d.release();
+    ctx->shots_redo.release();
+    ctx->viol.release();
+    ctx->fsm_T.release();
+    ctx->fsm_shots.release();
+    ctx->fsm_bar.release();
     ctx->rec.release();
     ctx->t_recv.release();
     for (auto &ev : ctx->ev)
@@ -292,31 +301,50 @@ int tomo_eik_brick_shapes(int *xyz, int cap)
     return 1;
 }
 
-int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows, int nrec,
-                   const tomo_point *receivers, float *t_recv, const tomo_eik_opts *opts,
-                   tomo_eik_stats *stats)
-{
-    if (!ctx) return TOMO_ERR_INVALID_ARG;
-    if (nshots < 1 || !shots) return fail(ctx, TOMO_ERR_INVALID_ARG, "nshots must be >= 1 with shot positions");
-    if (nrec < 0 || (nrec > 0 && !receivers)) return fail(ctx, TOMO_ERR_INVALID_ARG, "bad receivers");
-    if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
-    if (opts && opts->op != TOMO_OP_JW && opts->op != TOMO_OP_NGB)
-        return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown eikonal operator");
-    const tomo_grid &g = ctx->g;
-    const int max_inner = (opts && opts->max_inner > 0) ? opts->max_inner : kDefaultMaxInner;
-    const int max_rounds = (opts && opts->max_rounds > 0) ? opts->max_rounds : kDefaultMaxRounds;
-    const int block_warps = (opts && opts->block_warps > 0) ? opts->block_warps : 8;
-    const int occupancy = (opts && opts->occupancy > 0) ? opts->occupancy : 4;
-    // Default: the reference's convergence threshold EPS = 1e-6 s (cuda_kernel.cuh:8).
-    float change_tol = kDefaultChangeTol;
-    if (opts && opts->change_tol > 0.f) change_tol = opts->change_tol;
-    if (opts && opts->change_tol < 0.f) change_tol = 0.f;
-    CK(cudaSetDevice(ctx->device));
+}  // extern "C"
 
-    // ---- per-shot descriptors --------------------------------------------------------
-    std::vector<ShotDesc> sd((size_t)nshots);
-    long long t_total = 0;
-    unsigned long long q_total = 0;
+namespace {
+
+// Solver settings of one call (defaults where opts is NULL or a field is 0).
+struct SolveCfg {
+    int max_inner, max_rounds, block_warps, occupancy;
+    float change_tol, inner_tol;
+    bool ieee_sqrt;
+};
+
+SolveCfg solve_cfg(const tomo_eik_opts *opts)
+{
+    SolveCfg c{};
+    c.max_inner = (opts && opts->max_inner > 0) ? opts->max_inner : kDefaultMaxInner;
+    c.max_rounds = (opts && opts->max_rounds > 0) ? opts->max_rounds : kDefaultMaxRounds;
+    c.block_warps = (opts && opts->block_warps > 0) ? opts->block_warps : 8;
+    c.occupancy = (opts && opts->occupancy > 0) ? opts->occupancy : 4;
+    // Default: the reference's convergence threshold EPS = 1e-6 s (cuda_kernel.cuh:8).
+    c.change_tol = kDefaultChangeTol;
+    if (opts && opts->change_tol > 0.f) c.change_tol = opts->change_tol;
+    if (opts && opts->change_tol < 0.f) c.change_tol = 0.f;
+    // Default: exact in-brick convergence.  Stopping the in-brick relaxation at the face
+    // tolerance is 13 % faster on config 2 but raises the error vs the exact fixed point
+    // from ~1e-6 to ~2e-5 relative, too close to the 1e-4 budget on larger grids.
+    c.inner_tol = (opts && opts->inner_tol > 0.f) ? opts->inner_tol : 0.f;
+    c.ieee_sqrt = opts && opts->ieee_sqrt;
+    return c;
+}
+
+// Validated per-shot descriptors of a batch and the sizes of its device arrays.
+struct Batch {
+    std::vector<ShotDesc> sd;
+    long long t_total = 0;            // traveltime pool (floats)
+    long long v_total = 0;            // all window volumes back to back (floats)
+    unsigned long long q_total = 0;   // bricks
+    unsigned local_bits = 1;
+};
+
+int make_batch(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows, int nrec,
+               const tomo_point *receivers, Batch &bt)
+{
+    const tomo_grid &g = ctx->g;
+    bt.sd.assign((size_t)nshots, ShotDesc{});
     int max_bricks = 1;
     for (int s = 0; s < nshots; s++) {
         tomo_window w{0, g.nx, 0, g.ny};
@@ -327,7 +355,7 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
             return fail(ctx, TOMO_ERR_INVALID_ARG,
                         "window " + std::to_string(s) + ": origin must be a multiple of 4 and the end a "
                         "multiple of 4 or the model edge");
-        ShotDesc &d = sd[(size_t)s];
+        ShotDesc &d = bt.sd[(size_t)s];
         d.wx0 = w.x0;
         d.wy0 = w.y0;
         d.wnx = w.x1 - w.x0;
@@ -349,15 +377,17 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
         d.src_brick = (sidz >> 2) + d.nbz * ((sidx >> 2) + d.nbx * (sidy >> 2));
         d.src_node = (sidz & 3) + 4 * (sidx & 3) + 16 * (sidy & 3);
         const long long nb = (long long)d.nbx * d.nby * d.nbz;
-        d.t_off = t_total;
-        d.qbase = q_total;
-        t_total += nb * tomo::kBrickNodes;
-        q_total += (unsigned long long)nb;
+        d.t_off = bt.t_total;
+        d.qbase = bt.q_total;
+        d.v_off = bt.v_total;
+        bt.t_total += nb * tomo::kBrickNodes;
+        bt.q_total += (unsigned long long)nb;
+        bt.v_total += (long long)g.nz * d.wnx * d.wny;
         if (nb > max_bricks) max_bricks = (int)nb;
     }
-    unsigned local_bits = 1;
-    while ((1ll << local_bits) < max_bricks) local_bits++;
-    if (local_bits + 1 >= 32 || ((unsigned long long)nshots << local_bits) >= (1ull << 32))
+    bt.local_bits = 1;
+    while ((1ll << bt.local_bits) < max_bricks) bt.local_bits++;
+    if (bt.local_bits + 1 >= 32 || ((unsigned long long)nshots << bt.local_bits) >= (1ull << 32))
         return fail(ctx, TOMO_ERR_CAPACITY, "too many shots x bricks for one batch; split the batch");
     for (int r = 0; r < nrec; r++) {
         const tomo_point &p = receivers[r];
@@ -365,11 +395,16 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
             p.z > (g.nz - 1) * g.dz)
             return fail(ctx, TOMO_ERR_INVALID_ARG, "receiver " + std::to_string(r) + " outside the model");
     }
+    return TOMO_OK;
+}
 
-    // ---- buffers ----------------------------------------------------------------------
-    CK(ctx->T.ensure((size_t)t_total));
-    CK(ctx->qflag.ensure((size_t)q_total));
-    CK(ctx->lists.ensure((size_t)q_total * 3));
+// Device buffers of a batch; uploads the descriptors and receiver positions.
+int upload_batch(tomo_ctx *ctx, const Batch &bt, int nrec, const tomo_point *receivers)
+{
+    const int nshots = (int)bt.sd.size();
+    CK(ctx->T.ensure((size_t)bt.t_total));
+    CK(ctx->qflag.ensure((size_t)bt.q_total));
+    CK(ctx->lists.ensure((size_t)bt.q_total * 3));
     CK(ctx->shots_d.ensure((size_t)nshots));
     if (nrec > 0) {
         CK(ctx->rec.ensure((size_t)nrec * 3));
@@ -382,43 +417,32 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
         }
         CK(cudaMemcpyAsync(ctx->rec.ptr, rh.data(), rh.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     }
-    CK(cudaMemcpyAsync(ctx->shots_d.ptr, sd.data(), sd.size() * sizeof(ShotDesc), cudaMemcpyHostToDevice,
+    CK(cudaMemcpyAsync(ctx->shots_d.ptr, bt.sd.data(), bt.sd.size() * sizeof(ShotDesc), cudaMemcpyHostToDevice,
                        ctx->stream));
+    return TOMO_OK;
+}
 
-    // ---- launch -----------------------------------------------------------------------
-    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    const bool ngb = opts && opts->op == TOMO_OP_NGB;
-    if (ngb) {
-        const int rc = launch_ngb(ctx, sd, shots, nshots, nrec, opts ? opts->sweep_groups : 0);
-        if (rc != TOMO_OK) return rc;
-    } else {
-    CK(tomo::fim_init(ctx->T.ptr, (size_t)t_total, ctx->qflag.ptr, (size_t)q_total, ctx->ctrl.ptr, ctx->stats.ptr,
-                      ctx->stream));
-    CK(tomo::fim_seed(ctx->shots_d.ptr, nshots, ctx->S.ptr, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
-                      ctx->lists.ptr, local_bits, ctx->ctrl.ptr, ctx->stream));
+tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, int nrec)
+{
+    const tomo_grid &g = ctx->g;
     tomo::FimLaunch p{};
     p.S = ctx->S.ptr;
     p.T = ctx->T.ptr;
     p.shots = ctx->shots_d.ptr;
-    p.nshots = nshots;
+    p.nshots = (int)bt.sd.size();
     p.qflag = ctx->qflag.ptr;
     p.lists = ctx->lists.ptr;
-    p.list_cap = (unsigned)q_total;
+    p.list_cap = (unsigned)bt.q_total;
     p.ctrl = ctx->ctrl.ptr;
     p.stats = ctx->stats.ptr;
     p.gbx = ctx->gbx;
     p.gbz = ctx->gbz;
     p.h = g.dx;  // isotropic spacing h = dx (block_FIM.cpp:173)
-    p.max_inner = max_inner;
-    p.change_tol = change_tol;
-    // Default: exact in-brick convergence.  Stopping the in-brick relaxation at the face
-    // tolerance is 13 % faster on config 2 but raises the error vs the exact fixed point
-    // from ~1e-6 to ~2e-5 relative, too close to the 1e-4 budget on larger grids.
-    p.inner_tol = 0.f;
-    if (opts && opts->inner_tol > 0.f) p.inner_tol = opts->inner_tol;
-    if (opts && opts->inner_tol < 0.f) p.inner_tol = 0.f;
-    p.max_rounds = max_rounds;
-    p.local_bits = local_bits;
+    p.max_inner = c.max_inner;
+    p.change_tol = c.change_tol;
+    p.inner_tol = c.inner_tol;
+    p.max_rounds = c.max_rounds;
+    p.local_bits = bt.local_bits;
     p.spin_limit = kSpinLimit;
     p.nrec = nrec;
     p.rx = nrec ? ctx->rec.ptr : nullptr;
@@ -429,42 +453,213 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     p.dy = g.dy;
     p.dz = g.dz;
     p.nz = g.nz;
-    int grid = 0;
-    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
-    CK(tomo::fim_solve(p, block_warps, occupancy, opts && opts->ieee_sqrt, &grid, ctx->stream));
-    }
-    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    return p;
+}
+
+// Reads the control words and counters of the last persistent solve (synchronises).
+int read_solve(tomo_ctx *ctx, unsigned &rounds, unsigned long long &act, unsigned long long &inner,
+               const SolveCfg &c)
+{
     CK(cudaMemcpyAsync(ctx->pinned_ctrl, ctx->ctrl.ptr, tomo::kCtrlWords * sizeof(unsigned), cudaMemcpyDeviceToHost,
                        ctx->stream));
     CK(cudaMemcpyAsync(ctx->pinned_ctrl + tomo::kCtrlWords, ctx->stats.ptr, 2 * sizeof(unsigned long long),
                        cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned long long st[2];
+    std::memcpy(st, ctx->pinned_ctrl + tomo::kCtrlWords, sizeof(st));
+    rounds = ctx->pinned_ctrl[tomo::kRounds];
+    act = st[0];
+    inner = st[1];
+    const unsigned derr = ctx->pinned_ctrl[tomo::kErr];
+    if (derr == tomo::kDevRoundCap)
+        return fail(ctx, TOMO_ERR_NOT_CONVERGED,
+                    "eikonal solve hit the round cap (" + std::to_string(c.max_rounds) + ")");
+    if (derr != tomo::kDevOk) return fail(ctx, TOMO_ERR_TIMEOUT, "eikonal solve: device barrier wait timed out");
+    return TOMO_OK;
+}
+
+void keep_batch(tomo_ctx *ctx, const Batch &bt, const tomo_point *shots, int nrec, const tomo_point *receivers)
+{
+    ctx->shots_h = bt.sd;
+    ctx->shot_pos.assign(shots, shots + bt.sd.size());
+    ctx->rec_h.assign(receivers, receivers + nrec);
+    ctx->nshots = (int)bt.sd.size();
+    ctx->nrec = nrec;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows, int nrec,
+                   const tomo_point *receivers, float *t_recv, const tomo_eik_opts *opts,
+                   tomo_eik_stats *stats)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (nshots < 1 || !shots) return fail(ctx, TOMO_ERR_INVALID_ARG, "nshots must be >= 1 with shot positions");
+    if (nrec < 0 || (nrec > 0 && !receivers)) return fail(ctx, TOMO_ERR_INVALID_ARG, "bad receivers");
+    if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
+    if (opts && opts->op != TOMO_OP_JW && opts->op != TOMO_OP_NGB)
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown eikonal operator");
+    const SolveCfg cfg = solve_cfg(opts);
+    CK(cudaSetDevice(ctx->device));
+    Batch bt;
+    int rc = make_batch(ctx, nshots, shots, windows, nrec, receivers, bt);
+    if (rc != TOMO_OK) return rc;
+    rc = upload_batch(ctx, bt, nrec, receivers);
+    if (rc != TOMO_OK) return rc;
+
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    if (opts && opts->op == TOMO_OP_NGB) {
+        rc = launch_ngb(ctx, bt.sd, shots, nshots, nrec, opts->sweep_groups);
+        if (rc != TOMO_OK) return rc;
+    } else {
+        CK(tomo::fim_init(ctx->T.ptr, (size_t)bt.t_total, ctx->qflag.ptr, (size_t)bt.q_total, ctx->ctrl.ptr,
+                          ctx->stats.ptr, ctx->stream));
+        CK(tomo::fim_seed(ctx->shots_d.ptr, nshots, ctx->S.ptr, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
+                          ctx->lists.ptr, bt.local_bits, ctx->ctrl.ptr, ctx->stream));
+        const tomo::FimLaunch p = fim_params(ctx, bt, cfg, nrec);
+        int grid = 0;
+        CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+        CK(tomo::fim_solve(p, cfg.block_warps, cfg.occupancy, cfg.ieee_sqrt, &grid, ctx->stream));
+    }
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     if (t_recv && nrec > 0)
         CK(cudaMemcpyAsync(t_recv, ctx->t_recv.ptr, (size_t)nshots * nrec * sizeof(float), cudaMemcpyDeviceToHost,
                            ctx->stream));
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-
-    ctx->shots_h = sd;
-    ctx->shot_pos.assign(shots, shots + nshots);
-    ctx->rec_h.assign(receivers, receivers + nrec);
-    ctx->nshots = nshots;
-    ctx->nrec = nrec;
-    const unsigned derr = ctx->pinned_ctrl[tomo::kErr];
-    ctx->have_solve = (derr == tomo::kDevOk);
+    unsigned rounds = 0;
+    unsigned long long act = 0, inner = 0;
+    rc = read_solve(ctx, rounds, act, inner, cfg);
+    keep_batch(ctx, bt, shots, nrec, receivers);
+    ctx->have_solve = (rc == TOMO_OK);
     if (stats) {
-        unsigned long long st[2];
-        std::memcpy(st, ctx->pinned_ctrl + tomo::kCtrlWords, sizeof(st));
-        stats->rounds = ctx->pinned_ctrl[tomo::kRounds];
-        stats->activations = (long long)st[0];
-        stats->inner_iterations = (long long)st[1];
+        stats->rounds = rounds;
+        stats->activations = (long long)act;
+        stats->inner_iterations = (long long)inner;
         stats->nodes_per_brick = tomo::kBrickNodes;
         cudaEventElapsedTime(&stats->setup_ms, ctx->ev[0], ctx->ev[3]);
         cudaEventElapsedTime(&stats->solve_ms, ctx->ev[3], ctx->ev[1]);
         cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[2]);
     }
-    if (derr == tomo::kDevRoundCap)
-        return fail(ctx, TOMO_ERR_NOT_CONVERGED, "eikonal solve hit the round cap (" + std::to_string(max_rounds) + ")");
-    if (derr != tomo::kDevOk) return fail(ctx, TOMO_ERR_TIMEOUT, "eikonal solve: device barrier wait timed out");
+    return rc;
+}
+
+int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows, int nrec,
+                          const tomo_point *receivers, float *t_recv, const float *ceiling, float inflate,
+                          const tomo_eik_opts *opts, tomo_eik_stats *stats, tomo_seed_stats *seed_stats)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (nshots < 1 || !shots) return fail(ctx, TOMO_ERR_INVALID_ARG, "nshots must be >= 1 with shot positions");
+    if (nshots > 65535) return fail(ctx, TOMO_ERR_CAPACITY, "a warm-started batch holds at most 65535 shots");
+    if (nrec < 0 || (nrec > 0 && !receivers)) return fail(ctx, TOMO_ERR_INVALID_ARG, "bad receivers");
+    if (!ceiling) return fail(ctx, TOMO_ERR_INVALID_ARG, "ceiling must be a device array");
+    if (!(inflate >= 0.f) || !(inflate < 1.f)) return fail(ctx, TOMO_ERR_INVALID_ARG, "inflate must be in [0, 1)");
+    if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
+    if (opts && opts->op != TOMO_OP_JW)
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "the warm-started solve runs the JW operator only");
+    const SolveCfg cfg = solve_cfg(opts);
+    CK(cudaSetDevice(ctx->device));
+    Batch bt;
+    int rc = make_batch(ctx, nshots, shots, windows, nrec, receivers, bt);
+    if (rc != TOMO_OK) return rc;
+    rc = upload_batch(ctx, bt, nrec, receivers);
+    if (rc != TOMO_OK) return rc;
+    CK(ctx->viol.ensure((size_t)nshots));
+    cudaEvent_t *ev = ctx->ev;
+
+    // 1. pool from the ceiling, source seed, persistent solve (receivers after the check)
+    CK(cudaEventRecord(ev[0], ctx->stream));
+    CK(tomo::fim_init(ctx->T.ptr, (size_t)bt.t_total, ctx->qflag.ptr, (size_t)bt.q_total, ctx->ctrl.ptr,
+                      ctx->stats.ptr, ctx->stream));
+    CK(tomo::fim_ceiling(ctx->T.ptr, ctx->shots_d.ptr, nshots, ctx->g.nz, ceiling, 1.0f + inflate, ctx->stream));
+    CK(tomo::fim_seed(ctx->shots_d.ptr, nshots, ctx->S.ptr, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
+                      ctx->lists.ptr, bt.local_bits, ctx->ctrl.ptr, ctx->stream));
+    CK(cudaEventRecord(ev[3], ctx->stream));
+    tomo::FimLaunch p = fim_params(ctx, bt, cfg, 0);
+    int grid = 0;
+    CK(tomo::fim_solve(p, cfg.block_warps, cfg.occupancy, cfg.ieee_sqrt, &grid, ctx->stream));
+    CK(cudaEventRecord(ev[4], ctx->stream));
+    // 2. check: a node below what its neighbours give came from a ceiling below the truth
+    CK(cudaMemsetAsync(ctx->viol.ptr, 0, (size_t)nshots * sizeof(unsigned long long), ctx->stream));
+    CK(tomo::fim_verify(ctx->T.ptr, ctx->S.ptr, ctx->shots_d.ptr, nshots, ctx->gbx, ctx->gbz, ctx->g.dx,
+                        kVerifyRelTol, cfg.ieee_sqrt, ctx->viol.ptr, ctx->stream));
+    CK(cudaEventRecord(ev[5], ctx->stream));
+    std::vector<unsigned long long> viol((size_t)nshots);
+    CK(cudaMemcpyAsync(viol.data(), ctx->viol.ptr, viol.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    unsigned rounds = 0, rounds2 = 0;
+    unsigned long long act = 0, inner = 0, act2 = 0, inner2 = 0;
+    rc = read_solve(ctx, rounds, act, inner, cfg);
+    if (rc != TOMO_OK) return rc;
+
+    // 3. fallback: shots with violations are solved again from INF (plain FIM)
+    std::vector<ShotDesc> redo;
+    long long nviol = 0;
+    for (int s = 0; s < nshots; s++) {
+        nviol += (long long)viol[(size_t)s];
+        if (viol[(size_t)s]) redo.push_back(bt.sd[(size_t)s]);
+    }
+    const int nredo = (int)redo.size();
+    CK(cudaEventRecord(ev[6], ctx->stream));
+    if (nredo > 0) {
+        CK(ctx->shots_redo.ensure((size_t)nredo));
+        CK(cudaMemcpyAsync(ctx->shots_redo.ptr, redo.data(), redo.size() * sizeof(ShotDesc), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(tomo::fim_reset_shots(ctx->T.ptr, ctx->qflag.ptr, ctx->shots_redo.ptr, nredo, ctx->stream));
+        CK(tomo::fim_init(nullptr, 0, nullptr, 0, ctx->ctrl.ptr, ctx->stats.ptr, ctx->stream));
+        CK(tomo::fim_seed(ctx->shots_redo.ptr, nredo, ctx->S.ptr, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
+                          ctx->lists.ptr, bt.local_bits, ctx->ctrl.ptr, ctx->stream));
+        tomo::FimLaunch p2 = p;
+        p2.shots = ctx->shots_redo.ptr;
+        p2.nshots = nredo;
+        CK(tomo::fim_solve(p2, cfg.block_warps, cfg.occupancy, cfg.ieee_sqrt, &grid, ctx->stream));
+        rc = read_solve(ctx, rounds2, act2, inner2, cfg);
+        if (rc != TOMO_OK) return rc;
+    }
+    CK(cudaEventRecord(ev[7], ctx->stream));
+    if (nrec > 0)
+        CK(tomo::receivers_sample(ctx->T.ptr, ctx->shots_d.ptr, nshots, ctx->rec.ptr, ctx->rec.ptr + nrec,
+                                  ctx->rec.ptr + 2 * nrec, nrec, ctx->g.dx, ctx->g.dy, ctx->g.dz, ctx->g.nz,
+                                  ctx->t_recv.ptr, ctx->stream));
+    CK(cudaEventRecord(ev[1], ctx->stream));
+    if (t_recv && nrec > 0)
+        CK(cudaMemcpyAsync(t_recv, ctx->t_recv.ptr, (size_t)nshots * nrec * sizeof(float), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    CK(cudaEventRecord(ev[2], ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    keep_batch(ctx, bt, shots, nrec, receivers);
+    ctx->have_solve = true;
+    if (stats) {
+        stats->rounds = (long long)rounds + rounds2;
+        stats->activations = (long long)(act + act2);
+        stats->inner_iterations = (long long)(inner + inner2);
+        stats->nodes_per_brick = tomo::kBrickNodes;
+        cudaEventElapsedTime(&stats->setup_ms, ev[0], ev[3]);
+        cudaEventElapsedTime(&stats->solve_ms, ev[3], ev[1]);
+        cudaEventElapsedTime(&stats->total_ms, ev[0], ev[2]);
+    }
+    if (seed_stats) {
+        seed_stats->violations = nviol;
+        seed_stats->shots_fallback = nredo;
+        seed_stats->rounds_seeded = rounds;
+        seed_stats->activations_seeded = (long long)act;
+        seed_stats->inner_iterations_seeded = (long long)inner;
+        cudaEventElapsedTime(&seed_stats->seeded_ms, ev[3], ev[4]);
+        cudaEventElapsedTime(&seed_stats->verify_ms, ev[4], ev[5]);
+        cudaEventElapsedTime(&seed_stats->fallback_ms, ev[6], ev[7]);
+    }
+    return TOMO_OK;
+}
+
+int tomo_eik_volumes(tomo_ctx *ctx, float *dst)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (!dst) return fail(ctx, TOMO_ERR_INVALID_ARG, "output is NULL");
+    if (!ctx->have_solve) return fail(ctx, TOMO_ERR_STATE, "no eikonal solve");
+    CK(cudaSetDevice(ctx->device));
+    CK(tomo::fim_unbrick_all(ctx->T.ptr, ctx->shots_d.ptr, ctx->nshots, ctx->g.nz, dst, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return TOMO_OK;
 }
 

@@ -61,6 +61,8 @@ struct tomo_ctx {
     tomo::DevBuf<unsigned> fsm_bar;
     tomo::DevBuf<unsigned long long> stats;
     tomo::DevBuf<tomo::ShotDesc> shots_d;
+    tomo::DevBuf<tomo::ShotDesc> shots_redo;        // warm start: shots solved again from INF
+    tomo::DevBuf<unsigned long long> viol;          // warm start: per-shot check counts
     std::vector<tomo::ShotDesc> shots_h;
     std::vector<tomo_point> shot_pos;
     tomo::DevBuf<float> rec;       // 3*nrec: x | y | z
@@ -69,7 +71,7 @@ struct tomo_ctx {
     int nshots = 0, nrec = 0;
     bool have_solve = false;
 
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev[8] = {};
     unsigned *pinned_ctrl = nullptr;  // kCtrlWords + stats
 
     // ---- tomography (api_tomography.cpp) -----------------------------------------------

@@ -132,8 +132,7 @@ struct WarpStats {
     unsigned long long act, inner;
 };
 
-// Data of one work item, loaded one item ahead of its relaxation (software prefetch: the
-// loads of the next brick are in flight while the warp relaxes the current one).
+// Data of one work item as loaded from global memory.
 struct BrickLoad {
     unsigned s, b;
     float s0, s1;      // slowness of the lane's two nodes
@@ -331,8 +330,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
             p.ctrl[kCur0 + (round + 2u) % 3u] = 0u;
         }
         // Items are fetched one at a time from the round's cursor (warps that draw cheap
-        // bricks take more of them), and each warp loads its next brick before relaxing
-        // the current one.  A prefetched halo may predate a neighbour's update in this
+        // bricks take more of them).  A halo read may predate a neighbour's update in this
         // round; that neighbour then re-queues the brick, as for any concurrent update.
         const unsigned *list = p.lists + (size_t)cur * p.list_cap;
         unsigned *cursor = p.ctrl + kCur0 + cur;
@@ -442,6 +440,100 @@ __global__ void k_unbrick(const float *T, const ShotDesc *shots, int shot, int n
 }
 
 // -------------------------------------------------------------------------------------
+// Warm start: ceiling, verification, per-shot reset, export
+// -------------------------------------------------------------------------------------
+// Grid: x strides over one shot's pool nodes, y = shot.
+__device__ __forceinline__ void pool_node(const ShotDesc &d, long long i, int &z, int &x, int &y)
+{
+    const long long b = i / kBrickNodes;
+    const int node = (int)(i % kBrickNodes);
+    const int bz = (int)(b % d.nbz);
+    const long long t = b / d.nbz;
+    const int bx = (int)(t % d.nbx), by = (int)(t / d.nbx);
+    z = bz * kBrick + (node & 3);
+    x = bx * kBrick + ((node >> 2) & 3);
+    y = by * kBrick + (node >> 4);
+}
+
+__global__ void k_fim_ceiling(float *T, const ShotDesc *shots, int nz, const float *ceiling, float scale)
+{
+    const ShotDesc d = shots[blockIdx.y];
+    const long long n = (long long)d.nbx * d.nby * d.nbz * kBrickNodes;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int z, x, y;
+        pool_node(d, i, z, x, y);
+        if (z >= nz || x >= d.wnx || y >= d.wny) continue;
+        const float c = __ldg(ceiling + d.v_off + z + (long long)nz * (x + (long long)d.wnx * y));
+        if (c > 0.0f && c < kInf) {
+            const float u = c * scale;
+            if (u < kInf) __stcg(T + d.t_off + i, u);
+        }
+    }
+}
+
+template <bool kFastSqrt>
+__global__ void k_fim_verify(const float *T, const float *S, const ShotDesc *shots, int gbx, int gbz, float h,
+                             float rel_tol, unsigned long long *viol)
+{
+    const int s = blockIdx.y;
+    const ShotDesc d = shots[s];
+    const int ex = d.nbx * kBrick, ey = d.nby * kBrick, ez = d.nbz * kBrick;
+    const long long n = (long long)d.nbx * d.nby * d.nbz * kBrickNodes;
+    const long long src = (long long)d.src_brick * kBrickNodes + d.src_node;
+    unsigned cnt = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (i == src) continue;
+        int z, x, y;
+        pool_node(d, i, z, x, y);
+        const float t = __ldcg(T + d.t_off + i);
+        // neighbours as the solver sees them: nodes of the window's brick grid, INF beyond
+        const float xm = x > 0 ? brick_T(T, d, x - 1, y, z) : kInf, xp = x < ex - 1 ? brick_T(T, d, x + 1, y, z) : kInf;
+        const float ym = y > 0 ? brick_T(T, d, x, y - 1, z) : kInf, yp = y < ey - 1 ? brick_T(T, d, x, y + 1, z) : kInf;
+        const float zm = z > 0 ? brick_T(T, d, x, y, z - 1) : kInf, zp = z < ez - 1 ? brick_T(T, d, x, y, z + 1) : kInf;
+        const long long gb = (z >> 2) + (long long)gbz * (((x + d.wx0) >> 2) + (long long)gbx * ((y + d.wy0) >> 2));
+        const float sl = __ldg(S + gb * kBrickNodes + (i % kBrickNodes));
+        const float g = godunov_jw<kFastSqrt>(fminf(xm, xp), fminf(ym, yp), fminf(zm, zp), h, sl);
+        if (g < kInf && t < g - rel_tol * g) cnt++;
+    }
+    // block reduction, one atomic per block
+    cnt = __reduce_add_sync(kFull, cnt);
+    __shared__ unsigned part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += part[w];
+        if (tot) atomicAdd(viol + s, (unsigned long long)tot);
+    }
+}
+
+__global__ void k_fim_reset_shots(float *T, unsigned *qflag, const ShotDesc *shots)
+{
+    const ShotDesc d = shots[blockIdx.y];
+    const long long nb = (long long)d.nbx * d.nby * d.nbz;
+    const float4 inf4 = make_float4(kInf, kInf, kInf, kInf);
+    float4 *T4 = reinterpret_cast<float4 *>(T + d.t_off);  // t_off is a multiple of 64 floats
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nb * (kBrickNodes / 4);
+         i += (long long)gridDim.x * blockDim.x)
+        __stcg(T4 + i, inf4);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nb; i += (long long)gridDim.x * blockDim.x)
+        qflag[d.qbase + i] = 0u;
+}
+
+__global__ void k_unbrick_all(const float *T, const ShotDesc *shots, int nz, float *out)
+{
+    const ShotDesc d = shots[blockIdx.y];
+    const long long total = (long long)nz * d.wnx * d.wny;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int z = (int)(i % nz);
+        const long long r = i / nz;
+        const int x = (int)(r % d.wnx), y = (int)(r / d.wnx);
+        out[d.v_off + i] = brick_T(T, d, x, y, z);
+    }
+}
+
+// -------------------------------------------------------------------------------------
 // Launchers
 // -------------------------------------------------------------------------------------
 static int grid_for(size_t n, int threads)
@@ -522,6 +614,41 @@ cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, bool i
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out, cudaStream_t st)
 {
     k_unbrick<<<148 * 8, 256, 0, st>>>(T, shots, shot, nz, out);
+    return cudaGetLastError();
+}
+
+static dim3 per_shot_grid(int nshots) { return dim3(nshots >= 64 ? 32 : 128, (unsigned)nshots); }
+
+cudaError_t fim_ceiling(float *T, const ShotDesc *shots, int nshots, int nz, const float *ceiling, float scale,
+                        cudaStream_t st)
+{
+    if (nshots < 1 || nshots > 65535) return cudaErrorInvalidValue;
+    k_fim_ceiling<<<per_shot_grid(nshots), 256, 0, st>>>(T, shots, nz, ceiling, scale);
+    return cudaGetLastError();
+}
+
+cudaError_t fim_verify(const float *T, const float *S, const ShotDesc *shots, int nshots, int gbx, int gbz, float h,
+                       float rel_tol, bool ieee_sqrt, unsigned long long *viol, cudaStream_t st)
+{
+    if (nshots < 1 || nshots > 65535) return cudaErrorInvalidValue;
+    if (ieee_sqrt)
+        k_fim_verify<false><<<per_shot_grid(nshots), 256, 0, st>>>(T, S, shots, gbx, gbz, h, rel_tol, viol);
+    else
+        k_fim_verify<true><<<per_shot_grid(nshots), 256, 0, st>>>(T, S, shots, gbx, gbz, h, rel_tol, viol);
+    return cudaGetLastError();
+}
+
+cudaError_t fim_reset_shots(float *T, unsigned *qflag, const ShotDesc *shots, int nshots, cudaStream_t st)
+{
+    if (nshots < 1 || nshots > 65535) return cudaErrorInvalidValue;
+    k_fim_reset_shots<<<per_shot_grid(nshots), 256, 0, st>>>(T, qflag, shots);
+    return cudaGetLastError();
+}
+
+cudaError_t fim_unbrick_all(const float *T, const ShotDesc *shots, int nshots, int nz, float *out, cudaStream_t st)
+{
+    if (nshots < 1 || nshots > 65535) return cudaErrorInvalidValue;
+    k_unbrick_all<<<per_shot_grid(nshots), 256, 0, st>>>(T, shots, nz, out);
     return cudaGetLastError();
 }
 

@@ -20,6 +20,8 @@ struct ShotDesc {
     float src_dist;      // distance source -> seed node (m); seed = S(seed) * src_dist
     long long t_off;     // offset of the shot's field in the traveltime pool (floats)
     unsigned long long qbase;  // offset of the shot's bricks in the queue-flag array
+    long long v_off;     // offset of the shot's window volume (nz*wnx*wny, z fastest) in
+                         // arrays that hold all shots' volumes back to back
 };
 
 struct FimLaunch {
@@ -59,5 +61,24 @@ cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, bool i
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out,
                         cudaStream_t st);
 cudaError_t velocity_to_slowness(const float *v, float *s, size_t n, cudaStream_t st);
+
+// Warm start (fim.cu): every window node of every shot starts at ceiling * scale
+// (volumes at ShotDesc::v_off) instead of INF; non-finite or non-positive entries and
+// padding nodes stay INF.
+cudaError_t fim_ceiling(float *T, const ShotDesc *shots, int nshots, int nz, const float *ceiling, float scale,
+                        cudaStream_t st);
+// Per shot, the number of nodes (source node excepted) whose traveltime is below the
+// local update of its final neighbours by more than rel_tol (relative): values that no
+// neighbour explains, i.e. a ceiling below the true time.  viol[nshots] is accumulated.
+cudaError_t fim_verify(const float *T, const float *S, const ShotDesc *shots, int nshots, int gbx, int gbz, float h,
+                       float rel_tol, bool ieee_sqrt, unsigned long long *viol, cudaStream_t st);
+// Resets the pool regions (T = INF, queue flags 0) of the listed shots only.
+cudaError_t fim_reset_shots(float *T, unsigned *qflag, const ShotDesc *shots, int nshots, cudaStream_t st);
+// All shots' window volumes, back to back at ShotDesc::v_off (z fastest, then x, then y).
+cudaError_t fim_unbrick_all(const float *T, const ShotDesc *shots, int nshots, int nz, float *out,
+                            cudaStream_t st);
+cudaError_t receivers_sample(const float *T, const ShotDesc *shots, int nshots, const float *rx, const float *ry,
+                             const float *rz, int nrec, float dx, float dy, float dz, int nz, float *t_recv,
+                             cudaStream_t st);
 
 }  // namespace tomo

@@ -33,8 +33,5 @@ struct FsmLaunch {
 };
 
 cudaError_t fsm_solve(const FsmLaunch &p, int *grid_out, cudaStream_t st);
-cudaError_t receivers_sample(const float *T, const ShotDesc *shots, int nshots, const float *rx, const float *ry,
-                             const float *rz, int nrec, float dx, float dy, float dz, int nz, float *t_recv,
-                             cudaStream_t st);
 
 }  // namespace tomo

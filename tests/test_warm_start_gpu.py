@@ -1,0 +1,102 @@
+"""Warm-started solve (tomo_eik_solve_seeded) through the C ABI.
+
+The ceiling only prunes work: with any ceiling the result must equal the plain solve.
+  * a true upper bound (the plain solution inflated) gives the plain result, no fallback;
+  * a ceiling below the true times is detected by the check and the shot is solved again
+    from INF, again giving the plain result;
+  * entries <= 0 / non-finite mean "no ceiling".
+Tolerance: 1e-5 relative on nodes with T >= 2h/v_max against the plain FIM (both runs
+converge to the same FP32 fixed point; the 1e-4 budget is kept with margin).
+"""
+import numpy as np
+import pytest
+
+from seismic_tomography_3d_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def rel_err(T, Tref, h, vmax):
+    m = Tref >= 2.0 * h / vmax
+    return float(np.max(np.abs(T[m] - Tref[m]) / Tref[m])) if m.any() else 0.0
+
+
+@pytest.fixture(scope="module")
+def case(tomo):
+    import torch
+
+    sv = wl.small(77, 40, 36, 20, nshots=3, windows=True)
+    ctx = tomo.Context(sv.nx, sv.ny, sv.nz, sv.h)
+    ctx.set_velocity(sv.velocity)
+    t_plain, st = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers)
+    plain = [ctx.eik_volume(i) for i in range(len(sv.shots))]
+    sizes = ctx.volume_sizes(len(sv.shots), sv.windows)
+    dev = torch.empty(sum(sizes), dtype=torch.float32, device="cuda")
+    ctx.eik_volumes_to(dev.data_ptr())
+    torch.cuda.synchronize()
+    yield sv, ctx, plain, t_plain, st, dev, sizes
+    ctx.close()
+
+
+def check_equal(ctx, sv, plain):
+    for i in range(len(sv.shots)):
+        assert rel_err(ctx.eik_volume(i), plain[i], sv.h, float(sv.velocity.max())) < TOL
+
+
+def test_volumes_export_matches_per_shot_copy(case):
+    sv, ctx, plain, _, _, dev, sizes = case
+    flat = dev.cpu().numpy()
+    off = 0
+    for i, n in enumerate(sizes):
+        np.testing.assert_array_equal(flat[off:off + n].reshape(plain[i].shape), plain[i])
+        off += n
+
+
+@pytest.mark.parametrize("inflate", [0.001, 0.02, 0.1])
+def test_true_upper_bound_gives_plain_result(case, inflate):
+    sv, ctx, plain, t_plain, st_plain, dev, _ = case
+    t, st, ss = ctx.eik_solve_seeded(sv.shots, dev.data_ptr(), inflate, windows=sv.windows, receivers=sv.receivers)
+    assert ss["shots_fallback"] == 0 and ss["violations"] == 0
+    check_equal(ctx, sv, plain)
+    fin = np.isfinite(t_plain) & (t_plain < 1e5)
+    np.testing.assert_allclose(t[fin], t_plain[fin], rtol=TOL, atol=1e-7)
+    assert st["activations"] == ss["activations_seeded"]
+
+
+def test_ceiling_below_truth_falls_back(case):
+    import torch
+
+    sv, ctx, plain, t_plain, _, dev, sizes = case
+    low = dev.clone()
+    # shot 1's ceiling 5 % below the truth: must be detected and solved again from INF
+    off = sizes[0]
+    low[off:off + sizes[1]] *= 0.95
+    torch.cuda.synchronize()
+    t, st, ss = ctx.eik_solve_seeded(sv.shots, low.data_ptr(), 0.0, windows=sv.windows, receivers=sv.receivers)
+    assert ss["violations"] > 0
+    assert ss["shots_fallback"] == 1
+    check_equal(ctx, sv, plain)
+    fin = np.isfinite(t_plain) & (t_plain < 1e5)
+    np.testing.assert_allclose(t[fin], t_plain[fin], rtol=TOL, atol=1e-7)
+
+
+def test_no_ceiling_entries_equal_plain(case):
+    import torch
+
+    sv, ctx, plain, _, st_plain, dev, _ = case
+    none = torch.full_like(dev, float("inf"))
+    none[::2] = 0.0
+    torch.cuda.synchronize()
+    _, st, ss = ctx.eik_solve_seeded(sv.shots, none.data_ptr(), 0.02, windows=sv.windows)
+    assert ss["shots_fallback"] == 0
+    check_equal(ctx, sv, plain)
+
+
+def test_bad_arguments(case, tomo):
+    sv, ctx, _, _, _, dev, _ = case
+    with pytest.raises(tomo.TomoError):
+        ctx.eik_solve_seeded(sv.shots, 0, 0.02, windows=sv.windows)
+    with pytest.raises(tomo.TomoError):
+        ctx.eik_solve_seeded(sv.shots, dev.data_ptr(), -0.5, windows=sv.windows)
