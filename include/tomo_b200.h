@@ -146,6 +146,7 @@ int tomo_eik_volumes(tomo_ctx *ctx, float *dst);
 
 typedef struct {
     long long violations;              /* nodes below the update of their final neighbours   */
+    float max_deficit;                 /* largest (update - time) / update over those nodes   */
     int shots_fallback;                /* shots solved again from INF (plain FIM)            */
     long long rounds_seeded;           /* outer rounds of the warm-started launch            */
     long long activations_seeded;      /* brick activations of the warm-started launch       */

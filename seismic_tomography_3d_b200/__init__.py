@@ -63,7 +63,7 @@ class EikStats(ctypes.Structure):
 
 
 class SeedStats(ctypes.Structure):
-    _fields_ = [("violations", ctypes.c_longlong), ("shots_fallback", ctypes.c_int),
+    _fields_ = [("violations", ctypes.c_longlong), ("max_deficit", ctypes.c_float), ("shots_fallback", ctypes.c_int),
                 ("rounds_seeded", ctypes.c_longlong), ("activations_seeded", ctypes.c_longlong),
                 ("inner_iterations_seeded", ctypes.c_longlong), ("seeded_ms", ctypes.c_float),
                 ("verify_ms", ctypes.c_float), ("fallback_ms", ctypes.c_float)]

@@ -481,6 +481,7 @@ __global__ void k_fim_verify(const float *T, const float *S, const ShotDesc *sho
     const long long n = (long long)d.nbx * d.nby * d.nbz * kBrickNodes;
     const long long src = (long long)d.src_brick * kBrickNodes + d.src_node;
     unsigned cnt = 0;
+    float worst = 0.0f;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         if (i == src) continue;
         int z, x, y;
@@ -493,8 +494,18 @@ __global__ void k_fim_verify(const float *T, const float *S, const ShotDesc *sho
         const long long gb = (z >> 2) + (long long)gbz * (((x + d.wx0) >> 2) + (long long)gbx * ((y + d.wy0) >> 2));
         const float sl = __ldg(S + gb * kBrickNodes + (i % kBrickNodes));
         const float g = godunov_jw<kFastSqrt>(fminf(xm, xp), fminf(ym, yp), fminf(zm, zp), h, sl);
-        if (g < kInf && t < g - rel_tol * g) cnt++;
+        if (g < kInf && t < g - rel_tol * g) {
+            cnt++;
+            worst = fmaxf(worst, (g - t) / g);
+        }
     }
+    worst = fmaxf(worst, __shfl_xor_sync(kFull, worst, 16));
+    worst = fmaxf(worst, __shfl_xor_sync(kFull, worst, 8));
+    worst = fmaxf(worst, __shfl_xor_sync(kFull, worst, 4));
+    worst = fmaxf(worst, __shfl_xor_sync(kFull, worst, 2));
+    worst = fmaxf(worst, __shfl_xor_sync(kFull, worst, 1));
+    if ((threadIdx.x & 31) == 0 && worst > 0.0f)  // non-negative floats order as their bits
+        atomicMax(viol + gridDim.y + s, (unsigned long long)__float_as_uint(worst));
     // block reduction, one atomic per block
     cnt = __reduce_add_sync(kFull, cnt);
     __shared__ unsigned part[32];

@@ -69,7 +69,8 @@ cudaError_t fim_ceiling(float *T, const ShotDesc *shots, int nshots, int nz, con
                         cudaStream_t st);
 // Per shot, the number of nodes (source node excepted) whose traveltime is below the
 // local update of its final neighbours by more than rel_tol (relative): values that no
-// neighbour explains, i.e. a ceiling below the true time.  viol[nshots] is accumulated.
+// neighbour explains, i.e. a ceiling below the true time.  viol[s] accumulates the count
+// of shot s, viol[nshots + s] the largest relative deficit (float bits, atomicMax).
 cudaError_t fim_verify(const float *T, const float *S, const ShotDesc *shots, int nshots, int gbx, int gbz, float h,
                        float rel_tol, bool ieee_sqrt, unsigned long long *viol, cudaStream_t st);
 // Resets the pool regions (T = INF, queue flags 0) of the listed shots only.

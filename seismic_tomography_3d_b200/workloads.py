@@ -167,6 +167,16 @@ def config5(seed=5) -> Survey:
     return Survey("config5", nx, ny, nz, h, v.astype(np.float32), shots, None, rec)
 
 
+def config5_inversion(seed=5):
+    """(true Survey, starting velocity, inversion settings) of the large device-resident
+    inversion: 401x401x201 @10 m, 256 shots x 10,000 receivers, 5 iterations."""
+    s = config5(seed)
+    start = gradient_model(s.nx, s.ny, s.nz, s.h, 1500.0, 1.0)
+    inv = dict(d_tomo=(50.0, 50.0, 50.0), tk_order=2, tk_param=0.1, cg_iterations=30, iterations=5,
+               smooth=True, filter_samples=5, standard_deviation=2.0, pick_noise=0.002)
+    return s, start, inv
+
+
 def small(seed, nx, ny, nz, h=25.0, nshots=1, windows=False, layered=True, nrec=16):
     """Small seeded case for parity tests."""
     rng = np.random.default_rng(seed)
