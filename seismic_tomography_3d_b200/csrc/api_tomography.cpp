@@ -16,6 +16,7 @@ int rebrick_model(tomo_ctx *ctx);  // api_eikonal.cpp
 namespace {
 
 constexpr unsigned long long kSpinLimit = 1ull << 26;
+constexpr float kRayLengthFactor = 4.0f;  // default per-ray cap: 4 x (traveltime x v_max)
 
 int fail(tomo_ctx *c, int code, const std::string &msg)
 {
@@ -160,6 +161,24 @@ int tomo_build_jacobian(tomo_ctx *ctx, const tomo_jacobian_opts *opts, tomo_jaco
     const float dmax = std::fmax(g.dx, std::fmax(g.dy, g.dz));
     const int max_steps = opts->max_ray_steps > 0 ? opts->max_ray_steps
                                                   : (int)(20.0f * (g.nx + g.ny + g.nz) * dmax / rayStep);
+    // Default cap per ray: the reference marches until the source cell with no cap
+    // (least_squares.cpp:216-280), so a ray circling a flat spot of the field never ends.
+    // A ray of traveltime T is at most T x v_max long; 4x that (plus 256 steps) leaves
+    // every terminating ray untouched and stops circling ones early.
+    float steps_per_second = 0.f;
+    if (opts->max_ray_steps <= 0) {
+        const size_t nmodel = (size_t)g.nx * g.ny * g.nz;
+        size_t tb = 0;
+        CK(tomo::reduce_min(ctx->slow.ptr, nullptr, nmodel, nullptr, &tb, ctx->stream));
+        const size_t off = (tb + 255) / 256 * 256;
+        CK(ctx->cub_temp.ensure(off + sizeof(float)));
+        float *smin_d = reinterpret_cast<float *>(ctx->cub_temp.ptr + off);
+        CK(tomo::reduce_min(ctx->slow.ptr, smin_d, nmodel, ctx->cub_temp.ptr, &tb, ctx->stream));
+        float smin = 0.f;
+        CK(cudaMemcpyAsync(&smin, smin_d, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (smin > 0.f && std::isfinite(smin)) steps_per_second = kRayLengthFactor / (smin * rayStep);
+    }
     const int cap_runs = opts->max_cells_per_ray > 0 ? opts->max_cells_per_ray : 1024;
     bool full = true;
     for (const auto &d : ctx->shots_h) full = full && d.wx0 == 0 && d.wy0 == 0 && d.wnx == g.nx && d.wny == g.ny;
@@ -208,6 +227,7 @@ int tomo_build_jacobian(tomo_ctx *ctx, const tomo_jacobian_opts *opts, tomo_jaco
     rl.nyt = nyt;
     rl.nzt = nzt;
     rl.max_steps = max_steps;
+    rl.steps_per_second = steps_per_second;
     rl.cap_runs = cap_runs;
     rl.runs = ctx->runs.ptr;
     rl.nuniq = ctx->nuniq.ptr;

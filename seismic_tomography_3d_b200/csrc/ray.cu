@@ -63,8 +63,15 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
             st = kRayOutside;  // receiver outside this shot's window
             L = p.max_steps;   // skip the march
         }
+        int cap = p.max_steps;
+        if (p.steps_per_second > 0.0f && L == 0) {
+            const float t0 = t_exp(p.T, d, p.nz, trunc_div(zi, p.dz) + 1, trunc_div(xi, p.dx) + 1,
+                                   trunc_div(yi, p.dy) + 1);
+            const float c = t0 * p.steps_per_second + 256.0f;
+            if (c < (float)cap) cap = (int)c;
+        }
         const float two_dz = fmul(2.0f, p.dz), two_dx = fmul(2.0f, p.dx), two_dy = fmul(2.0f, p.dy);
-        while (L < p.max_steps) {
+        while (L < cap) {
             const int i = trunc_div(zi, p.dz) + 1, j = trunc_div(xi, p.dx) + 1, k = trunc_div(yi, p.dy) + 1;
             const float dTz = fdiv(fsub(t_exp(p.T, d, p.nz, i + 1, j, k), t_exp(p.T, d, p.nz, i - 1, j, k)), two_dz);
             const float dTx = fdiv(fsub(t_exp(p.T, d, p.nz, i, j + 1, k), t_exp(p.T, d, p.nz, i, j - 1, k)), two_dx);
@@ -256,6 +263,11 @@ cudaError_t csr_transpose_finish(const int *sorted_pos, const int *rows_of, cons
 cudaError_t scan_exclusive(const int *in, int *out, int n, void *temp, size_t *temp_bytes, cudaStream_t st)
 {
     return cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, in, out, n, st);
+}
+
+cudaError_t reduce_min(const float *in, float *out, size_t n, void *temp, size_t *temp_bytes, cudaStream_t st)
+{
+    return cub::DeviceReduce::Min(temp, *temp_bytes, in, out, (long long)n, st);
 }
 
 cudaError_t sort_pairs(const int *keys_in, int *keys_out, const int *vals_in, int *vals_out, long long n, int key_bits,

@@ -31,6 +31,8 @@ struct RayLaunch {
     float dxt, dyt, dzt;  // inversion cell size
     int nxt, nyt, nzt;    // inversion grid
     int max_steps;
+    float steps_per_second;  // > 0: a ray also stops (capped) after T(start node) x this + 256
+                             // steps -- a ray of traveltime T cannot be longer than T x v_max
     int cap_runs;         // per-ray capacity of distinct cells
     uint2 *runs;          // nrays*cap_runs (cell, count), sorted by cell on exit
     int *nuniq;           // per ray: distinct cells
@@ -48,6 +50,7 @@ cudaError_t csr_transpose_prepare(const int *row_ptr, const int *cols, int nrows
                                   int *pos, int *rows_of, cudaStream_t st);
 // CUB device-wide primitives (temp == nullptr queries *temp_bytes).
 cudaError_t scan_exclusive(const int *in, int *out, int n, void *temp, size_t *temp_bytes, cudaStream_t st);
+cudaError_t reduce_min(const float *in, float *out, size_t n, void *temp, size_t *temp_bytes, cudaStream_t st);
 cudaError_t sort_pairs(const int *keys_in, int *keys_out, const int *vals_in, int *vals_out, long long n, int key_bits,
                        void *temp, size_t *temp_bytes, cudaStream_t st);
 cudaError_t csr_transpose_finish(const int *sorted_pos, const int *rows_of, const float *vals, long long nnz, int ncols,

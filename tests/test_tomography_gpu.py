@@ -232,3 +232,23 @@ def test_full_iteration_recovered_model(tomo, oracle_mod, small_survey):
     rms = np.sqrt(np.mean(((vel - vel_o) / vel_o) ** 2))
     assert rms < 5e-3
     assert np.count_nonzero(vel != sv["start_v"]) > 1000
+
+
+def test_default_ray_cap_keeps_terminating_rays(tomo, small_survey):
+    """The default per-ray cap (4 x traveltime x v_max) leaves every ray that reaches the
+    source cell exactly as under a plain step cap."""
+    sv = small_survey
+    ctx, _, _ = _solve(tomo, sv, sv["start_v"], sv["shots"], sv["nodes"])
+    with ctx:
+        ctx.build_jacobian(sv["d"], tk_order=2, tk_param=0.5, max_ray_steps=MAX_STEPS)
+        rp0, c0, v0 = ctx.jacobian()
+        s0 = ctx.ray_status()
+        ctx.build_jacobian(sv["d"], tk_order=2, tk_param=0.5)
+        rp1, c1, v1 = ctx.jacobian()
+        s1 = ctx.ray_status()
+    ok = np.flatnonzero(s0 == 0)
+    assert len(ok) > 0
+    np.testing.assert_array_equal(s1[ok], 0)
+    for r in ok:
+        np.testing.assert_array_equal(c1[rp1[r]:rp1[r + 1]], c0[rp0[r]:rp0[r + 1]])
+        np.testing.assert_array_equal(v1[rp1[r]:rp1[r + 1]], v0[rp0[r]:rp0[r + 1]])
