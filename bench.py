@@ -439,7 +439,9 @@ def run_inversion(args):
         iters.append({"residual_l2_s": res, "eikonal_ms": ms[0], "jacobian_ms": ms[1], "cgls_ms": ms[2],
                       "update_ms": ms[3], "total_ms": ev[0].elapsed_time(ev[4]),
                       "activations": est["activations"], "rounds": est["rounds"], "nnz": jst["nnz"],
-                      "rays_ok": jst["rays_ok"], "rays_stalled": jst["rays_stalled"],
+                      "rays_ok": jst["rays_ok"], "rays_stalled": jst["rays_stalled"], "rays_capped": jst["rays_capped"],
+                      "rays_nonfinite": jst["rays_nonfinite"], "rays_outside": jst["rays_outside"],
+                      "rays_overflow": jst["rays_overflow"], "ray_steps": jst["ray_steps"],
                       "cgls_rnorm": cst["rnorm"]})
     ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False)
     final_res = ctx.data_residual()

@@ -177,6 +177,22 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
  * returns how many there are. */
 int tomo_eik_brick_shapes(int *xyz_triples, int cap);
 
+typedef struct {
+    int trials;        /* launch shapes timed                                           */
+    float best_ms;     /* device time of the persistent solve with the chosen shape      */
+    float default_ms;  /* the same with the built-in default shape                      */
+} tomo_tune_stats;
+
+/* Autotuner of the JW solve (no counterpart in the reference, whose launch shape is fixed).
+ * Solves this batch (no receivers) with every launch shape -- warps per CTA {4, 8}, CTAs
+ * per SM {2, 3, 4}, in-brick iteration cap {8, 16, 32}, each brick shape of
+ * tomo_eik_brick_shapes -- `repeats` times each (0: 2), keeps the fastest in the context
+ * and writes it to *best (may be NULL).  Later solves on this context use the tuned value
+ * for every tomo_eik_opts field they leave 0.  The traveltime pool holds the last trial's
+ * fields afterwards. */
+int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows,
+                      int repeats, tomo_eik_opts *best, tomo_tune_stats *stats);
+
 /* Allocation-free single-shot solve, for callers that cannot call cudaMalloc (their
  * application already owns the GPU's memory through its own pool, or must stay within
  * a fixed device-memory budget).  No counterpart in the reference: it has no library

@@ -62,6 +62,10 @@ class EikStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class TuneStats(ctypes.Structure):
+    _fields_ = [("trials", ctypes.c_int), ("best_ms", ctypes.c_float), ("default_ms", ctypes.c_float)]
+
+
 class SeedStats(ctypes.Structure):
     _fields_ = [("violations", ctypes.c_longlong), ("max_deficit", ctypes.c_float), ("shots_fallback", ctypes.c_int),
                 ("rounds_seeded", ctypes.c_longlong), ("activations_seeded", ctypes.c_longlong),
@@ -102,6 +106,7 @@ def load_library(path: str = LIB_PATH):
     lib.tomo_eik_window.argtypes = [V, I, P(Window)]
     lib.tomo_eik_brick_shapes.argtypes = [P(I), I]
     lib.tomo_eik_volumes.argtypes = [V, V]
+    lib.tomo_eik_autotune.argtypes = [V, I, P(Point), P(Window), I, P(EikOpts), P(TuneStats)]
     lib.tomo_eik_solve_seeded.argtypes = [V, I, P(Point), P(Window), I, P(Point), V, V, F, P(EikOpts),
                                           P(EikStats), P(SeedStats)]
     _bind_tomography(lib)
@@ -289,6 +294,17 @@ class Context:
                                                    ctypes.c_void_p(ceiling_ptr), float(inflate), ctypes.byref(opts),
                                                    ctypes.byref(st), ctypes.byref(ss)))
         return out, st.as_dict(), ss.as_dict()
+
+    def eik_autotune(self, shots, windows=None, repeats=0):
+        """Autotunes the launch shape on this batch; returns (chosen shape dict, stats dict)."""
+        sp, ns, _s = _points(shots)
+        wp = _w = None
+        if windows is not None:
+            wp, _w = _windows(windows)
+        best, st = EikOpts(), TuneStats()
+        self._check(self.lib.tomo_eik_autotune(self.h, ns, sp, wp, repeats, ctypes.byref(best), ctypes.byref(st)))
+        shape = {"block_warps": best.block_warps, "occupancy": best.occupancy, "max_inner": best.max_inner}
+        return shape, {f: getattr(st, f) for f, _ in st._fields_}
 
     def volume_sizes(self, nshots, windows=None):
         """Floats of each shot's window volume (nz*wx*wy) in the back-to-back layout."""

@@ -316,13 +316,17 @@ struct SolveCfg {
     bool ieee_sqrt;
 };
 
-SolveCfg solve_cfg(const tomo_eik_opts *opts)
+SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
 {
     SolveCfg c{};
-    c.max_inner = (opts && opts->max_inner > 0) ? opts->max_inner : kDefaultMaxInner;
+    // fields left 0: the autotuned launch shape if there is one, else the defaults
+    const int inner0 = ctx->tuned_max_inner > 0 ? ctx->tuned_max_inner : kDefaultMaxInner;
+    const int warps0 = ctx->tuned_block_warps > 0 ? ctx->tuned_block_warps : 8;
+    const int occ0 = ctx->tuned_occupancy > 0 ? ctx->tuned_occupancy : 4;
+    c.max_inner = (opts && opts->max_inner > 0) ? opts->max_inner : inner0;
     c.max_rounds = (opts && opts->max_rounds > 0) ? opts->max_rounds : kDefaultMaxRounds;
-    c.block_warps = (opts && opts->block_warps > 0) ? opts->block_warps : 8;
-    c.occupancy = (opts && opts->occupancy > 0) ? opts->occupancy : 4;
+    c.block_warps = (opts && opts->block_warps > 0) ? opts->block_warps : warps0;
+    c.occupancy = (opts && opts->occupancy > 0) ? opts->occupancy : occ0;
     // Default: the reference's convergence threshold EPS = 1e-6 s (cuda_kernel.cuh:8).
     c.change_tol = kDefaultChangeTol;
     if (opts && opts->change_tol > 0.f) c.change_tol = opts->change_tol;
@@ -505,7 +509,7 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
     if (opts && opts->op != TOMO_OP_JW && opts->op != TOMO_OP_NGB)
         return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown eikonal operator");
-    const SolveCfg cfg = solve_cfg(opts);
+    const SolveCfg cfg = solve_cfg(ctx, opts);
     CK(cudaSetDevice(ctx->device));
     Batch bt;
     int rc = make_batch(ctx, nshots, shots, windows, nrec, receivers, bt);
@@ -562,7 +566,7 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
     if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
     if (opts && opts->op != TOMO_OP_JW)
         return fail(ctx, TOMO_ERR_INVALID_ARG, "the warm-started solve runs the JW operator only");
-    const SolveCfg cfg = solve_cfg(opts);
+    const SolveCfg cfg = solve_cfg(ctx, opts);
     CK(cudaSetDevice(ctx->device));
     Batch bt;
     int rc = make_batch(ctx, nshots, shots, windows, nrec, receivers, bt);
@@ -658,6 +662,65 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
         cudaEventElapsedTime(&seed_stats->seeded_ms, ev[3], ev[4]);
         cudaEventElapsedTime(&seed_stats->verify_ms, ev[4], ev[5]);
         cudaEventElapsedTime(&seed_stats->fallback_ms, ev[6], ev[7]);
+    }
+    return TOMO_OK;
+}
+
+int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows, int repeats,
+                      tomo_eik_opts *best, tomo_tune_stats *stats)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (repeats < 0) return fail(ctx, TOMO_ERR_INVALID_ARG, "repeats must be >= 0");
+    if (repeats == 0) repeats = 2;
+    // untuned defaults while timing (an earlier tuning must not leak into the trials)
+    ctx->tuned_block_warps = ctx->tuned_occupancy = ctx->tuned_max_inner = 0;
+    const int warps[] = {8, 4};
+    const int occs[] = {4, 3, 2};
+    const int inners[] = {16, 8, 32};
+    tomo_eik_opts o{};
+    o.op = TOMO_OP_JW;
+    tomo_eik_stats st{};
+    // warm-up (first launch of each kernel variant pays for module loading)
+    int rc = tomo_eik_solve(ctx, nshots, shots, windows, 0, nullptr, nullptr, &o, &st);
+    if (rc != TOMO_OK) return rc;
+    float best_ms = 0.f, default_ms = 0.f;
+    int trials = 0, bw = 8, bo = 4, bi = kDefaultMaxInner;
+    for (int w : warps)
+        for (int oc : occs)
+            for (int in : inners) {
+                o.block_warps = w;
+                o.occupancy = oc;
+                o.max_inner = in;
+                float ms = 0.f;
+                for (int r = 0; r < repeats + 1; r++) {
+                    rc = tomo_eik_solve(ctx, nshots, shots, windows, 0, nullptr, nullptr, &o, &st);
+                    if (rc != TOMO_OK) return rc;
+                    if (r == 0) continue;  // first launch of this variant: not timed
+                    ms = (r == 1) ? st.solve_ms : std::min(ms, st.solve_ms);
+                }
+                if (trials == 0) default_ms = ms;
+                if (trials == 0 || ms < best_ms) {
+                    best_ms = ms;
+                    bw = w;
+                    bo = oc;
+                    bi = in;
+                }
+                ++trials;
+            }
+    ctx->tuned_block_warps = bw;
+    ctx->tuned_occupancy = bo;
+    ctx->tuned_max_inner = bi;
+    if (best) {
+        *best = tomo_eik_opts{};
+        best->op = TOMO_OP_JW;
+        best->block_warps = bw;
+        best->occupancy = bo;
+        best->max_inner = bi;
+    }
+    if (stats) {
+        stats->trials = trials;
+        stats->best_ms = best_ms;
+        stats->default_ms = default_ms;
     }
     return TOMO_OK;
 }

@@ -70,6 +70,8 @@ struct tomo_ctx {
     std::vector<tomo_point> rec_h;
     int nshots = 0, nrec = 0;
     bool have_solve = false;
+    // launch shape chosen by tomo_eik_autotune (0: not tuned)
+    int tuned_block_warps = 0, tuned_occupancy = 0, tuned_max_inner = 0;
 
     cudaEvent_t ev[8] = {};
     unsigned *pinned_ctrl = nullptr;  // kCtrlWords + stats

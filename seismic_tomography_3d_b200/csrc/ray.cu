@@ -59,6 +59,12 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
         int nr = 0, L = 0, st = kRayCapped;
         bool overflow = false;
         unsigned cur = 0xffffffffu, cnt = 0;
+        int ci = -1;  // run that collects the steps in cell `cur`
+        // The four cells most recently entered and their runs: a ray running along a cell
+        // face alternates between two or three cells, and their steps go to one run each
+        // instead of a new run per re-entry (the per-cell totals are the same).
+        unsigned c0 = 0xffffffffu, c1 = 0xffffffffu, c2 = 0xffffffffu, c3 = 0xffffffffu;
+        int r0 = -1, r1 = -1, r2 = -1, r3 = -1;
         if (xi < 0.0f || yi < 0.0f || xi > fmul((float)(d.wnx - 1), p.dx) || yi > fmul((float)(d.wny - 1), p.dy)) {
             st = kRayOutside;  // receiver outside this shot's window
             L = p.max_steps;   // skip the march
@@ -94,10 +100,21 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
             if (cell == cur) {
                 ++cnt;
             } else {
-                if (cnt) {
-                    if (nr < p.cap_runs) runs[nr++] = make_uint2(cur, cnt);
-                    else overflow = true;
+                if (cnt && ci >= 0) runs[ci].y += cnt;
+                int hit = cell == c0 ? r0 : cell == c1 ? r1 : cell == c2 ? r2 : cell == c3 ? r3 : -1;
+                if (hit < 0) {
+                    if (nr < p.cap_runs) {
+                        runs[nr] = make_uint2(cell, 0u);
+                        hit = nr++;
+                        c3 = c2; r3 = r2;
+                        c2 = c1; r2 = r1;
+                        c1 = c0; r1 = r0;
+                        c0 = cell; r0 = hit;
+                    } else {
+                        overflow = true;
+                    }
                 }
+                ci = hit;
                 cur = cell;
                 cnt = 1;
             }
@@ -114,10 +131,7 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
                 break;
             }
         }
-        if (cnt) {
-            if (nr < p.cap_runs) runs[nr++] = make_uint2(cur, cnt);
-            else overflow = true;
-        }
+        if (cnt && ci >= 0) runs[ci].y += cnt;
         // sort the runs by cell and merge repeated cells (std::sort + run-length, :241-263)
         for (int a = 1; a < nr; a++) {
             const uint2 key = runs[a];

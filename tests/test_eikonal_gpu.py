@@ -169,3 +169,21 @@ def test_config1_full_size(tomo, oracle_mod):
     ref_recv = oracle_mod.first_arrival(Tref.astype(np.float32), sv.h, *sv.receivers.T)
     m = ref_recv >= 2 * sv.h / sv.velocity.max()
     assert np.max(np.abs(t_recv[0][m] - ref_recv[m]) / ref_recv[m]) < REL_TOL
+
+
+def test_autotune_picks_a_shape_and_keeps_results(tomo):
+    """tomo_eik_autotune times the launch shapes, keeps the fastest in the context, and the
+    tuned solve converges to the same field as the default one."""
+    sv = wl.small(5, 48, 40, 24, nshots=4, windows=True)
+    with tomo.Context(sv.nx, sv.ny, sv.nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(sv.shots, windows=sv.windows)
+        ref = [ctx.eik_volume(i) for i in range(len(sv.shots))]
+        shape, st = ctx.eik_autotune(sv.shots, windows=sv.windows, repeats=1)
+        assert st["trials"] == 18
+        assert shape["block_warps"] in (4, 8) and shape["occupancy"] in (2, 3, 4)
+        assert shape["max_inner"] in (8, 16, 32)
+        assert 0 < st["best_ms"] <= st["default_ms"]
+        ctx.eik_solve(sv.shots, windows=sv.windows)
+        for i in range(len(sv.shots)):
+            assert rel_err(ctx.eik_volume(i), ref[i], sv.h, float(sv.velocity.max())) < 1e-5
