@@ -302,6 +302,49 @@ int tomo_model_update(tomo_ctx *ctx, const tomo_update_opts *opts, float *veloci
 int tomo_sparse_cgls_gpu(const int *iA, const int *jA, const float *vA, const float *B, float *x, int N, int M,
                          int NNZ, int NIT, float TOL);
 
+/* ------------------------------------------------ learned warm start (surrogate) ------ */
+/* No counterpart in the reference (it has no learned component).  A 3D U-Net (4 levels,
+ * 16/32/48/64 channels, 3x3x3 convolutions, ReLU) predicts the factored traveltime
+ * tau = T / (s_src |x - x_src|) of one source from the slowness around it; BF16 tensor-core
+ * convolutions with FP32 accumulation, trained on the device by the library's own
+ * backward kernels and Adam.  Its prediction feeds tomo_eik_solve_seeded. */
+typedef struct tomo_net tomo_net;
+
+typedef struct {
+    const float *slow;          /* DEVICE: model slowness, nz*nx*ny, z fastest            */
+    int model_nx, model_ny, nz; /* that model's size                                      */
+    tomo_window window;         /* the sample: lateral window (any origin), full depth    */
+    tomo_point source;          /* metres, model coordinates, inside the window           */
+    const float *T;             /* DEVICE: the window's traveltimes (nz*wx*wy, z fastest);
+                                   training targets, unused by tomo_net_predict            */
+} tomo_net_sample;
+
+int tomo_net_create(int device, void *stream, unsigned long long seed, tomo_net **out);
+int tomo_net_destroy(tomo_net *net);
+const char *tomo_net_last_error(const tomo_net *net);
+long long tomo_net_param_count(const tomo_net *net);
+/* FP32 parameters (host): per convolution w[cout][27][cin] then b[cout], then the head. */
+int tomo_net_get_params(tomo_net *net, float *out);
+int tomo_net_set_params(tomo_net *net, const float *in);  /* also resets the optimiser */
+/* Loss (mean squared tau error over nodes at distance >= h from the source) and its
+ * gradient w.r.t. every parameter (host, may be NULL), without an update. */
+int tomo_net_gradients(tomo_net *net, int n, const tomo_net_sample *samples, float h, double *loss, float *grads);
+/* One Adam step (lr) on a batch of n samples of equal padded size; returns the loss. */
+int tomo_net_train_step(tomo_net *net, int n, const tomo_net_sample *samples, float h, float lr, double *loss);
+int tomo_net_evaluate(tomo_net *net, int n, const tomo_net_sample *samples, float h, double *loss);
+/* Predicted traveltimes tau x s_src x distance for n samples, written to the DEVICE array
+ * t_pred back to back (sample i's window volume, z fastest) -- the layout of
+ * tomo_eik_volumes and of the ceiling of tomo_eik_solve_seeded; 0 within h of the source.
+ * ms (may be NULL): device time. */
+int tomo_net_predict(tomo_net *net, int n, const tomo_net_sample *samples, float h, float *t_pred, float *ms);
+
+/* Training data: fills ctx's model with seeded random tiles (tile x tile nodes laterally,
+ * full depth): 3-6 dipping layers of 1500-4500 m/s and 0-12 Gaussian anomalies of up to
+ * +-15 %.  nx and ny must be multiples of tile. */
+int tomo_random_tiles(tomo_ctx *ctx, int tile, unsigned long long seed);
+/* The context's current slowness model on the device (nz*nx*ny, z fastest). */
+const float *tomo_ctx_slowness_device(tomo_ctx *ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -143,8 +143,34 @@ class UpdateOpts(ctypes.Structure):
                 ("standard_deviation", ctypes.c_float), ("use_reference_masks", ctypes.c_int)]
 
 
+class NetSample(ctypes.Structure):
+    _fields_ = [("slow", ctypes.c_void_p), ("model_nx", ctypes.c_int), ("model_ny", ctypes.c_int),
+                ("nz", ctypes.c_int), ("window", Window), ("source", Point), ("T", ctypes.c_void_p)]
+
+
+def _bind_net(lib):
+    """Bindings of the surrogate (learned warm start) part of the ABI."""
+    P, I, V, F, D = ctypes.POINTER, ctypes.c_int, ctypes.c_void_p, ctypes.c_float, ctypes.c_double
+    lib.tomo_net_create.argtypes = [I, V, ctypes.c_ulonglong, P(V)]
+    lib.tomo_net_destroy.argtypes = [V]
+    lib.tomo_net_last_error.argtypes = [V]
+    lib.tomo_net_last_error.restype = ctypes.c_char_p
+    lib.tomo_net_param_count.argtypes = [V]
+    lib.tomo_net_param_count.restype = ctypes.c_longlong
+    lib.tomo_net_get_params.argtypes = [V, V]
+    lib.tomo_net_set_params.argtypes = [V, V]
+    lib.tomo_net_gradients.argtypes = [V, I, P(NetSample), F, P(D), V]
+    lib.tomo_net_train_step.argtypes = [V, I, P(NetSample), F, F, P(D)]
+    lib.tomo_net_evaluate.argtypes = [V, I, P(NetSample), F, P(D)]
+    lib.tomo_net_predict.argtypes = [V, I, P(NetSample), F, V, P(F)]
+    lib.tomo_random_tiles.argtypes = [V, I, ctypes.c_ulonglong]
+    lib.tomo_ctx_slowness_device.argtypes = [V]
+    lib.tomo_ctx_slowness_device.restype = V
+
+
 def _bind_tomography(lib):
     """Bindings of the tomography half of the ABI."""
+    _bind_net(lib)
     P, I, V = ctypes.POINTER, ctypes.c_int, ctypes.c_void_p
     lib.tomo_build_jacobian.argtypes = [V, P(JacobianOpts), P(JacobianStats)]
     lib.tomo_jacobian_copy.argtypes = [V, V, V, V]
@@ -317,6 +343,14 @@ class Context:
         """All window volumes of the last solve into the device array at dst_ptr."""
         self._check(self.lib.tomo_eik_volumes(self.h, ctypes.c_void_p(dst_ptr)))
 
+    def random_tiles(self, tile, seed):
+        """Seeded random layered tiles as the model (surrogate training data)."""
+        self._check(self.lib.tomo_random_tiles(self.h, tile, seed))
+
+    def slowness_device(self):
+        """Device address of the current slowness model (z fastest)."""
+        return self.lib.tomo_ctx_slowness_device(self.h)
+
     def eik_window(self, shot):
         w = Window()
         self._check(self.lib.tomo_eik_window(self.h, shot, ctypes.byref(w)))
@@ -380,3 +414,81 @@ class Context:
         out = np.empty((y1 - y0, x1 - x0, self.grid.nz), np.float32)
         self._check(self.lib.tomo_eik_volume(self.h, shot, out.ctypes.data))
         return out
+
+
+def net_samples(items):
+    """ctypes array of tomo_net_sample from dicts with keys slow (device address),
+    model_nx, model_ny, nz, window (x0, x1, y0, y1), source (x, y, z), T (device address or 0)."""
+    arr = (NetSample * len(items))()
+    for i, it in enumerate(items):
+        arr[i].slow = it["slow"]
+        arr[i].model_nx, arr[i].model_ny, arr[i].nz = it["model_nx"], it["model_ny"], it["nz"]
+        arr[i].window = Window(*[int(v) for v in it["window"]])
+        arr[i].source = Point(*[float(v) for v in it["source"]])
+        arr[i].T = it.get("T") or None
+    return arr
+
+
+class Net:
+    """The traveltime surrogate (tomo_net): 3D U-Net trained and run on the device."""
+
+    def __init__(self, device=0, seed=0, stream=None):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.tomo_net_create(device, ctypes.c_void_p(stream) if stream else None, seed, ctypes.byref(h))
+        if rc != TOMO_OK:
+            raise TomoError(rc, self.lib.tomo_status_string(rc).decode())
+        self.h = h
+        self.n_params = int(self.lib.tomo_net_param_count(self.h))
+
+    def _check(self, rc):
+        if rc != TOMO_OK:
+            raise TomoError(rc, self.lib.tomo_net_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tomo_net_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self):
+        out = np.empty(self.n_params, np.float32)
+        self._check(self.lib.tomo_net_get_params(self.h, out.ctypes.data))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.n_params
+        self._check(self.lib.tomo_net_set_params(self.h, p.ctypes.data))
+
+    def gradients(self, samples, h):
+        arr = net_samples(samples)
+        loss = ctypes.c_double()
+        g = np.empty(self.n_params, np.float32)
+        self._check(self.lib.tomo_net_gradients(self.h, len(arr), arr, h, ctypes.byref(loss), g.ctypes.data))
+        return loss.value, g
+
+    def train_step(self, samples, h, lr):
+        arr = net_samples(samples)
+        loss = ctypes.c_double()
+        self._check(self.lib.tomo_net_train_step(self.h, len(arr), arr, h, lr, ctypes.byref(loss)))
+        return loss.value
+
+    def evaluate(self, samples, h):
+        arr = net_samples(samples)
+        loss = ctypes.c_double()
+        self._check(self.lib.tomo_net_evaluate(self.h, len(arr), arr, h, ctypes.byref(loss)))
+        return loss.value
+
+    def predict(self, samples, h, out_ptr):
+        """Predicted traveltimes into the device array at out_ptr (back-to-back windows);
+        returns the device time in ms."""
+        arr = net_samples(samples)
+        ms = ctypes.c_float()
+        self._check(self.lib.tomo_net_predict(self.h, len(arr), arr, h, ctypes.c_void_p(out_ptr), ctypes.byref(ms)))
+        return ms.value

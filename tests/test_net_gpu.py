@@ -1,0 +1,135 @@
+"""The traveltime surrogate on the device, through the C ABI.
+
+  * forward output and the gradients of every parameter (BF16 tensor-core convolutions,
+    FP32 accumulation) against the FP64 oracle (oracle/unet.py, itself pinned to torch
+    autograd): loss within 3 %, each parameter tensor's gradient at cosine >= 0.98;
+  * training on solver-generated fields lowers the loss;
+  * the trained network's prediction, used as the ceiling of tomo_eik_solve_seeded, leaves
+    the solution unchanged (the plain solve judges it) -- and the test reports what it saves.
+"""
+import numpy as np
+import pytest
+
+from oracle import unet
+from seismic_tomography_3d_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def _case(tomo, seed=4, nx=20, ny=24, nz=14, h=20.0):
+    """A small layered model, one source, its plain-FIM traveltimes."""
+    sv = wl.small(seed, nx, ny, nz, h=h, nshots=1)
+    with tomo.Context(nx, ny, nz, h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(sv.shots)
+        T = ctx.eik_volume(0)
+    slow = (1.0 / sv.velocity).astype(np.float32)
+    return sv, slow, T
+
+
+def _cos(a, b):
+    return float(np.dot(a, b) / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-300))
+
+
+def test_gradients_match_oracle(tomo):
+    sv, slow, T = _case(tomo)
+    h = sv.h
+    net = tomo.Net(seed=11)
+    p = unet.init_params(11)
+    convs, head, _ = unet.layout()
+    rng = np.random.default_rng(0)
+    for w, b, ci, co in convs:
+        p[b:b + co] = rng.uniform(-0.05, 0.05, co)
+    net.set_params(p)
+    p = net.get_params()
+    slow_d, T_d = _dev(slow), _dev(T)
+    win = (0, sv.nx, 0, sv.ny)
+    sample = dict(slow=slow_d.data_ptr(), model_nx=sv.nx, model_ny=sv.ny, nz=sv.nz, window=win,
+                  source=sv.shots[0], T=T_d.data_ptr())
+    loss, g = net.gradients([sample], h)
+    pad = tuple(-(-n // 8) * 8 for n in (sv.ny, sv.nx, sv.nz))
+    f, dist, s_src, inside = unet.features(slow, win, sv.nz, sv.shots[0], h, pad)
+    tgt = unet.target(T, dist, s_src, inside, h)
+    loss_o, tau_o, g_o = unet.forward_backward(p, f[None], tgt[None])
+    assert abs(loss - loss_o) <= 0.03 * loss_o, (loss, loss_o)
+    for i, (w, b, ci, co) in enumerate(convs):
+        gw, gw_o = g[w:w + 27 * ci * co], g_o[w:w + 27 * ci * co]
+        if i == 0:  # input channels 2..15 are zero: only the first two carry gradient
+            gw, gw_o = gw.reshape(co, 27, ci)[..., :2].ravel(), gw_o.reshape(co, 27, ci)[..., :2].ravel()
+        assert _cos(gw, gw_o) >= 0.98, (i, _cos(gw, gw_o))
+        assert _cos(g[b:b + co], g_o[b:b + co]) >= 0.98, (i, "bias")
+    assert _cos(g[head:head + 17], g_o[head:head + 17]) >= 0.98
+    # prediction = oracle tau * s_src * distance on the window
+    import torch
+
+    out = torch.zeros(sv.nx * sv.ny * sv.nz, dtype=torch.float32, device="cuda")
+    net.predict([sample], h, out.data_ptr())
+    t_pred = out.cpu().numpy().reshape(sv.ny, sv.nx, sv.nz)
+    t_o = (tau_o[0] * s_src * dist)[:sv.ny, :sv.nx, :sv.nz]
+    m = dist[:sv.ny, :sv.nx, :sv.nz] >= h
+    assert np.max(np.abs(t_pred[m] - t_o[m]) / t_o[m]) < 0.02
+    assert np.all(t_pred[~m] == 0.0)
+    net.close()
+
+
+def _tiles(tomo, ctx, tile, nz, h, seed):
+    """Random tiles as the model, one surface source per tile; returns net samples."""
+    import torch
+
+    ctx.random_tiles(tile, seed)
+    rng = np.random.default_rng(seed)
+    tx, ty = ctx.grid.nx // tile, ctx.grid.ny // tile
+    wins, shots = [], []
+    for j in range(ty):
+        for i in range(tx):
+            wins.append((i * tile, (i + 1) * tile, j * tile, (j + 1) * tile))
+            shots.append(((i * tile + rng.integers(0, tile)) * h, (j * tile + rng.integers(0, tile)) * h, 0.0))
+    wins, shots = np.array(wins, np.int32), np.array(shots, np.float32)
+    ctx.eik_solve(shots, windows=wins)
+    T = torch.empty(len(shots) * tile * tile * nz, dtype=torch.float32, device="cuda")
+    ctx.eik_volumes_to(T.data_ptr())
+    # the model is rewritten by the next random_tiles call: keep a copy
+    slow = torch.from_numpy(ctx.get_slowness().ravel()).cuda()
+    vol = tile * tile * nz
+    samples = [dict(slow=slow.data_ptr(), model_nx=ctx.grid.nx, model_ny=ctx.grid.ny, nz=nz, window=tuple(wins[k]),
+                    source=shots[k], T=T.data_ptr() + 4 * k * vol) for k in range(len(shots))]
+    return samples, (slow, T), wins, shots
+
+
+def test_training_lowers_loss_and_warm_start_keeps_the_solution(tomo):
+    import torch
+
+    tile, nz, h = 32, 32, 20.0
+    ctx = tomo.Context(4 * tile, 4 * tile, nz, h)
+    train, keep, _, _ = _tiles(tomo, ctx, tile, nz, h, seed=1)
+    net = tomo.Net(seed=5)
+    first = net.evaluate(train, h)
+    for it in range(60):
+        k = (4 * it) % len(train)
+        net.train_step(train[k:k + 4], h, 2e-3)
+    last = net.evaluate(train, h)
+    assert last < 0.5 * first, (first, last)
+
+    # warm start on a fresh set of tiles: prediction -> ceiling -> seeded solve
+    test, keep2, wins, shots = _tiles(tomo, ctx, tile, nz, h, seed=99)
+    _, st_plain = ctx.eik_solve(shots, windows=wins)
+    plain = [ctx.eik_volume(i) for i in range(len(shots))]
+    pred = torch.zeros(len(shots) * tile * tile * nz, dtype=torch.float32, device="cuda")
+    net.predict(test, h, pred.data_ptr())
+    torch.cuda.synchronize()
+    _, st, ss = ctx.eik_solve_seeded(shots, pred.data_ptr(), 0.02, windows=wins)
+    vmax = 4500.0 * 1.15
+    for i in range(len(shots)):
+        T = ctx.eik_volume(i)
+        m = plain[i] >= 2 * h / vmax
+        assert np.max(np.abs(T[m] - plain[i][m]) / plain[i][m]) < 1e-5
+    print(f"\nwarm start with the trained surrogate: activations {st['activations']} vs plain "
+          f"{st_plain['activations']}, fallback shots {ss['shots_fallback']}/{len(shots)}")
+    net.close()
+    ctx.close()
