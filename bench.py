@@ -467,6 +467,67 @@ def run_inversion(args):
     return 0
 
 
+def run_warm_start(args):
+    """Config 4: the learned warm start end to end -- solver-generated training fields on
+    seeded random models, the U-Net trained on the device, then used on the config-2 batch:
+    prediction -> ceiling (x 1.02) -> warm-started FIM, against the plain FIM.  Prints its own
+    JSON line (not the headline metric)."""
+    import torch
+
+    import seismic_tomography_3d_b200 as tomo
+    from seismic_tomography_3d_b200 import surrogate
+
+    t0 = time.perf_counter()
+    ds = surrogate.make_dataset(nfields=args.fields, tile=64, nz=64, h=12.5)
+    net = tomo.Net(seed=0)
+    summ = surrogate.train(net, ds, epochs=args.epochs, batch=8, lr=1e-3)
+    gen_s, gen_solve_ms = ds.gen_s, ds.solve_ms
+    del ds
+    torch.cuda.empty_cache()
+    sv = workload(0)
+    ns = len(sv.shots)
+    ctx = tomo.Context(sv.nx, sv.ny, sv.nz, sv.h)
+    ctx.set_velocity(sv.velocity)
+    for _ in range(2):
+        _, st_plain = ctx.eik_solve(sv.shots, windows=sv.windows)
+    plain_ms = statistics.median(ctx.eik_solve(sv.shots, windows=sv.windows)[1]["total_ms"] for _ in range(5))
+    sizes = ctx.volume_sizes(ns, sv.windows)
+    exact = torch.empty(sum(sizes), dtype=torch.float32, device="cuda")
+    ctx.eik_volumes_to(exact.data_ptr())
+    pred, infer_ms = surrogate.predict_ceiling(net, ctx, sv.shots, sv.windows)
+    pred, infer_ms = surrogate.predict_ceiling(net, ctx, sv.shots, sv.windows)
+    m = (exact >= 2.0 * sv.h / float(sv.velocity.max())) & (pred > 0)
+    rel = ((pred - exact) / exact)[m]
+    runs = [ctx.eik_solve_seeded(sv.shots, pred.data_ptr(), 0.02, windows=sv.windows) for _ in range(3)]
+    _, st_w, ss_w = runs[-1]
+    warm_ms = statistics.median(r[1]["total_ms"] for r in runs)
+    out = torch.empty_like(exact)
+    ctx.eik_volumes_to(out.data_ptr())
+    torch.cuda.synchronize()
+    err = float(((out - exact).abs() / exact)[exact >= 2.0 * sv.h / float(sv.velocity.max())].max())
+    line = {"metric": "learned warm start vs plain FIM (config 4 surrogate on the config-2 batch)",
+            "value": ns / ((warm_ms + infer_ms) / 1000.0), "unit": UNIT, "higher_is_better": True,
+            "plain": {"value": ns / (plain_ms / 1000.0), "ms_per_batch": plain_ms,
+                      "activations": st_plain["activations"], "inner_iterations": st_plain["inner_iterations"]},
+            "warm": {"ms_per_batch_solve": warm_ms, "ms_inference": infer_ms,
+                     "activations": st_w["activations"], "inner_iterations": st_w["inner_iterations"],
+                     "activations_seeded_launch": ss_w["activations_seeded"], "shots_fallback": ss_w["shots_fallback"],
+                     "violations": ss_w["violations"], "max_rel_err_vs_plain": err},
+            "speedup_vs_plain": plain_ms / (warm_ms + infer_ms),
+            "predictor_rel_err": {"median_abs": float(rel.abs().median()), "p99_abs": float(rel.abs().quantile(0.99))
+                                  if rel.numel() < 16_000_000 else None,
+                                  "frac_below_truth_by_2pct": float((rel < -0.02).float().mean())},
+            "training": {k: v for k, v in summ.items() if k != "history"}, "history": summ["history"],
+            "data": {"fields": args.fields, "tile": [64, 64, 64], "h_m": 12.5,
+                     "models": "seeded random: 3-6 dipping layers 1500-4500 m/s, 0-12 Gaussian anomalies +-15 %",
+                     "generation_s": gen_s, "generation_solve_ms": gen_solve_ms},
+            "wall_s": time.perf_counter() - t0}
+    print(json.dumps(line), flush=True)
+    net.close()
+    ctx.close()
+    return 0
+
+
 def run_tomography(args):
     """Config 3: one full tomography iteration on the device (64 shots x 2,500 receivers,
     201x201x101 at 12.5 m, 50x50x25 cells, Tikhonov order 2, lambda 0.1, 30 CGLS
@@ -539,7 +600,13 @@ def main():
                     help="time one config-3 tomography iteration instead (separate JSON line)")
     ap.add_argument("--inversion", action="store_true",
                     help="run the config-5 device-resident inversion instead (separate JSON line)")
+    ap.add_argument("--warm-start", action="store_true",
+                    help="run the config-4 learned warm start instead (separate JSON line)")
+    ap.add_argument("--fields", type=int, default=20000, help="training fields (--warm-start)")
+    ap.add_argument("--epochs", type=int, default=3, help="training epochs (--warm-start)")
     args = ap.parse_args()
+    if args.warm_start:
+        return run_warm_start(args)
     if args.tomography:
         return run_tomography(args)
     if args.inversion:
