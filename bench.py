@@ -36,6 +36,11 @@ sys.path.insert(0, ROOT)
 METRIC = "shot solves/s on 201x201x101, learned-warm vs plain FIM, at 1e-4 rel err"
 UNIT = "shots/s"
 BYTES_PER_NODE_ACT = 12  # slowness read + traveltime read + traveltime write (float32)
+# Solver tolerances of the timed runs: the metric is quoted at 1e-4 relative traveltime
+# error, so the face-change and in-brick tolerances are loosened until the measured error
+# against the fully converged field (checked every run, reported as "accuracy") sits well
+# inside that budget: 2.7e-5 on this batch.  The library default is the exact fixed point.
+SOLVER = dict(change_tol=1e-5, inner_tol=1e-6)
 
 
 def rank_info():
@@ -236,7 +241,7 @@ def run_ours(args):
     ctx.set_velocity(sv.velocity)
 
     def step_resident():
-        _, st = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=False)
+        _, st = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=False, **SOLVER)
         return st
 
     def barrier():
@@ -274,7 +279,7 @@ def run_ours(args):
     for _ in range(args.steps):
         tomo_rc = lib.tomo_set_velocity(ctx.h, vel_pinned.data_ptr())
         assert tomo_rc == 0
-        t_out, _ = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=True)
+        t_out, _ = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=True, **SOLVER)
     e1.record(stream)
     barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
@@ -300,6 +305,9 @@ def run_ours(args):
                 if ln.startswith("dram_bytes_per_activation:"):
                     traffic = float(ln.split(":")[1]) * act
 
+    # ---- accuracy of the timed setting against the fully converged field ----------------
+    accuracy = solver_accuracy(ctx, sv)
+
     # ---- the NGB operator: the reference's own Accurate_FSM sweeps, bit-exact ------------
     ngb_steps = max(1, min(args.steps, 5))
     ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=False, op=1)
@@ -324,6 +332,7 @@ def run_ours(args):
             "data": "synthetic (seeded config-2 model, shots, windows, receivers)",
             "config": {"workload": "config2: 64 shots/GPU, 201x201x101 @12.5 m, brick-aligned windows "
                                    "60-100 % lateral, 2500 receivers, plain FIM (JW operator)",
+                       "tolerances_s": SOLVER,
                        "shots_per_gpu": ns, "grid": [sv.nx, sv.ny, sv.nz], "h_m": sv.h,
                        "l2": "traveltime pool 1.1 GB > 126 MB L2 (inputs larger than L2)",
                        "parallelism": f"shot-sharded x{world}"},
@@ -337,7 +346,8 @@ def run_ours(args):
             "clocks": clk.summary(),
             "gpu_launches": 3 * args.steps,
             "solver": {"rounds": stats[-1]["rounds"], "activations": stats[-1]["activations"],
-                       "inner_iterations": stats[-1]["inner_iterations"]},
+                       "inner_iterations": stats[-1]["inner_iterations"], **SOLVER},
+            "accuracy": accuracy,
             "ngb_fsm": {"value": world * ns / (ngb_ms / 1000.0), "unit": UNIT, "ms_per_step": ngb_ms,
                         "steps": ngb_steps,
                         "what": "TOMO_OP_NGB: the reference Accurate_FSM's 8+8 sweeps on the same batch, "
@@ -354,6 +364,26 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def solver_accuracy(ctx, sv):
+    """Max relative error of the timed setting against the fully converged field (any face
+    drop re-queues, exact in-brick convergence) on nodes with T >= 2h/v_max."""
+    import torch
+
+    ns = len(sv.shots)
+    sizes = ctx.volume_sizes(ns, sv.windows)
+    ref = torch.empty(sum(sizes), dtype=torch.float32, device="cuda")
+    out = torch.empty_like(ref)
+    ctx.eik_solve(sv.shots, windows=sv.windows, want_recv=False, change_tol=-1.0)
+    ctx.eik_volumes_to(ref.data_ptr())
+    ctx.eik_solve(sv.shots, windows=sv.windows, want_recv=False, **SOLVER)
+    ctx.eik_volumes_to(out.data_ptr())
+    torch.cuda.synchronize()
+    m = ref >= 2.0 * sv.h / float(sv.velocity.max())
+    err = float(((out - ref).abs() / ref)[m].max())
+    return {"max_rel_err_vs_converged": err, "budget": 1e-4, "nodes_checked": int(m.sum()),
+            "reference": "same batch with change_tol < 0 (any drop re-queues) and exact in-brick convergence"}
 
 
 def warm_start_bound(ctx, sv, stream, steps, barrier, dist, world, inflate=0.02):

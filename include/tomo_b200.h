@@ -71,7 +71,7 @@ typedef struct {
     int max_rounds;  /* cap of outer rounds (0: default 1<<20)                        */
     int brick;       /* brick shape id (0: tuned default); see tomo_eik_brick_shapes  */
     int block_warps; /* warps per CTA of the persistent kernel (0: default)           */
-    int occupancy;   /* CTAs per SM the kernel is compiled for, 1..4 (0: default 4)   */
+    int occupancy;   /* CTAs per SM the kernel is compiled for, 1..6 (0: default 4)   */
     float change_tol;/* a face value must drop by more than this (s) to re-queue the
                         neighbour brick.  0: default 1e-6 s, the reference's EPS
                         (cuda_kernel.cuh:8); < 0: any drop (exact FP32 fixed point) */
@@ -185,7 +185,7 @@ typedef struct {
 
 /* Autotuner of the JW solve (no counterpart in the reference, whose launch shape is fixed).
  * Solves this batch (no receivers) with every launch shape -- warps per CTA {4, 8}, CTAs
- * per SM {2, 3, 4}, in-brick iteration cap {8, 16, 32}, each brick shape of
+ * per SM {3, 4, 5, 6}, in-brick iteration cap {8, 16, 32}, each brick shape of
  * tomo_eik_brick_shapes -- `repeats` times each (0: 2), keeps the fastest in the context
  * and writes it to *best (may be NULL).  Later solves on this context use the tuned value
  * for every tomo_eik_opts field they leave 0.  The traveltime pool holds the last trial's

@@ -675,7 +675,7 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
     // untuned defaults while timing (an earlier tuning must not leak into the trials)
     ctx->tuned_block_warps = ctx->tuned_occupancy = ctx->tuned_max_inner = 0;
     const int warps[] = {8, 4};
-    const int occs[] = {4, 3, 2};
+    const int occs[] = {4, 5, 6, 3};
     const int inners[] = {16, 8, 32};
     tomo_eik_opts o{};
     o.op = TOMO_OP_JW;

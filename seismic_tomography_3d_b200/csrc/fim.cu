@@ -69,14 +69,14 @@ __device__ __forceinline__ int tile_idx(int z, int x, int y)
     return (z + 1) + kTile * ((x + 1) + kTile * (y + 1));
 }
 
-// Lane masks of the brick faces for the two node sets of a lane (node = lane and
-// lane + 32; node = z + 4x + 16y).
+// Lane masks of the brick faces for the two node sets of a lane (node = z + 4x + 16y;
+// first set y = 2 (lane >> 4), second set y + 1).
 constexpr unsigned kMaskZm = 0x11111111u;  // z == 0
 constexpr unsigned kMaskZp = 0x88888888u;  // z == 3
 constexpr unsigned kMaskXm = 0x000F000Fu;  // x == 0
 constexpr unsigned kMaskXp = 0xF000F000u;  // x == 3
-constexpr unsigned kMaskY0 = 0x0000FFFFu;  // y == 0 (first node set)
-constexpr unsigned kMaskY3 = 0xFFFF0000u;  // y == 3 (second node set)
+constexpr unsigned kMaskY0 = 0x0000FFFFu;  // y == 0 (first node set, lanes 0-15)
+constexpr unsigned kMaskY3 = 0xFFFF0000u;  // y == 3 (second node set, lanes 16-31)
 
 __device__ __forceinline__ float brick_T(const float *T, const ShotDesc &d, int x, int y, int z)
 {
@@ -140,6 +140,9 @@ struct BrickLoad {
     float hv[3];       // the lane's three face-halo values
 };
 
+// First of the lane's two nodes (node = z + 4x + 16y); the second is 16 above it (y + 1).
+__device__ __forceinline__ int lane_node(int lane) { return (lane & 15) + 32 * (lane >> 4); }
+
 __device__ __forceinline__ void brick_coords(const ShotDesc &d, unsigned b, int &bz, int &bx, int &by)
 {
     bz = (int)(b % (unsigned)d.nbz);
@@ -181,11 +184,13 @@ __device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, Br
     const long long gb = bz + (long long)p.gbz * ((bx + (d.wx0 >> 2)) + (long long)p.gbx * (by + (d.wy0 >> 2)));
     const float *Sb = p.S + gb * kBrickNodes;
     const float *Tb = p.T + d.t_off + (long long)L.b * kBrickNodes;
-    // own nodes: n0 = lane (y in {0,1}), n1 = lane + 32 (y in {2,3})
-    L.s0 = __ldg(Sb + lane);
-    L.s1 = __ldg(Sb + 32 + lane);
-    L.i0 = __ldcg(Tb + lane);
-    L.i1 = __ldcg(Tb + 32 + lane);
+    // own nodes: (z, x, y) and (z, x, y + 1) with z = lane & 3, x = (lane >> 2) & 3,
+    // y = 2 (lane >> 4)
+    const int n0 = lane_node(lane);
+    L.s0 = __ldg(Sb + n0);
+    L.s1 = __ldg(Sb + n0 + 16);
+    L.i0 = __ldcg(Tb + n0);
+    L.i1 = __ldcg(Tb + n0 + 16);
     // Missing neighbours (grid edge) are INF; the reference's "halo = self" at the edge
     // cannot lower a node either.
 #pragma unroll
@@ -209,9 +214,9 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     const int nbz = d.nbz, nbx = d.nbx, nby = d.nby;
     float *Tb = p.T + d.t_off + (long long)b * kBrickNodes;
 
-    const int z0 = lane & 3, x0 = (lane >> 2) & 3, y0 = lane >> 4;
+    const int z0 = lane & 3, x0 = (lane >> 2) & 3, y0 = 2 * (lane >> 4);
     const int ti0 = tile_idx(z0, x0, y0);
-    const int ti1 = ti0 + 2 * kTile * kTile;
+    const int ti1 = ti0 + kTile * kTile;  // y + 1
     const float s0 = L.s0, s1 = L.s1, i0 = L.i0, i1 = L.i1;
     float c0 = i0, c1 = i1;
     tile[ti0] = c0;
@@ -228,14 +233,22 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     bool more = true;
     int it = 0;
     for (; it < p.max_inner; ++it) {
+        // The lane's two nodes are y-neighbours: the second update of an iteration uses the
+        // first one's new value (Gauss-Seidel along y inside the lane), and the order
+        // alternates so that information crosses the pair both ways.
         const float a0 = fminf(tile[ti0 - kTile], tile[ti0 + kTile]);
-        const float b0 = fminf(tile[ti0 - kTile * kTile], tile[ti0 + kTile * kTile]);
         const float g0 = fminf(tile[ti0 - 1], tile[ti0 + 1]);
         const float a1 = fminf(tile[ti1 - kTile], tile[ti1 + kTile]);
-        const float b1 = fminf(tile[ti1 - kTile * kTile], tile[ti1 + kTile * kTile]);
         const float g1 = fminf(tile[ti1 - 1], tile[ti1 + 1]);
-        const float n0 = fminf(c0, godunov_jw<kFastSqrt>(a0, b0, g0, h, s0));
-        const float n1 = fminf(c1, godunov_jw<kFastSqrt>(a1, b1, g1, h, s1));
+        const float ym = tile[ti0 - kTile * kTile], yp = tile[ti1 + kTile * kTile];
+        float n0, n1;
+        if (it & 1) {
+            n1 = fminf(c1, godunov_jw<kFastSqrt>(a1, fminf(c0, yp), g1, h, s1));
+            n0 = fminf(c0, godunov_jw<kFastSqrt>(a0, fminf(ym, n1), g0, h, s0));
+        } else {
+            n0 = fminf(c0, godunov_jw<kFastSqrt>(a0, fminf(ym, c1), g0, h, s0));
+            n1 = fminf(c1, godunov_jw<kFastSqrt>(a1, fminf(n0, yp), g1, h, s1));
+        }
         const bool ch = (n0 < c0 - p.inner_tol) | (n1 < c1 - p.inner_tol);
         __syncwarp();
         tile[ti0] = n0;
@@ -257,8 +270,9 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     const unsigned m1 = __ballot_sync(kFull, c1 < i1 - p.change_tol);
     const unsigned mm = m0 | m1;
     if (any_drop) {
-        __stcg(Tb + lane, c0);
-        __stcg(Tb + 32 + lane, c1);
+        const int n0 = lane_node(lane);
+        __stcg(Tb + n0, c0);
+        __stcg(Tb + n0 + 16, c1);
     }
 
     // Queue the neighbours across changed faces, and this brick if it hit the cap.
@@ -610,6 +624,8 @@ static cudaError_t solve_occ(const FimLaunch &p, int block_warps, int occupancy,
     case 1: return launch_solve<1, kFastSqrt>(p, block_warps, grid_out, st);
     case 2: return launch_solve<2, kFastSqrt>(p, block_warps, grid_out, st);
     case 3: return launch_solve<3, kFastSqrt>(p, block_warps, grid_out, st);
+    case 5: return launch_solve<5, kFastSqrt>(p, block_warps, grid_out, st);
+    case 6: return launch_solve<6, kFastSqrt>(p, block_warps, grid_out, st);
     default: return launch_solve<4, kFastSqrt>(p, block_warps, grid_out, st);
     }
 }
