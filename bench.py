@@ -48,6 +48,18 @@ def rank_info():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
+def max_over_ranks(value, dist, device):
+    """The largest of every rank's value (the job's time is its slowest rank's); value
+    itself without a process group."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -263,10 +275,7 @@ def run_ours(args):
         barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
     ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, dist, 'cuda')
     value = world * ns / (ms_max / 1000.0)
 
     # ---- e2e: host buffers through the C ABI ---------------------------------------------
@@ -283,10 +292,7 @@ def run_ours(args):
     e1.record(stream)
     barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dist, 'cuda')
     e2e_value = world * ns / (e2e_ms / 1000.0)
 
     # ---- roofline of the dominant kernel -----------------------------------------------
@@ -319,10 +325,7 @@ def run_ours(args):
     n1.record(stream)
     barrier()
     ngb_ms = n0.elapsed_time(n1) / ngb_steps
-    if dist is not None:
-        t = torch.tensor([ngb_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ngb_ms = float(t.item())
+    ngb_ms = max_over_ranks(ngb_ms, dist, 'cuda')
 
     warm = warm_start_bound(ctx, sv, stream, ngb_steps, barrier, dist, world)
 
@@ -408,10 +411,7 @@ def warm_start_bound(ctx, sv, stream, steps, barrier, dist, world, inflate=0.02)
     w1.record(stream)
     barrier()
     warm_ms = w0.elapsed_time(w1) / steps
-    if dist is not None:
-        t = torch.tensor([warm_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        warm_ms = float(t.item())
+    warm_ms = max_over_ranks(warm_ms, dist, 'cuda')
     out = torch.empty_like(exact)
     ctx.eik_volumes_to(out.data_ptr())
     torch.cuda.synchronize()

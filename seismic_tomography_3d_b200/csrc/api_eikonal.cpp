@@ -20,6 +20,7 @@ const char *static_error_text();  // fim_static.cu
 namespace {
 
 constexpr int kDefaultMaxInner = 16;
+constexpr int kDefaultOccupancy = 5;  // 5 CTAs x 8 warps per SM (48 registers): fastest on config 2
 constexpr float kDefaultChangeTol = 1e-6f;
 constexpr int kDefaultMaxRounds = 1 << 20;
 constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~ seconds of polling, then error
@@ -322,7 +323,7 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     // fields left 0: the autotuned launch shape if there is one, else the defaults
     const int inner0 = ctx->tuned_max_inner > 0 ? ctx->tuned_max_inner : kDefaultMaxInner;
     const int warps0 = ctx->tuned_block_warps > 0 ? ctx->tuned_block_warps : 8;
-    const int occ0 = ctx->tuned_occupancy > 0 ? ctx->tuned_occupancy : 4;
+    const int occ0 = ctx->tuned_occupancy > 0 ? ctx->tuned_occupancy : kDefaultOccupancy;
     c.max_inner = (opts && opts->max_inner > 0) ? opts->max_inner : inner0;
     c.max_rounds = (opts && opts->max_rounds > 0) ? opts->max_rounds : kDefaultMaxRounds;
     c.block_warps = (opts && opts->block_warps > 0) ? opts->block_warps : warps0;
@@ -675,7 +676,7 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
     // untuned defaults while timing (an earlier tuning must not leak into the trials)
     ctx->tuned_block_warps = ctx->tuned_occupancy = ctx->tuned_max_inner = 0;
     const int warps[] = {8, 4};
-    const int occs[] = {4, 5, 6, 3};
+    const int occs[] = {5, 4, 6, 3};
     const int inners[] = {16, 8, 32};
     tomo_eik_opts o{};
     o.op = TOMO_OP_JW;
@@ -684,7 +685,7 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
     int rc = tomo_eik_solve(ctx, nshots, shots, windows, 0, nullptr, nullptr, &o, &st);
     if (rc != TOMO_OK) return rc;
     float best_ms = 0.f, default_ms = 0.f;
-    int trials = 0, bw = 8, bo = 4, bi = kDefaultMaxInner;
+    int trials = 0, bw = 8, bo = kDefaultOccupancy, bi = kDefaultMaxInner;
     for (int w : warps)
         for (int oc : occs)
             for (int in : inners) {
