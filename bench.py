@@ -450,7 +450,18 @@ def run_inversion(args):
     ctx.set_observed(dobs)
     free, total = torch.cuda.mem_get_info()
     iters = []
-    for it in range(inv["iterations"]):
+    for it in range(inv["iterations"] if not args.no_graph else 0):
+        # the whole iteration in one call, replayed from CUDA graphs after the first
+        st = ctx.iteration(sv.shots, sv.receivers, inv["d_tomo"], tk_order=inv["tk_order"], tk_param=inv["tk_param"],
+                           cg_iterations=inv["cg_iterations"], smooth=inv["smooth"],
+                           filter_samples=inv["filter_samples"], standard_deviation=inv["standard_deviation"],
+                           use_graph=True)
+        if it == 0:
+            free, total = torch.cuda.mem_get_info()
+        iters.append({"residual_l2_s": st["residual"], "total_ms": st["ms"], "nnz": st["nnz"],
+                      "activations": st["activations"], "captured": st["captured"], "replayed": st["replayed"],
+                      "cgls_rnorm": st["cg_rnorm"]})
+    for it in range(inv["iterations"] if args.no_graph else 0):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         ev[0].record(stream)
         _, est = ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False)
@@ -479,12 +490,31 @@ def run_inversion(args):
     v_true, v0 = sv.velocity.astype(np.float64), start.astype(np.float64)
     rms = float(np.sqrt(np.mean(((v_est - v_true) / v_true) ** 2)))
     rms0 = float(np.sqrt(np.mean(((v0 - v_true) / v_true) ** 2)))
-    med = {k: statistics.median(i[k] for i in iters) for k in ("eikonal_ms", "jacobian_ms", "cgls_ms", "update_ms",
-                                                                "total_ms")}
+    keys = ("total_ms",) if not args.no_graph else ("eikonal_ms", "jacobian_ms", "cgls_ms", "update_ms", "total_ms")
+    med = {k: statistics.median(i[k] for i in iters) for k in keys}
+    stages = None
+    if not args.no_graph:
+        # one more iteration stage by stage (after the model figures above): where the time goes
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        ev[0].record(stream)
+        ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False)
+        ev[1].record(stream)
+        ctx.build_jacobian(inv["d_tomo"], inv["tk_order"], inv["tk_param"])
+        ev[2].record(stream)
+        ctx.cgls(inv["cg_iterations"], want_x=False)
+        ev[3].record(stream)
+        ctx.model_update(inv["smooth"], inv["filter_samples"], inv["standard_deviation"], want_velocity=False)
+        ev[4].record(stream)
+        torch.cuda.synchronize()
+        stages = dict(zip(("eikonal_ms", "jacobian_ms", "cgls_ms", "update_ms"),
+                          (a.elapsed_time(b) for a, b in zip(ev[:4], ev[1:]))))
+        stages["total_ms"] = ev[0].elapsed_time(ev[4])
+    br = stages or med
     line = {"metric": "device-resident inversion iteration time (config 5)", "value": med["total_ms"], "unit": "ms",
-            "higher_is_better": False, "iterations": len(iters), "breakdown_ms_median": med,
-            "shots_per_s_eikonal": len(sv.shots) / (med["eikonal_ms"] / 1000.0),
-            "cgls_ms_per_iteration": med["cgls_ms"] / inv["cg_iterations"],
+            "higher_is_better": False, "iterations": len(iters), "iteration_ms_median": med["total_ms"],
+            "graph_captured": not args.no_graph, "stage_breakdown_ms": br,
+            "shots_per_s_eikonal": len(sv.shots) / (br["eikonal_ms"] / 1000.0),
+            "cgls_ms_per_iteration": br["cgls_ms"] / inv["cg_iterations"],
             "recovered_model_rms_rel_err": rms, "starting_model_rms_rel_err": rms0,
             "residual_l2_s": [i["residual_l2_s"] for i in iters] + [final_res],
             "hbm_used_gb": (total - free) / 1e9, "per_iteration": iters,
@@ -630,6 +660,8 @@ def main():
                     help="time one config-3 tomography iteration instead (separate JSON line)")
     ap.add_argument("--inversion", action="store_true",
                     help="run the config-5 device-resident inversion instead (separate JSON line)")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="--inversion: call the stages one by one instead of tomo_iteration's CUDA graphs")
     ap.add_argument("--warm-start", action="store_true",
                     help="run the config-4 learned warm start instead (separate JSON line)")
     ap.add_argument("--fields", type=int, default=20000, help="training fields (--warm-start)")

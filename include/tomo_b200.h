@@ -295,6 +295,37 @@ typedef struct {
  * reference updates Eikonal::slowness); velocity_out (host nz*nx*ny) may be NULL. */
 int tomo_model_update(tomo_ctx *ctx, const tomo_update_opts *opts, float *velocity_out);
 
+/* ---------------------------------------------------------- one whole iteration ------ */
+typedef struct {
+    tomo_jacobian_opts jacobian;  /* inversion grid, Tikhonov, ray caps                      */
+    int cg_iterations;            /* CGLS iterations (>= 1)                                   */
+    tomo_update_opts update;      /* model update                                             */
+    tomo_eik_opts eik;            /* eikonal solve (TOMO_OP_JW)                               */
+    int use_graph;                /* 1: capture the iteration in CUDA graphs once, then replay */
+    float nnz_headroom;           /* Jacobian capacity over the first non-zero count (0: 1.25) */
+} tomo_iteration_opts;
+
+typedef struct {
+    double residual;        /* ||dobs - dcal|| of this iteration's forward model            */
+    double cg_rnorm;        /* ||B - A x|| after the last CGLS iteration                     */
+    long long nnz;          /* non-zeros of A = [G; lambda L]                                 */
+    long long activations;  /* brick activations of the eikonal solve                         */
+    int replayed;           /* 1: ran as replays of graphs captured by an earlier call         */
+    int captured;           /* 1: a graph was (re)captured in this call                        */
+    float ms;               /* device time of the iteration                                   */
+} tomo_iteration_stats;
+
+/* One tomography iteration on the device: eikonal solve of the batch with receiver times,
+ * ray tracing into A = [G; lambda L], CGLS on B = [dobs - dcal; 0], model update -- the
+ * body of the reference's loop (src/tomography/tomography_main.cpp:19-30: forward_modeling,
+ * import_cal_data, converged, optimization, model_update).  Needs tomo_set_observed with
+ * nshots x nrec picks.  With use_graph the device work runs as two CUDA graphs captured on
+ * the first call (the second sized by the Jacobian's non-zero count x headroom) and
+ * replayed on later calls; the host only reads the non-zero count in between.  Afterwards
+ * the context holds the new model, the fields, A and x as after the per-stage calls. */
+int tomo_iteration(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows, int nrec,
+                   const tomo_point *receivers, const tomo_iteration_opts *opts, tomo_iteration_stats *stats);
+
 /* The reference's GPU CGLS entry point, sparse_cgls_gpu (src/utils/cgls/cgls.cuh:47):
  * host COO (iA, jA, vA; rows need not be sorted), host B and x, N rows, M columns, NIT
  * iterations, stop when ||A'(B - A x)|| < TOL.  Self-contained (own device buffers);

@@ -168,6 +168,20 @@ def _bind_net(lib):
     lib.tomo_ctx_slowness_device.restype = V
 
 
+class IterationOpts(ctypes.Structure):
+    _fields_ = [("jacobian", JacobianOpts), ("cg_iterations", ctypes.c_int), ("update", UpdateOpts),
+                ("eik", EikOpts), ("use_graph", ctypes.c_int), ("nnz_headroom", ctypes.c_float)]
+
+
+class IterationStats(ctypes.Structure):
+    _fields_ = [("residual", ctypes.c_double), ("cg_rnorm", ctypes.c_double), ("nnz", ctypes.c_longlong),
+                ("activations", ctypes.c_longlong), ("replayed", ctypes.c_int), ("captured", ctypes.c_int),
+                ("ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 def _bind_tomography(lib):
     """Bindings of the tomography half of the ABI."""
     _bind_net(lib)
@@ -183,6 +197,7 @@ def _bind_tomography(lib):
     lib.tomo_cgls.argtypes = [V, I, V, V, P(CglsStats)]
     lib.tomo_model_update.argtypes = [V, P(UpdateOpts), V]
     lib.tomo_sparse_cgls_gpu.argtypes = [V, V, V, V, V, I, I, I, I, ctypes.c_float]
+    lib.tomo_iteration.argtypes = [V, I, P(Point), P(Window), I, P(Point), P(IterationOpts), P(IterationStats)]
 
 
 def sparse_cgls_gpu(iA, jA, vA, B, N, M, nit, tol=0.0):
@@ -408,6 +423,26 @@ class Context:
         v = np.empty(self.shape, np.float32) if want_velocity else None
         self._check(self.lib.tomo_model_update(self.h, ctypes.byref(o), v.ctypes.data if v is not None else None))
         return v
+
+    def iteration(self, shots, receivers, d_tomo, windows=None, tk_order=2, tk_param=0.1, cg_iterations=30,
+                  smooth=True, filter_samples=5, standard_deviation=2.0, reference_masks=True, use_graph=True,
+                  max_ray_steps=0, max_cells_per_ray=0, nnz_headroom=0.0, change_tol=0.0, inner_tol=0.0):
+        """One whole tomography iteration on the device (tomo_iteration); returns its stats."""
+        sp, ns, _s = _points(shots)
+        rp, nr, _r = _points(receivers)
+        wp = _w = None
+        if windows is not None:
+            wp, _w = _windows(windows)
+        o = IterationOpts()
+        o.jacobian = JacobianOpts(*map(float, d_tomo), tk_order, tk_param, max_ray_steps, max_cells_per_ray, 0)
+        o.cg_iterations = cg_iterations
+        o.update = UpdateOpts(int(smooth), filter_samples, standard_deviation, int(reference_masks))
+        o.eik = EikOpts(0, 0, 0, 0, 0, 0, change_tol, inner_tol, 0, 0)
+        o.use_graph = int(use_graph)
+        o.nnz_headroom = nnz_headroom
+        st = IterationStats()
+        self._check(self.lib.tomo_iteration(self.h, ns, sp, wp, nr, rp, ctypes.byref(o), ctypes.byref(st)))
+        return st.as_dict()
 
     def eik_volume(self, shot):
         x0, x1, y0, y1 = self.eik_window(shot)

@@ -9,6 +9,7 @@
 #include "common.cuh"
 #include "context.hpp"
 #include "fsm.cuh"
+#include "internal.hpp"
 
 using tomo::ShotDesc;
 
@@ -235,12 +236,14 @@ int tomo_ctx_create(const tomo_grid *grid, int device, tomo_ctx **out)
 }
 
 void tomo_release_tomography(tomo_ctx *ctx);  // api_tomography.cpp
+void tomo_release_iteration(tomo_ctx *ctx);   // api_iteration.cpp
 
 int tomo_ctx_destroy(tomo_ctx *ctx)
 {
     if (!ctx) return TOMO_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    tomo_release_iteration(ctx);
     tomo_release_tomography(ctx);
     ctx->slow.release();
     ctx->S.release();
@@ -497,6 +500,44 @@ void keep_batch(tomo_ctx *ctx, const Batch &bt, const tomo_point *shots, int nre
 }
 
 }  // namespace
+
+namespace tomo {
+
+int eik_plan(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows, int nrec,
+             const tomo_point *receivers, const tomo_eik_opts *opts, EikPlan &plan)
+{
+    if (nshots < 1 || !shots) return fail(ctx, TOMO_ERR_INVALID_ARG, "nshots must be >= 1 with shot positions");
+    if (nrec < 0 || (nrec > 0 && !receivers)) return fail(ctx, TOMO_ERR_INVALID_ARG, "bad receivers");
+    if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
+    if (opts && opts->op != TOMO_OP_JW) return fail(ctx, TOMO_ERR_INVALID_ARG, "the plan runs the JW operator only");
+    const SolveCfg cfg = solve_cfg(ctx, opts);
+    Batch bt;
+    int rc = make_batch(ctx, nshots, shots, windows, nrec, receivers, bt);
+    if (rc != TOMO_OK) return rc;
+    rc = upload_batch(ctx, bt, nrec, receivers);
+    if (rc != TOMO_OK) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));  // host staging of upload_batch
+    keep_batch(ctx, bt, shots, nrec, receivers);
+    plan.p = fim_params(ctx, bt, cfg, nrec);
+    plan.block_warps = cfg.block_warps;
+    plan.occupancy = cfg.occupancy;
+    plan.ieee_sqrt = cfg.ieee_sqrt;
+    plan.t_total = (size_t)bt.t_total;
+    plan.q_total = (size_t)bt.q_total;
+    return TOMO_OK;
+}
+
+int eik_enqueue(tomo_ctx *ctx, const EikPlan &plan)
+{
+    const FimLaunch &p = plan.p;
+    CK(tomo::fim_init(p.T, plan.t_total, p.qflag, plan.q_total, p.ctrl, p.stats, ctx->stream));
+    CK(tomo::fim_seed(p.shots, p.nshots, p.S, p.gbx, p.gbz, p.T, p.qflag, p.lists, p.local_bits, p.ctrl, ctx->stream));
+    int grid = 0;
+    CK(tomo::fim_solve(p, plan.block_warps, plan.occupancy, plan.ieee_sqrt, &grid, ctx->stream));
+    return TOMO_OK;
+}
+
+}  // namespace tomo
 
 extern "C" {
 

@@ -7,6 +7,7 @@
 #include "cgls.cuh"
 #include "common.cuh"
 #include "context.hpp"
+#include "internal.hpp"
 #include "ray.cuh"
 
 namespace tomo {
@@ -85,27 +86,43 @@ int bits_for(long long n)
 }
 
 // Transposed CSR of (ptr, idx, val) with nrows rows and ncols columns: a stable radix
-// sort of the column keys keeps each column's entries in row order (deterministic).
+// sort of the column keys keeps each column's entries in row order (deterministic).  The
+// sort runs over a fixed capacity `cap` >= nnz (sizes[1], on the device), the padding keyed
+// after every column, so the same launches serve any nnz up to cap.
 template <class Ctx>
-int build_transpose(Ctx *ctx, const int *ptr, const int *idx, const float *val, int nrows, int ncols, long long nnz,
-                    tomo::DevBuf<int> &t_ptr, tomo::DevBuf<int> &t_idx, tomo::DevBuf<float> &t_val,
-                    tomo::DevBuf<int> &k0, tomo::DevBuf<int> &k1, tomo::DevBuf<int> &p0, tomo::DevBuf<int> &p1,
-                    tomo::DevBuf<int> &rows_of, tomo::DevBuf<unsigned char> &temp, cudaStream_t st)
+int transpose_ensure(Ctx *ctx, int ncols, long long cap, tomo::DevBuf<int> &t_ptr, tomo::DevBuf<int> &t_idx,
+                     tomo::DevBuf<float> &t_val, tomo::DevBuf<int> &k0, tomo::DevBuf<int> &k1, tomo::DevBuf<int> &p0,
+                     tomo::DevBuf<int> &p1, tomo::DevBuf<int> &rows_of, tomo::DevBuf<unsigned char> &temp,
+                     cudaStream_t st)
 {
-    CK(k0.ensure((size_t)nnz));
-    CK(k1.ensure((size_t)nnz));
-    CK(p0.ensure((size_t)nnz));
-    CK(p1.ensure((size_t)nnz));
-    CK(rows_of.ensure((size_t)nnz));
+    if (cap >= (1ll << 31) - 1) return fail(ctx, TOMO_ERR_CAPACITY, "Jacobian has more than 2^31 non-zeros");
+    CK(k0.ensure((size_t)cap));
+    CK(k1.ensure((size_t)cap));
+    CK(p0.ensure((size_t)cap));
+    CK(p1.ensure((size_t)cap));
+    CK(rows_of.ensure((size_t)cap));
     CK(t_ptr.ensure((size_t)ncols + 1));
-    CK(t_idx.ensure((size_t)nnz));
-    CK(t_val.ensure((size_t)nnz));
-    CK(tomo::csr_transpose_prepare(ptr, idx, nrows, nnz, k0.ptr, p0.ptr, rows_of.ptr, st));
+    CK(t_idx.ensure((size_t)cap));
+    CK(t_val.ensure((size_t)cap));
     size_t tb = 0;
-    CK(tomo::sort_pairs(k0.ptr, k1.ptr, p0.ptr, p1.ptr, nnz, bits_for(ncols + 1), nullptr, &tb, st));
+    CK(tomo::sort_pairs(k0.ptr, k1.ptr, p0.ptr, p1.ptr, cap, bits_for(ncols + 1), nullptr, &tb, st));
     CK(temp.ensure(tb));
-    CK(tomo::sort_pairs(k0.ptr, k1.ptr, p0.ptr, p1.ptr, nnz, bits_for(ncols + 1), temp.ptr, &tb, st));
-    CK(tomo::csr_transpose_finish(p1.ptr, rows_of.ptr, val, nnz, ncols, k1.ptr, t_ptr.ptr, t_idx.ptr, t_val.ptr, st));
+    return TOMO_OK;
+}
+
+template <class Ctx>
+int transpose_enqueue(Ctx *ctx, const int *ptr, const int *idx, const float *val, int nrows, int ncols,
+                      const long long *sizes, long long cap, tomo::DevBuf<int> &t_ptr, tomo::DevBuf<int> &t_idx,
+                      tomo::DevBuf<float> &t_val, tomo::DevBuf<int> &k0, tomo::DevBuf<int> &k1, tomo::DevBuf<int> &p0,
+                      tomo::DevBuf<int> &p1, tomo::DevBuf<int> &rows_of, tomo::DevBuf<unsigned char> &temp,
+                      cudaStream_t st)
+{
+    CK(tomo::csr_transpose_prepare(ptr, idx, nrows, cap, k0.ptr, p0.ptr, rows_of.ptr, st));
+    CK(tomo::sort_tail(k0.ptr, p0.ptr, sizes, cap, ncols, st));
+    size_t tb = temp.cap;
+    CK(tomo::sort_pairs(k0.ptr, k1.ptr, p0.ptr, p1.ptr, cap, bits_for(ncols + 1), temp.ptr, &tb, st));
+    CK(tomo::csr_transpose_finish(p1.ptr, rows_of.ptr, val, sizes, cap, ncols, k1.ptr, t_ptr.ptr, t_idx.ptr, t_val.ptr,
+                                  st));
     return TOMO_OK;
 }
 
@@ -139,75 +156,87 @@ void tomo_release_tomography(tomo_ctx *ctx)
     for (auto *b : {&ctx->cg_x, &ctx->cg_s, &ctx->cg_r, &ctx->cg_p, &ctx->cg_q}) b->release();
 }
 
-int tomo_build_jacobian(tomo_ctx *ctx, const tomo_jacobian_opts *opts, tomo_jacobian_stats *stats)
+}  // extern "C"
+
+namespace tomo {
+
+int jac_prepare(tomo_ctx *ctx, const tomo_jacobian_opts *opts, JacGeom &jg)
 {
-    if (!ctx) return TOMO_ERR_INVALID_ARG;
     if (!opts || !(opts->dx > 0) || !(opts->dy > 0) || !(opts->dz > 0) || opts->tk_order < 0)
         return fail(ctx, TOMO_ERR_INVALID_ARG, "bad inversion grid / Tikhonov options");
     if (!ctx->have_solve || ctx->nrec < 1) return fail(ctx, TOMO_ERR_STATE, "no eikonal solve with receivers");
-    CK(cudaSetDevice(ctx->device));
     const tomo_grid &g = ctx->g;
     // Least_squares::set_parameters (least_squares.cpp:124-126)
-    const int nzt = (int)((g.nz - 1) * g.dz / opts->dz) + 1;
-    const int nxt = (int)((g.nx - 1) * g.dx / opts->dx) + 1;
-    const int nyt = (int)((g.ny - 1) * g.dy / opts->dy) + 1;
-    const long long M = (long long)nxt * nyt * nzt;
-    const int ord = opts->tk_order;
-    if (M <= ord || M >= (1ll << 30)) return fail(ctx, TOMO_ERR_INVALID_ARG, "inversion grid too small or too large");
-    const long long nrays = (long long)ctx->nshots * ctx->nrec;
-    const long long N = nrays + M - ord;
-    if (N >= (1ll << 31) - 1) return fail(ctx, TOMO_ERR_CAPACITY, "too many rows");
-    const float rayStep = 0.2f * g.dz;
+    jg.nzt = (int)((g.nz - 1) * g.dz / opts->dz) + 1;
+    jg.nxt = (int)((g.nx - 1) * g.dx / opts->dx) + 1;
+    jg.nyt = (int)((g.ny - 1) * g.dy / opts->dy) + 1;
+    jg.M = (long long)jg.nxt * jg.nyt * jg.nzt;
+    jg.ord = opts->tk_order;
+    if (jg.M <= jg.ord || jg.M >= (1ll << 30))
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "inversion grid too small or too large");
+    jg.nrays = (long long)ctx->nshots * ctx->nrec;
+    jg.N = jg.nrays + jg.M - jg.ord;
+    if (jg.N >= (1ll << 31) - 1) return fail(ctx, TOMO_ERR_CAPACITY, "too many rows");
+    jg.tk_entries = (long long)(jg.ord + 1) * (jg.M - jg.ord);
+    jg.rayStep = 0.2f * g.dz;
     const float dmax = std::fmax(g.dx, std::fmax(g.dy, g.dz));
-    const int max_steps = opts->max_ray_steps > 0 ? opts->max_ray_steps
-                                                  : (int)(20.0f * (g.nx + g.ny + g.nz) * dmax / rayStep);
+    jg.max_steps = opts->max_ray_steps > 0 ? opts->max_ray_steps
+                                           : (int)(20.0f * (g.nx + g.ny + g.nz) * dmax / jg.rayStep);
     // Default cap per ray: the reference marches until the source cell with no cap
     // (least_squares.cpp:216-280), so a ray circling a flat spot of the field never ends.
     // A ray of traveltime T is at most T x v_max long; 4x that (plus 256 steps) leaves
     // every terminating ray untouched and stops circling ones early.
-    float steps_per_second = 0.f;
-    if (opts->max_ray_steps <= 0) {
-        const size_t nmodel = (size_t)g.nx * g.ny * g.nz;
-        size_t tb = 0;
-        CK(tomo::reduce_min(ctx->slow.ptr, nullptr, nmodel, nullptr, &tb, ctx->stream));
-        const size_t off = (tb + 255) / 256 * 256;
-        CK(ctx->cub_temp.ensure(off + sizeof(float)));
-        float *smin_d = reinterpret_cast<float *>(ctx->cub_temp.ptr + off);
-        CK(tomo::reduce_min(ctx->slow.ptr, smin_d, nmodel, ctx->cub_temp.ptr, &tb, ctx->stream));
-        float smin = 0.f;
-        CK(cudaMemcpyAsync(&smin, smin_d, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        if (smin > 0.f && std::isfinite(smin)) steps_per_second = kRayLengthFactor / (smin * rayStep);
-    }
-    const int cap_runs = opts->max_cells_per_ray > 0 ? opts->max_cells_per_ray : 1024;
+    jg.ray_cap = opts->max_ray_steps <= 0;
+    jg.cap_runs = opts->max_cells_per_ray > 0 ? opts->max_cells_per_ray : 1024;
+    jg.illum = opts->illumination != 0;
+    jg.dx = opts->dx;
+    jg.dy = opts->dy;
+    jg.dz = opts->dz;
     bool full = true;
     for (const auto &d : ctx->shots_h) full = full && d.wx0 == 0 && d.wy0 == 0 && d.wnx == g.nx && d.wny == g.ny;
-    if (opts->illumination && !full)
-        return fail(ctx, TOMO_ERR_INVALID_ARG, "illumination needs full-model windows");
+    if (jg.illum && !full) return fail(ctx, TOMO_ERR_INVALID_ARG, "illumination needs full-model windows");
 
-    CK(ctx->runs.ensure((size_t)nrays * cap_runs));
+    const long long nrays = jg.nrays;
+    CK(ctx->runs.ensure((size_t)nrays * jg.cap_runs));
     CK(ctx->nuniq.ensure((size_t)nrays + 1));
     CK(ctx->ray_status.ensure((size_t)nrays));
     CK(ctx->ray_steps.ensure((size_t)nrays));
     CK(ctx->final_dist.ensure((size_t)nrays));
     CK(ctx->spos.ensure((size_t)ctx->nshots * 3));
-    CK(ctx->a_ptr.ensure((size_t)N + 1));
+    CK(ctx->a_ptr.ensure((size_t)jg.N + 1));
+    CK(ctx->csr_sizes.ensure(2));
+    CK(ctx->smin.ensure(1));
+    if (jg.illum) CK(ctx->illum.ensure((size_t)g.nx * g.ny * g.nz));
     std::vector<float> sp((size_t)ctx->nshots * 3);
     for (int s = 0; s < ctx->nshots; s++) {
         sp[(size_t)s] = ctx->shot_pos[(size_t)s].x;
         sp[(size_t)ctx->nshots + s] = ctx->shot_pos[(size_t)s].y;
         sp[(size_t)2 * ctx->nshots + s] = ctx->shot_pos[(size_t)s].z;
     }
-    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     CK(cudaMemcpyAsync(ctx->spos.ptr, sp.data(), sp.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-    const size_t npts = (size_t)g.nx * g.ny * g.nz;
-    if (opts->illumination) {
-        CK(ctx->illum.ensure(npts));
-        CK(cudaMemsetAsync(ctx->illum.ptr, 0, npts * sizeof(float), ctx->stream));
-    }
-    CK(cudaMemsetAsync(ctx->nuniq.ptr + nrays, 0, sizeof(int), ctx->stream));
+    // Tikhonov rows lambda * df (least_squares.cpp:412-417)
+    const std::vector<int> df = tk_coefficients(jg.ord);
+    std::vector<float> coef((size_t)jg.ord + 1);
+    for (int k = 0; k <= jg.ord; k++) coef[(size_t)k] = opts->tk_param * (float)df[(size_t)k];
+    CK(ctx->tk_coef.ensure(coef.size()));
+    CK(cudaMemcpyAsync(ctx->tk_coef.ptr, coef.data(), coef.size() * sizeof(float), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    // CUB scratch of the scan and the min-reduction (sizes depend on the counts only)
+    size_t tb = 0;
+    CK(tomo::scan_exclusive(ctx->nuniq.ptr, ctx->a_ptr.ptr, (int)nrays + 1, nullptr, &tb, ctx->stream));
+    CK(ctx->scan_temp.ensure(tb));
+    tb = 0;
+    CK(tomo::reduce_min(ctx->slow.ptr, nullptr, (size_t)g.nx * g.ny * g.nz, nullptr, &tb, ctx->stream));
+    CK(ctx->reduce_temp.ensure(tb));
+    // the sync keeps the host staging vectors alive until the copies are done
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TOMO_OK;
+}
 
-    tomo::RayLaunch rl{};
+RayLaunch ray_launch(tomo_ctx *ctx, const JacGeom &jg)
+{
+    const tomo_grid &g = ctx->g;
+    RayLaunch rl{};
     rl.T = ctx->T.ptr;
     rl.shots = ctx->shots_d.ptr;
     rl.nshots = ctx->nshots;
@@ -220,79 +249,121 @@ int tomo_build_jacobian(tomo_ctx *ctx, const tomo_jacobian_opts *opts, tomo_jaco
     rl.dx = g.dx;
     rl.dy = g.dy;
     rl.dz = g.dz;
-    rl.dxt = opts->dx;
-    rl.dyt = opts->dy;
-    rl.dzt = opts->dz;
-    rl.nxt = nxt;
-    rl.nyt = nyt;
-    rl.nzt = nzt;
-    rl.max_steps = max_steps;
-    rl.steps_per_second = steps_per_second;
-    rl.cap_runs = cap_runs;
+    rl.dxt = jg.dx;
+    rl.dyt = jg.dy;
+    rl.dzt = jg.dz;
+    rl.nxt = jg.nxt;
+    rl.nyt = jg.nyt;
+    rl.nzt = jg.nzt;
+    rl.max_steps = jg.max_steps;
+    rl.smin = jg.ray_cap ? ctx->smin.ptr : nullptr;
+    rl.length_factor = kRayLengthFactor;
+    rl.cap_runs = jg.cap_runs;
     rl.runs = ctx->runs.ptr;
     rl.nuniq = ctx->nuniq.ptr;
     rl.status = ctx->ray_status.ptr;
     rl.steps = ctx->ray_steps.ptr;
     rl.final_dist = ctx->final_dist.ptr;
-    rl.illum = opts->illumination ? ctx->illum.ptr : nullptr;
+    rl.illum = jg.illum ? ctx->illum.ptr : nullptr;
     rl.model_nx = g.nx;
     rl.model_ny = g.ny;
+    return rl;
+}
+
+int jac_march(tomo_ctx *ctx, const JacGeom &jg)
+{
+    const tomo_grid &g = ctx->g;
+    const size_t npts = (size_t)g.nx * g.ny * g.nz;
+    if (jg.illum) CK(cudaMemsetAsync(ctx->illum.ptr, 0, npts * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(ctx->nuniq.ptr + jg.nrays, 0, sizeof(int), ctx->stream));
+    if (jg.ray_cap) {
+        size_t tb = ctx->reduce_temp.cap;
+        CK(tomo::reduce_min(ctx->slow.ptr, ctx->smin.ptr, npts, ctx->reduce_temp.ptr, &tb, ctx->stream));
+    }
+    const RayLaunch rl = ray_launch(ctx, jg);
     CK(tomo::ray_march(rl, ctx->stream));
-    size_t tb = 0;
-    CK(tomo::scan_exclusive(ctx->nuniq.ptr, ctx->a_ptr.ptr, (int)nrays + 1, nullptr, &tb, ctx->stream));
-    CK(ctx->cub_temp.ensure(tb));
-    CK(tomo::scan_exclusive(ctx->nuniq.ptr, ctx->a_ptr.ptr, (int)nrays + 1, ctx->cub_temp.ptr, &tb, ctx->stream));
-    int nnz_g = 0;
-    CK(cudaMemcpyAsync(&nnz_g, ctx->a_ptr.ptr + nrays, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    const long long nL = M - ord;
-    const long long nnz = (long long)nnz_g + (long long)(ord + 1) * nL;
-    if (nnz >= (1ll << 31) - 1) return fail(ctx, TOMO_ERR_CAPACITY, "Jacobian has more than 2^31 non-zeros");
-    CK(ctx->a_idx.ensure((size_t)nnz));
-    CK(ctx->a_val.ensure((size_t)nnz));
+    size_t tb = ctx->scan_temp.cap;
+    CK(tomo::scan_exclusive(ctx->nuniq.ptr, ctx->a_ptr.ptr, (int)jg.nrays + 1, ctx->scan_temp.ptr, &tb, ctx->stream));
+    CK(tomo::csr_sizes(ctx->a_ptr.ptr, (int)jg.nrays, jg.tk_entries, ctx->csr_sizes.ptr, ctx->stream));
+    return TOMO_OK;
+}
+
+int jac_ensure(tomo_ctx *ctx, const JacGeom &jg, long long cap)
+{
+    CK(ctx->a_idx.ensure((size_t)cap));
+    CK(ctx->a_val.ensure((size_t)cap));
+    return transpose_ensure(ctx, (int)jg.M, cap, ctx->t_ptr, ctx->t_idx, ctx->t_val, ctx->sort_keys,
+                            ctx->sort_keys_out, ctx->sort_pos, ctx->sort_pos_out, ctx->rows_of, ctx->sort_temp,
+                            ctx->stream);
+}
+
+int jac_emit(tomo_ctx *ctx, const JacGeom &jg, long long cap)
+{
+    const RayLaunch rl = ray_launch(ctx, jg);
     CK(tomo::ray_emit(rl, ctx->a_ptr.ptr, ctx->a_idx.ptr, ctx->a_val.ptr, ctx->stream));
-    // Tikhonov rows lambda * df (least_squares.cpp:412-417)
-    const std::vector<int> df = tk_coefficients(ord);
-    std::vector<float> coef((size_t)ord + 1);
-    for (int k = 0; k <= ord; k++) coef[(size_t)k] = opts->tk_param * (float)df[(size_t)k];
-    CK(ctx->tk_coef.ensure(coef.size()));
-    CK(cudaMemcpyAsync(ctx->tk_coef.ptr, coef.data(), coef.size() * sizeof(float), cudaMemcpyHostToDevice,
-                       ctx->stream));
-    CK(tomo::tk_rows((int)nrays, nnz_g, (int)M, ord, ctx->tk_coef.ptr, ctx->a_ptr.ptr, ctx->a_idx.ptr, ctx->a_val.ptr,
-                     ctx->stream));
-    int rc = build_transpose(ctx, ctx->a_ptr.ptr, ctx->a_idx.ptr, ctx->a_val.ptr, (int)N, (int)M, nnz, ctx->t_ptr,
-                             ctx->t_idx, ctx->t_val, ctx->sort_keys, ctx->sort_keys_out, ctx->sort_pos,
-                             ctx->sort_pos_out, ctx->rows_of, ctx->cub_temp, ctx->stream);
+    CK(tomo::tk_rows((int)jg.nrays, ctx->csr_sizes.ptr, (int)jg.M, jg.ord, ctx->tk_coef.ptr, ctx->a_ptr.ptr,
+                     ctx->a_idx.ptr, ctx->a_val.ptr, ctx->stream));
+    return transpose_enqueue(ctx, ctx->a_ptr.ptr, ctx->a_idx.ptr, ctx->a_val.ptr, (int)jg.N, (int)jg.M,
+                             ctx->csr_sizes.ptr, cap, ctx->t_ptr, ctx->t_idx, ctx->t_val, ctx->sort_keys,
+                             ctx->sort_keys_out, ctx->sort_pos, ctx->sort_pos_out, ctx->rows_of, ctx->sort_temp,
+                             ctx->stream);
+}
+
+void jac_commit(tomo_ctx *ctx, const JacGeom &jg, long long nnz_g, long long nnz)
+{
+    ctx->n_data = (int)jg.nrays;
+    ctx->n_model = (int)jg.M;
+    ctx->n_rows = (int)jg.N;
+    ctx->tk_order = jg.ord;
+    ctx->nxt = jg.nxt;
+    ctx->nyt = jg.nyt;
+    ctx->nzt = jg.nzt;
+    ctx->dxt = jg.dx;
+    ctx->dyt = jg.dy;
+    ctx->dzt = jg.dz;
+    ctx->nnz_g = nnz_g;
+    ctx->nnz = nnz;
+    ctx->have_jacobian = true;
+    ctx->have_illum = jg.illum;
+    ctx->have_x = false;
+}
+
+}  // namespace tomo
+
+extern "C" {
+
+int tomo_build_jacobian(tomo_ctx *ctx, const tomo_jacobian_opts *opts, tomo_jacobian_stats *stats)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    CK(cudaSetDevice(ctx->device));
+    tomo::JacGeom jg{};
+    int rc = tomo::jac_prepare(ctx, opts, jg);
+    if (rc != TOMO_OK) return rc;
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    rc = tomo::jac_march(ctx, jg);
+    if (rc != TOMO_OK) return rc;
+    long long sizes[2] = {0, 0};
+    CK(cudaMemcpyAsync(sizes, ctx->csr_sizes.ptr, sizeof(sizes), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const long long nnz_g = sizes[0], nnz = sizes[1];
+    rc = tomo::jac_ensure(ctx, jg, nnz);
+    if (rc == TOMO_OK) rc = tomo::jac_emit(ctx, jg, nnz);
     if (rc != TOMO_OK) return rc;
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    const long long nrays = jg.nrays;
     std::vector<int> st((size_t)nrays), steps((size_t)nrays);
     CK(cudaMemcpyAsync(st.data(), ctx->ray_status.ptr, st.size() * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(steps.data(), ctx->ray_steps.ptr, steps.size() * sizeof(int), cudaMemcpyDeviceToHost,
                        ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-
-    ctx->n_data = (int)nrays;
-    ctx->n_model = (int)M;
-    ctx->n_rows = (int)N;
-    ctx->tk_order = ord;
-    ctx->nxt = nxt;
-    ctx->nyt = nyt;
-    ctx->nzt = nzt;
-    ctx->dxt = opts->dx;
-    ctx->dyt = opts->dy;
-    ctx->dzt = opts->dz;
-    ctx->nnz_g = nnz_g;
-    ctx->nnz = nnz;
-    ctx->have_jacobian = true;
-    ctx->have_illum = opts->illumination != 0;
-    ctx->have_x = false;
+    tomo::jac_commit(ctx, jg, nnz_g, nnz);
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
-        stats->nx = nxt;
-        stats->ny = nyt;
-        stats->nz = nzt;
-        stats->rows = N;
-        stats->cols = M;
+        stats->nx = jg.nxt;
+        stats->ny = jg.nyt;
+        stats->nz = jg.nzt;
+        stats->rows = jg.N;
+        stats->cols = jg.M;
         stats->nnz_rays = nnz_g;
         stats->nnz = nnz;
         stats->rays = nrays;
@@ -447,16 +518,13 @@ int cuda_fail(Plain *c, cudaError_t e, const char *where)
 
 extern "C" {
 
-int tomo_cgls(tomo_ctx *ctx, int iterations, float *x_out, double *history, tomo_cgls_stats *stats)
+}  // extern "C"
+
+namespace tomo {
+
+int cgls_prepare(tomo_ctx *ctx, int iterations)
 {
-    if (!ctx) return TOMO_ERR_INVALID_ARG;
-    if (iterations < 0) return fail(ctx, TOMO_ERR_INVALID_ARG, "iterations < 0");
-    if (!ctx->have_jacobian) return fail(ctx, TOMO_ERR_STATE, "no Jacobian (tomo_build_jacobian)");
-    if (!ctx->have_dobs) return fail(ctx, TOMO_ERR_STATE, "no observed data (tomo_set_observed)");
-    if (ctx->n_dobs != ctx->n_data)
-        return fail(ctx, TOMO_ERR_INVALID_ARG, "observed data size does not match the Jacobian's rays");
-    CK(cudaSetDevice(ctx->device));
-    const int N = ctx->n_rows, M = ctx->n_model, nd = ctx->n_data;
+    const int N = ctx->n_rows, M = ctx->n_model;
     CK(ctx->rhs.ensure((size_t)N));
     CK(ctx->x.ensure((size_t)M));
     CK(ctx->cg_x.ensure((size_t)M));
@@ -466,27 +534,126 @@ int tomo_cgls(tomo_ctx *ctx, int iterations, float *x_out, double *history, tomo
     CK(ctx->cg_p.ensure((size_t)M));
     CK(ctx->hist.ensure((size_t)(iterations > 0 ? iterations : 1)));
     CK(ctx->norm2.ensure(1));
-    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    int grid = 0;
+    CK(tomo::cgls_grid(&grid));
+    CK(ctx->partials.ensure((size_t)grid * 3));
+    CK(ctx->cg_ctrl.ensure(tomo::kCtrlWords));
+    return TOMO_OK;
+}
+
+int cgls_enqueue(tomo_ctx *ctx, int iterations)
+{
+    const int N = ctx->n_rows, M = ctx->n_model, nd = ctx->n_data;
     // B = [dobs - dcal ; 0] (least_squares.cpp:335-336)
     CK(tomo::data_residual(ctx->dobs.ptr, ctx->t_recv.ptr, ctx->rhs.ptr, nd, N, ctx->norm2.ptr, ctx->stream));
-    int iters = 0;
-    int rc = run_cgls(ctx, N, M, ctx->a_ptr.ptr, ctx->a_idx.ptr, ctx->a_val.ptr, ctx->t_ptr.ptr, ctx->t_idx.ptr,
-                      ctx->t_val.ptr, ctx->rhs.ptr, ctx->cg_x.ptr, ctx->cg_s.ptr, ctx->cg_r.ptr, ctx->cg_p.ptr,
-                      ctx->cg_q.ptr, ctx->x.ptr, ctx->partials, ctx->hist.ptr, ctx->cg_ctrl, iterations, 0.0, ctx->stream, &iters);
+    CK(cudaMemsetAsync(ctx->cg_ctrl.ptr, 0, tomo::kCtrlWords * sizeof(unsigned), ctx->stream));
+    int grid = 0;
+    CK(tomo::cgls_grid(&grid));
+    tomo::CglsLaunch cl{};
+    cl.N = N;
+    cl.M = M;
+    cl.a_ptr = ctx->a_ptr.ptr;
+    cl.a_idx = ctx->a_idx.ptr;
+    cl.a_val = ctx->a_val.ptr;
+    cl.t_ptr = ctx->t_ptr.ptr;
+    cl.t_idx = ctx->t_idx.ptr;
+    cl.t_val = ctx->t_val.ptr;
+    cl.B = ctx->rhs.ptr;
+    cl.x = ctx->cg_x.ptr;
+    cl.x32 = ctx->x.ptr;
+    cl.s = ctx->cg_s.ptr;
+    cl.r = ctx->cg_r.ptr;
+    cl.p = ctx->cg_p.ptr;
+    cl.q = ctx->cg_q.ptr;
+    cl.partials = ctx->partials.ptr;
+    cl.hist = ctx->hist.ptr;
+    cl.ctrl = ctx->cg_ctrl.ptr;
+    cl.nit = iterations;
+    cl.tol = 0.0;
+    cl.spin_limit = kSpinLimit;
+    CK(tomo::cgls_run(cl, grid, ctx->stream));
+    return TOMO_OK;
+}
+
+int update_prepare(tomo_ctx *ctx, const tomo_update_opts *opts)
+{
+    const int smooth = opts ? opts->smooth : 1;
+    const int samples = opts ? opts->filter_samples : 5;
+    const float stdv = opts ? opts->standard_deviation : 2.0f;
+    if (smooth && (samples < 1 || samples % 2 == 0))
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "filter_samples must be odd and >= 1");
+    const tomo_grid &g = ctx->g;
+    const size_t n = (size_t)g.nx * g.ny * g.nz;
+    CK(ctx->dm.ensure(n));
+    if (smooth) {
+        const std::vector<float> k = gaussian_weights(samples, stdv);
+        CK(ctx->gauss_kernel.ensure(k.size()));
+        CK(cudaMemcpyAsync(ctx->gauss_kernel.ptr, k.data(), k.size() * sizeof(float), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(ctx->dm_smooth.ensure(n));
+        CK(cudaStreamSynchronize(ctx->stream));  // k is a host temporary
+    }
+    return TOMO_OK;
+}
+
+// dm from the CGLS solution, optional smoothing, slowness += dm, re-brick (velocity_out:
+// device array or nullptr).
+int update_enqueue_v(tomo_ctx *ctx, const tomo_update_opts *opts, float *velocity_out)
+{
+    const int smooth = opts ? opts->smooth : 1;
+    const int samples = opts ? opts->filter_samples : 5;
+    const int ref_masks = opts ? opts->use_reference_masks : 1;
+    const tomo_grid &g = ctx->g;
+    const tomo::UpdateMasks m = ref_masks ? reference_masks() : tomo::UpdateMasks{0, 0, 0, 0, 0, 0, 0, 0};
+    CK(tomo::model_dm(ctx->x.ptr, ctx->dm.ptr, g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, ctx->dxt, ctx->dyt, ctx->dzt,
+                      ctx->nxt, ctx->nyt, ctx->nzt, m, ctx->stream));
+    const float *dm = ctx->dm.ptr;
+    if (smooth) {
+        CK(tomo::gaussian_smooth(ctx->dm.ptr, ctx->dm_smooth.ptr, g.nx, g.ny, g.nz, samples, ctx->gauss_kernel.ptr,
+                                 ctx->stream));
+        dm = ctx->dm_smooth.ptr;
+    }
+    CK(tomo::model_apply(ctx->slow.ptr, dm, velocity_out, g.nx, g.ny, g.nz, m, ctx->stream));
+    return tomo::rebrick_model(ctx);
+}
+
+int update_enqueue(tomo_ctx *ctx, const tomo_update_opts *opts) { return update_enqueue_v(ctx, opts, nullptr); }
+
+}  // namespace tomo
+
+extern "C" {
+
+int tomo_cgls(tomo_ctx *ctx, int iterations, float *x_out, double *history, tomo_cgls_stats *stats)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (iterations < 0) return fail(ctx, TOMO_ERR_INVALID_ARG, "iterations < 0");
+    if (!ctx->have_jacobian) return fail(ctx, TOMO_ERR_STATE, "no Jacobian (tomo_build_jacobian)");
+    if (!ctx->have_dobs) return fail(ctx, TOMO_ERR_STATE, "no observed data (tomo_set_observed)");
+    if (ctx->n_dobs != ctx->n_data)
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "observed data size does not match the Jacobian's rays");
+    CK(cudaSetDevice(ctx->device));
+    const int M = ctx->n_model;
+    int rc = tomo::cgls_prepare(ctx, iterations);
+    if (rc != TOMO_OK) return rc;
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    rc = tomo::cgls_enqueue(ctx, iterations);
     if (rc != TOMO_OK) return rc;
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     std::vector<double> h((size_t)(iterations > 0 ? iterations : 1), 0.0);
     double b2 = 0.0;
+    unsigned words[tomo::kCtrlWords];
+    CK(cudaMemcpyAsync(words, ctx->cg_ctrl.ptr, sizeof(words), cudaMemcpyDeviceToHost, ctx->stream));
     if (iterations > 0)
         CK(cudaMemcpyAsync(h.data(), ctx->hist.ptr, (size_t)iterations * sizeof(double), cudaMemcpyDeviceToHost,
                            ctx->stream));
     CK(cudaMemcpyAsync(&b2, ctx->norm2.ptr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (x_out) CK(cudaMemcpyAsync(x_out, ctx->x.ptr, (size_t)M * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (words[tomo::kErr] != 0) return fail(ctx, TOMO_ERR_TIMEOUT, "CGLS: device barrier wait timed out");
     if (history && iterations > 0) std::memcpy(history, h.data(), (size_t)iterations * sizeof(double));
     ctx->have_x = true;
     if (stats) {
-        stats->iterations = iters;
+        stats->iterations = (int)words[tomo::kRounds];
         stats->rnorm0 = std::sqrt(b2);
         stats->rnorm = iterations > 0 ? h[(size_t)iterations - 1] : std::sqrt(b2);
         cudaEventElapsedTime(&stats->ms, ctx->ev[0], ctx->ev[1]);
@@ -498,37 +665,16 @@ int tomo_model_update(tomo_ctx *ctx, const tomo_update_opts *opts, float *veloci
 {
     if (!ctx) return TOMO_ERR_INVALID_ARG;
     if (!ctx->have_x) return fail(ctx, TOMO_ERR_STATE, "no CGLS solution (tomo_cgls)");
-    const int smooth = opts ? opts->smooth : 1;
-    const int samples = opts ? opts->filter_samples : 5;
-    const float stdv = opts ? opts->standard_deviation : 2.0f;
-    const int ref_masks = opts ? opts->use_reference_masks : 1;
-    if (smooth && (samples < 1 || samples % 2 == 0))
-        return fail(ctx, TOMO_ERR_INVALID_ARG, "filter_samples must be odd and >= 1");
     CK(cudaSetDevice(ctx->device));
-    const tomo_grid &g = ctx->g;
-    const size_t n = (size_t)g.nx * g.ny * g.nz;
-    const tomo::UpdateMasks m = ref_masks ? reference_masks() : tomo::UpdateMasks{0, 0, 0, 0, 0, 0, 0, 0};
-    CK(ctx->dm.ensure(n));
-    CK(tomo::model_dm(ctx->x.ptr, ctx->dm.ptr, g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, ctx->dxt, ctx->dyt, ctx->dzt,
-                      ctx->nxt, ctx->nyt, ctx->nzt, m, ctx->stream));
-    const float *dm = ctx->dm.ptr;
-    if (smooth) {
-        const std::vector<float> k = gaussian_weights(samples, stdv);
-        CK(ctx->gauss_kernel.ensure(k.size()));
-        CK(cudaMemcpyAsync(ctx->gauss_kernel.ptr, k.data(), k.size() * sizeof(float), cudaMemcpyHostToDevice,
-                           ctx->stream));
-        CK(ctx->dm_smooth.ensure(n));
-        CK(tomo::gaussian_smooth(ctx->dm.ptr, ctx->dm_smooth.ptr, g.nx, g.ny, g.nz, samples, ctx->gauss_kernel.ptr,
-                                 ctx->stream));
-        dm = ctx->dm_smooth.ptr;
-    }
+    const size_t n = (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz;
+    int rc = tomo::update_prepare(ctx, opts);
+    if (rc != TOMO_OK) return rc;
     float *vel = nullptr;
     if (velocity_out) {
         CK(ctx->vel_out.ensure(n));
         vel = ctx->vel_out.ptr;
     }
-    CK(tomo::model_apply(ctx->slow.ptr, dm, vel, g.nx, g.ny, g.nz, m, ctx->stream));
-    int rc = tomo::rebrick_model(ctx);
+    rc = tomo::update_enqueue_v(ctx, opts, vel);
     if (rc != TOMO_OK) return rc;
     if (velocity_out)
         CK(cudaMemcpyAsync(velocity_out, vel, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
@@ -562,9 +708,11 @@ int tomo_sparse_cgls_gpu(const int *iA, const int *jA, const float *vA, const fl
     tomo::DevBuf<double> partials;
     tomo::DevBuf<unsigned> ctrl;
     tomo::DevBuf<unsigned char> temp;
+    tomo::DevBuf<long long> sizes;
     cudaStream_t st = nullptr;
     int rc = TOMO_OK;
     auto cleanup = [&]() {
+        sizes.release();
         for (auto *b : {&a_ptr, &a_idx, &t_ptr, &t_idx, &k0, &k1, &p0, &p1, &rows_of}) b->release();
         for (auto *b : {&a_val, &t_val, &dB, &dx_}) b->release();
         for (auto *b : {&x64, &s, &r, &p, &q}) b->release();
@@ -589,8 +737,13 @@ int tomo_sparse_cgls_gpu(const int *iA, const int *jA, const float *vA, const fl
         CK(cudaMemcpyAsync(a_idx.ptr, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(a_val.ptr, val.data(), val.size() * sizeof(float), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(dB.ptr, B, (size_t)N * sizeof(float), cudaMemcpyHostToDevice, st));
-        int r2 = build_transpose(ctx, a_ptr.ptr, a_idx.ptr, a_val.ptr, N, M, NNZ, t_ptr, t_idx, t_val, k0, k1, p0, p1,
-                                 rows_of, temp, st);
+        const long long hs[2] = {NNZ, NNZ};
+        CK(sizes.ensure(2));
+        CK(cudaMemcpyAsync(sizes.ptr, hs, sizeof(hs), cudaMemcpyHostToDevice, st));
+        int r2 = transpose_ensure(ctx, M, NNZ, t_ptr, t_idx, t_val, k0, k1, p0, p1, rows_of, temp, st);
+        if (r2 == TOMO_OK)
+            r2 = transpose_enqueue(ctx, a_ptr.ptr, a_idx.ptr, a_val.ptr, N, M, sizes.ptr, NNZ, t_ptr, t_idx, t_val, k0,
+                                   k1, p0, p1, rows_of, temp, st);
         if (r2 != TOMO_OK) return r2;
         r2 = run_cgls(ctx, N, M, a_ptr.ptr, a_idx.ptr, a_val.ptr, t_ptr.ptr, t_idx.ptr, t_val.ptr, dB.ptr, x64.ptr,
                       s.ptr, r.ptr, p.ptr, q.ptr, dx_.ptr, partials, nullptr, ctrl, NIT, (double)TOL, st, nullptr);

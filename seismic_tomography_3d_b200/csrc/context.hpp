@@ -37,6 +37,15 @@ struct DevBuf {
 
 struct Jacobian;  // ray tracing output (ray.cu)
 
+// CUDA graphs of tomo_iteration (api_iteration.cpp) and what they were captured with.
+struct IterGraphs {
+    cudaGraphExec_t a = nullptr, b = nullptr;
+    std::vector<char> key_a, key_b;  // options, sizes and device addresses baked in
+    long long cap = 0;               // Jacobian capacity graph B was built for
+    unsigned long long *pinned = nullptr;
+    bool broken = false;             // capture refused once: run eagerly from then on
+};
+
 }  // namespace tomo
 
 struct tomo_ctx {
@@ -85,7 +94,9 @@ struct tomo_ctx {
     tomo::DevBuf<int> a_ptr, a_idx, t_ptr, t_idx;
     tomo::DevBuf<float> a_val, t_val;
     tomo::DevBuf<int> sort_keys, sort_keys_out, sort_pos, sort_pos_out, rows_of;
-    tomo::DevBuf<unsigned char> cub_temp;
+    tomo::DevBuf<unsigned char> cub_temp, scan_temp, reduce_temp, sort_temp;
+    tomo::DevBuf<long long> csr_sizes;  // [0] ray non-zeros, [1] all non-zeros (device side)
+    tomo::DevBuf<float> smin;           // smallest slowness of the model (per-ray cap)
     int n_data = 0, n_model = 0, n_rows = 0, tk_order = 0;
     int nxt = 0, nyt = 0, nzt = 0;
     float dxt = 0, dyt = 0, dzt = 0;
@@ -99,4 +110,5 @@ struct tomo_ctx {
     tomo::DevBuf<float> dm, dm_smooth, vel_out, gauss_kernel;
     bool have_dobs = false, have_x = false;
     int n_dobs = 0;
+    tomo::IterGraphs iter;
 };

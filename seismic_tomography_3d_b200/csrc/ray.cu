@@ -70,11 +70,14 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
             L = p.max_steps;   // skip the march
         }
         int cap = p.max_steps;
-        if (p.steps_per_second > 0.0f && L == 0) {
+        if (p.smin && L == 0) {
             const float t0 = t_exp(p.T, d, p.nz, trunc_div(zi, p.dz) + 1, trunc_div(xi, p.dx) + 1,
                                    trunc_div(yi, p.dy) + 1);
-            const float c = t0 * p.steps_per_second + 256.0f;
-            if (c < (float)cap) cap = (int)c;
+            const float smin = *p.smin;
+            if (smin > 0.0f) {
+                const float c = t0 * (p.length_factor / (smin * rayStep)) + 256.0f;
+                if (c < (float)cap) cap = (int)c;
+            }
         }
         const float two_dz = fmul(2.0f, p.dz), two_dx = fmul(2.0f, p.dx), two_dy = fmul(2.0f, p.dy);
         while (L < cap) {
@@ -188,9 +191,19 @@ __global__ void __launch_bounds__(128) k_ray_emit(RayLaunch p, const int *row_pt
 }
 
 // Least_squares::tk_reg_matrix (:358-422): row n_data + t holds lambda*df[k] at column t+k.
-__global__ void k_tk_rows(int n_data_rows, long long nnz_g, int n_model, int tk_order, const float *coef, int *row_ptr,
-                          int *cols, float *vals)
+// sizes[0] = ray non-zeros (the scan total), sizes[1] = all non-zeros with the Tikhonov rows
+__global__ void k_csr_sizes(const int *row_ptr, int n_data_rows, long long tk_entries, long long *sizes)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sizes[0] = row_ptr[n_data_rows];
+        sizes[1] = sizes[0] + tk_entries;
+    }
+}
+
+__global__ void k_tk_rows(int n_data_rows, const long long *sizes, int n_model, int tk_order, const float *coef,
+                          int *row_ptr, int *cols, float *vals)
+{
+    const long long nnz_g = sizes[0];
     const int e = tk_order + 1;
     const int nL = n_model - tk_order;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t <= nL; t += gridDim.x * blockDim.x) {
@@ -213,9 +226,22 @@ __global__ void k_transpose_prepare(const int *row_ptr, const int *cols, int nro
         }
 }
 
-__global__ void k_transpose_finish(const int *sorted_pos, const int *rows_of, const float *vals, long long nnz, int ncols,
-                                   const int *sorted_keys, int *t_ptr, int *t_rows, float *t_vals)
+// Sort padding: entries [nnz, cap) get the key ncols (after every column) and their own
+// position, so a sort over a fixed capacity leaves the real entries in front, in order.
+__global__ void k_sort_tail(int *keys, int *pos, const long long *sizes, long long cap, int ncols)
 {
+    for (long long k = sizes[1] + blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cap;
+         k += (long long)gridDim.x * blockDim.x) {
+        keys[k] = ncols;
+        pos[k] = (int)k;
+    }
+}
+
+__global__ void k_transpose_finish(const int *sorted_pos, const int *rows_of, const float *vals,
+                                   const long long *sizes, int ncols, const int *sorted_keys, int *t_ptr, int *t_rows,
+                                   float *t_vals)
+{
+    const long long nnz = sizes[1];
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nnz; k += (long long)gridDim.x * blockDim.x) {
         const int src = sorted_pos[k];
         t_rows[k] = rows_of[src];
@@ -249,11 +275,23 @@ cudaError_t ray_emit(const RayLaunch &p, const int *row_ptr, int *cols, float *v
     return cudaGetLastError();
 }
 
-cudaError_t tk_rows(int n_data_rows, long long nnz_g, int n_model, int tk_order, const float *coef, int *row_ptr,
+cudaError_t csr_sizes(const int *row_ptr, int n_data_rows, long long tk_entries, long long *sizes, cudaStream_t st)
+{
+    k_csr_sizes<<<1, 32, 0, st>>>(row_ptr, n_data_rows, tk_entries, sizes);
+    return cudaGetLastError();
+}
+
+cudaError_t tk_rows(int n_data_rows, const long long *sizes, int n_model, int tk_order, const float *coef, int *row_ptr,
                     int *cols, float *vals, cudaStream_t st)
 {
-    k_tk_rows<<<grid_for(n_model + 1, 256), 256, 0, st>>>(n_data_rows, nnz_g, n_model, tk_order, coef, row_ptr, cols,
+    k_tk_rows<<<grid_for(n_model + 1, 256), 256, 0, st>>>(n_data_rows, sizes, n_model, tk_order, coef, row_ptr, cols,
                                                           vals);
+    return cudaGetLastError();
+}
+
+cudaError_t sort_tail(int *keys, int *pos, const long long *sizes, long long cap, int ncols, cudaStream_t st)
+{
+    k_sort_tail<<<grid_for(cap > 0 ? cap : 1, 256), 256, 0, st>>>(keys, pos, sizes, cap, ncols);
     return cudaGetLastError();
 }
 
@@ -265,10 +303,11 @@ cudaError_t csr_transpose_prepare(const int *row_ptr, const int *cols, int nrows
     return cudaGetLastError();
 }
 
-cudaError_t csr_transpose_finish(const int *sorted_pos, const int *rows_of, const float *vals, long long nnz, int ncols,
-                                 const int *sorted_keys, int *t_ptr, int *t_rows, float *t_vals, cudaStream_t st)
+cudaError_t csr_transpose_finish(const int *sorted_pos, const int *rows_of, const float *vals, const long long *sizes,
+                                 long long cap, int ncols, const int *sorted_keys, int *t_ptr, int *t_rows,
+                                 float *t_vals, cudaStream_t st)
 {
-    k_transpose_finish<<<grid_for(nnz > 0 ? nnz : 1, 256), 256, 0, st>>>(sorted_pos, rows_of, vals, nnz, ncols,
+    k_transpose_finish<<<grid_for(cap > 0 ? cap : 1, 256), 256, 0, st>>>(sorted_pos, rows_of, vals, sizes, ncols,
                                                                         sorted_keys, t_ptr, t_rows, t_vals);
     return cudaGetLastError();
 }

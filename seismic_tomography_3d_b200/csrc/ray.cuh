@@ -31,8 +31,9 @@ struct RayLaunch {
     float dxt, dyt, dzt;  // inversion cell size
     int nxt, nyt, nzt;    // inversion grid
     int max_steps;
-    float steps_per_second;  // > 0: a ray also stops (capped) after T(start node) x this + 256
-                             // steps -- a ray of traveltime T cannot be longer than T x v_max
+    const float *smin;       // device: smallest slowness of the model, or nullptr.  Given, a ray
+    float length_factor;     // also stops (capped) after length_factor x T(start) / smin / step
+                             // + 256 steps -- a ray of traveltime T is at most T x v_max long
     int cap_runs;         // per-ray capacity of distinct cells
     uint2 *runs;          // nrays*cap_runs (cell, count), sorted by cell on exit
     int *nuniq;           // per ray: distinct cells
@@ -44,8 +45,11 @@ struct RayLaunch {
 
 cudaError_t ray_march(const RayLaunch &p, cudaStream_t st);
 cudaError_t ray_emit(const RayLaunch &p, const int *row_ptr, int *cols, float *vals, cudaStream_t st);
-cudaError_t tk_rows(int n_data_rows, long long nnz_g, int n_model, int tk_order, const float *coef, int *row_ptr,
+// sizes[0] = row_ptr[n_data_rows] (ray non-zeros), sizes[1] = sizes[0] + tk_entries
+cudaError_t csr_sizes(const int *row_ptr, int n_data_rows, long long tk_entries, long long *sizes, cudaStream_t st);
+cudaError_t tk_rows(int n_data_rows, const long long *sizes, int n_model, int tk_order, const float *coef, int *row_ptr,
                     int *cols, float *vals, cudaStream_t st);
+cudaError_t sort_tail(int *keys, int *pos, const long long *sizes, long long cap, int ncols, cudaStream_t st);
 cudaError_t csr_transpose_prepare(const int *row_ptr, const int *cols, int nrows, long long nnz, int *keys,
                                   int *pos, int *rows_of, cudaStream_t st);
 // CUB device-wide primitives (temp == nullptr queries *temp_bytes).
@@ -53,7 +57,8 @@ cudaError_t scan_exclusive(const int *in, int *out, int n, void *temp, size_t *t
 cudaError_t reduce_min(const float *in, float *out, size_t n, void *temp, size_t *temp_bytes, cudaStream_t st);
 cudaError_t sort_pairs(const int *keys_in, int *keys_out, const int *vals_in, int *vals_out, long long n, int key_bits,
                        void *temp, size_t *temp_bytes, cudaStream_t st);
-cudaError_t csr_transpose_finish(const int *sorted_pos, const int *rows_of, const float *vals, long long nnz, int ncols,
-                                 const int *sorted_keys, int *t_ptr, int *t_rows, float *t_vals, cudaStream_t st);
+cudaError_t csr_transpose_finish(const int *sorted_pos, const int *rows_of, const float *vals, const long long *sizes,
+                                 long long cap, int ncols, const int *sorted_keys, int *t_ptr, int *t_rows,
+                                 float *t_vals, cudaStream_t st);
 
 }  // namespace tomo

@@ -1,0 +1,89 @@
+"""tomo_iteration: a whole tomography iteration in one call, eager or replayed from CUDA
+graphs, against the same stages called one by one (tomo_eik_solve, tomo_build_jacobian,
+tomo_cgls, tomo_model_update).  The eikonal runs to its exact FP32 fixed point
+(change_tol < 0) so that the three paths see the same fields; the updated models must agree
+to 1e-5 relative RMS, and the second graph call must be a pure replay."""
+import numpy as np
+import pytest
+
+from seismic_tomography_3d_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+H = 25.0
+D = (100.0, 100.0, 100.0)
+
+
+@pytest.fixture(scope="module")
+def survey():
+    nx, ny, nz = 48, 44, 24
+    rng = np.random.default_rng(8)
+    true_v = wl.layered_model(rng, nx, ny, nz, H) * wl._anomalies(rng, nx, ny, nz, H, 3, sigma=3 * H)
+    start = wl.gradient_model(nx, ny, nz, H, 1500.0, 1.0)
+    shots = np.array([(x * H, y * H, 0.0) for x in (6, 24, 40) for y in (5, 22, 38)], np.float32)
+    rec = wl.regular_receivers(12, 2 * H, (nx - 3) * H).astype(np.float32)
+    return dict(nx=nx, ny=ny, nz=nz, true_v=true_v.astype(np.float32), start=start.astype(np.float32), shots=shots,
+                rec=rec)
+
+
+def _observed(tomo, sv):
+    with tomo.Context(sv["nx"], sv["ny"], sv["nz"], H) as ctx:
+        ctx.set_velocity(sv["true_v"])
+        dobs, _ = ctx.eik_solve(sv["shots"], receivers=sv["rec"], change_tol=-1.0)
+    return dobs
+
+
+def _per_stage(tomo, sv, dobs, iters):
+    ctx = tomo.Context(sv["nx"], sv["ny"], sv["nz"], H)
+    ctx.set_velocity(sv["start"])
+    ctx.set_observed(dobs)
+    for _ in range(iters):
+        ctx.eik_solve(sv["shots"], receivers=sv["rec"], want_recv=False, change_tol=-1.0)
+        ctx.build_jacobian(D, 2, 0.1)
+        ctx.cgls(10, want_x=False)
+        ctx.model_update(True, 5, 2.0, want_velocity=False)
+    s = ctx.get_slowness()
+    ctx.close()
+    return s
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_iteration_matches_per_stage_calls(tomo, survey, use_graph):
+    sv = survey
+    dobs = _observed(tomo, sv)
+    ref = _per_stage(tomo, sv, dobs, 3)
+    with tomo.Context(sv["nx"], sv["ny"], sv["nz"], H) as ctx:
+        ctx.set_velocity(sv["start"])
+        ctx.set_observed(dobs)
+        stats = [ctx.iteration(sv["shots"], sv["rec"], D, cg_iterations=10, use_graph=use_graph, change_tol=-1.0)
+                 for _ in range(3)]
+        s = ctx.get_slowness()
+    rms = float(np.sqrt(np.mean(((s - ref) / ref) ** 2)))
+    assert rms < 1e-5, rms
+    assert stats[0]["residual"] > stats[-1]["residual"]
+    if use_graph:
+        assert stats[0]["captured"] == 1
+        assert any(st["replayed"] == 1 for st in stats[1:]), stats
+    else:
+        assert all(st["replayed"] == 0 and st["captured"] == 0 for st in stats)
+
+
+def test_iteration_recaptures_when_the_jacobian_outgrows_its_capacity(tomo, survey):
+    """headroom 1.0: capacity = the first iteration's non-zeros; a later iteration with more
+    non-zeros must grow it and capture again, with the same result as the eager path."""
+    sv = survey
+    dobs = _observed(tomo, sv)
+    out = []
+    for use_graph in (False, True):
+        with tomo.Context(sv["nx"], sv["ny"], sv["nz"], H) as ctx:
+            ctx.set_velocity(sv["start"])
+            ctx.set_observed(dobs)
+            st = [ctx.iteration(sv["shots"], sv["rec"], D, cg_iterations=10, use_graph=use_graph, change_tol=-1.0,
+                                nnz_headroom=1.0) for _ in range(3)]
+            out.append((ctx.get_slowness(), st))
+    (s0, st0), (s1, st1) = out
+    assert [a["nnz"] for a in st0] == [b["nnz"] for b in st1]
+    assert float(np.sqrt(np.mean(((s1 - s0) / s0) ** 2))) < 1e-5
+    grew = [i for i in range(1, 3) if st1[i]["nnz"] > max(st1[j]["nnz"] for j in range(i))]
+    for i in grew:
+        assert st1[i]["captured"] == 1
