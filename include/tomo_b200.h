@@ -302,7 +302,7 @@ typedef struct {
     tomo_update_opts update;      /* model update                                             */
     tomo_eik_opts eik;            /* eikonal solve (TOMO_OP_JW)                               */
     int use_graph;                /* 1: capture the iteration in CUDA graphs once, then replay */
-    float nnz_headroom;           /* Jacobian capacity over the first non-zero count (0: 1.25) */
+    float nnz_headroom;           /* Jacobian capacity / first non-zero count, >= 1 (else 1.25) */
 } tomo_iteration_opts;
 
 typedef struct {

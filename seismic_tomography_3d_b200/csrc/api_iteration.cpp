@@ -102,7 +102,7 @@ extern "C" int tomo_iteration(tomo_ctx *ctx, int nshots, const tomo_point *shots
     if (opts->cg_iterations < 1) return fail(ctx, TOMO_ERR_INVALID_ARG, "cg_iterations must be >= 1");
     if (!ctx->have_dobs || (long long)ctx->n_dobs != (long long)nshots * nrec)
         return fail(ctx, TOMO_ERR_STATE, "observed data (tomo_set_observed) must hold nshots x nrec picks");
-    const float headroom = opts->nnz_headroom > 1.0f ? opts->nnz_headroom : 1.25f;
+    const float headroom = opts->nnz_headroom >= 1.0f ? opts->nnz_headroom : 1.25f;
     const int nit = opts->cg_iterations;
     tomo::IterGraphs &G = ctx->iter;
     CK(cudaSetDevice(ctx->device));
