@@ -71,7 +71,7 @@ typedef struct {
     int max_rounds;  /* cap of outer rounds (0: default 1<<20)                        */
     int brick;       /* brick shape id (0: tuned default); see tomo_eik_brick_shapes  */
     int block_warps; /* warps per CTA of the persistent kernel (0: default)           */
-    int occupancy;   /* CTAs per SM the kernel is compiled for, 1..6 (0: default 5)   */
+    int occupancy;   /* CTAs per SM the kernel is compiled for, 1..6 (0: default 4)   */
     float change_tol;/* a face value must drop by more than this (s) to re-queue the
                         neighbour brick.  0: default 1e-6 s, the reference's EPS
                         (cuda_kernel.cuh:8); < 0: any drop (exact FP32 fixed point) */

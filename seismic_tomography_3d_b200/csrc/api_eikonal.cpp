@@ -21,7 +21,7 @@ const char *static_error_text();  // fim_static.cu
 namespace {
 
 constexpr int kDefaultMaxInner = 16;
-constexpr int kDefaultOccupancy = 5;  // 5 CTAs x 8 warps per SM (48 registers): fastest on config 2
+constexpr int kDefaultOccupancy = 4;  // 4 CTAs x 8 warps per SM (64 registers): fastest on config 2
 constexpr float kDefaultChangeTol = 1e-6f;
 constexpr int kDefaultMaxRounds = 1 << 20;
 constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~ seconds of polling, then error
@@ -717,7 +717,7 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
     // untuned defaults while timing (an earlier tuning must not leak into the trials)
     ctx->tuned_block_warps = ctx->tuned_occupancy = ctx->tuned_max_inner = 0;
     const int warps[] = {8, 4};
-    const int occs[] = {5, 4, 6, 3};
+    const int occs[] = {4, 5, 6, 3};
     const int inners[] = {16, 8, 32};
     tomo_eik_opts o{};
     o.op = TOMO_OP_JW;

@@ -35,29 +35,46 @@ __device__ __forceinline__ float sqrt_fast(float v)
 }
 
 template <bool kFastSqrt>
-__device__ __forceinline__ float godunov_jw(float a, float b, float c, float h, float s)
+__device__ __forceinline__ float sqrt_sel(float v)
+{
+    return kFastSqrt ? sqrt_fast(v) : sqrtf(v);
+}
+
+// Loop-invariant part of the local update of a node: h*s and the two discriminant terms.
+struct NodeConst {
+    float hs, q2c, q3c;  // h s, 2 (h s)^2, 3 (h s)^2
+};
+
+__device__ __forceinline__ NodeConst node_const(float h, float s)
+{
+    NodeConst k;
+    k.hs = h * s;
+    k.q2c = 2.0f * k.hs * k.hs;
+    k.q3c = 3.0f * k.hs * k.hs;
+    return k;
+}
+
+// Branch-free: all three candidates are computed and the causal one selected, so the lanes
+// of a warp (which need different candidates) never diverge.  A candidate whose root is
+// imaginary is NaN and fails every comparison, exactly as the sequential tests skip it.
+template <bool kFastSqrt>
+__device__ __forceinline__ float godunov_jw(float a, float b, float c, const NodeConst &k)
 {
     const float lo = fminf(a, b), hi = fmaxf(a, b);
     const float u0 = fminf(lo, c);
     const float mid = fmaxf(lo, c);
     const float u1 = fminf(mid, hi), u2 = fmaxf(mid, hi);
-    if (!(u0 < kInf)) return kInf;
-    const float hs = h * s;
-    float t = u0 + hs;
-    if (t > u1) {
-        const float d01 = u1 - u0;
-        const float q2 = 2.0f * hs * hs - d01 * d01;
-        const float t2 = 0.5f * ((u0 + u1) + (kFastSqrt ? sqrt_fast(q2) : sqrtf(q2)));
-        if (t2 > u1) t = t2;
-        if (t > u2) {
-            const float sum = u0 + u1 + u2;
-            const float d12 = u2 - u1, d02 = u2 - u0;
-            const float disc = 3.0f * hs * hs - (d01 * d01 + d12 * d12 + d02 * d02);
-            const float t3 = (sum + (kFastSqrt ? sqrt_fast(disc) : sqrtf(disc))) * (1.0f / 3.0f);
-            if (t3 > u2) t = t3;
-        }
-    }
-    return t;
+    const float t1 = u0 + k.hs;
+    const float d01 = u1 - u0;
+    const float t2 = 0.5f * ((u0 + u1) + sqrt_sel<kFastSqrt>(k.q2c - d01 * d01));
+    const float sum = u0 + u1 + u2;
+    const float d12 = u2 - u1, d02 = u2 - u0;
+    const float t3 = (sum + sqrt_sel<kFastSqrt>(k.q3c - (d01 * d01 + d12 * d12 + d02 * d02))) * (1.0f / 3.0f);
+    // sequential rule: t1; if t1 > u1 { t2 if causal; then t3 if the result exceeds u2 and t3 is causal }
+    const float ta = (t2 > u1) ? t2 : t1;
+    const float tb = (ta > u2 && t3 > u2) ? t3 : ta;
+    const float t = (t1 > u1) ? tb : t1;
+    return (u0 < kInf) ? t : kInf;
 }
 
 // Tile of one warp: (4+2)^3 nodes, the brick plus a one-node face halo.
@@ -135,6 +152,7 @@ struct WarpStats {
 // Data of one work item as loaded from global memory.
 struct BrickLoad {
     unsigned s, b;
+    int bz, bx, by;    // brick coordinates in the shot's window
     float s0, s1;      // slowness of the lane's two nodes
     float i0, i1;      // traveltimes of the lane's two nodes at load time
     float hv[3];       // the lane's three face-halo values
@@ -151,26 +169,34 @@ __device__ __forceinline__ void brick_coords(const ShotDesc &d, unsigned b, int 
     by = (int)(tq / (unsigned)d.nbx);
 }
 
-// Face halo slot q (0..2) of a lane: 6 faces x 16 nodes, three per lane.  Returns the
-// neighbour brick (-1 at the grid edge), the node index inside it and the tile index.
+// Face halo slot q (0..2) of a lane: slot q covers the two faces of axis q (z, x, y); lanes
+// 0-15 the lower face, 16-31 the upper, one face node each.  Returns the neighbour brick
+// (-1 at the grid edge); node = its node index, ti = the tile index of the halo cell.
 __device__ __forceinline__ long long halo_slot(const ShotDesc &d, unsigned b, int bz, int bx, int by, int lane, int q,
                                                int &node, int &ti)
 {
-    const int k = lane + 32 * q;
-    const int f = k >> 4, j = k & 15, u = j & 3, v = j >> 2;
-    const int nbz = d.nbz, nbx = d.nbx, nby = d.nby;
-    long long nb = -1;
-    int tz = 0, tx = 0, ty = 0;
-    switch (f) {
-    case 0: if (bz > 0) nb = (long long)b - 1;                      node = 3 + 4 * u + 16 * v; tz = -1; tx = u; ty = v; break;
-    case 1: if (bz < nbz - 1) nb = (long long)b + 1;                node = 0 + 4 * u + 16 * v; tz = 4;  tx = u; ty = v; break;
-    case 2: if (bx > 0) nb = (long long)b - nbz;                    node = u + 12 + 16 * v;    tz = u;  tx = -1; ty = v; break;
-    case 3: if (bx < nbx - 1) nb = (long long)b + nbz;              node = u + 0 + 16 * v;     tz = u;  tx = 4;  ty = v; break;
-    case 4: if (by > 0) nb = (long long)b - (long long)nbz * nbx;   node = u + 4 * v + 48;     tz = u;  tx = v;  ty = -1; break;
-    default: if (by < nby - 1) nb = (long long)b + (long long)nbz * nbx; node = u + 4 * v;     tz = u;  tx = v;  ty = 4; break;
+    const bool lower = lane < 16;
+    const int j = lane & 15, u = j & 3, v = j >> 2;
+    const int e = lower ? -1 : kBrick;      // halo plane in tile coordinates
+    long long step;
+    bool ok;
+    if (q == 0) {
+        node = (lower ? 3 : 0) + 4 * u + 16 * v;
+        ti = tile_idx(e, u, v);
+        ok = lower ? bz > 0 : bz < d.nbz - 1;
+        step = 1;
+    } else if (q == 1) {
+        node = u + (lower ? 12 : 0) + 16 * v;
+        ti = tile_idx(u, e, v);
+        ok = lower ? bx > 0 : bx < d.nbx - 1;
+        step = d.nbz;
+    } else {
+        node = u + 4 * v + (lower ? 48 : 0);
+        ti = tile_idx(u, v, e);
+        ok = lower ? by > 0 : by < d.nby - 1;
+        step = (long long)d.nbz * d.nbx;
     }
-    ti = tile_idx(tz, tx, ty);
-    return nb;
+    return ok ? (long long)b + (lower ? -step : step) : -1;
 }
 
 __device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, BrickLoad &L)
@@ -179,9 +205,9 @@ __device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, Br
     L.s = item >> p.local_bits;
     L.b = item & ((1u << p.local_bits) - 1u);
     const ShotDesc &d = p.shots[L.s];
-    int bz, bx, by;
-    brick_coords(d, L.b, bz, bx, by);
-    const long long gb = bz + (long long)p.gbz * ((bx + (d.wx0 >> 2)) + (long long)p.gbx * (by + (d.wy0 >> 2)));
+    brick_coords(d, L.b, L.bz, L.bx, L.by);
+    const long long gb =
+        L.bz + (long long)p.gbz * ((L.bx + (d.wx0 >> 2)) + (long long)p.gbx * (L.by + (d.wy0 >> 2)));
     const float *Sb = p.S + gb * kBrickNodes;
     const float *Tb = p.T + d.t_off + (long long)L.b * kBrickNodes;
     // own nodes: (z, x, y) and (z, x, y + 1) with z = lane & 3, x = (lane >> 2) & 3,
@@ -196,7 +222,7 @@ __device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, Br
 #pragma unroll
     for (int q = 0; q < 3; q++) {
         int node, ti;
-        const long long nb = halo_slot(d, L.b, bz, bx, by, lane, q, node, ti);
+        const long long nb = halo_slot(d, L.b, L.bz, L.bx, L.by, lane, q, node, ti);
         L.hv[q] = nb >= 0 ? __ldcg(p.T + d.t_off + nb * kBrickNodes + node) : kInf;
     }
 }
@@ -209,16 +235,19 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     const int lane = threadIdx.x & 31;
     const unsigned s = L.s, b = L.b;
     const ShotDesc &d = p.shots[s];
-    int bz, bx, by;
-    brick_coords(d, b, bz, bx, by);
+    const int bz = L.bz, bx = L.bx, by = L.by;
     const int nbz = d.nbz, nbx = d.nbx, nby = d.nby;
     float *Tb = p.T + d.t_off + (long long)b * kBrickNodes;
 
     const int z0 = lane & 3, x0 = (lane >> 2) & 3, y0 = 2 * (lane >> 4);
     const int ti0 = tile_idx(z0, x0, y0);
     const int ti1 = ti0 + kTile * kTile;  // y + 1
-    const float s0 = L.s0, s1 = L.s1, i0 = L.i0, i1 = L.i1;
+    const float i0 = L.i0, i1 = L.i1;
     float c0 = i0, c1 = i1;
+    // Two tile buffers: iteration k reads one and writes the other, so one __syncwarp per
+    // iteration orders both the reads before the next writes and the writes before the
+    // next reads.  The halo is written to both.
+    float *tile1 = tile + kTileNodes;
     tile[ti0] = c0;
     tile[ti1] = c1;
 #pragma unroll
@@ -226,33 +255,29 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
         int node, ti;
         (void)halo_slot(d, b, bz, bx, by, lane, q, node, ti);
         tile[ti] = L.hv[q];
+        tile1[ti] = L.hv[q];
     }
     __syncwarp();
 
-    const float h = p.h;
+    const NodeConst k0 = node_const(p.h, L.s0), k1 = node_const(p.h, L.s1);
     bool more = true;
     int it = 0;
     for (; it < p.max_inner; ++it) {
-        // The lane's two nodes are y-neighbours: the second update of an iteration uses the
-        // first one's new value (Gauss-Seidel along y inside the lane), and the order
-        // alternates so that information crosses the pair both ways.
-        const float a0 = fminf(tile[ti0 - kTile], tile[ti0 + kTile]);
-        const float g0 = fminf(tile[ti0 - 1], tile[ti0 + 1]);
-        const float a1 = fminf(tile[ti1 - kTile], tile[ti1 + kTile]);
-        const float g1 = fminf(tile[ti1 - 1], tile[ti1 + 1]);
-        const float ym = tile[ti0 - kTile * kTile], yp = tile[ti1 + kTile * kTile];
-        float n0, n1;
-        if (it & 1) {
-            n1 = fminf(c1, godunov_jw<kFastSqrt>(a1, fminf(c0, yp), g1, h, s1));
-            n0 = fminf(c0, godunov_jw<kFastSqrt>(a0, fminf(ym, n1), g0, h, s0));
-        } else {
-            n0 = fminf(c0, godunov_jw<kFastSqrt>(a0, fminf(ym, c1), g0, h, s0));
-            n1 = fminf(c1, godunov_jw<kFastSqrt>(a1, fminf(n0, yp), g1, h, s1));
-        }
+        const float *rd = (it & 1) ? tile1 : tile;
+        float *wr = (it & 1) ? tile : tile1;
+        // Jacobi: both nodes from the previous iteration's values, two independent chains
+        // for the scheduler to interleave.
+        const float a0 = fminf(rd[ti0 - kTile], rd[ti0 + kTile]);
+        const float g0 = fminf(rd[ti0 - 1], rd[ti0 + 1]);
+        const float a1 = fminf(rd[ti1 - kTile], rd[ti1 + kTile]);
+        const float g1 = fminf(rd[ti1 - 1], rd[ti1 + 1]);
+        const float b0 = fminf(rd[ti0 - kTile * kTile], c1);
+        const float b1 = fminf(c0, rd[ti1 + kTile * kTile]);
+        const float n0 = fminf(c0, godunov_jw<kFastSqrt>(a0, b0, g0, k0));
+        const float n1 = fminf(c1, godunov_jw<kFastSqrt>(a1, b1, g1, k1));
         const bool ch = (n0 < c0 - p.inner_tol) | (n1 < c1 - p.inner_tol);
-        __syncwarp();
-        tile[ti0] = n0;
-        tile[ti1] = n1;
+        wr[ti0] = n0;
+        wr[ti1] = n1;
         c0 = n0;
         c1 = n1;
         __syncwarp();
@@ -325,7 +350,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
 {
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5;
-    float *tile = smem + warp * kTileNodes;
+    float *tile = smem + warp * 2 * kTileNodes;
     WarpStats ws{0ull, 0ull};
 
     unsigned round = 0;
@@ -348,12 +373,19 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
         // round; that neighbour then re-queues the brick, as for any concurrent update.
         const unsigned *list = p.lists + (size_t)cur * p.list_cap;
         unsigned *cursor = p.ctrl + kCur0 + cur;
-        // one item at a time: fetching the next item's brick before relaxing this one
-        // (software prefetch) doubles the live registers and measured 4 % slower
-        for (unsigned i = fetch_item(cursor); i < n; i = fetch_item(cursor)) {
+        // One brick at a time (loading the next brick's data ahead doubles the live
+        // registers and measured 4 % slower), but the cursor atomic for the next item is
+        // issued before this brick is relaxed and its result read only afterwards, so its
+        // round trip overlaps the relaxation.
+        unsigned i = fetch_item(cursor);
+        while (i < n) {
+            const unsigned item = __ldcg(list + i);
+            unsigned next = 0;
+            if ((threadIdx.x & 31) == 0) next = atomicAdd(cursor, 1u);
             BrickLoad A;
-            load_brick(p, __ldcg(list + i), A);
+            load_brick(p, item, A);
             relax_brick<kFastSqrt>(p, A, round, tile, ws);
+            i = __shfl_sync(kFull, next, 0);
         }
         if (!grid_barrier(p.ctrl, p.spin_limit)) { ok = false; break; }
         ++round;
@@ -507,7 +539,7 @@ __global__ void k_fim_verify(const float *T, const float *S, const ShotDesc *sho
         const float zm = z > 0 ? brick_T(T, d, x, y, z - 1) : kInf, zp = z < ez - 1 ? brick_T(T, d, x, y, z + 1) : kInf;
         const long long gb = (z >> 2) + (long long)gbz * (((x + d.wx0) >> 2) + (long long)gbx * ((y + d.wy0) >> 2));
         const float sl = __ldg(S + gb * kBrickNodes + (i % kBrickNodes));
-        const float g = godunov_jw<kFastSqrt>(fminf(xm, xp), fminf(ym, yp), fminf(zm, zp), h, sl);
+        const float g = godunov_jw<kFastSqrt>(fminf(xm, xp), fminf(ym, yp), fminf(zm, zp), node_const(h, sl));
         if (g < kInf && t < g - rel_tol * g) {
             cnt++;
             worst = fmaxf(worst, (g - t) / g);
@@ -600,7 +632,7 @@ template <int MINB, bool kFastSqrt>
 static cudaError_t launch_solve(const FimLaunch &p, int block_warps, int *grid_out, cudaStream_t st)
 {
     const int threads = 32 * block_warps;
-    const size_t smem = (size_t)block_warps * kTileNodes * sizeof(float);
+    const size_t smem = (size_t)block_warps * 2 * kTileNodes * sizeof(float);
     int dev = 0, nsm = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;

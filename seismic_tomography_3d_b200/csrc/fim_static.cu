@@ -161,7 +161,7 @@ extern "C" int tomo_eik_solve_static(const float *slowness, int nx, int ny, int 
     p.inner_tol = 0.f;
     p.local_bits = local_bits;
     p.spin_limit = 1ull << 26;
-    CKS(fim_solve(p, 8, 5, false, nullptr, st));
+    CKS(fim_solve(p, 8, 4, false, nullptr, st));
     CKS(fim_unbrick(T, desc, 0, nz, t_out, st));
     unsigned err_word = 0;
     CKS(cudaMemcpyAsync(&err_word, ctrl + kErr, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
