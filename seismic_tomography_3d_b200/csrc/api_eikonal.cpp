@@ -15,6 +15,7 @@ using tomo::ShotDesc;
 
 namespace tomo {
 int rebrick_model(tomo_ctx *ctx);
+int model_buffers(tomo_ctx *ctx);
 const char *static_error_text();  // fim_static.cu
 }
 
@@ -64,8 +65,9 @@ int upload_model(tomo_ctx *ctx, const float *host, bool is_velocity)
     } else {
         CK(cudaMemcpyAsync(ctx->slow.ptr, host, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     }
-    CK(ctx->S.ensure((size_t)ctx->nxx * ctx->nyy * ctx->nzz));
-    int rc = tomo::rebrick_model(ctx);
+    int rc = tomo::model_buffers(ctx);
+    if (rc != TOMO_OK) return rc;
+    rc = tomo::rebrick_model(ctx);
     if (rc != TOMO_OK) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->have_model = true;
@@ -156,7 +158,15 @@ int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point 
 }  // namespace
 
 namespace tomo {
-// Bricks the device model (after an upload or a model update).
+int model_buffers(tomo_ctx *ctx)
+{
+    CK(ctx->slow.ensure((size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz));
+    CK(ctx->S.ensure((size_t)ctx->nxx * ctx->nyy * ctx->nzz));
+    return TOMO_OK;
+}
+
+// Bricks the device model (after an upload or a model update; enqueue only, buffers from
+// model_buffers).
 int rebrick_model(tomo_ctx *ctx)
 {
     CK(fim_brick_model(ctx->slow.ptr, ctx->S.ptr, ctx->g.nx, ctx->g.ny, ctx->g.nz, ctx->nxx, ctx->nyy, ctx->nzz,

@@ -486,6 +486,7 @@ int tomo_net_predict(tomo_net *net, int n, const tomo_net_sample *samples, float
 // ----------------------------------------------------------------------------------------
 namespace tomo {
 int rebrick_model(tomo_ctx *ctx);
+int model_buffers(tomo_ctx *ctx);
 }
 
 extern "C" int tomo_random_tiles(tomo_ctx *ctx, int tile, unsigned long long seed)
@@ -535,13 +536,13 @@ extern "C" int tomo_random_tiles(tomo_ctx *ctx, int tile, unsigned long long see
         e = cudaMemcpyAsync(d.ptr, tm.data(), tm.size() * sizeof(tomo::net::TileModel), cudaMemcpyHostToDevice,
                             ctx->stream);
     if (e == cudaSuccess) e = tomo::net::random_models(d.ptr, (int)tm.size(), ctx->slow.ptr, g.nx, g.ny, g.nz, ctx->stream);
-    if (e == cudaSuccess) e = ctx->S.ensure((size_t)ctx->nxx * ctx->nyy * ctx->nzz);
     if (e != cudaSuccess) {
         ctx->err = std::string("tomo_random_tiles: ") + cudaGetErrorString(e);
         d.release();
         return TOMO_ERR_CUDA;
     }
-    int rc = tomo::rebrick_model(ctx);
+    int rc = tomo::model_buffers(ctx);
+    if (rc == TOMO_OK) rc = tomo::rebrick_model(ctx);
     if (rc == TOMO_OK) {
         e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) {

@@ -86,15 +86,6 @@ __device__ __forceinline__ int tile_idx(int z, int x, int y)
     return (z + 1) + kTile * ((x + 1) + kTile * (y + 1));
 }
 
-// Lane masks of the brick faces for the two node sets of a lane (node = z + 4x + 16y;
-// first set y = 2 (lane >> 4), second set y + 1).
-constexpr unsigned kMaskZm = 0x11111111u;  // z == 0
-constexpr unsigned kMaskZp = 0x88888888u;  // z == 3
-constexpr unsigned kMaskXm = 0x000F000Fu;  // x == 0
-constexpr unsigned kMaskXp = 0xF000F000u;  // x == 3
-constexpr unsigned kMaskY0 = 0x0000FFFFu;  // y == 0 (first node set, lanes 0-15)
-constexpr unsigned kMaskY3 = 0xFFFF0000u;  // y == 3 (second node set, lanes 16-31)
-
 __device__ __forceinline__ float brick_T(const float *T, const ShotDesc &d, int x, int y, int z)
 {
     const long long b = (z >> 2) + (long long)d.nbz * ((x >> 2) + (long long)d.nbx * (y >> 2));
@@ -291,27 +282,41 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     ws.inner += (unsigned long long)it;
 
     const bool any_drop = __any_sync(kFull, (c0 < i0) | (c1 < i1));
-    const unsigned m0 = __ballot_sync(kFull, c0 < i0 - p.change_tol);
-    const unsigned m1 = __ballot_sync(kFull, c1 < i1 - p.change_tol);
-    const unsigned mm = m0 | m1;
     if (any_drop) {
         const int n0 = lane_node(lane);
         __stcg(Tb + n0, c0);
         __stcg(Tb + n0 + 16, c1);
     }
 
-    // Queue the neighbours across changed faces, and this brick if it hit the cap.
+    // Queue a neighbour when a node on the shared face dropped by more than change_tol AND
+    // its new time is below the neighbour's adjacent node y: a local update of y exceeds
+    // every neighbour value it uses (causality), so a face node at or above T(y) cannot lower
+    // y.  T(y) is the halo cell loaded at the start of this activation; a concurrent drop of
+    // y only makes the test more permissive.
+    const bool d0 = c0 < i0 - p.change_tol, d1 = c1 < i1 - p.change_tol;
+    const int kT2 = kTile * kTile;
+    const bool fzm = (z0 == 0) && ((d0 && c0 < tile[ti0 - 1]) || (d1 && c1 < tile[ti1 - 1]));
+    const bool fzp = (z0 == 3) && ((d0 && c0 < tile[ti0 + 1]) || (d1 && c1 < tile[ti1 + 1]));
+    const bool fxm = (x0 == 0) && ((d0 && c0 < tile[ti0 - kTile]) || (d1 && c1 < tile[ti1 - kTile]));
+    const bool fxp = (x0 == 3) && ((d0 && c0 < tile[ti0 + kTile]) || (d1 && c1 < tile[ti1 + kTile]));
+    const bool fym = (y0 == 0) && d0 && c0 < tile[ti0 - kT2];
+    const bool fyp = (y0 == 2) && d1 && c1 < tile[ti1 + kT2];
+    const unsigned face = (__ballot_sync(kFull, fzm) ? 1u : 0u) | (__ballot_sync(kFull, fzp) ? 2u : 0u) |
+                          (__ballot_sync(kFull, fxm) ? 4u : 0u) | (__ballot_sync(kFull, fxp) ? 8u : 0u) |
+                          (__ballot_sync(kFull, fym) ? 16u : 0u) | (__ballot_sync(kFull, fyp) ? 32u : 0u);
+
+    // Queue the neighbours across those faces, and this brick if it hit the cap.
     bool want = false;
     long long tgt = -1;
     if (lane < 6) {
-        bool chg = false;
+        bool chg = (face >> lane) & 1u;
         switch (lane) {
-        case 0: chg = (mm & kMaskZm) && bz > 0;        tgt = (long long)b - 1; break;
-        case 1: chg = (mm & kMaskZp) && bz < nbz - 1;  tgt = (long long)b + 1; break;
-        case 2: chg = (mm & kMaskXm) && bx > 0;        tgt = (long long)b - nbz; break;
-        case 3: chg = (mm & kMaskXp) && bx < nbx - 1;  tgt = (long long)b + nbz; break;
-        case 4: chg = (m0 & kMaskY0) && by > 0;        tgt = (long long)b - (long long)nbz * nbx; break;
-        default: chg = (m1 & kMaskY3) && by < nby - 1; tgt = (long long)b + (long long)nbz * nbx; break;
+        case 0: chg = chg && bz > 0;        tgt = (long long)b - 1; break;
+        case 1: chg = chg && bz < nbz - 1;  tgt = (long long)b + 1; break;
+        case 2: chg = chg && bx > 0;        tgt = (long long)b - nbz; break;
+        case 3: chg = chg && bx < nbx - 1;  tgt = (long long)b + nbz; break;
+        case 4: chg = chg && by > 0;        tgt = (long long)b - (long long)nbz * nbx; break;
+        default: chg = chg && by < nby - 1; tgt = (long long)b + (long long)nbz * nbx; break;
         }
         want = chg;
     } else if (lane == 6) {
@@ -373,19 +378,14 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
         // round; that neighbour then re-queues the brick, as for any concurrent update.
         const unsigned *list = p.lists + (size_t)cur * p.list_cap;
         unsigned *cursor = p.ctrl + kCur0 + cur;
-        // One brick at a time (loading the next brick's data ahead doubles the live
-        // registers and measured 4 % slower), but the cursor atomic for the next item is
-        // issued before this brick is relaxed and its result read only afterwards, so its
-        // round trip overlaps the relaxation.
-        unsigned i = fetch_item(cursor);
-        while (i < n) {
-            const unsigned item = __ldcg(list + i);
-            unsigned next = 0;
-            if ((threadIdx.x & 31) == 0) next = atomicAdd(cursor, 1u);
+        // One item at a time, fetched only when the warp is free: loading the next brick
+        // ahead doubles the live registers (4 % slower), and even reserving the next item
+        // index early (its atomic overlapping the relaxation) is 5 % slower, because busy
+        // warps then hold items that idle warps could take at the end of a round.
+        for (unsigned i = fetch_item(cursor); i < n; i = fetch_item(cursor)) {
             BrickLoad A;
-            load_brick(p, item, A);
+            load_brick(p, __ldcg(list + i), A);
             relax_brick<kFastSqrt>(p, A, round, tile, ws);
-            i = __shfl_sync(kFull, next, 0);
         }
         if (!grid_barrier(p.ctrl, p.spin_limit)) { ok = false; break; }
         ++round;
