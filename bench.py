@@ -301,6 +301,9 @@ def run_ours(args):
     alg_bytes = act * stats[0]["nodes_per_brick"] * BYTES_PER_NODE_ACT
     peak, peak_kind = peaks()
     achieved = alg_bytes / (kern_ms / 1000.0) / 1e9
+    # compulsory traffic of the batch whatever the algorithm: slowness read + traveltime
+    # written once per window node (8 B/node)
+    compulsory = 8.0 * sum(ctx.volume_sizes(ns, sv.windows))
     # DRAM bytes per brick activation from the committed ncu summary (one capture of a
     # 16-shot launch of the same workload), scaled to this launch's activations
     traffic = None
@@ -345,7 +348,9 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "k_fim_solve", "kernel_ms": kern_ms,
-                         "alg_bytes_per_launch": alg_bytes, "activations_per_launch": act},
+                         "alg_bytes_per_launch": alg_bytes, "activations_per_launch": act,
+                         "compulsory_bytes_per_launch": compulsory,
+                         "compulsory_frac": compulsory / (kern_ms / 1000.0) / 1e9 / peak},
             "clocks": clk.summary(),
             "gpu_launches": 3 * args.steps,
             "solver": {"rounds": stats[-1]["rounds"], "activations": stats[-1]["activations"],
