@@ -175,7 +175,12 @@ extern "C" int tomo_iteration(tomo_ctx *ctx, int nshots, const tomo_point *shots
                           (const void *)ctx->ray_steps.ptr, (const void *)ctx->final_dist.ptr,
                           (const void *)ctx->spos.ptr, (const void *)ctx->a_ptr.ptr, (const void *)ctx->csr_sizes.ptr,
                           (const void *)ctx->smin.ptr, (const void *)ctx->illum.ptr, (const void *)ctx->slow.ptr,
-                          (const void *)ctx->scan_temp.ptr, (const void *)ctx->reduce_temp.ptr, (const void *)pin})
+                          (const void *)ctx->scan_temp.ptr, (const void *)ctx->reduce_temp.ptr, (const void *)pin,
+                          (const void *)ctx->ray_keys.ptr, (const void *)ctx->ray_keys_out.ptr,
+                          (const void *)ctx->ray_iota.ptr, (const void *)ctx->ray_order.ptr,
+                          (const void *)ctx->order_temp.ptr, (const void *)ctx->t_recv.ptr, (const void *)ctx->T.ptr,
+                          (const void *)ctx->qflag.ptr, (const void *)ctx->lists.ptr, (const void *)ctx->S.ptr,
+                          (const void *)ctx->shots_d.ptr, (const void *)ctx->rec.ptr})
         push(key_a, p);
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     if (graphs && (!G.a || key_a != G.key_a)) {

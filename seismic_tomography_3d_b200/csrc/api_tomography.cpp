@@ -139,6 +139,16 @@ extern "C" {
 void tomo_release_tomography(tomo_ctx *ctx)
 {
     if (!ctx) return;
+    ctx->ray_keys.release();
+    ctx->ray_keys_out.release();
+    ctx->ray_iota.release();
+    ctx->ray_order.release();
+    ctx->order_temp.release();
+    ctx->scan_temp.release();
+    ctx->reduce_temp.release();
+    ctx->sort_temp.release();
+    ctx->csr_sizes.release();
+    ctx->smin.release();
     for (auto *b : {&ctx->nuniq, &ctx->ray_status, &ctx->ray_steps, &ctx->a_ptr, &ctx->a_idx, &ctx->t_ptr,
                     &ctx->t_idx, &ctx->sort_keys, &ctx->sort_keys_out, &ctx->sort_pos, &ctx->sort_pos_out,
                     &ctx->rows_of})
@@ -228,6 +238,14 @@ int jac_prepare(tomo_ctx *ctx, const tomo_jacobian_opts *opts, JacGeom &jg)
     tb = 0;
     CK(tomo::reduce_min(ctx->slow.ptr, nullptr, (size_t)g.nx * g.ny * g.nz, nullptr, &tb, ctx->stream));
     CK(ctx->reduce_temp.ensure(tb));
+    CK(ctx->ray_keys.ensure((size_t)nrays));
+    CK(ctx->ray_keys_out.ensure((size_t)nrays));
+    CK(ctx->ray_iota.ensure((size_t)nrays));
+    CK(ctx->ray_order.ensure((size_t)nrays));
+    tb = 0;
+    CK(tomo::ray_order(ctx->t_recv.ptr, ctx->ray_keys.ptr, ctx->ray_keys_out.ptr, ctx->ray_iota.ptr,
+                       ctx->ray_order.ptr, (int)nrays, nullptr, &tb, ctx->stream));
+    CK(ctx->order_temp.ensure(tb));
     // the sync keeps the host staging vectors alive until the copies are done
     CK(cudaStreamSynchronize(ctx->stream));
     return TOMO_OK;
@@ -280,7 +298,11 @@ int jac_march(tomo_ctx *ctx, const JacGeom &jg)
         size_t tb = ctx->reduce_temp.cap;
         CK(tomo::reduce_min(ctx->slow.ptr, ctx->smin.ptr, npts, ctx->reduce_temp.ptr, &tb, ctx->stream));
     }
-    const RayLaunch rl = ray_launch(ctx, jg);
+    size_t ob = ctx->order_temp.cap;
+    CK(tomo::ray_order(ctx->t_recv.ptr, ctx->ray_keys.ptr, ctx->ray_keys_out.ptr, ctx->ray_iota.ptr, ctx->ray_order.ptr,
+                       (int)jg.nrays, ctx->order_temp.ptr, &ob, ctx->stream));
+    RayLaunch rl = ray_launch(ctx, jg);
+    rl.order = ctx->ray_order.ptr;
     CK(tomo::ray_march(rl, ctx->stream));
     size_t tb = ctx->scan_temp.cap;
     CK(tomo::scan_exclusive(ctx->nuniq.ptr, ctx->a_ptr.ptr, (int)jg.nrays + 1, ctx->scan_temp.ptr, &tb, ctx->stream));

@@ -97,6 +97,9 @@ struct tomo_ctx {
     tomo::DevBuf<unsigned char> cub_temp, scan_temp, reduce_temp, sort_temp;
     tomo::DevBuf<long long> csr_sizes;  // [0] ray non-zeros, [1] all non-zeros (device side)
     tomo::DevBuf<float> smin;           // smallest slowness of the model (per-ray cap)
+    tomo::DevBuf<unsigned> ray_keys, ray_keys_out;  // march order of the rays
+    tomo::DevBuf<int> ray_iota, ray_order;
+    tomo::DevBuf<unsigned char> order_temp;
     int n_data = 0, n_model = 0, n_rows = 0, tk_order = 0;
     int nxt = 0, nyt = 0, nzt = 0;
     float dxt = 0, dyt = 0, dzt = 0;

@@ -43,8 +43,11 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
 {
     const long long nrays = (long long)p.nshots * p.nrec;
     const float rayStep = fmul(0.2f, p.dz);  // least_squares.cpp:203
-    for (long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x; ray < nrays;
-         ray += (long long)gridDim.x * blockDim.x) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nrays;
+         t += (long long)gridDim.x * blockDim.x) {
+        // march order: longest (largest receiver time) first, so that the lanes of a warp
+        // carry rays of similar length; results stay indexed by the ray itself
+        const long long ray = p.order ? (long long)p.order[t] : t;
         const int s = (int)(ray / p.nrec), r = (int)(ray % p.nrec);
         const ShotDesc &d = p.shots[s];
         const float ox = fmul((float)d.wx0, p.dx), oy = fmul((float)d.wy0, p.dy);
@@ -316,6 +319,28 @@ cudaError_t csr_transpose_finish(const int *sorted_pos, const int *rows_of, cons
 cudaError_t scan_exclusive(const int *in, int *out, int n, void *temp, size_t *temp_bytes, cudaStream_t st)
 {
     return cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, in, out, n, st);
+}
+
+// Rays by descending receiver time: keys are the time bits (non-negative floats order as
+// their bits), values the ray index.
+__global__ void k_ray_order_init(const float *t_recv, unsigned *keys, int *vals, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float t = t_recv[i];
+        keys[i] = t > 0.0f ? __float_as_uint(t) : 0u;
+        vals[i] = i;
+    }
+}
+
+cudaError_t ray_order(const float *t_recv, unsigned *keys, unsigned *keys_out, int *vals, int *order, int n,
+                      void *temp, size_t *temp_bytes, cudaStream_t st)
+{
+    if (temp) {
+        k_ray_order_init<<<grid_for(n, 256), 256, 0, st>>>(t_recv, keys, vals, n);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cub::DeviceRadixSort::SortPairsDescending(temp, *temp_bytes, keys, keys_out, vals, order, n, 0, 32, st);
 }
 
 cudaError_t reduce_min(const float *in, float *out, size_t n, void *temp, size_t *temp_bytes, cudaStream_t st)
