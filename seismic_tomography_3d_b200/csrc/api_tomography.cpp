@@ -304,6 +304,7 @@ int jac_march(tomo_ctx *ctx, const JacGeom &jg)
     RayLaunch rl = ray_launch(ctx, jg);
     rl.order = ctx->ray_order.ptr;
     CK(tomo::ray_march(rl, ctx->stream));
+    CK(tomo::ray_sort(rl, ctx->stream));
     size_t tb = ctx->scan_temp.cap;
     CK(tomo::scan_exclusive(ctx->nuniq.ptr, ctx->a_ptr.ptr, (int)jg.nrays + 1, ctx->scan_temp.ptr, &tb, ctx->stream));
     CK(tomo::csr_sizes(ctx->a_ptr.ptr, (int)jg.nrays, jg.tk_entries, ctx->csr_sizes.ptr, ctx->stream));

@@ -138,31 +138,92 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
             }
         }
         if (cnt && ci >= 0) runs[ci].y += cnt;
-        // sort the runs by cell and merge repeated cells (std::sort + run-length, :241-263)
-        for (int a = 1; a < nr; a++) {
-            const uint2 key = runs[a];
-            int b = a - 1;
-            while (b >= 0 && runs[b].x > key.x) {
-                runs[b + 1] = runs[b];
-                --b;
-            }
-            runs[b + 1] = key;
-        }
-        int w = 0;
-        for (int a = 0; a < nr; a++) {
-            const uint2 e = runs[a];
-            if (w > 0 && runs[w - 1].x == e.x) runs[w - 1].y += e.y;
-            else runs[w++] = e;
-        }
         if (overflow) {
             st = kRayOverflow;
-            w = 0;
+            nr = 0;
         }
-        p.nuniq[ray] = w;
+        p.nuniq[ray] = nr;  // raw run count; k_ray_sort sorts, merges and rewrites it
         p.status[ray] = st;
         p.steps[ray] = L;
         const float ez = fsub(zi, sz), ex = fsub(xi, sx), ey = fsub(yi, sy);
         p.final_dist[ray] = __fsqrt_rn(fadd(fadd(fmul(ez, ez), fmul(ex, ex)), fmul(ey, ey)));
+    }
+}
+
+
+// Sorts each ray's runs by cell and merges repeated cells -- the reference's std::sort of
+// the step cells and run-length count (least_squares.cpp:241-263), on the runs recorded
+// while marching.  One warp per ray: a bitonic sort in shared memory over the next power
+// of two of the run count, then one lane merges equal cells (their step counts add).
+// Rays with more runs than the shared buffer (possible only with max_cells_per_ray > 1024)
+// are sorted by one lane in place.
+constexpr int kSortWarps = 4;
+constexpr int kSortCap = 1024;
+
+__global__ void __launch_bounds__(32 * kSortWarps) k_ray_sort(RayLaunch p)
+{
+    __shared__ uint2 sbuf[kSortWarps][kSortCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint2 *buf = sbuf[warp];
+    const long long nrays = (long long)p.nshots * p.nrec;
+    for (long long ray = blockIdx.x * (long long)kSortWarps + warp; ray < nrays;
+         ray += (long long)gridDim.x * kSortWarps) {
+        uint2 *runs = p.runs + ray * (long long)p.cap_runs;
+        const int n = p.nuniq[ray];
+        if (n <= 1) continue;
+        if (n > kSortCap) {
+            if (lane == 0) {
+                for (int a = 1; a < n; a++) {
+                    const uint2 key = runs[a];
+                    int b = a - 1;
+                    while (b >= 0 && runs[b].x > key.x) {
+                        runs[b + 1] = runs[b];
+                        --b;
+                    }
+                    runs[b + 1] = key;
+                }
+                int w = 0;
+                for (int a = 0; a < n; a++) {
+                    const uint2 e = runs[a];
+                    if (w > 0 && runs[w - 1].x == e.x) runs[w - 1].y += e.y;
+                    else runs[w++] = e;
+                }
+                p.nuniq[ray] = w;
+            }
+            __syncwarp();
+            continue;
+        }
+        int P = 2;
+        while (P < n) P <<= 1;
+        for (int i = lane; i < P; i += 32) buf[i] = i < n ? runs[i] : make_uint2(0xffffffffu, 0u);
+        __syncwarp();
+        for (int k = 2; k <= P; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = lane; i < P; i += 32) {
+                    const int ixj = i ^ j;
+                    if (ixj > i) {
+                        const uint2 a = buf[i], b = buf[ixj];
+                        if ((a.x > b.x) == ((i & k) == 0)) {
+                            buf[i] = b;
+                            buf[ixj] = a;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        int w = 0;
+        if (lane == 0) {
+            for (int a = 0; a < n; a++) {
+                const uint2 e = buf[a];
+                if (w > 0 && buf[w - 1].x == e.x) buf[w - 1].y += e.y;
+                else buf[w++] = e;
+            }
+            p.nuniq[ray] = w;
+        }
+        w = __shfl_sync(0xffffffffu, w, 0);
+        __syncwarp();
+        for (int i = lane; i < w; i += 32) runs[i] = buf[i];
+        __syncwarp();
     }
 }
 
@@ -269,6 +330,15 @@ static int grid_for(long long n, int threads)
 cudaError_t ray_march(const RayLaunch &p, cudaStream_t st)
 {
     k_ray_march<<<grid_for((long long)p.nshots * p.nrec, 128), 128, 0, st>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t ray_sort(const RayLaunch &p, cudaStream_t st)
+{
+    const long long nrays = (long long)p.nshots * p.nrec;
+    long long g = (nrays + kSortWarps - 1) / kSortWarps;
+    if (g > 148LL * 16) g = 148LL * 16;
+    k_ray_sort<<<(int)(g > 0 ? g : 1), 32 * kSortWarps, 0, st>>>(p);
     return cudaGetLastError();
 }
 

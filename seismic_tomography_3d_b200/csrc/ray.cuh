@@ -45,6 +45,8 @@ struct RayLaunch {
 };
 
 cudaError_t ray_march(const RayLaunch &p, cudaStream_t st);
+// per ray: runs sorted by cell with repeated cells merged; nuniq = distinct cells
+cudaError_t ray_sort(const RayLaunch &p, cudaStream_t st);
 cudaError_t ray_emit(const RayLaunch &p, const int *row_ptr, int *cols, float *vals, cudaStream_t st);
 // sizes[0] = row_ptr[n_data_rows] (ray non-zeros), sizes[1] = sizes[0] + tk_entries
 cudaError_t csr_sizes(const int *row_ptr, int n_data_rows, long long tk_entries, long long *sizes, cudaStream_t st);
