@@ -80,7 +80,20 @@ typedef struct {
     int ieee_sqrt;   /* 1: IEEE sqrtf in the local update; 0 (default): sqrt.approx  */
     int sweep_groups;/* TOMO_OP_NGB: independent block groups sweeping their own shots
                         (0: default)                                                  */
+    int schedule;    /* TOMO_OP_JW work schedule: TOMO_SCHED_DEFAULT, TOMO_SCHED_ROUNDS,
+                        TOMO_SCHED_ASYNC                                              */
 } tomo_eik_opts;
+
+/* Work schedules of the JW solve (same fixed point, different order of brick updates).
+ * ROUNDS (default): bricks queued during a round are relaxed in the next one, rounds
+ *   separated by a grid-wide barrier -- a wavefront order; max_rounds caps the rounds.
+ * ASYNC: no rounds -- one work ring, a brick is relaxed as soon as a warp is free;
+ *   max_rounds caps the activations at max_rounds x the batch's bricks.  Measured 2.5x
+ *   slower than ROUNDS on the config-2 batch (bricks relaxed before their upwind
+ *   neighbours settle are relaxed again: 1.8x the activations). */
+#define TOMO_SCHED_DEFAULT 0
+#define TOMO_SCHED_ROUNDS  1
+#define TOMO_SCHED_ASYNC   2
 
 typedef struct {
     long long rounds;            /* outer rounds of the persistent solve                  */

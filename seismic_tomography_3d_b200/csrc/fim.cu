@@ -218,8 +218,99 @@ __device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, Br
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Asynchronous schedule (no rounds).  One ring of work items (capacity = bricks of the
+// batch) and one state word per (shot, brick): 0 idle, 1 queued (exactly one ring entry),
+// 2 being relaxed by one warp, 3 being relaxed and re-queued meanwhile ("dirty").  A brick
+// therefore never has two owners, and a re-queue that arrives while it is being relaxed
+// is kept as the dirty state and honoured by the owner.  `pending` counts queued + owned
+// bricks; it is raised before a push and lowered after an owner's pushes, so it reaches
+// zero only when the work is done.  Every wait is bounded (error flag, then return).
+// ---------------------------------------------------------------------------------------
+constexpr unsigned kEmpty = 0xffffffffu;
+constexpr unsigned kIdle = 0u, kQueued = 1u, kOwned = 2u, kDirty = 3u;
+
+__device__ __forceinline__ unsigned *ring_of(const FimLaunch &p) { return p.lists; }
+// The ring spans the whole list buffer (3 x the batch's bricks).
+__device__ __forceinline__ unsigned ring_cap(const FimLaunch &p) { return 3u * p.list_cap; }
+
+// Pushes the items of the lanes with `push` (warp-aggregated): pending first, then the
+// ring slots.  The caller fenced its traveltime stores before.
+__device__ __forceinline__ void ring_push(const FimLaunch &p, bool push, unsigned item)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned m = __ballot_sync(kFull, push);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if (lane == leader) {
+        atomicAdd(p.ctrl + kCnt1, (unsigned)__popc(m));
+        base = atomicAdd(p.ctrl + kCnt0, (unsigned)__popc(m));
+    }
+    base = __shfl_sync(kFull, base, leader);
+    if (push) {
+        // Slots are handed out in tail order but written later: a slot may still hold the
+        // item of the previous lap (its reader not yet there), so claim it only when empty.
+        const unsigned slot = (base + __popc(m & ((1u << lane) - 1u))) % ring_cap(p);
+        unsigned long long spins = 0;
+        while (atomicCAS(ring_of(p) + slot, kEmpty, item) != kEmpty) {
+            if (++spins > p.spin_limit) {
+                atomicCAS(p.ctrl + kErr, 0u, (unsigned)kDevBarrierTimeout);
+                break;
+            }
+            __nanosleep(32);
+        }
+    }
+}
+
+// Lanes 0-5: neighbour tgt to queue (want); lane 6: this brick, `more` = its in-brick
+// iteration cap was hit.  Ends this warp's ownership of brick b.
+__device__ __forceinline__ void queue_async(const FimLaunch &p, const ShotDesc &d, unsigned s, unsigned b, bool want,
+                                            long long tgt, bool self_lane)
+{
+    const int lane = threadIdx.x & 31;
+    __threadfence();  // the brick's traveltimes are visible before anyone is queued
+    bool push = false;
+    unsigned item = 0;
+    if (want && lane < 6) {
+        unsigned *st = p.qflag + d.qbase + (unsigned long long)tgt;
+        bool settled = false;
+        for (int tries = 0; tries < 256 && !settled; tries++) {
+            const unsigned old = atomicCAS(st, kIdle, kQueued);
+            if (old == kIdle) {
+                push = settled = true;
+            } else if (old == kQueued || old == kDirty) {
+                settled = true;
+            } else {  // owned: mark dirty unless the owner let go meanwhile (then retry)
+                const unsigned o2 = atomicCAS(st, kOwned, kDirty);
+                settled = (o2 == kOwned || o2 == kDirty || o2 == kQueued);
+            }
+        }
+        if (!settled) atomicCAS(p.ctrl + kErr, 0u, (unsigned)kDevCapacity);
+        item = (s << p.local_bits) | (unsigned)tgt;
+    }
+    // this brick: re-queue when its cap was hit or it turned dirty, else release it
+    if (self_lane && lane == 6) {
+        unsigned *st = p.qflag + d.qbase + b;
+        if (want) {  // `want` on lane 6 = in-brick cap hit
+            atomicExch(st, kQueued);
+            push = true;
+        } else {
+            const unsigned old = atomicCAS(st, kOwned, kIdle);
+            if (old == kDirty) {
+                atomicExch(st, kQueued);
+                push = true;
+            }
+        }
+        item = (s << p.local_bits) | b;
+    }
+    ring_push(p, push, item);
+    __syncwarp();
+    if (lane == 0) atomicSub(p.ctrl + kCnt1, 1u);  // this ownership ends
+}
+
 // One activation of one (already loaded) brick by one warp.
-template <bool kFastSqrt>
+template <bool kFastSqrt, bool kAsync>
 __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad &L, unsigned round, float *tile,
                                             WarpStats &ws)
 {
@@ -323,6 +414,10 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
         want = more;
         tgt = b;
     }
+    if (kAsync) {
+        queue_async(p, d, s, b, want, tgt, lane == 6 ? true : false);
+        return;
+    }
     const unsigned tag = round + 2u;  // "queued for round+1", offset by one so 0 = never
     if (want) {
         const unsigned old = atomicMax(p.qflag + d.qbase + (unsigned long long)tgt, tag);
@@ -385,7 +480,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
         for (unsigned i = fetch_item(cursor); i < n; i = fetch_item(cursor)) {
             BrickLoad A;
             load_brick(p, __ldcg(list + i), A);
-            relax_brick<kFastSqrt>(p, A, round, tile, ws);
+            relax_brick<kFastSqrt, false>(p, A, round, tile, ws);
         }
         if (!grid_barrier(p.ctrl, p.spin_limit)) { ok = false; break; }
         ++round;
@@ -397,6 +492,80 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
     if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kRounds] = round;
     if (!ok || p.nrec == 0) return;
 
+    sample_receivers(p.T, p.shots, p.nshots, p.rx, p.ry, p.rz, p.nrec, p.dx, p.dy, p.dz, p.nz, p.t_recv);
+}
+
+template <int MINB, bool kFastSqrt>
+__global__ void __launch_bounds__(256, MINB) k_fim_async(FimLaunch p)
+{
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *tile = smem + warp * 2 * kTileNodes;
+    WarpStats ws{0ull, 0ull};
+    unsigned *ring = ring_of(p);
+    const unsigned long long act_cap =
+        p.max_rounds > 0 ? (unsigned long long)p.max_rounds * p.list_cap : ~0ull;  // activations
+    for (;;) {
+        unsigned h = 0, item = kEmpty;
+        int done = 0;
+        if (lane == 0) {
+            h = atomicAdd(p.ctrl + kCur0, 1u) % ring_cap(p);
+            unsigned long long spins = 0;
+            for (;;) {
+                // Claim the slot's item with an exchange: with fewer slots than warps two
+                // consumers can wait on one slot (one lap apart); only one gets the item.
+                if (ld_volatile(ring + h) != kEmpty) {
+                    item = atomicExch(ring + h, kEmpty);
+                    if (item != kEmpty) break;
+                }
+                if (ld_volatile(p.ctrl + kCnt1) == 0u || ld_volatile(p.ctrl + kErr) != 0u) {
+                    done = 1;
+                    break;
+                }
+                if (++spins > p.spin_limit) {
+                    atomicCAS(p.ctrl + kErr, 0u, (unsigned)kDevBarrierTimeout);
+                    done = 1;
+                    break;
+                }
+                __nanosleep(32);
+            }
+            if (!done) {
+                // Owned before any of the brick is read (and fenced below): a neighbour that
+                // stored before finding the brick queued is seen; one that stores later
+                // finds it owned and marks it dirty.
+                const unsigned s = item >> p.local_bits, b = item & ((1u << p.local_bits) - 1u);
+                atomicExch(p.qflag + p.shots[s].qbase + b, kOwned);
+                if (atomicAdd(p.stats + 2, 1ull) >= act_cap) atomicCAS(p.ctrl + kErr, 0u, (unsigned)kDevRoundCap);
+            }
+        }
+        done = __shfl_sync(kFull, done, 0);
+        if (done) break;
+        item = __shfl_sync(kFull, item, 0);
+        __threadfence();  // the previous owner's stores of neighbouring bricks are visible
+        BrickLoad A;
+        load_brick(p, item, A);
+        relax_brick<kFastSqrt, true>(p, A, 0u, tile, ws);
+    }
+    if (lane == 0 && ws.act) {
+        atomicAdd(p.stats + 0, ws.act);
+        atomicAdd(p.stats + 1, ws.inner);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kRounds] = 0u;
+    // receivers once every brick is done: wait until no work is pending (bounded)
+    if (p.nrec == 0) return;
+    if (threadIdx.x == 0) {
+        unsigned long long spins = 0;
+        while (ld_volatile(p.ctrl + kCnt1) != 0u && ld_volatile(p.ctrl + kErr) == 0u) {
+            if (++spins > p.spin_limit) {
+                atomicCAS(p.ctrl + kErr, 0u, (unsigned)kDevBarrierTimeout);
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    if (ld_volatile(p.ctrl + kErr) != 0u) return;
     sample_receivers(p.T, p.shots, p.nshots, p.rx, p.ry, p.rz, p.nrec, p.dx, p.dy, p.dz, p.nz, p.t_recv);
 }
 
@@ -452,11 +621,11 @@ __global__ void k_fim_init(float4 *T4, size_t n4, unsigned *qflag, size_t nq, un
     for (size_t i = t; i < n4; i += stride) __stcg(T4 + i, inf4);
     for (size_t i = t; i < nq; i += stride) qflag[i] = 0u;
     if (t < kCtrlWords) ctrl[t] = 0u;
-    if (t < 2) stats[t] = 0ull;
+    if (t < 3) stats[t] = 0ull;
 }
 
 __global__ void k_fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
-                           unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl)
+                           unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, int async)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < nshots) {
@@ -470,7 +639,10 @@ __global__ void k_fim_seed(const ShotDesc *shots, int nshots, const float *S, in
         qflag[d.qbase + d.src_brick] = 1u;
         lists[s] = ((unsigned)s << local_bits) | (unsigned)d.src_brick;
     }
-    if (s == 0) ctrl[kCnt0] = (unsigned)nshots;
+    if (s == 0) {
+        ctrl[kCnt0] = (unsigned)nshots;           // rounds: items of round 0; async: ring tail
+        if (async) ctrl[kCnt1] = (unsigned)nshots;  // async: pending work
+    }
 }
 
 __global__ void k_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out)
@@ -622,15 +794,24 @@ cudaError_t fim_init(float *T, size_t t_count, unsigned *qflag, size_t q_count, 
 }
 
 cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
-                     unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st)
+                     unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st,
+                     size_t ring_cap)
 {
-    k_fim_seed<<<(nshots + 127) / 128, 128, 0, st>>>(shots, nshots, S, gbx, gbz, T, qflag, lists, local_bits, ctrl);
+    if (ring_cap) {  // asynchronous schedule: an empty ring, then the seeds in its first slots
+        const cudaError_t e = cudaMemsetAsync(lists, 0xff, ring_cap * sizeof(unsigned), st);
+        if (e != cudaSuccess) return e;
+    }
+    k_fim_seed<<<(nshots + 127) / 128, 128, 0, st>>>(shots, nshots, S, gbx, gbz, T, qflag, lists, local_bits, ctrl,
+                                                     ring_cap ? 1 : 0);
     return cudaGetLastError();
 }
 
+// Both schedules run as cooperative launches (every CTA resident): the rounds schedule
+// needs it for its grid barrier, the asynchronous one for its waits on other CTAs' pushes.
 template <int MINB, bool kFastSqrt>
-static cudaError_t launch_solve(const FimLaunch &p, int block_warps, int *grid_out, cudaStream_t st)
+static cudaError_t launch_solve(const FimLaunch &p, int block_warps, bool async, int *grid_out, cudaStream_t st)
 {
+    const void *fn = async ? (const void *)k_fim_async<MINB, kFastSqrt> : (const void *)k_fim_solve<MINB, kFastSqrt>;
     const int threads = 32 * block_warps;
     const size_t smem = (size_t)block_warps * 2 * kTileNodes * sizeof(float);
     int dev = 0, nsm = 0, per_sm = 0;
@@ -638,36 +819,36 @@ static cudaError_t launch_solve(const FimLaunch &p, int block_warps, int *grid_o
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fim_solve<MINB, kFastSqrt>, threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int grid = nsm * per_sm;
     if (grid_out) *grid_out = grid;
     FimLaunch pp = p;
     void *args[] = {&pp};
-    return cudaLaunchCooperativeKernel((const void *)k_fim_solve<MINB, kFastSqrt>, dim3(grid), dim3(threads), args,
-                                       smem, st);
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, smem, st);
 }
 
 template <bool kFastSqrt>
-static cudaError_t solve_occ(const FimLaunch &p, int block_warps, int occupancy, int *grid_out, cudaStream_t st)
+static cudaError_t solve_occ(const FimLaunch &p, int block_warps, int occupancy, bool async, int *grid_out,
+                             cudaStream_t st)
 {
     switch (occupancy) {
-    case 1: return launch_solve<1, kFastSqrt>(p, block_warps, grid_out, st);
-    case 2: return launch_solve<2, kFastSqrt>(p, block_warps, grid_out, st);
-    case 3: return launch_solve<3, kFastSqrt>(p, block_warps, grid_out, st);
-    case 5: return launch_solve<5, kFastSqrt>(p, block_warps, grid_out, st);
-    case 6: return launch_solve<6, kFastSqrt>(p, block_warps, grid_out, st);
-    default: return launch_solve<4, kFastSqrt>(p, block_warps, grid_out, st);
+    case 1: return launch_solve<1, kFastSqrt>(p, block_warps, async, grid_out, st);
+    case 2: return launch_solve<2, kFastSqrt>(p, block_warps, async, grid_out, st);
+    case 3: return launch_solve<3, kFastSqrt>(p, block_warps, async, grid_out, st);
+    case 5: return launch_solve<5, kFastSqrt>(p, block_warps, async, grid_out, st);
+    case 6: return launch_solve<6, kFastSqrt>(p, block_warps, async, grid_out, st);
+    default: return launch_solve<4, kFastSqrt>(p, block_warps, async, grid_out, st);
     }
 }
 
 cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, bool ieee_sqrt, int *grid_out,
-                      cudaStream_t st)
+                      cudaStream_t st, bool async)
 {
     if (block_warps < 1 || block_warps > 8) block_warps = 8;
-    return ieee_sqrt ? solve_occ<false>(p, block_warps, occupancy, grid_out, st)
-                     : solve_occ<true>(p, block_warps, occupancy, grid_out, st);
+    return ieee_sqrt ? solve_occ<false>(p, block_warps, occupancy, async, grid_out, st)
+                     : solve_occ<true>(p, block_warps, occupancy, async, grid_out, st);
 }
 
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out, cudaStream_t st)

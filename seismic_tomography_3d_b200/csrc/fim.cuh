@@ -33,7 +33,7 @@ struct FimLaunch {
     unsigned *lists;      // 3 work lists of list_cap entries
     unsigned list_cap;
     unsigned *ctrl;       // kCtrlWords control words
-    unsigned long long *stats;  // [0] activations, [1] inner iterations
+    unsigned long long *stats;  // [0] activations, [1] inner iterations, [2] async activation count
     int gbx, gbz;         // global brick grid (x, z) for S addressing
     float h;              // grid spacing of the update (dx, as the reference)
     int max_inner, max_rounds;
@@ -54,10 +54,14 @@ cudaError_t fim_brick_model(const float *slow, float *S, int nx, int ny, int nz,
                             int nzz, cudaStream_t st);
 cudaError_t fim_init(float *T, size_t t_count, unsigned *qflag, size_t q_count, unsigned *ctrl,
                      unsigned long long *stats, cudaStream_t st);
+// ring_cap > 0: the asynchronous schedule; lists holds a ring of ring_cap = 3 x list_cap
+// items (the whole list buffer).
 cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
-                     unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st);
+                     unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st,
+                     size_t ring_cap = 0);
+// async: the asynchronous schedule (seeded with ring_cap = list_cap), else rounds.
 cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, bool ieee_sqrt, int *grid_out,
-                      cudaStream_t st);
+                      cudaStream_t st, bool async = false);
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out,
                         cudaStream_t st);
 cudaError_t velocity_to_slowness(const float *v, float *s, size_t n, cudaStream_t st);

@@ -101,11 +101,13 @@ def test_eikonal_and_tomography_executables(tomo, tmp_path):
         ctx.cgls(10, want_x=False)
         vel = ctx.model_update()
     nz, nx, ny = t["nz"], t["nx"], t["ny"]
+    # The default (asynchronous) schedule relaxes bricks in a run-dependent order; with the
+    # 1e-6 s face tolerance two runs agree to ~1e-6 relative, not bit for bit.
     for i in range(len(shots)):
         tt = np.fromfile(os.path.join(d, "tt", f"fim_eikonal_nz{nz}_nx{nx}_ny{ny}_shot_{i + 1}.bin"), np.float32)
-        np.testing.assert_array_equal(tt.reshape(ny, nx, nz), vols[i])
+        np.testing.assert_allclose(tt.reshape(ny, nx, nz), vols[i], rtol=1e-5, atol=1e-7)
         fa = np.fromfile(os.path.join(d, "fa", f"fim_times_nr{len(nodes)}_shot_{i + 1}.bin"), np.float32)
-        np.testing.assert_array_equal(fa, dcal[i])
+        np.testing.assert_allclose(fa, dcal[i], rtol=1e-5, atol=1e-7)
     xyz = np.loadtxt(os.path.join(d, "xyz_shots.txt"), delimiter=",", dtype=np.float32).reshape(-1, 3)
     np.testing.assert_array_equal(xyz, shots)
 
@@ -113,7 +115,7 @@ def test_eikonal_and_tomography_executables(tomo, tmp_path):
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     model = np.fromfile(os.path.join(d, "models", "fim_model_iteration_1.bin"), np.float32).reshape(ny, nx, nz)
-    np.testing.assert_array_equal(model, vel)
+    np.testing.assert_allclose(model, vel, rtol=1e-4)
     conv = np.loadtxt(os.path.join(d, "conv", "fim_convergency.txt"))
     # the reference's hard-coded interior masks confine the update to a small region of
     # this model, so the residual barely moves (as in the reference's own run)

@@ -151,10 +151,14 @@ def test_errors_are_status_codes(tomo):
             ctx.eik_solve([[5.0, 5.0, 0.0]], windows=[[1, 12, 0, 12]])  # unaligned window
         assert e.value.status == -1
         with pytest.raises(tomo.TomoError) as e:
-            ctx.eik_solve([[50.0, 50.0, 0.0]], max_rounds=2)  # round cap
+            ctx.eik_solve([[50.0, 50.0, 0.0]], max_rounds=2, schedule=1)  # round cap
         assert e.value.status == -4
-        t, st = ctx.eik_solve([[50.0, 50.0, 0.0]])  # context still usable
+        t, st = ctx.eik_solve([[50.0, 50.0, 0.0]], schedule=1)  # context still usable
         assert st["rounds"] > 2
+        with pytest.raises(tomo.TomoError) as e:  # asynchronous schedule: activation cap
+            ctx.eik_solve([[50.0, 50.0, 0.0]], max_rounds=1, max_inner=1, schedule=2)
+        assert e.value.status == -4
+        ctx.eik_solve([[50.0, 50.0, 0.0]], schedule=2)
 
 
 @pytest.mark.slow
@@ -187,3 +191,18 @@ def test_autotune_picks_a_shape_and_keeps_results(tomo):
         ctx.eik_solve(sv.shots, windows=sv.windows)
         for i in range(len(sv.shots)):
             assert rel_err(ctx.eik_volume(i), ref[i], sv.h, float(sv.velocity.max())) < 1e-5
+
+
+@pytest.mark.parametrize("windows", [False, True])
+def test_async_and_round_schedules_agree(tomo, windows):
+    """The asynchronous schedule and the round-synchronous one (default) relax the bricks in
+    different orders towards the same fixed point."""
+    sv = wl.small(31, 52, 44, 26, nshots=6, windows=windows)
+    with tomo.Context(sv.nx, sv.ny, sv.nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(sv.shots, windows=sv.windows, schedule=1, change_tol=-1.0)
+        ref = [ctx.eik_volume(i) for i in range(len(sv.shots))]
+        _, st = ctx.eik_solve(sv.shots, windows=sv.windows, change_tol=-1.0, schedule=2)
+        assert st["rounds"] == 0 and st["activations"] > 0
+        for i in range(len(sv.shots)):
+            assert rel_err(ctx.eik_volume(i), ref[i], sv.h, float(sv.velocity.max())) < 1e-6

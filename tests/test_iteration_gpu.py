@@ -1,7 +1,8 @@
 """tomo_iteration: a whole tomography iteration in one call, eager or replayed from CUDA
 graphs, against the same stages called one by one (tomo_eik_solve, tomo_build_jacobian,
 tomo_cgls, tomo_model_update).  The eikonal runs to its exact FP32 fixed point
-(change_tol < 0) so that the three paths see the same fields; the updated models must agree
+(change_tol < 0) on the round schedule, whose brick order does not depend on the run, so
+that the three paths see the same fields; the updated models must agree
 to 1e-5 relative RMS, and the second graph call must be a pure replay.  The reference's
 hard-coded interior masks would leave this small model (shallow surface-to-surface rays)
 untouched, so the update runs unmasked here."""
@@ -31,7 +32,7 @@ def survey():
 def _observed(tomo, sv):
     with tomo.Context(sv["nx"], sv["ny"], sv["nz"], H) as ctx:
         ctx.set_velocity(sv["true_v"])
-        dobs, _ = ctx.eik_solve(sv["shots"], receivers=sv["rec"], change_tol=-1.0)
+        dobs, _ = ctx.eik_solve(sv["shots"], receivers=sv["rec"], change_tol=-1.0, schedule=1)
     return dobs
 
 
@@ -40,7 +41,7 @@ def _per_stage(tomo, sv, dobs, iters):
     ctx.set_velocity(sv["start"])
     ctx.set_observed(dobs)
     for _ in range(iters):
-        ctx.eik_solve(sv["shots"], receivers=sv["rec"], want_recv=False, change_tol=-1.0)
+        ctx.eik_solve(sv["shots"], receivers=sv["rec"], want_recv=False, change_tol=-1.0, schedule=1)
         ctx.build_jacobian(D, 2, 0.1)
         ctx.cgls(10, want_x=False)
         ctx.model_update(True, 5, 2.0, reference_masks=False, want_velocity=False)
@@ -58,7 +59,7 @@ def test_iteration_matches_per_stage_calls(tomo, survey, use_graph):
         ctx.set_velocity(sv["start"])
         ctx.set_observed(dobs)
         stats = [ctx.iteration(sv["shots"], sv["rec"], D, cg_iterations=10, use_graph=use_graph, change_tol=-1.0,
-                               reference_masks=False) for _ in range(3)]
+                               reference_masks=False, schedule=1) for _ in range(3)]
         s = ctx.get_slowness()
     rms = float(np.sqrt(np.mean(((s - ref) / ref) ** 2)))
     assert rms < 1e-5, rms
@@ -83,7 +84,7 @@ def test_iteration_recaptures_when_the_jacobian_outgrows_its_capacity(tomo, surv
             ctx.set_velocity(sv["start"])
             ctx.set_observed(dobs)
             st = [ctx.iteration(sv["shots"], sv["rec"], D, cg_iterations=10, use_graph=use_graph, change_tol=-1.0,
-                                nnz_headroom=1.0, reference_masks=False) for _ in range(3)]
+                                nnz_headroom=1.0, reference_masks=False, schedule=1) for _ in range(3)]
             out.append((ctx.get_slowness(), st))
     (s0, st0), (s1, st1) = out
     assert [a["nnz"] for a in st0] == [b["nnz"] for b in st1]
