@@ -474,9 +474,9 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
         const unsigned *list = p.lists + (size_t)cur * p.list_cap;
         unsigned *cursor = p.ctrl + kCur0 + cur;
         // One item at a time, fetched only when the warp is free: loading the next brick
-        // ahead doubles the live registers (4 % slower), and even reserving the next item
-        // index early (its atomic overlapping the relaxation) is 5 % slower, because busy
-        // warps then hold items that idle warps could take at the end of a round.
+        // ahead doubles the live registers (4 % slower), and reserving the next item index
+        // early (its atomic overlapping the relaxation) is 2-5 % slower even when limited
+        // to rounds with many items left.
         for (unsigned i = fetch_item(cursor); i < n; i = fetch_item(cursor)) {
             BrickLoad A;
             load_brick(p, __ldcg(list + i), A);
