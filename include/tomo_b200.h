@@ -100,6 +100,7 @@ typedef struct {
     long long activations;       /* brick activations (sum over shots)                    */
     long long inner_iterations;  /* sum over activations of in-brick iterations           */
     long long nodes_per_brick;   /* nodes of one brick                                    */
+    long long idle_activations;  /* activations that lowered no node (JW)                 */
     float setup_ms;              /* device time of the pool reset + seeding kernels       */
     float solve_ms;              /* device time of the persistent solve kernel             */
     float total_ms;              /* device time of the whole call incl. copies             */

@@ -56,6 +56,7 @@ class EikOpts(ctypes.Structure):
 class EikStats(ctypes.Structure):
     _fields_ = [("rounds", ctypes.c_longlong), ("activations", ctypes.c_longlong),
                 ("inner_iterations", ctypes.c_longlong), ("nodes_per_brick", ctypes.c_longlong),
+                ("idle_activations", ctypes.c_longlong),
                 ("setup_ms", ctypes.c_float), ("solve_ms", ctypes.c_float), ("total_ms", ctypes.c_float)]
 
     def as_dict(self):

@@ -484,18 +484,19 @@ tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, in
 
 // Reads the control words and counters of the last persistent solve (synchronises).
 int read_solve(tomo_ctx *ctx, unsigned &rounds, unsigned long long &act, unsigned long long &inner,
-               const SolveCfg &c)
+               const SolveCfg &c, unsigned long long *idle = nullptr)
 {
     CK(cudaMemcpyAsync(ctx->pinned_ctrl, ctx->ctrl.ptr, tomo::kCtrlWords * sizeof(unsigned), cudaMemcpyDeviceToHost,
                        ctx->stream));
-    CK(cudaMemcpyAsync(ctx->pinned_ctrl + tomo::kCtrlWords, ctx->stats.ptr, 2 * sizeof(unsigned long long),
+    CK(cudaMemcpyAsync(ctx->pinned_ctrl + tomo::kCtrlWords, ctx->stats.ptr, 4 * sizeof(unsigned long long),
                        cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    unsigned long long st[2];
+    unsigned long long st[4];
     std::memcpy(st, ctx->pinned_ctrl + tomo::kCtrlWords, sizeof(st));
     rounds = ctx->pinned_ctrl[tomo::kRounds];
     act = st[0];
     inner = st[1];
+    if (idle) *idle = st[3];
     const unsigned derr = ctx->pinned_ctrl[tomo::kErr];
     if (derr == tomo::kDevRoundCap)
         return fail(ctx, TOMO_ERR_NOT_CONVERGED,
@@ -595,14 +596,15 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
                            ctx->stream));
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     unsigned rounds = 0;
-    unsigned long long act = 0, inner = 0;
-    rc = read_solve(ctx, rounds, act, inner, cfg);
+    unsigned long long act = 0, inner = 0, idle = 0;
+    rc = read_solve(ctx, rounds, act, inner, cfg, &idle);
     keep_batch(ctx, bt, shots, nrec, receivers);
     ctx->have_solve = (rc == TOMO_OK);
     if (stats) {
         stats->rounds = rounds;
         stats->activations = (long long)act;
         stats->inner_iterations = (long long)inner;
+        stats->idle_activations = (long long)idle;
         stats->nodes_per_brick = tomo::kBrickNodes;
         cudaEventElapsedTime(&stats->setup_ms, ctx->ev[0], ctx->ev[3]);
         cudaEventElapsedTime(&stats->solve_ms, ctx->ev[3], ctx->ev[1]);

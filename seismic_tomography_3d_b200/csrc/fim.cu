@@ -137,7 +137,7 @@ __device__ void sample_receivers(const float *T, const ShotDesc *shots, int nsho
 }
 
 struct WarpStats {
-    unsigned long long act, inner;
+    unsigned long long act, inner, idle;  // idle: activations that lowered no node
 };
 
 // Data of one work item as loaded from global memory.
@@ -373,6 +373,7 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     ws.inner += (unsigned long long)it;
 
     const bool any_drop = __any_sync(kFull, (c0 < i0) | (c1 < i1));
+    if (!any_drop) ws.idle += 1;
     if (any_drop) {
         const int n0 = lane_node(lane);
         __stcg(Tb + n0, c0);
@@ -451,7 +452,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5;
     float *tile = smem + warp * 2 * kTileNodes;
-    WarpStats ws{0ull, 0ull};
+    WarpStats ws{0ull, 0ull, 0ull};
 
     unsigned round = 0;
     bool ok = true;
@@ -488,6 +489,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
     if ((threadIdx.x & 31) == 0 && ws.act) {
         atomicAdd(p.stats + 0, ws.act);
         atomicAdd(p.stats + 1, ws.inner);
+        atomicAdd(p.stats + 3, ws.idle);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kRounds] = round;
     if (!ok || p.nrec == 0) return;
@@ -501,7 +503,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_async(FimLaunch p)
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float *tile = smem + warp * 2 * kTileNodes;
-    WarpStats ws{0ull, 0ull};
+    WarpStats ws{0ull, 0ull, 0ull};
     unsigned *ring = ring_of(p);
     const unsigned long long act_cap =
         p.max_rounds > 0 ? (unsigned long long)p.max_rounds * p.list_cap : ~0ull;  // activations
@@ -549,6 +551,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_async(FimLaunch p)
     if (lane == 0 && ws.act) {
         atomicAdd(p.stats + 0, ws.act);
         atomicAdd(p.stats + 1, ws.inner);
+        atomicAdd(p.stats + 3, ws.idle);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kRounds] = 0u;
     // receivers once every brick is done: wait until no work is pending (bounded)
@@ -621,7 +624,7 @@ __global__ void k_fim_init(float4 *T4, size_t n4, unsigned *qflag, size_t nq, un
     for (size_t i = t; i < n4; i += stride) __stcg(T4 + i, inf4);
     for (size_t i = t; i < nq; i += stride) qflag[i] = 0u;
     if (t < kCtrlWords) ctrl[t] = 0u;
-    if (t < 3) stats[t] = 0ull;
+    if (t < 4) stats[t] = 0ull;
 }
 
 __global__ void k_fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,

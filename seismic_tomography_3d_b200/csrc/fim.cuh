@@ -33,7 +33,8 @@ struct FimLaunch {
     unsigned *lists;      // 3 work lists of list_cap entries
     unsigned list_cap;
     unsigned *ctrl;       // kCtrlWords control words
-    unsigned long long *stats;  // [0] activations, [1] inner iterations, [2] async activation count
+    unsigned long long *stats;  // [0] activations, [1] inner iterations, [2] async activation
+                                // count, [3] activations that lowered no node
     int gbx, gbz;         // global brick grid (x, z) for S addressing
     float h;              // grid spacing of the update (dx, as the reference)
     int max_inner, max_rounds;
