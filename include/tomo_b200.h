@@ -69,7 +69,7 @@ typedef struct {
     int op;          /* TOMO_OP_*                                                     */
     int max_inner;   /* cap of in-brick iterations per activation (0: default 16)     */
     int max_rounds;  /* cap of outer rounds (0: default 1<<20)                        */
-    int brick;       /* brick shape id (0: tuned default); see tomo_eik_brick_shapes  */
+    int brick;       /* brick shape: 0 or 1 = 4x4x4, the one shape of tomo_eik_brick_shapes */
     int block_warps; /* warps per CTA of the persistent kernel (0: default)           */
     int occupancy;   /* CTAs per SM the kernel is compiled for, 1..6 (0: default 4)   */
     float change_tol;/* a face value must drop by more than this (s) to re-queue the
@@ -141,7 +141,7 @@ int tomo_get_slowness(tomo_ctx *ctx, float *slowness_out);
  *   t_recv     host nshots*nrec (row-major shot, receiver) receiver times by trilinear
  *              interpolation (block_FIM.cpp:228-262); NULL keeps them on the device only
  *   opts/stats may be NULL.
- * Traveltime fields stay on the device for tomo_eik_volume / tomo_raytrace. */
+ * Traveltime fields stay on the device for tomo_eik_volume(s) and tomo_build_jacobian. */
 int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows,
                    int nrec, const tomo_point *receivers, float *t_recv,
                    const tomo_eik_opts *opts, tomo_eik_stats *stats);

@@ -568,6 +568,10 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
     if (opts && opts->op != TOMO_OP_JW && opts->op != TOMO_OP_NGB)
         return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown eikonal operator");
+    if (opts && (opts->brick < 0 || opts->brick > 1))
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown brick shape (tomo_eik_brick_shapes lists 1: 4x4x4)");
+    if (opts && (opts->schedule < TOMO_SCHED_DEFAULT || opts->schedule > TOMO_SCHED_ASYNC))
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown work schedule");
     const SolveCfg cfg = solve_cfg(ctx, opts);
     CK(cudaSetDevice(ctx->device));
     Batch bt;
