@@ -577,6 +577,7 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     Batch bt;
     int rc = make_batch(ctx, nshots, shots, windows, nrec, receivers, bt);
     if (rc != TOMO_OK) return rc;
+    ctx->have_solve = false;  // the pool is about to be overwritten
     rc = upload_batch(ctx, bt, nrec, receivers);
     if (rc != TOMO_OK) return rc;
 
@@ -635,6 +636,7 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
     Batch bt;
     int rc = make_batch(ctx, nshots, shots, windows, nrec, receivers, bt);
     if (rc != TOMO_OK) return rc;
+    ctx->have_solve = false;  // the pool is about to be overwritten
     rc = upload_batch(ctx, bt, nrec, receivers);
     if (rc != TOMO_OK) return rc;
     CK(ctx->viol.ensure((size_t)nshots * 2));
