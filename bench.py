@@ -460,7 +460,7 @@ def run_inversion(args):
         st = ctx.iteration(sv.shots, sv.receivers, inv["d_tomo"], tk_order=inv["tk_order"], tk_param=inv["tk_param"],
                            cg_iterations=inv["cg_iterations"], smooth=inv["smooth"],
                            filter_samples=inv["filter_samples"], standard_deviation=inv["standard_deviation"],
-                           use_graph=True)
+                           use_graph=True, **SOLVER)
         if it == 0:
             free, total = torch.cuda.mem_get_info()
         iters.append({"residual_l2_s": st["residual"], "total_ms": st["ms"], "nnz": st["nnz"],
@@ -469,7 +469,7 @@ def run_inversion(args):
     for it in range(inv["iterations"] if args.no_graph else 0):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         ev[0].record(stream)
-        _, est = ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False)
+        _, est = ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False, **SOLVER)
         ev[1].record(stream)
         res = ctx.data_residual()
         jst = ctx.build_jacobian(inv["d_tomo"], inv["tk_order"], inv["tk_param"])
@@ -489,7 +489,7 @@ def run_inversion(args):
                       "rays_nonfinite": jst["rays_nonfinite"], "rays_outside": jst["rays_outside"],
                       "rays_overflow": jst["rays_overflow"], "ray_steps": jst["ray_steps"],
                       "cgls_rnorm": cst["rnorm"]})
-    ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False)
+    ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False, **SOLVER)
     final_res = ctx.data_residual()
     v_est = 1.0 / ctx.get_slowness()
     v_true, v0 = sv.velocity.astype(np.float64), start.astype(np.float64)
@@ -502,7 +502,7 @@ def run_inversion(args):
         # one more iteration stage by stage (after the model figures above): where the time goes
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         ev[0].record(stream)
-        ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False)
+        ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False, **SOLVER)
         ev[1].record(stream)
         ctx.build_jacobian(inv["d_tomo"], inv["tk_order"], inv["tk_param"])
         ev[2].record(stream)
@@ -525,6 +525,7 @@ def run_inversion(args):
             "hbm_used_gb": (total - free) / 1e9, "per_iteration": iters,
             "config": {"workload": "config5: 401x401x201 @10 m (32.3 M nodes), 256 shots x 10,000 receivers, "
                                    "full windows, 50 m cells (81x81x41), tk order 2 lambda 0.1, 30 CGLS, 5 iterations",
+                       "eikonal_tolerances_s": SOLVER,
                        "start": "v(z) = 1500 + 1.0 z", "picks": "plain FIM on the true model + N(0, 2 ms)"},
             "data": "synthetic (seeded config-5 model, shots, receivers)"}
     print(json.dumps(line), flush=True)
@@ -615,7 +616,7 @@ def run_tomography(args):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         ev[0].record(stream)
         ctx.set_velocity(start)
-        _, est = ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False)
+        _, est = ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False, **SOLVER)
         ev[1].record(stream)
         jst = ctx.build_jacobian(inv["d_tomo"], inv["tk_order"], inv["tk_param"])
         ev[2].record(stream)
@@ -647,6 +648,7 @@ def run_tomography(args):
                      "roofline": {"bound": "hbm", "achieved": cg_bytes / (cg_ms_it / 1000.0) / 1e9, "peak": peak,
                                   "unit": "GB/s", "frac": cg_bytes / (cg_ms_it / 1000.0) / 1e9 / peak,
                                   "peak_kind": peak_kind, "alg_bytes_per_iteration": cg_bytes}},
+            "eikonal_tolerances_s": SOLVER,
             "data": "synthetic (seeded config-3 model, 64 shots x 2500 receivers, picks + N(0, 2 ms))"}
     print(json.dumps(line), flush=True)
     ctx.close()
