@@ -77,13 +77,17 @@ __device__ __forceinline__ float godunov_jw(float a, float b, float c, const Nod
     return (u0 < kInf) ? t : kInf;
 }
 
-// Tile of one warp: (4+2)^3 nodes, the brick plus a one-node face halo.
-constexpr int kTile = kBrick + 2;
-constexpr int kTileNodes = kTile * kTile * kTile;
+// Tile of one warp: (4+2)^3 nodes, the brick plus a one-node face halo, z fastest.  The x
+// and y strides are padded (8 and 52 words instead of 6 and 36) so that every shared-memory
+// access of the relaxation -- a phase's six neighbour reads and its store, over the 32 lanes
+// -- falls in 32 distinct banks.
+constexpr int kTileX = 8;
+constexpr int kTileY = 52;
+constexpr int kTileNodes = kTileY * (kBrick + 2);
 
 __device__ __forceinline__ int tile_idx(int z, int x, int y)
 {
-    return (z + 1) + kTile * ((x + 1) + kTile * (y + 1));
+    return (z + 1) + kTileX * (x + 1) + kTileY * (y + 1);
 }
 
 __device__ __forceinline__ float brick_T(const float *T, const ShotDesc &d, int x, int y, int z)
@@ -323,45 +327,47 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
 
     const int z0 = lane & 3, x0 = (lane >> 2) & 3, y0 = 2 * (lane >> 4);
     const int ti0 = tile_idx(z0, x0, y0);
-    const int ti1 = ti0 + kTile * kTile;  // y + 1
+    const int ti1 = ti0 + kTileY;  // y + 1
     const float i0 = L.i0, i1 = L.i1;
-    float c0 = i0, c1 = i1;
-    // Two tile buffers: iteration k reads one and writes the other, so one __syncwarp per
-    // iteration orders both the reads before the next writes and the writes before the
-    // next reads.  The halo is written to both.
-    float *tile1 = tile + kTileNodes;
-    tile[ti0] = c0;
-    tile[ti1] = c1;
+    tile[ti0] = i0;
+    tile[ti1] = i1;
 #pragma unroll
     for (int q = 0; q < 3; q++) {
         int node, ti;
         (void)halo_slot(d, b, bz, bx, by, lane, q, node, ti);
         tile[ti] = L.hv[q];
-        tile1[ti] = L.hv[q];
     }
     __syncwarp();
 
-    const NodeConst k0 = node_const(p.h, L.s0), k1 = node_const(p.h, L.s1);
+    // Red-black Gauss-Seidel.  A lane's two nodes are y-adjacent, so one is red (z + x + y
+    // even) and the other black: phase A relaxes the lane's red node from black neighbours,
+    // phase B its black node from the new red ones.  Every neighbour of a node has the other
+    // colour, so each phase reads only what the other phase writes, and a dependency chain
+    // -- alternating in colour -- advances two nodes per iteration where Jacobi advances one.
+    // Of a phase's two y-neighbours one is the lane's other node (a register), the other is
+    // in the tile at offset yA (phase A) or -yA (phase B).
+    const bool red0 = ((z0 + x0) & 1) == 0;
+    const int tA = red0 ? ti0 : ti1, tB = red0 ? ti1 : ti0;
+    const int yA = red0 ? -kTileY : kTileY;
+    float cA = red0 ? i0 : i1, cB = red0 ? i1 : i0;
+    const NodeConst kA = node_const(p.h, red0 ? L.s0 : L.s1), kB = node_const(p.h, red0 ? L.s1 : L.s0);
     bool more = true;
     int it = 0;
     for (; it < p.max_inner; ++it) {
-        const float *rd = (it & 1) ? tile1 : tile;
-        float *wr = (it & 1) ? tile : tile1;
-        // Jacobi: both nodes from the previous iteration's values, two independent chains
-        // for the scheduler to interleave.
-        const float a0 = fminf(rd[ti0 - kTile], rd[ti0 + kTile]);
-        const float g0 = fminf(rd[ti0 - 1], rd[ti0 + 1]);
-        const float a1 = fminf(rd[ti1 - kTile], rd[ti1 + kTile]);
-        const float g1 = fminf(rd[ti1 - 1], rd[ti1 + 1]);
-        const float b0 = fminf(rd[ti0 - kTile * kTile], c1);
-        const float b1 = fminf(c0, rd[ti1 + kTile * kTile]);
-        const float n0 = fminf(c0, godunov_jw<kFastSqrt>(a0, b0, g0, k0));
-        const float n1 = fminf(c1, godunov_jw<kFastSqrt>(a1, b1, g1, k1));
-        const bool ch = (n0 < c0 - p.inner_tol) | (n1 < c1 - p.inner_tol);
-        wr[ti0] = n0;
-        wr[ti1] = n1;
-        c0 = n0;
-        c1 = n1;
+        const float aA = fminf(tile[tA - kTileX], tile[tA + kTileX]);
+        const float gA = fminf(tile[tA - 1], tile[tA + 1]);
+        const float bA = fminf(tile[tA + yA], cB);
+        const float nA = fminf(cA, godunov_jw<kFastSqrt>(aA, bA, gA, kA));
+        tile[tA] = nA;
+        __syncwarp();
+        const float aB = fminf(tile[tB - kTileX], tile[tB + kTileX]);
+        const float gB = fminf(tile[tB - 1], tile[tB + 1]);
+        const float bB = fminf(tile[tB - yA], nA);
+        const float nB = fminf(cB, godunov_jw<kFastSqrt>(aB, bB, gB, kB));
+        tile[tB] = nB;
+        const bool ch = (nA < cA - p.inner_tol) | (nB < cB - p.inner_tol);
+        cA = nA;
+        cB = nB;
         __syncwarp();
         if (!__any_sync(kFull, ch)) {
             more = false;
@@ -369,6 +375,7 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
             break;
         }
     }
+    const float c0 = red0 ? cA : cB, c1 = red0 ? cB : cA;
     ws.act += 1;
     ws.inner += (unsigned long long)it;
 
@@ -386,13 +393,12 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     // y.  T(y) is the halo cell loaded at the start of this activation; a concurrent drop of
     // y only makes the test more permissive.
     const bool d0 = c0 < i0 - p.change_tol, d1 = c1 < i1 - p.change_tol;
-    const int kT2 = kTile * kTile;
     const bool fzm = (z0 == 0) && ((d0 && c0 < tile[ti0 - 1]) || (d1 && c1 < tile[ti1 - 1]));
     const bool fzp = (z0 == 3) && ((d0 && c0 < tile[ti0 + 1]) || (d1 && c1 < tile[ti1 + 1]));
-    const bool fxm = (x0 == 0) && ((d0 && c0 < tile[ti0 - kTile]) || (d1 && c1 < tile[ti1 - kTile]));
-    const bool fxp = (x0 == 3) && ((d0 && c0 < tile[ti0 + kTile]) || (d1 && c1 < tile[ti1 + kTile]));
-    const bool fym = (y0 == 0) && d0 && c0 < tile[ti0 - kT2];
-    const bool fyp = (y0 == 2) && d1 && c1 < tile[ti1 + kT2];
+    const bool fxm = (x0 == 0) && ((d0 && c0 < tile[ti0 - kTileX]) || (d1 && c1 < tile[ti1 - kTileX]));
+    const bool fxp = (x0 == 3) && ((d0 && c0 < tile[ti0 + kTileX]) || (d1 && c1 < tile[ti1 + kTileX]));
+    const bool fym = (y0 == 0) && d0 && c0 < tile[ti0 - kTileY];
+    const bool fyp = (y0 == 2) && d1 && c1 < tile[ti1 + kTileY];
     const unsigned face = (__ballot_sync(kFull, fzm) ? 1u : 0u) | (__ballot_sync(kFull, fzp) ? 2u : 0u) |
                           (__ballot_sync(kFull, fxm) ? 4u : 0u) | (__ballot_sync(kFull, fxp) ? 8u : 0u) |
                           (__ballot_sync(kFull, fym) ? 16u : 0u) | (__ballot_sync(kFull, fyp) ? 32u : 0u);
@@ -451,7 +457,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
 {
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5;
-    float *tile = smem + warp * 2 * kTileNodes;
+    float *tile = smem + warp * kTileNodes;
     WarpStats ws{0ull, 0ull, 0ull};
 
     unsigned round = 0;
@@ -502,7 +508,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_async(FimLaunch p)
 {
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float *tile = smem + warp * 2 * kTileNodes;
+    float *tile = smem + warp * kTileNodes;
     WarpStats ws{0ull, 0ull, 0ull};
     unsigned *ring = ring_of(p);
     const unsigned long long act_cap =
@@ -816,7 +822,7 @@ static cudaError_t launch_solve(const FimLaunch &p, int block_warps, bool async,
 {
     const void *fn = async ? (const void *)k_fim_async<MINB, kFastSqrt> : (const void *)k_fim_solve<MINB, kFastSqrt>;
     const int threads = 32 * block_warps;
-    const size_t smem = (size_t)block_warps * 2 * kTileNodes * sizeof(float);
+    const size_t smem = (size_t)block_warps * kTileNodes * sizeof(float);
     int dev = 0, nsm = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
