@@ -415,6 +415,7 @@ int make_batch(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_wi
     while ((1ll << bt.local_bits) < max_bricks) bt.local_bits++;
     if (bt.local_bits + 1 >= 32 || ((unsigned long long)nshots << bt.local_bits) >= (1ull << 32))
         return fail(ctx, TOMO_ERR_CAPACITY, "too many shots x bricks for one batch; split the batch");
+    for (ShotDesc &d : bt.sd) tomo::set_brick_division(d, bt.local_bits);
     for (int r = 0; r < nrec; r++) {
         const tomo_point &p = receivers[r];
         if (!(p.x >= 0.f) || !(p.y >= 0.f) || !(p.z >= 0.f) || p.x > (g.nx - 1) * g.dx || p.y > (g.ny - 1) * g.dy ||

@@ -144,13 +144,13 @@ struct WarpStats {
     unsigned long long act, inner, idle;  // idle: activations that lowered no node
 };
 
-// Data of one work item as loaded from global memory.
+// Data of one work item as loaded from global memory (the face halo goes straight to the
+// warp's tile).
 struct BrickLoad {
     unsigned s, b;
     int bz, bx, by;    // brick coordinates in the shot's window
     float s0, s1;      // slowness of the lane's two nodes
     float i0, i1;      // traveltimes of the lane's two nodes at load time
-    float hv[3];       // the lane's three face-halo values
 };
 
 // First of the lane's two nodes (node = z + 4x + 16y); the second is 16 above it (y + 1).
@@ -158,10 +158,11 @@ __device__ __forceinline__ int lane_node(int lane) { return (lane & 15) + 32 * (
 
 __device__ __forceinline__ void brick_coords(const ShotDesc &d, unsigned b, int &bz, int &bx, int &by)
 {
-    bz = (int)(b % (unsigned)d.nbz);
-    const unsigned tq = b / (unsigned)d.nbz;
-    bx = (int)(tq % (unsigned)d.nbx);
-    by = (int)(tq / (unsigned)d.nbx);
+    const unsigned tq = (unsigned)(((unsigned long long)b * d.divz_m) >> d.divz_sh);  // b / nbz
+    bz = (int)(b - tq * (unsigned)d.nbz);
+    const unsigned q2 = (unsigned)(((unsigned long long)tq * d.divx_m) >> d.divx_sh);  // tq / nbx
+    bx = (int)(tq - q2 * (unsigned)d.nbx);
+    by = (int)q2;
 }
 
 // Face halo slot q (0..2) of a lane: slot q covers the two faces of axis q (z, x, y); lanes
@@ -194,7 +195,9 @@ __device__ __forceinline__ long long halo_slot(const ShotDesc &d, unsigned b, in
     return ok ? (long long)b + (lower ? -step : step) : -1;
 }
 
-__device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, BrickLoad &L)
+// Loads work item `item` into L and into the warp's tile: the lane's two nodes and its three
+// face-halo cells.  The caller synchronises the warp before the tile is read.
+__device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, BrickLoad &L, float *tile)
 {
     const int lane = threadIdx.x & 31;
     L.s = item >> p.local_bits;
@@ -212,13 +215,16 @@ __device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, Br
     L.s1 = __ldg(Sb + n0 + 16);
     L.i0 = __ldcg(Tb + n0);
     L.i1 = __ldcg(Tb + n0 + 16);
+    const int ti0 = tile_idx(lane & 3, (lane >> 2) & 3, 2 * (lane >> 4));
+    tile[ti0] = L.i0;
+    tile[ti0 + kTileY] = L.i1;
     // Missing neighbours (grid edge) are INF; the reference's "halo = self" at the edge
     // cannot lower a node either.
 #pragma unroll
     for (int q = 0; q < 3; q++) {
         int node, ti;
         const long long nb = halo_slot(d, L.b, L.bz, L.bx, L.by, lane, q, node, ti);
-        L.hv[q] = nb >= 0 ? __ldcg(p.T + d.t_off + nb * kBrickNodes + node) : kInf;
+        tile[ti] = nb >= 0 ? __ldcg(p.T + d.t_off + nb * kBrickNodes + node) : kInf;
     }
 }
 
@@ -329,15 +335,7 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     const int ti0 = tile_idx(z0, x0, y0);
     const int ti1 = ti0 + kTileY;  // y + 1
     const float i0 = L.i0, i1 = L.i1;
-    tile[ti0] = i0;
-    tile[ti1] = i1;
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-        int node, ti;
-        (void)halo_slot(d, b, bz, bx, by, lane, q, node, ti);
-        tile[ti] = L.hv[q];
-    }
-    __syncwarp();
+    __syncwarp();  // the tile as load_brick wrote it
 
     // Red-black Gauss-Seidel.  A lane's two nodes are y-adjacent, so one is red (z + x + y
     // even) and the other black: phase A relaxes the lane's red node from black neighbours,
@@ -393,33 +391,29 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     // y.  T(y) is the halo cell loaded at the start of this activation; a concurrent drop of
     // y only makes the test more permissive.
     const bool d0 = c0 < i0 - p.change_tol, d1 = c1 < i1 - p.change_tol;
-    const bool fzm = (z0 == 0) && ((d0 && c0 < tile[ti0 - 1]) || (d1 && c1 < tile[ti1 - 1]));
-    const bool fzp = (z0 == 3) && ((d0 && c0 < tile[ti0 + 1]) || (d1 && c1 < tile[ti1 + 1]));
-    const bool fxm = (x0 == 0) && ((d0 && c0 < tile[ti0 - kTileX]) || (d1 && c1 < tile[ti1 - kTileX]));
-    const bool fxp = (x0 == 3) && ((d0 && c0 < tile[ti0 + kTileX]) || (d1 && c1 < tile[ti1 + kTileX]));
-    const bool fym = (y0 == 0) && d0 && c0 < tile[ti0 - kTileY];
-    const bool fyp = (y0 == 2) && d1 && c1 < tile[ti1 + kTileY];
-    const unsigned face = (__ballot_sync(kFull, fzm) ? 1u : 0u) | (__ballot_sync(kFull, fzp) ? 2u : 0u) |
-                          (__ballot_sync(kFull, fxm) ? 4u : 0u) | (__ballot_sync(kFull, fxp) ? 8u : 0u) |
-                          (__ballot_sync(kFull, fym) ? 16u : 0u) | (__ballot_sync(kFull, fyp) ? 32u : 0u);
+    unsigned fl = 0;  // faces: 1 z-, 2 z+, 4 x-, 8 x+, 16 y-, 32 y+
+    if (z0 == 0 && ((d0 && c0 < tile[ti0 - 1]) || (d1 && c1 < tile[ti1 - 1]))) fl |= 1u;
+    if (z0 == 3 && ((d0 && c0 < tile[ti0 + 1]) || (d1 && c1 < tile[ti1 + 1]))) fl |= 2u;
+    if (x0 == 0 && ((d0 && c0 < tile[ti0 - kTileX]) || (d1 && c1 < tile[ti1 - kTileX]))) fl |= 4u;
+    if (x0 == 3 && ((d0 && c0 < tile[ti0 + kTileX]) || (d1 && c1 < tile[ti1 + kTileX]))) fl |= 8u;
+    if (y0 == 0 && d0 && c0 < tile[ti0 - kTileY]) fl |= 16u;
+    if (y0 == 2 && d1 && c1 < tile[ti1 + kTileY]) fl |= 32u;
+    const unsigned face = __reduce_or_sync(kFull, fl);
 
-    // Queue the neighbours across those faces, and this brick if it hit the cap.
+    // Queue the neighbours across those faces (lane 2 axis + up), and this brick (lane 6)
+    // if it hit the cap.
     bool want = false;
-    long long tgt = -1;
+    int tgt = (int)b;
     if (lane < 6) {
-        bool chg = (face >> lane) & 1u;
-        switch (lane) {
-        case 0: chg = chg && bz > 0;        tgt = (long long)b - 1; break;
-        case 1: chg = chg && bz < nbz - 1;  tgt = (long long)b + 1; break;
-        case 2: chg = chg && bx > 0;        tgt = (long long)b - nbz; break;
-        case 3: chg = chg && bx < nbx - 1;  tgt = (long long)b + nbz; break;
-        case 4: chg = chg && by > 0;        tgt = (long long)b - (long long)nbz * nbx; break;
-        default: chg = chg && by < nby - 1; tgt = (long long)b + (long long)nbz * nbx; break;
-        }
-        want = chg;
+        const int axis = lane >> 1;
+        const bool up = lane & 1;
+        const int c = axis == 0 ? bz : (axis == 1 ? bx : by);
+        const int nmax = axis == 0 ? nbz : (axis == 1 ? nbx : nby);
+        const int stride = axis == 0 ? 1 : (axis == 1 ? nbz : nbz * nbx);
+        want = ((face >> lane) & 1u) && (up ? c < nmax - 1 : c > 0);
+        tgt += up ? stride : -stride;
     } else if (lane == 6) {
         want = more;
-        tgt = b;
     }
     if (kAsync) {
         queue_async(p, d, s, b, want, tgt, lane == 6 ? true : false);
@@ -486,7 +480,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
         // to rounds with many items left.
         for (unsigned i = fetch_item(cursor); i < n; i = fetch_item(cursor)) {
             BrickLoad A;
-            load_brick(p, __ldcg(list + i), A);
+            load_brick(p, __ldcg(list + i), A, tile);
             relax_brick<kFastSqrt, false>(p, A, round, tile, ws);
         }
         if (!grid_barrier(p.ctrl, p.spin_limit)) { ok = false; break; }
@@ -551,7 +545,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_async(FimLaunch p)
         item = __shfl_sync(kFull, item, 0);
         __threadfence();  // the previous owner's stores of neighbouring bricks are visible
         BrickLoad A;
-        load_brick(p, item, A);
+        load_brick(p, item, A, tile);
         relax_brick<kFastSqrt, true>(p, A, 0u, tile, ws);
     }
     if (lane == 0 && ws.act) {

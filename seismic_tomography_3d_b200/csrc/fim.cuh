@@ -22,7 +22,30 @@ struct ShotDesc {
     unsigned long long qbase;  // offset of the shot's bricks in the queue-flag array
     long long v_off;     // offset of the shot's window volume (nz*wnx*wny, z fastest) in
                          // arrays that hold all shots' volumes back to back
+    // Brick index -> coordinates without integer division: b / nbz and (b / nbz) / nbx as
+    // (n * m) >> sh, exact for every n below 2^local_bits (set by set_brick_division).
+    unsigned long long divz_m, divx_m;
+    unsigned divz_sh, divx_sh;
 };
+
+// Multiply-shift constants for an exact n / d over 0 <= n < 2^nbits (nbits <= 31): with
+// l = ceil(log2 d) and m = ceil(2^(nbits + l) / d), floor(n / d) = (n m) >> (nbits + l)
+// (Granlund & Montgomery, "Division by invariant integers using multiplication", 1994,
+// Theorem 4.2: 2^(N+l) <= m d <= 2^(N+l) + 2^l).  n m < 2^63, so it is one 64-bit product.
+inline void fastdiv_consts(unsigned d, unsigned nbits, unsigned long long &m, unsigned &sh)
+{
+    unsigned l = 0;
+    while ((1ull << l) < d) l++;
+    sh = nbits + l;
+    m = ((1ull << sh) + d - 1) / d;
+}
+
+// Fills a descriptor's division constants once nbz, nbx and the batch's local_bits are set.
+inline void set_brick_division(ShotDesc &d, unsigned local_bits)
+{
+    fastdiv_consts((unsigned)d.nbz, local_bits, d.divz_m, d.divz_sh);
+    fastdiv_consts((unsigned)d.nbx, local_bits, d.divx_m, d.divx_sh);
+}
 
 struct FimLaunch {
     const float *S;       // slowness, brick-major over the padded model

@@ -127,6 +127,7 @@ extern "C" int tomo_eik_solve_static(const float *slowness, int nx, int ny, int 
     const long long nbricks = (long long)d.nbx * d.nby * d.nbz;
     unsigned local_bits = 1;
     while ((1ll << local_bits) < nbricks) local_bits++;
+    set_brick_division(d, local_bits);
 
     float *S = reinterpret_cast<float *>(base + kOffS);
     float *T = reinterpret_cast<float *>(base + kOffT);
