@@ -25,6 +25,7 @@ constexpr int kDefaultMaxInner = 16;
 constexpr int kDefaultOccupancy = 4;  // 4 CTAs x 8 warps per SM (64 registers): fastest on config 2
 constexpr float kDefaultChangeTol = 1e-6f;
 constexpr int kDefaultMaxRounds = 1 << 20;
+constexpr int kMaxRounds = 1 << 22;
 constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~ seconds of polling, then error
 // Warm-start check: a node more than this (relative) below the update of its final
 // neighbours flags its shot.  The converged FP32 field itself holds such deficits up to
@@ -340,6 +341,8 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     const int occ0 = ctx->tuned_occupancy > 0 ? ctx->tuned_occupancy : kDefaultOccupancy;
     c.max_inner = (opts && opts->max_inner > 0) ? opts->max_inner : inner0;
     c.max_rounds = (opts && opts->max_rounds > 0) ? opts->max_rounds : kDefaultMaxRounds;
+    // the round barrier counts arrivals of up to ~1,000 blocks per round in 32 bits
+    c.max_rounds = std::min(c.max_rounds, kMaxRounds);
     c.block_warps = (opts && opts->block_warps > 0) ? opts->block_warps : warps0;
     c.occupancy = (opts && opts->occupancy > 0) ? opts->occupancy : occ0;
     // Default: the reference's convergence threshold EPS = 1e-6 s (cuda_kernel.cuh:8).

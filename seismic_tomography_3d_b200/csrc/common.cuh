@@ -64,6 +64,32 @@ __device__ __forceinline__ bool grid_barrier(unsigned *ctrl, unsigned long long 
     return ld_volatile(ctrl + kErr) == 0u;
 }
 
+// Grid-wide barrier on a monotone arrival counter: the k-th barrier of a launch (k = epoch,
+// counted by every block) completes when ctrl[kBarCount] reaches (k + 1) * blocks.  There is
+// no reset and no generation word, so the last block to arrive does no extra atomics.  The
+// counter starts at 0 for the launch; the waits are bounded as in grid_barrier.
+__device__ __forceinline__ bool grid_sync(unsigned *ctrl, unsigned &epoch, unsigned long long spin_limit)
+{
+    __syncthreads();
+    ++epoch;
+    if (threadIdx.x == 0) {
+        const unsigned target = epoch * (gridDim.x * gridDim.y * gridDim.z);
+        __threadfence();
+        atomicAdd(ctrl + kBarCount, 1u);
+        unsigned long long spins = 0;
+        while (ld_volatile(ctrl + kBarCount) < target) {
+            if (++spins > spin_limit) {
+                atomicCAS(ctrl + kErr, 0u, (unsigned)kDevBarrierTimeout);
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ld_volatile(ctrl + kErr) == 0u;
+}
+
 // IEEE FP32 arithmetic that the compiler may not contract into FMAs: used wherever the
 // reference's FP32 operation order is restated bit for bit.
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }

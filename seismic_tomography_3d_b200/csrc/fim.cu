@@ -349,6 +349,9 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     const int yA = red0 ? -kTileY : kTileY;
     float cA = red0 ? i0 : i1, cB = red0 ? i1 : i0;
     const NodeConst kA = node_const(p.h, red0 ? L.s0 : L.s1), kB = node_const(p.h, red0 ? L.s1 : L.s0);
+    // The relaxation has converged as soon as one phase changes nothing, once every black
+    // node has been relaxed at least once: the other colour then reads the same inputs as in
+    // its previous phase and would reproduce its values.
     bool more = true;
     int it = 0;
     for (; it < p.max_inner; ++it) {
@@ -357,17 +360,23 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
         const float bA = fminf(tile[tA + yA], cB);
         const float nA = fminf(cA, godunov_jw<kFastSqrt>(aA, bA, gA, kA));
         tile[tA] = nA;
+        const bool chA = nA < cA - p.inner_tol;
+        cA = nA;
         __syncwarp();
+        if (it > 0 && !__any_sync(kFull, chA)) {
+            more = false;
+            ++it;
+            break;
+        }
         const float aB = fminf(tile[tB - kTileX], tile[tB + kTileX]);
         const float gB = fminf(tile[tB - 1], tile[tB + 1]);
         const float bB = fminf(tile[tB - yA], nA);
         const float nB = fminf(cB, godunov_jw<kFastSqrt>(aB, bB, gB, kB));
         tile[tB] = nB;
-        const bool ch = (nA < cA - p.inner_tol) | (nB < cB - p.inner_tol);
-        cA = nA;
+        const bool chB = nB < cB - p.inner_tol;
         cB = nB;
         __syncwarp();
-        if (!__any_sync(kFull, ch)) {
+        if (!__any_sync(kFull, chB)) {
             more = false;
             ++it;
             break;
@@ -453,8 +462,10 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
     const int warp = threadIdx.x >> 5;
     float *tile = smem + warp * kTileNodes;
     WarpStats ws{0ull, 0ull, 0ull};
+    const unsigned nwarps = gridDim.x * (blockDim.x >> 5);
+    const unsigned gwarp = blockIdx.x * (blockDim.x >> 5) + warp;
 
-    unsigned round = 0;
+    unsigned round = 0, epoch = 0;
     bool ok = true;
     for (;;) {
         const unsigned cur = round % 3u;
@@ -478,12 +489,13 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
         // ahead doubles the live registers (4 % slower), and reserving the next item index
         // early (its atomic overlapping the relaxation) is 2-5 % slower even when limited
         // to rounds with many items left.
-        for (unsigned i = fetch_item(cursor); i < n; i = fetch_item(cursor)) {
+        // A warp's first item of the round is its own index; the cursor hands out the rest.
+        for (unsigned i = gwarp; i < n; i = nwarps + fetch_item(cursor)) {
             BrickLoad A;
             load_brick(p, __ldcg(list + i), A, tile);
             relax_brick<kFastSqrt, false>(p, A, round, tile, ws);
         }
-        if (!grid_barrier(p.ctrl, p.spin_limit)) { ok = false; break; }
+        if (!grid_sync(p.ctrl, epoch, p.spin_limit)) { ok = false; break; }
         ++round;
     }
     if ((threadIdx.x & 31) == 0 && ws.act) {
