@@ -78,11 +78,12 @@ __device__ __forceinline__ float godunov_jw(float a, float b, float c, const Nod
 }
 
 // Tile of one warp: (4+2)^3 nodes, the brick plus a one-node face halo, z fastest.  The x
-// and y strides are padded (8 and 52 words instead of 6 and 36) so that every shared-memory
+// and y strides are padded (12 and 72 words instead of 6 and 36) so that every shared-memory
 // access of the relaxation -- a phase's six neighbour reads and its store, over the 32 lanes
-// -- falls in 32 distinct banks.
-constexpr int kTileX = 8;
-constexpr int kTileY = 52;
+// -- falls in 32 distinct banks, and so do the face tests; of the tile fill, two of the
+// three halo stores are 2-way conflicted.
+constexpr int kTileX = 12;
+constexpr int kTileY = 72;
 constexpr int kTileNodes = kTileY * (kBrick + 2);
 
 __device__ __forceinline__ int tile_idx(int z, int x, int y)
@@ -319,10 +320,43 @@ __device__ __forceinline__ void queue_async(const FimLaunch &p, const ShotDesc &
     if (lane == 0) atomicSub(p.ctrl + kCnt1, 1u);  // this ownership ends
 }
 
+// Per-warp buffer of queue candidates (items for the next round), in shared memory.  An
+// activation adds at most 7, and the buffer is flushed once it holds more than
+// kPushCap - 7, so it never overflows.
+constexpr unsigned kPushCap = 32;
+
+// Queues the buffered candidates for round+1: one lane per candidate marks its brick
+// "queued for round+1" (atomicMax on the brick's flag; only the first marker of the round
+// appends it), and the survivors are appended to the next list with one atomic.
+__device__ __forceinline__ void flush_pushes(const FimLaunch &p, unsigned *pbuf, unsigned &pcnt, unsigned round)
+{
+    const int lane = threadIdx.x & 31;
+    __syncwarp();  // the buffer as the lanes wrote it
+    const unsigned tag = round + 2u;  // "queued for round+1", offset by one so 0 = never
+    bool want = false;
+    unsigned item = 0;
+    if ((unsigned)lane < pcnt) {
+        item = pbuf[lane];
+        const unsigned s = item >> p.local_bits, b = item & ((1u << p.local_bits) - 1u);
+        const unsigned old = atomicMax(p.qflag + p.shots[s].qbase + b, tag);
+        want = old < tag;
+    }
+    const unsigned wm = __ballot_sync(kFull, want);
+    if (wm) {
+        const int leader = __ffs(wm) - 1;
+        const unsigned nxt = (round + 1u) % 3u;
+        unsigned base = 0;
+        if (lane == leader) base = atomicAdd(p.ctrl + kCnt0 + nxt, (unsigned)__popc(wm));
+        base = __shfl_sync(kFull, base, leader);
+        if (want) p.lists[(size_t)nxt * p.list_cap + base + __popc(wm & ((1u << lane) - 1u))] = item;
+    }
+    pcnt = 0;
+}
+
 // One activation of one (already loaded) brick by one warp.
 template <bool kFastSqrt, bool kAsync>
 __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad &L, unsigned round, float *tile,
-                                            WarpStats &ws)
+                                            WarpStats &ws, unsigned *pbuf, unsigned &pcnt)
 {
     const int lane = threadIdx.x & 31;
     const unsigned s = L.s, b = L.b;
@@ -428,23 +462,12 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
         queue_async(p, d, s, b, want, tgt, lane == 6 ? true : false);
         return;
     }
-    const unsigned tag = round + 2u;  // "queued for round+1", offset by one so 0 = never
-    if (want) {
-        const unsigned old = atomicMax(p.qflag + d.qbase + (unsigned long long)tgt, tag);
-        want = old < tag;
-    }
+    // Candidates go to the warp's push buffer; the global dedup and append happen 32 at a
+    // time (flush_pushes), so most activations end without a global atomic.
     const unsigned wm = __ballot_sync(kFull, want);
-    if (wm) {
-        const int leader = __ffs(wm) - 1;
-        const unsigned nxt = (round + 1u) % 3u;
-        unsigned base = 0;
-        if (lane == leader) base = atomicAdd(p.ctrl + kCnt0 + nxt, (unsigned)__popc(wm));
-        base = __shfl_sync(kFull, base, leader);
-        if (want) {
-            const unsigned slot = base + __popc(wm & ((1u << lane) - 1u));
-            p.lists[(size_t)nxt * p.list_cap + slot] = (s << p.local_bits) | (unsigned)tgt;
-        }
-    }
+    if (want) pbuf[pcnt + __popc(wm & ((1u << lane) - 1u))] = (s << p.local_bits) | (unsigned)tgt;
+    pcnt += __popc(wm);
+    if (pcnt > kPushCap - 7u) flush_pushes(p, pbuf, pcnt, round);
 }
 
 // Next item index of the round: one atomic per warp on the round's cursor.
@@ -461,6 +484,8 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5;
     float *tile = smem + warp * kTileNodes;
+    unsigned *pbuf = reinterpret_cast<unsigned *>(smem + (blockDim.x >> 5) * kTileNodes) + warp * kPushCap;
+    unsigned pcnt = 0;
     WarpStats ws{0ull, 0ull, 0ull};
     const unsigned nwarps = gridDim.x * (blockDim.x >> 5);
     const unsigned gwarp = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -488,13 +513,17 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
         // One item at a time, fetched only when the warp is free: loading the next brick
         // ahead doubles the live registers (4 % slower), and reserving the next item index
         // early (its atomic overlapping the relaxation) is 2-5 % slower even when limited
-        // to rounds with many items left.
+        // to rounds with many items left; so is handing out all but the last ~2 items per
+        // warp by stride, with the next item read early (5 % slower), and so are chunks of
+        // 1/(G W) of the remaining items per fetch (guided self-scheduling, G = 2, 4, 8:
+        // 3-9 % slower): an item held by a busy warp lengthens the round's tail.
         // A warp's first item of the round is its own index; the cursor hands out the rest.
         for (unsigned i = gwarp; i < n; i = nwarps + fetch_item(cursor)) {
             BrickLoad A;
             load_brick(p, __ldcg(list + i), A, tile);
-            relax_brick<kFastSqrt, false>(p, A, round, tile, ws);
+            relax_brick<kFastSqrt, false>(p, A, round, tile, ws, pbuf, pcnt);
         }
+        if (pcnt) flush_pushes(p, pbuf, pcnt, round);
         if (!grid_sync(p.ctrl, epoch, p.spin_limit)) { ok = false; break; }
         ++round;
     }
@@ -558,7 +587,8 @@ __global__ void __launch_bounds__(256, MINB) k_fim_async(FimLaunch p)
         __threadfence();  // the previous owner's stores of neighbouring bricks are visible
         BrickLoad A;
         load_brick(p, item, A, tile);
-        relax_brick<kFastSqrt, true>(p, A, 0u, tile, ws);
+        unsigned unused = 0;
+        relax_brick<kFastSqrt, true>(p, A, 0u, tile, ws, nullptr, unused);
     }
     if (lane == 0 && ws.act) {
         atomicAdd(p.stats + 0, ws.act);
@@ -828,7 +858,7 @@ static cudaError_t launch_solve(const FimLaunch &p, int block_warps, bool async,
 {
     const void *fn = async ? (const void *)k_fim_async<MINB, kFastSqrt> : (const void *)k_fim_solve<MINB, kFastSqrt>;
     const int threads = 32 * block_warps;
-    const size_t smem = (size_t)block_warps * kTileNodes * sizeof(float);
+    const size_t smem = (size_t)block_warps * (kTileNodes * sizeof(float) + kPushCap * sizeof(unsigned));
     int dev = 0, nsm = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
