@@ -516,7 +516,9 @@ __global__ void __launch_bounds__(256, MINB) k_fim_solve(FimLaunch p)
         // to rounds with many items left; so is handing out all but the last ~2 items per
         // warp by stride, with the next item read early (5 % slower), and so are chunks of
         // 1/(G W) of the remaining items per fetch (guided self-scheduling, G = 2, 4, 8:
-        // 3-9 % slower): an item held by a busy warp lengthens the round's tail.
+        // 3-9 % slower): an item held by a busy warp lengthens the round's tail.  Sixteen
+        // cursors on separate lines, each over a stripe of the list, are 6 % slower: the
+        // one cursor is not contended enough to matter, and the stripe scan lengthens the tail.
         // A warp's first item of the round is its own index; the cursor hands out the rest.
         for (unsigned i = gwarp; i < n; i = nwarps + fetch_item(cursor)) {
             BrickLoad A;
