@@ -70,10 +70,12 @@ __device__ __forceinline__ float godunov_jw(float a, float b, float c, const Nod
     const float sum = u0 + u1 + u2;
     const float d12 = u2 - u1, d02 = u2 - u0;
     const float t3 = (sum + sqrt_sel<kFastSqrt>(k.q3c - (d01 * d01 + d12 * d12 + d02 * d02))) * (1.0f / 3.0f);
-    // sequential rule: t1; if t1 > u1 { t2 if causal; then t3 if the result exceeds u2 and t3 is causal }
-    const float ta = (t2 > u1) ? t2 : t1;
-    const float tb = (ta > u2 && t3 > u2) ? t3 : ta;
-    const float t = (t1 > u1) ? tb : t1;
+    // Sequential rule: t1 unless it exceeds u1; then t2 unless it exceeds u2; then t3 if
+    // causal.  t2's causality needs no test: t1 > u1 means u1 - u0 < hs, so the
+    // discriminant exceeds (hs)^2 and t2 > u1.  t3's test stays: when t2 only just exceeds
+    // u2 the discriminant of t3 is near zero and may round negative (NaN), and t2 is then
+    // the right value to within rounding.
+    const float t = (t1 > u1) ? ((t2 > u2 && t3 > u2) ? t3 : t2) : t1;
     return (u0 < kInf) ? t : kInf;
 }
 
