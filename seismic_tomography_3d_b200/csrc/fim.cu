@@ -57,7 +57,10 @@ __device__ __forceinline__ NodeConst node_const(float h, float s)
 // Branch-free: all three candidates are computed and the causal one selected, so the lanes
 // of a warp (which need different candidates) never diverge.  A candidate whose root is
 // imaginary is NaN and fails every comparison, exactly as the sequential tests skip it.
-template <bool kFastSqrt>
+// kGate: return kInf when every neighbour is unreached.  Callers that take the minimum with
+// the node's own value (at most kInf) can skip it: with all neighbours at kInf every
+// candidate is at least kInf.
+template <bool kFastSqrt, bool kGate = true>
 __device__ __forceinline__ float godunov_jw(float a, float b, float c, const NodeConst &k)
 {
     const float lo = fminf(a, b), hi = fmaxf(a, b);
@@ -76,7 +79,7 @@ __device__ __forceinline__ float godunov_jw(float a, float b, float c, const Nod
     // u2 the discriminant of t3 is near zero and may round negative (NaN), and t2 is then
     // the right value to within rounding.
     const float t = (t1 > u1) ? ((t2 > u2 && t3 > u2) ? t3 : t2) : t1;
-    return (u0 < kInf) ? t : kInf;
+    return (!kGate || u0 < kInf) ? t : kInf;
 }
 
 // Tile of one warp: (4+2)^3 nodes, the brick plus a one-node face halo, z fastest.  The x
@@ -395,7 +398,7 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
         const float aA = fminf(tile[tA - kTileX], tile[tA + kTileX]);
         const float gA = fminf(tile[tA - 1], tile[tA + 1]);
         const float bA = fminf(tile[tA + yA], cB);
-        const float nA = fminf(cA, godunov_jw<kFastSqrt>(aA, bA, gA, kA));
+        const float nA = fminf(cA, godunov_jw<kFastSqrt, false>(aA, bA, gA, kA));
         tile[tA] = nA;
         const bool chA = nA < cA - p.inner_tol;
         cA = nA;
@@ -408,7 +411,7 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
         const float aB = fminf(tile[tB - kTileX], tile[tB + kTileX]);
         const float gB = fminf(tile[tB - 1], tile[tB + 1]);
         const float bB = fminf(tile[tB - yA], nA);
-        const float nB = fminf(cB, godunov_jw<kFastSqrt>(aB, bB, gB, kB));
+        const float nB = fminf(cB, godunov_jw<kFastSqrt, false>(aB, bB, gB, kB));
         tile[tB] = nB;
         const bool chB = nB < cB - p.inner_tol;
         cB = nB;
