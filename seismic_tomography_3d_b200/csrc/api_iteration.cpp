@@ -168,6 +168,7 @@ extern "C" int tomo_iteration(tomo_ctx *ctx, int nshots, const tomo_point *shots
     push(key_a, plan.block_warps);
     push(key_a, plan.occupancy);
     push(key_a, plan.ieee_sqrt);
+    push(key_a, plan.async);
     push(key_a, plan.t_total);
     push(key_a, plan.q_total);
     push(key_a, jg);

@@ -35,9 +35,12 @@ __device__ __forceinline__ unsigned ld_volatile(const unsigned *p)
 
 // Software grid barrier for a cooperatively launched (co-resident) grid.  The wait is
 // bounded: after `spin_limit` polls it records kDevBarrierTimeout and returns false, so a
-// lost block can never hang the GPU.  Returns false if any block recorded an error.
+// lost block can never hang the GPU.  Returns false if any block recorded an error; every
+// thread of a block gets the same answer (thread 0's read of the error word), so a block
+// never splits over an error raised while it passes the barrier.
 __device__ __forceinline__ bool grid_barrier(unsigned *ctrl, unsigned long long spin_limit)
 {
+    __shared__ unsigned err;
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
@@ -59,9 +62,10 @@ __device__ __forceinline__ bool grid_barrier(unsigned *ctrl, unsigned long long 
             }
         }
         __threadfence();
+        err = ld_volatile(ctrl + kErr);
     }
     __syncthreads();
-    return ld_volatile(ctrl + kErr) == 0u;
+    return err == 0u;
 }
 
 // Grid-wide barrier on a monotone arrival counter: the k-th barrier of a launch (k = epoch,
@@ -70,6 +74,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *ctrl, unsigned long long 
 // counter starts at 0 for the launch; the waits are bounded as in grid_barrier.
 __device__ __forceinline__ bool grid_sync(unsigned *ctrl, unsigned &epoch, unsigned long long spin_limit)
 {
+    __shared__ unsigned err;  // the error word as thread 0 read it: one answer for the block
     __syncthreads();
     ++epoch;
     if (threadIdx.x == 0) {
@@ -85,9 +90,10 @@ __device__ __forceinline__ bool grid_sync(unsigned *ctrl, unsigned &epoch, unsig
             __nanosleep(32);
         }
         __threadfence();
+        err = ld_volatile(ctrl + kErr);
     }
     __syncthreads();
-    return ld_volatile(ctrl + kErr) == 0u;
+    return err == 0u;
 }
 
 // IEEE FP32 arithmetic that the compiler may not contract into FMAs: used wherever the
