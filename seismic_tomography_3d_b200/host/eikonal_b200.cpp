@@ -114,12 +114,15 @@ void Eikonal_B200::eikonal_equation()
     check(tomo_eik_volume(ctx, shot_id, travel_time), "traveltime copy");
 }
 
+// Files go to the background writer (same bytes, path and message as write_binary_float);
+// the call returns before the disk write.
 void Eikonal_B200::write_time_volume()
 {
     if (export_time_volume)
-        write_binary_float(time_volume_folder + name + "_eikonal_nz" + std::to_string(nz) + "_nx" + std::to_string(nx) +
-                               "_ny" + std::to_string(ny) + "_shot_" + std::to_string(shot_id + 1) + ".bin",
-                           travel_time, nPoints);
+        tomo_io::AsyncWriter::instance().write_floats(time_volume_folder + name + "_eikonal_nz" + std::to_string(nz) +
+                                                          "_nx" + std::to_string(nx) + "_ny" + std::to_string(ny) +
+                                                          "_shot_" + std::to_string(shot_id + 1) + ".bin",
+                                                      travel_time, (size_t)nPoints);
 }
 
 void Eikonal_B200::write_first_arrival()
@@ -128,9 +131,10 @@ void Eikonal_B200::write_first_arrival()
     // receiver times were sampled on the device with the reference's trilinear rule
     std::memcpy(first_arrival, recv_times.data() + (size_t)shot_id * total_nodes, sizeof(float) * total_nodes);
     if (export_first_arrival)
-        write_binary_float(first_arrival_folder + name + "_times_nr" + std::to_string(total_nodes) + "_shot_" +
-                               std::to_string(shot_id + 1) + ".bin",
-                           first_arrival, total_nodes);
+        tomo_io::AsyncWriter::instance().write_floats(first_arrival_folder + name + "_times_nr" +
+                                                          std::to_string(total_nodes) + "_shot_" +
+                                                          std::to_string(shot_id + 1) + ".bin",
+                                                      first_arrival, (size_t)total_nodes);
 }
 
 void Eikonal_B200::destroy_volumes() { batch_ready = false; }

@@ -20,6 +20,7 @@
 #else
 #include "tomo_b200_interface.hpp"
 #endif
+#include "async_writer.hpp"
 #include "tomo_b200.h"
 
 class Eikonal_B200 : public Eikonal {

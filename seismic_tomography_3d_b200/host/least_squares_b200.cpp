@@ -105,14 +105,24 @@ void Least_squares_B200::forward_modeling()
                   << " rays cut (stalled next to the source: " << st.rays_stalled << ")\n";
     std::vector<float> illum((size_t)eikonal->nPoints);
     check(b200->context(), tomo_illumination(b200->context(), illum.data()), "illumination");
-    write_binary_float(illumination_folder + eikonal->name + "_illumination_iteration_" + std::to_string(iteration) +
-                           ".bin",
-                       illum.data(), eikonal->nPoints);
+    tomo_io::AsyncWriter::instance().write_floats(illumination_folder + eikonal->name + "_illumination_iteration_" +
+                                                      std::to_string(iteration) + ".bin",
+                                                  illum.data(), (size_t)eikonal->nPoints);
     eikonal->destroy_volumes();
 }
 
 void Least_squares_B200::import_cal_data()
 {
+    // The receiver times this iteration's forward_modeling() wrote to the first-arrival
+    // files are still in memory: take them from there (the same floats, bit for bit) and
+    // let the files finish in the background.  Without them, read the files back as the
+    // reference does, once every queued write is on disk.
+    const std::vector<float> &rt = b200->receiver_times();
+    if (rt.size() == (size_t)n_data) {
+        std::copy(rt.begin(), rt.end(), dcal);
+        return;
+    }
+    tomo_io::AsyncWriter::instance().drain();
     std::vector<float> data((size_t)eikonal->total_nodes);
     for (int shot = 0; shot < eikonal->total_shots; shot++) {
         read_binary_float(cal_data_folder + eikonal->name + "_times_nr" + std::to_string(eikonal->total_nodes) +
@@ -156,14 +166,17 @@ void Least_squares_B200::model_update()
     check(ctx, tomo_model_update(ctx, &o, velocity.data()), "model update");
     // the host slowness stays the model state, as Eikonal::slowness in the reference
     check(ctx, tomo_get_slowness(ctx, eikonal->slowness), "slowness copy");
-    write_binary_float(estimated_model_folder + eikonal->name + "_model_iteration_" + std::to_string(iteration) + ".bin",
-                       velocity.data(), eikonal->nPoints);
+    tomo_io::AsyncWriter::instance().write_floats(estimated_model_folder + eikonal->name + "_model_iteration_" +
+                                                      std::to_string(iteration) + ".bin",
+                                                  velocity.data(), (size_t)eikonal->nPoints);
 }
 
 void Least_squares_B200::export_convergency()
 {
     std::ofstream f(convergency_folder + eikonal->name + "_convergency.txt", std::ios::out);
     for (float r : residuo) f << r << "\n";
+    // the run ends here: every model, illumination and first-arrival file is on disk
+    tomo_io::AsyncWriter::instance().drain();
 }
 
 Least_squares_B200::Least_squares_B200()

@@ -4,13 +4,15 @@
 // Tikhonov CGLS and model update.  Parameter keys, the iteration logic of
 // tomography_main.cpp:19-30 and every file the reference reads or writes are kept:
 //   <dobs_folder>obsData_<nodes>_samples_shot_<k>.bin          (read)
-//   <first_arrival_folder><name>_times_nr<nodes>_shot_<k>.bin  (written, read back)
+//   <first_arrival_folder><name>_times_nr<nodes>_shot_<k>.bin  (written; the same values are
+//                                                                then taken from memory)
 //   <illumination_folder><name>_illumination_iteration_<i>.bin (written; default folder
 //                                                                ../outputs/illumination/)
 //   <estimated_models_folder><name>_model_iteration_<i>.bin    (written, velocity)
 //   <convergency_folder><name>_convergency.txt                 (written)
 // Extra optional keys: cg_iterations (default 10, the reference's hard-coded count) and
-// illumination_folder.
+// illumination_folder.  The binary files are written by a background thread
+// (async_writer.hpp) while the iteration goes on; export_convergency() waits for all of them.
 #ifndef LEAST_SQUARES_B200_HPP
 #define LEAST_SQUARES_B200_HPP
 
