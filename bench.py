@@ -655,6 +655,45 @@ def run_tomography(args):
     return 0
 
 
+def run_jacobian(args):
+    """Ray tracing into the Jacobian at config-5 scale: the config-5 starting model and its
+    first --shots shots (default all 256) x 10,000 receivers, solved once; then the Jacobian
+    (ray march, run sort, emit, Tikhonov rows, transpose) built warmup + steps times.
+    Prints its own JSON line (not the headline metric)."""
+    import torch
+
+    import seismic_tomography_3d_b200 as tomo
+    from seismic_tomography_3d_b200 import workloads as wl
+
+    sv, start, inv = wl.config5_inversion()
+    shots = sv.shots[:args.shots] if args.shots else sv.shots
+    ctx = tomo.Context(sv.nx, sv.ny, sv.nz, sv.h)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    ctx.set_velocity(start)
+    ctx.eik_solve(shots, receivers=sv.receivers, want_recv=False, **SOLVER)
+    ms = []
+    for it in range(args.warmup + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        j = ctx.build_jacobian(inv["d_tomo"], inv["tk_order"], inv["tk_param"])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            ms.append(e0.elapsed_time(e1))
+    med = statistics.median(ms)
+    line = {"metric": "Jacobian build time (config-5 model)", "value": med, "unit": "ms",
+            "higher_is_better": False, "steps": args.steps, "warmup": args.warmup,
+            "ray_steps_per_s": j["ray_steps"] / (med / 1000.0),
+            "jacobian": {k: j[k] for k in ("rows", "cols", "nnz", "rays", "rays_ok", "rays_stalled", "rays_capped",
+                                           "rays_nonfinite", "rays_outside", "ray_steps")},
+            "config": {"workload": "config-5 starting model, first %d shots x 10,000 receivers, 50 m cells"
+                                   % len(shots)},
+            "data": "synthetic (seeded config-5 model, shots, receivers)"}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -667,6 +706,8 @@ def main():
                     help="time one config-3 tomography iteration instead (separate JSON line)")
     ap.add_argument("--inversion", action="store_true",
                     help="run the config-5 device-resident inversion instead (separate JSON line)")
+    ap.add_argument("--jacobian", action="store_true",
+                    help="time the Jacobian build on the config-5 model (first --shots shots) instead")
     ap.add_argument("--no-graph", action="store_true",
                     help="--inversion: call the stages one by one instead of tomo_iteration's CUDA graphs")
     ap.add_argument("--warm-start", action="store_true",
@@ -680,6 +721,8 @@ def main():
         return run_tomography(args)
     if args.inversion:
         return run_inversion(args)
+    if args.jacobian:
+        return run_jacobian(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
