@@ -234,7 +234,8 @@ extern "C" int tomo_iteration(tomo_ctx *ctx, int nshots, const tomo_point *shots
           (const void *)ctx->x.ptr, (const void *)ctx->cg_x.ptr, (const void *)ctx->cg_s.ptr,
           (const void *)ctx->cg_r.ptr, (const void *)ctx->cg_p.ptr, (const void *)ctx->cg_q.ptr,
           (const void *)ctx->partials.ptr, (const void *)ctx->hist.ptr, (const void *)ctx->norm2.ptr,
-          (const void *)ctx->cg_ctrl.ptr, (const void *)ctx->dm.ptr, (const void *)ctx->dm_smooth.ptr,
+          (const void *)ctx->cg_ctrl.ptr, (const void *)ctx->cg_long.ptr, (const void *)ctx->cg_ltemp.ptr,
+          (const void *)ctx->dm.ptr, (const void *)ctx->dm_smooth.ptr,
           (const void *)ctx->gauss_kernel.ptr, (const void *)ctx->slow.ptr, (const void *)ctx->S.ptr,
           (const void *)ctx->T.ptr, (const void *)ctx->shots_d.ptr, (const void *)ctx->rec.ptr, (const void *)pin})
         push(key_b, p);

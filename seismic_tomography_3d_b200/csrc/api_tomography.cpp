@@ -163,6 +163,8 @@ void tomo_release_tomography(tomo_ctx *ctx)
     ctx->hist.release();
     ctx->norm2.release();
     ctx->cg_ctrl.release();
+    ctx->cg_long.release();
+    ctx->cg_ltemp.release();
     for (auto *b : {&ctx->cg_x, &ctx->cg_s, &ctx->cg_r, &ctx->cg_p, &ctx->cg_q}) b->release();
 }
 
@@ -484,15 +486,23 @@ template <class Ctx>
 int run_cgls(Ctx *ctx, int N, int M, const int *a_ptr, const int *a_idx, const float *a_val, const int *t_ptr,
              const int *t_idx, const float *t_val, const float *B, double *x, double *s, double *r, double *p, double *q,
              float *x32,
-             tomo::DevBuf<double> &partials, double *hist, tomo::DevBuf<unsigned> &ctrl, int nit, double tol,
-             cudaStream_t st, int *iters_run)
+             tomo::DevBuf<double> &partials, double *hist, tomo::DevBuf<unsigned> &ctrl,
+             tomo::DevBuf<int> &longr, tomo::DevBuf<unsigned char> &ltemp, int nit, double tol, cudaStream_t st,
+             int *iters_run)
 {
     int grid = 0;
     CK(tomo::cgls_grid(&grid));
     CK(partials.ensure((size_t)grid * 3));
     CK(ctrl.ensure(tomo::kCtrlWords));
     CK(cudaMemsetAsync(ctrl.ptr, 0, tomo::kCtrlWords * sizeof(unsigned), st));
+    size_t lbytes = 0;
+    CK(tomo::cgls_long_rows(t_ptr, M, nullptr, nullptr, nullptr, &lbytes, st));
+    CK(longr.ensure((size_t)M + 1));
+    CK(ltemp.ensure(lbytes));
+    CK(tomo::cgls_long_rows(t_ptr, M, longr.ptr, longr.ptr + M, ltemp.ptr, &lbytes, st));
     tomo::CglsLaunch cl{};
+    cl.long_rows = longr.ptr;
+    cl.n_long = longr.ptr + M;
     cl.N = N;
     cl.M = M;
     cl.a_ptr = a_ptr;
@@ -561,6 +571,10 @@ int cgls_prepare(tomo_ctx *ctx, int iterations)
     CK(tomo::cgls_grid(&grid));
     CK(ctx->partials.ensure((size_t)grid * 3));
     CK(ctx->cg_ctrl.ensure(tomo::kCtrlWords));
+    size_t lbytes = 0;
+    CK(tomo::cgls_long_rows(ctx->t_ptr.ptr, M, nullptr, nullptr, nullptr, &lbytes, ctx->stream));
+    CK(ctx->cg_long.ensure((size_t)M + 1));
+    CK(ctx->cg_ltemp.ensure(lbytes));
     return TOMO_OK;
 }
 
@@ -594,6 +608,11 @@ int cgls_enqueue(tomo_ctx *ctx, int iterations)
     cl.nit = iterations;
     cl.tol = 0.0;
     cl.spin_limit = kSpinLimit;
+    size_t lbytes = ctx->cg_ltemp.cap;
+    CK(tomo::cgls_long_rows(ctx->t_ptr.ptr, M, ctx->cg_long.ptr, ctx->cg_long.ptr + M, ctx->cg_ltemp.ptr, &lbytes,
+                            ctx->stream));
+    cl.long_rows = ctx->cg_long.ptr;
+    cl.n_long = ctx->cg_long.ptr + M;
     CK(tomo::cgls_run(cl, grid, ctx->stream));
     return TOMO_OK;
 }
@@ -730,7 +749,8 @@ int tomo_sparse_cgls_gpu(const int *iA, const int *jA, const float *vA, const fl
     tomo::DevBuf<double> x64, s, r, p, q;
     tomo::DevBuf<double> partials;
     tomo::DevBuf<unsigned> ctrl;
-    tomo::DevBuf<unsigned char> temp;
+    tomo::DevBuf<unsigned char> temp, ltemp;
+    tomo::DevBuf<int> longr;
     tomo::DevBuf<long long> sizes;
     cudaStream_t st = nullptr;
     int rc = TOMO_OK;
@@ -742,6 +762,8 @@ int tomo_sparse_cgls_gpu(const int *iA, const int *jA, const float *vA, const fl
         partials.release();
         ctrl.release();
         temp.release();
+        ltemp.release();
+        longr.release();
         if (st) cudaStreamDestroy(st);
     };
     auto body = [&]() -> int {
@@ -769,7 +791,8 @@ int tomo_sparse_cgls_gpu(const int *iA, const int *jA, const float *vA, const fl
                                    k1, p0, p1, rows_of, temp, st);
         if (r2 != TOMO_OK) return r2;
         r2 = run_cgls(ctx, N, M, a_ptr.ptr, a_idx.ptr, a_val.ptr, t_ptr.ptr, t_idx.ptr, t_val.ptr, dB.ptr, x64.ptr,
-                      s.ptr, r.ptr, p.ptr, q.ptr, dx_.ptr, partials, nullptr, ctrl, NIT, (double)TOL, st, nullptr);
+                      s.ptr, r.ptr, p.ptr, q.ptr, dx_.ptr, partials, nullptr, ctrl, longr, ltemp, NIT, (double)TOL, st,
+                      nullptr);
         if (r2 != TOMO_OK) return r2;
         CK(cudaMemcpyAsync(x, dx_.ptr, (size_t)M * sizeof(float), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));

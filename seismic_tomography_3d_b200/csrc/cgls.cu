@@ -9,6 +9,14 @@
 // grid-wide dependencies per iteration are software grid barriers with bounded waits.
 // Reductions are deterministic: fixed row-to-thread mapping, fixed-order block and grid
 // sums computed identically by every block.
+//
+// A' has very uneven rows: a model cell is crossed by anything from no ray to thousands
+// (config 3: median 3 non-zeros, maximum 3,206).  Rows longer than kLongRow are listed
+// once per call (cgls_long_rows, in row order) and each is summed by a whole block; the
+// 32-lane groups take the rest, so the longest row no longer sets the length of A's.
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
 #include "common.cuh"
 #include "cgls.cuh"
 
@@ -18,6 +26,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+constexpr int kLongRow = 256;  // A' rows with more non-zeros are summed by a whole block
 
 // Block-wide FP64 sum in a fixed order; result valid in every thread.
 __device__ __forceinline__ double block_sum(double v, double *sh)
@@ -48,8 +57,9 @@ __device__ __forceinline__ double grid_sum(const double *partials, int nb, doubl
 }
 
 // y = M x for a CSR matrix with `G` lanes per row: FP32 matrix values, FP64 vectors and
-// row sums.  Returns this thread's share of y'y.
-template <int G>
+// row sums.  Returns this thread's share of y'y.  kSkipLong: rows longer than kLongRow
+// are left to spmv_long.
+template <int G, bool kSkipLong = false>
 __device__ __forceinline__ double spmv(const int *ptr, const int *idx, const float *val, const double *x, double *y,
                                        int nrows)
 {
@@ -62,17 +72,49 @@ __device__ __forceinline__ double spmv(const int *ptr, const int *idx, const flo
     for (long long it = 0; it < iters; it++) {
         const long long row = gthread / G + it * groups;
         double acc = 0.0;
-        if (row < nrows) {
+        bool mine = row < nrows;
+        if (mine) {
             const int b = __ldg(ptr + row), e = __ldg(ptr + row + 1);
-            for (int k = b + sub; k < e; k += G) acc += (double)__ldg(val + k) * __ldcg(x + __ldg(idx + k));
+            mine = !kSkipLong || e - b <= kLongRow;
+            if (mine)
+                for (int k = b + sub; k < e; k += G) acc += (double)__ldg(val + k) * __ldcg(x + __ldg(idx + k));
         }
         for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o, G);
-        if (row < nrows && sub == 0) {
+        if (mine && sub == 0) {
             y[row] = acc;
             local += acc * acc;
         }
     }
     return local;
+}
+
+// The listed long rows of y = M x, one block per row (block i takes rows i, i + grid, ...
+// of the list).  Returns this thread's share of y'y (thread 0 holds it).
+__device__ __forceinline__ double spmv_long(const int *ptr, const int *idx, const float *val, const double *x,
+                                            double *y, const int *rows, const int *nrows_long, double *sh)
+{
+    double local = 0.0;
+    const int nl = __ldcg(nrows_long);
+    for (int i = blockIdx.x; i < nl; i += gridDim.x) {
+        const int row = __ldcg(rows + i);
+        const int b = __ldg(ptr + row), e = __ldg(ptr + row + 1);
+        double acc = 0.0;
+        for (int k = b + (int)threadIdx.x; k < e; k += blockDim.x)
+            acc += (double)__ldg(val + k) * __ldcg(x + __ldg(idx + k));
+        acc = block_sum(acc, sh);
+        if (threadIdx.x == 0) {
+            y[row] = acc;
+            local += acc * acc;
+        }
+    }
+    return local;
+}
+
+// r = A' s: long rows by blocks, the rest by 32-lane groups.
+__device__ __forceinline__ double spmv_t(const CglsLaunch &p, const double *x, double *y, double *sh)
+{
+    const double l = spmv_long(p.t_ptr, p.t_idx, p.t_val, x, y, p.long_rows, p.n_long, sh);
+    return l + spmv<32, true>(p.t_ptr, p.t_idx, p.t_val, x, y, p.M);
 }
 
 }  // namespace
@@ -90,7 +132,7 @@ __global__ void __launch_bounds__(kThreads) k_cgls(CglsLaunch p)
     for (long long i = tid; i < p.M; i += nth) p.x[i] = 0.0;
     if (!grid_barrier(p.ctrl, p.spin_limit)) return;
     // r = A' s
-    double v = block_sum(spmv<32>(p.t_ptr, p.t_idx, p.t_val, p.s, p.r, p.M), sh);
+    double v = block_sum(spmv_t(p, p.s, p.r, sh), sh);
     if (threadIdx.x == 0) pa[blockIdx.x] = v;
     if (!grid_barrier(p.ctrl, p.spin_limit)) return;
     // p = r, q = A r (= A p)
@@ -121,7 +163,7 @@ __global__ void __launch_bounds__(kThreads) k_cgls(CglsLaunch p)
         // sparse_cgls_gpu's exit test on the r of this iteration (src/utils/cgls/cgls.cu:102)
         if (p.tol > 0.0 && sqrt(rTr) < p.tol) break;
         // r = A' s
-        v = block_sum(spmv<32>(p.t_ptr, p.t_idx, p.t_val, p.s, p.r, p.M), sh);
+        v = block_sum(spmv_t(p, p.s, p.r, sh), sh);
         if (threadIdx.x == 0) pa[blockIdx.x] = v;
         if (!grid_barrier(p.ctrl, p.spin_limit)) return;
         const double rTr_new = grid_sum(pa, nb, sh);
@@ -151,6 +193,20 @@ cudaError_t cgls_grid(int *grid)
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     *grid = nsm * (per_sm < 4 ? per_sm : 4);
     return cudaSuccess;
+}
+
+namespace {
+struct IsLongRow {
+    const int *ptr;
+    __host__ __device__ bool operator()(int r) const { return ptr[r + 1] - ptr[r] > kLongRow; }
+};
+}  // namespace
+
+cudaError_t cgls_long_rows(const int *t_ptr, int M, int *rows, int *n_long, void *temp, size_t *temp_bytes,
+                           cudaStream_t st)
+{
+    return cub::DeviceSelect::If(temp, *temp_bytes, thrust::counting_iterator<int>(0), rows, n_long, M,
+                                 IsLongRow{t_ptr}, st);
 }
 
 cudaError_t cgls_run(const CglsLaunch &p, int grid, cudaStream_t st)

@@ -9,6 +9,7 @@ struct CglsLaunch {
     int N, M;                                               // rows, columns
     const int *a_ptr, *a_idx; const float *a_val;           // A in CSR
     const int *t_ptr, *t_idx; const float *t_val;           // A' in CSR
+    const int *long_rows, *n_long;                          // A' rows summed by whole blocks
     const float *B;                                         // right-hand side (N)
     double *x, *s, *r, *p, *q;                              // M, N, M, M, N (FP64 vectors)
     float *x32;                                             // solution rounded to FP32 (M)
@@ -21,6 +22,10 @@ struct CglsLaunch {
 };
 
 cudaError_t cgls_grid(int *grid);
+// The rows of A' (t_ptr, M rows) too long for one 32-lane group, in row order, and their
+// count, on the device (temp == nullptr: *temp_bytes = the scratch needed).
+cudaError_t cgls_long_rows(const int *t_ptr, int M, int *rows, int *n_long, void *temp, size_t *temp_bytes,
+                           cudaStream_t st);
 cudaError_t cgls_run(const CglsLaunch &p, int grid, cudaStream_t st);
 
 // Model update (Least_squares::model_update, least_squares.cpp:498-570).

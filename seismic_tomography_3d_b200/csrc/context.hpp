@@ -110,6 +110,8 @@ struct tomo_ctx {
     tomo::DevBuf<double> cg_x, cg_s, cg_r, cg_p, cg_q;  // CGLS vectors (FP64)
     tomo::DevBuf<double> partials, hist, norm2;
     tomo::DevBuf<unsigned> cg_ctrl;
+    tomo::DevBuf<int> cg_long;                // long rows of A' (M) and their count (last entry)
+    tomo::DevBuf<unsigned char> cg_ltemp;     // scratch of the long-row selection
     tomo::DevBuf<float> dm, dm_smooth, vel_out, gauss_kernel;
     bool have_dobs = false, have_x = false;
     int n_dobs = 0;
