@@ -199,6 +199,27 @@ def test_sparse_cgls_gpu_entry_point(tomo, oracle_mod):
         tomo.sparse_cgls_gpu(iA, jA + M, vA, B, N, M, 5)  # column out of range
 
 
+def test_sparse_cgls_gpu_long_columns(tomo, oracle_mod):
+    """Columns of A (rows of A') with thousands of non-zeros -- the cells next to sources and
+    receivers that most rays cross -- take the block-per-row path of the transposed
+    product; the result matches the FP64 oracle and is identical from run to run."""
+    rng = np.random.default_rng(11)
+    N, M = 6000, 400
+    heavy = rng.integers(0, M, 40000)                # spread over every column
+    hot = rng.choice(8, 30000) * 37 % M               # 8 columns with ~3,750 entries each
+    jA = np.concatenate([heavy, hot]).astype(np.int32)
+    iA = rng.integers(0, N, jA.size).astype(np.int32)
+    vA = rng.uniform(0.1, 2.0, jA.size).astype(np.float32)
+    B = rng.standard_normal(N).astype(np.float32)
+    counts = np.bincount(jA, minlength=M)
+    assert counts.max() > 2000 and (counts > 256).sum() >= 8  # long rows of A' exist
+    x = tomo.sparse_cgls_gpu(iA, jA, vA, B, N, M, 20)
+    x64, _ = oracle_mod.cgls_f64(N, M, iA, jA, vA, B, 20)
+    assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-5
+    x2 = tomo.sparse_cgls_gpu(iA, jA, vA, B, N, M, 20)
+    np.testing.assert_array_equal(x, x2)  # fixed-order reductions: deterministic
+
+
 def test_full_iteration_recovered_model(tomo, oracle_mod, small_survey):
     """Device iteration vs the oracle pipeline on the device traveltimes: recovered
     velocity models agree within 0.5 % RMS; in practice ~1e-7."""
