@@ -272,11 +272,23 @@ int load_batch(tomo_net *net, int n, const tomo_net_sample *s, float h, bool tar
     return TOMO_OK;
 }
 
+// The tensor-core convolutions' error word (synchronises the stream): a bounded wait that
+// ran out is reported, and the word cleared, instead of returning garbage.
+int check_convolutions(tomo_net *net)
+{
+    unsigned err = 0;
+    NK(tomo::net::conv_tc_error(&err, true, net->stream));
+    if (err) return fail(net, TOMO_ERR_TIMEOUT, "tensor-core convolution: a device wait timed out");
+    return TOMO_OK;
+}
+
 int read_loss(tomo_net *net, double *loss)
 {
     double a[2];
     NK(cudaMemcpyAsync(a, net->acc.ptr, sizeof(a), cudaMemcpyDeviceToHost, net->stream));
     NK(cudaStreamSynchronize(net->stream));
+    const int rc = check_convolutions(net);
+    if (rc != TOMO_OK) return rc;
     if (loss) *loss = a[1] > 0 ? a[0] / a[1] : 0.0;
     return TOMO_OK;
 }
@@ -476,7 +488,7 @@ int tomo_net_predict(tomo_net *net, int n, const tomo_net_sample *samples, float
     NK(cudaEventRecord(net->ev[1], net->stream));
     NK(cudaStreamSynchronize(net->stream));
     if (ms) cudaEventElapsedTime(ms, net->ev[0], net->ev[1]);
-    return TOMO_OK;
+    return check_convolutions(net);
 }
 
 }  // extern "C"

@@ -4,8 +4,9 @@
 // of the model maps D = y, H = x, W = z, so channels-last order follows the model's
 // z-fastest layout.  Weights of a 3x3x3 convolution are BF16 [Cout][27][Cin] with
 // tap = (dd*3 + dh)*3 + dw (offsets -1..1); master weights, gradients and optimiser state
-// are FP32.  Convolutions are implicit GEMMs on the tensor cores (mma.sync m16n8k16,
-// BF16 operands, FP32 accumulation), zero padding, same-size output.
+// are FP32.  Convolutions are implicit GEMMs on the tensor cores with BF16 operands and
+// FP32 accumulation -- the forward on tcgen05 (accumulator in tensor memory), the weight
+// gradient on mma.sync -- zero padding, same-size output.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -25,6 +26,13 @@ struct Vol {
 // y = act(conv3x3x3(x, w) + bias); relu: 0/1; bias may be nullptr.
 cudaError_t conv_fwd(const bf16 *x, const bf16 *w, const float *bias, bf16 *y, Vol v, int cin, int cout, int relu,
                      cudaStream_t st);
+// The same convolution on the tcgen05 tensor cores (net_tc.cu): M = 128 voxels per CTA,
+// accumulator in tensor memory.
+cudaError_t conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, bf16 *y, Vol v, int cin, int cout, int relu,
+                        cudaStream_t st);
+// The tcgen05 convolution's error word (0, or 1 after a bounded wait ran out); synchronises
+// the stream; reset: clear it after reading.
+cudaError_t conv_tc_error(unsigned *err, bool reset, cudaStream_t st);
 // dW[co][tap][ci] += sum_v dy[v][co] * x[v + tap][ci]  (FP32, accumulated with atomics)
 cudaError_t conv_wgrad(const bf16 *x, const bf16 *dy, float *dw, Vol v, int cin, int cout, cudaStream_t st);
 // db[co] += sum_v dy[v][co]
