@@ -1,18 +1,21 @@
 // 3x3x3 convolution forward on the 5th-generation tensor cores (tcgen05, sm_100a).
 //
-// Implicit GEMM with the accumulator in tensor memory: a CTA of 4 warps owns M = 128 output
-// voxels -- 8 along W (the model's z) x 16 along H (x) x 1 along D (y) -- and N = NT output
-// channels.  For each 16-channel slice of the input, the CTA stages into shared memory
-//   * the slice of the 10 x 18 x 3 input halo, as [8-channel half][halo voxel][8 channels],
-//   * the 27 taps' weights for the slice, as [tap][8-channel half][output channel][8 ch],
+// Implicit GEMM with the accumulators in tensor memory: a CTA of 4 warps owns DS slices of
+// 128 output voxels -- 8 along W (the model's z) x 16 along H (x), DS consecutive along D
+// (y) -- and N = NT output channels, one M128 x N accumulator per slice.  For each
+// 16-channel slice of the input channels, the CTA stages into shared memory
+//   * the 10 x 18 x (DS + 2) input halo, as [8-channel half][halo voxel][8 channels],
+//   * the 27 taps' weights, as [tap][8-channel half][output channel][8 channels],
 // both in the canonical K-major, unswizzled operand layout (8 rows x 16 B core matrices),
-// and one thread issues 27 tcgen05.mma (M128 x N x K16, BF16 in, FP32 accumulate in TMEM).
-// A tap is only a different start address: the output row (w, h) reads halo voxel
-// (w + dw) + 10 (h + dh) + 180 dd, so the rows of each 8-row core matrix (w = 0..7) are
-// consecutive halo voxels and the core matrices (h) sit 10 voxels = 160 B apart -- the
+// and one thread issues 27 x DS tcgen05.mma (M128 x N x K16, BF16 in, FP32 accumulate):
+// the weights staged once serve all DS slices.  A tap and a slice are only a different
+// start address: output row (w, h) of slice s reads halo voxel
+// (w + dw) + 10 (h + dh) + 180 (s + dd), so the rows of each 8-row core matrix (w = 0..7)
+// are consecutive halo voxels and the core matrices (h) sit 10 voxels = 160 B apart -- the
 // operand's row-group stride.  The MMAs' completion arrives on an mbarrier
-// (tcgen05.commit); the epilogue reads the accumulator back with tcgen05.ld (each warp its
-// 32 lanes = 32 output voxels), adds the bias, applies ReLU and stores BF16 channels-last.
+// (tcgen05.commit); the epilogue reads the accumulators back with tcgen05.ld (each warp its
+// 32 lanes = 32 output voxels of each slice), adds the bias, applies ReLU and stores BF16
+// channels-last.
 //
 // Every wait is bounded: on a timeout the kernel records kConvTimeout in its error word,
 // still frees its tensor memory and returns.
@@ -29,10 +32,11 @@ __device__ unsigned g_conv_tc_error;  // 0, or kConvTimeout after a wait ran out
 namespace {
 
 constexpr unsigned kConvTimeout = 1u;
-constexpr int TW = 8, TH = 16;                          // output tile (W, H); D = 1
-constexpr int HW = TW + 2, HH = TH + 2, HD = 3;         // input halo
-constexpr int kHalo = HW * HH * HD;                     // 540 voxels
-constexpr unsigned kHalfBytes = kHalo * 16u;            // one 8-channel half of the halo slice
+constexpr int TW = 8, TH = 16;                          // output tile (W, H) of one slice
+constexpr int HW = TW + 2, HH = TH + 2;                 // input halo (W, H); D: DS + 2
+
+// One 8-channel half of the input halo of a CTA with DS slices (bytes).
+__host__ __device__ constexpr unsigned half_bytes(int ds) { return (unsigned)(HW * HH * (ds + 2)) * 16u; }
 constexpr long long kWaitLimit = 1ll << 22;             // mbarrier polls before giving up
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -103,31 +107,35 @@ struct TcTile {
     int b, d0, h0, w0;
 };
 
+template <int DS>
 __device__ __forceinline__ TcTile tc_tile(long long t, const Vol &v)
 {
-    const int nw = (v.W + TW - 1) / TW, nh = (v.H + TH - 1) / TH;
+    const int nw = (v.W + TW - 1) / TW, nh = (v.H + TH - 1) / TH, nd = (v.D + DS - 1) / DS;
     TcTile c;
     c.w0 = (int)(t % nw) * TW;
     t /= nw;
     c.h0 = (int)(t % nh) * TH;
     t /= nh;
-    c.d0 = (int)(t % v.D);
-    c.b = (int)(t / v.D);
+    c.d0 = (int)(t % nd) * DS;
+    c.b = (int)(t / nd);
     return c;
 }
 
-template <int NT>
+template <int NT, int DS>
 __global__ void __launch_bounds__(128) k_conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, bf16 *y,
                                                      Vol v, int cin, int cout, int relu)
 {
-    constexpr uint32_t kCols = NT <= 32 ? 32u : 64u;  // TMEM columns: a power of two >= 32
+    constexpr int kHalo = HW * HH * (DS + 2);
+    constexpr unsigned kHalfBytes = half_bytes(DS);
+    // TMEM columns for DS accumulators of NT columns: a power of two >= 32
+    constexpr uint32_t kCols = DS * NT <= 32 ? 32u : DS * NT <= 64 ? 64u : DS * NT <= 128 ? 128u : 256u;
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *s_a = smem;                                  // 2 x kHalfBytes
     unsigned char *s_b = smem + 2 * kHalfBytes;                 // 27 x 2 x NT x 16 B
     uint64_t *bar = reinterpret_cast<uint64_t *>(s_b + 27 * 2 * NT * 16);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const TcTile tc = tc_tile(blockIdx.x, v);
+    const TcTile tc = tc_tile<DS>(blockIdx.x, v);
     const int co0 = blockIdx.y * NT;
 
     if (warp == 0) {
@@ -175,10 +183,13 @@ __global__ void __launch_bounds__(128) k_conv_fwd_tc(const bf16 *x, const bf16 *
 #pragma unroll 1
             for (int tap = 0; tap < 27; tap++) {
                 const int dd = tap / 9, dh = (tap / 3) % 3, dw = tap % 3;
-                const uint32_t a_off = (uint32_t)(dw + HW * dh + HW * HH * dd) * 16u;
-                const uint64_t ad = operand_desc(a_base + a_off, kHalfBytes, HW * 16u);
                 const uint64_t bd = operand_desc(b_base + (uint32_t)tap * 2u * NT * 16u, NT * 16u, 128u);
-                mma_bf16(tmem, ad, bd, idesc, (ci0 > 0 || tap > 0) ? 1u : 0u);
+#pragma unroll
+                for (int sl = 0; sl < DS; sl++) {
+                    const uint32_t a_off = (uint32_t)(dw + HW * dh + HW * HH * (dd + sl)) * 16u;
+                    const uint64_t ad = operand_desc(a_base + a_off, kHalfBytes, HW * 16u);
+                    mma_bf16(tmem + (uint32_t)(sl * NT), ad, bd, idesc, (ci0 > 0 || tap > 0) ? 1u : 0u);
+                }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
                          : "memory");
@@ -192,16 +203,19 @@ __global__ void __launch_bounds__(128) k_conv_fwd_tc(const bf16 *x, const bf16 *
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     }
 
-    if (ok) {
-        // epilogue: row m = 32 warp + lane of the accumulator is output voxel (w, h) = (m % 8, m / 8)
-        const int m = 32 * warp + lane;
-        const int h = tc.h0 + m / TW, ws = tc.w0 + m % TW;
-        const bool inside = h < v.H && ws < v.W;
-        const long long vox = (((long long)tc.b * v.D + tc.d0) * v.H + h) * v.W + ws;
+    // epilogue: row m = 32 warp + lane of slice sl's accumulator is output voxel
+    // (w, h, d) = (m % 8, m / 8, d0 + sl)
+    const int m = 32 * warp + lane;
+    const int h = tc.h0 + m / TW, ws = tc.w0 + m % TW;
+#pragma unroll 1
+    for (int sl = 0; sl < DS && ok; sl++) {
+        const int d = tc.d0 + sl;
+        const bool inside = h < v.H && ws < v.W && d < v.D;
+        const long long vox = (((long long)tc.b * v.D + d) * v.H + h) * v.W + ws;
 #pragma unroll
         for (int c = 0; c < NT; c += 16) {
             float acc[16];
-            tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c, acc);
+            tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(sl * NT + c), acc);
             if (!inside || co0 + c >= cout) continue;
             uint32_t packed[8];
 #pragma unroll
@@ -231,18 +245,34 @@ __global__ void __launch_bounds__(128) k_conv_fwd_tc(const bf16 *x, const bf16 *
     }
 }
 
-template <int NT>
+template <int NT, int DS>
 cudaError_t launch_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, bf16 *y, Vol v, int cin, int cout, int relu,
-                          cudaStream_t st)
+                          long long tiles, cudaStream_t st)
 {
-    const size_t smem = 2 * (size_t)kHalfBytes + 27 * 2 * NT * 16 + 16;
-    cudaError_t e = cudaFuncSetAttribute(k_conv_fwd_tc<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = 2 * (size_t)half_bytes(DS) + 27 * 2 * NT * 16 + 16;
+    cudaError_t e = cudaFuncSetAttribute(k_conv_fwd_tc<NT, DS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const long long tiles = (long long)v.B * v.D * ((v.H + TH - 1) / TH) * ((v.W + TW - 1) / TW);
-    if (tiles >= (1LL << 31)) return cudaErrorInvalidValue;
     const dim3 grid((unsigned)tiles, (unsigned)((cout + NT - 1) / NT));
-    k_conv_fwd_tc<NT><<<grid, 128, smem, st>>>(x, w, bias, y, v, cin, cout, relu);
+    k_conv_fwd_tc<NT, DS><<<grid, 128, smem, st>>>(x, w, bias, y, v, cin, cout, relu);
     return cudaGetLastError();
+}
+
+long long tc_tiles(const Vol &v, int ds)
+{
+    return (long long)v.B * ((v.D + ds - 1) / ds) * ((v.H + TH - 1) / TH) * ((v.W + TW - 1) / TW);
+}
+
+// Slices per CTA: as many as keep about two CTAs per SM busy (more slices share one weight
+// staging; fewer give small volumes enough CTAs).
+template <int NT>
+cudaError_t launch_fwd_tc_ds(const bf16 *x, const bf16 *w, const float *bias, bf16 *y, Vol v, int cin, int cout,
+                             int relu, cudaStream_t st)
+{
+    const long long chunks = (cout + NT - 1) / NT, want = 2LL * 148;
+    if (tc_tiles(v, 1) >= (1LL << 31)) return cudaErrorInvalidValue;
+    if (tc_tiles(v, 4) * chunks >= want) return launch_fwd_tc<NT, 4>(x, w, bias, y, v, cin, cout, relu, tc_tiles(v, 4), st);
+    if (tc_tiles(v, 2) * chunks >= want) return launch_fwd_tc<NT, 2>(x, w, bias, y, v, cin, cout, relu, tc_tiles(v, 2), st);
+    return launch_fwd_tc<NT, 1>(x, w, bias, y, v, cin, cout, relu, tc_tiles(v, 1), st);
 }
 
 }  // namespace
@@ -252,10 +282,10 @@ cudaError_t conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, bf16 *y
 {
     if (cin % 16 || cout % 16 || cin < 16 || cout < 16) return cudaErrorInvalidValue;
     switch (cout >= 64 ? 64 : cout) {
-    case 16: return launch_fwd_tc<16>(x, w, bias, y, v, cin, cout, relu, st);
-    case 32: return launch_fwd_tc<32>(x, w, bias, y, v, cin, cout, relu, st);
-    case 48: return launch_fwd_tc<48>(x, w, bias, y, v, cin, cout, relu, st);
-    default: return launch_fwd_tc<64>(x, w, bias, y, v, cin, cout, relu, st);
+    case 16: return launch_fwd_tc_ds<16>(x, w, bias, y, v, cin, cout, relu, st);
+    case 32: return launch_fwd_tc_ds<32>(x, w, bias, y, v, cin, cout, relu, st);
+    case 48: return launch_fwd_tc_ds<48>(x, w, bias, y, v, cin, cout, relu, st);
+    default: return launch_fwd_tc_ds<64>(x, w, bias, y, v, cin, cout, relu, st);
     }
 }
 
