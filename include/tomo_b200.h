@@ -70,8 +70,10 @@ typedef struct {
     int max_inner;   /* cap of in-brick iterations per activation (0: default 16)     */
     int max_rounds;  /* cap of outer rounds (0: default 1<<20)                        */
     int brick;       /* brick shape: 0 or 1 = 4x4x4, the one shape of tomo_eik_brick_shapes */
-    int block_warps; /* warps per CTA of the persistent kernel (0: default)           */
-    int occupancy;   /* CTAs per SM the kernel is compiled for, 1..6 (0: default 4)   */
+    int block_warps; /* warps per CTA of the persistent kernel, 1-16 (0: default 16;
+                        the asynchronous schedule uses at most 8)                     */
+    int occupancy;   /* register budget of the kernel, in CTAs of 8 warps per SM, 1..6
+                        (0: default 4, i.e. 64 registers)                             */
     float change_tol;/* a face value must drop by more than this (s) to re-queue the
                         neighbour brick.  0: default 1e-6 s, the reference's EPS
                         (cuda_kernel.cuh:8); < 0: any drop (exact FP32 fixed point) */

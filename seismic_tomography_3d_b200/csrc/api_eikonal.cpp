@@ -22,7 +22,10 @@ const char *static_error_text();  // fim_static.cu
 namespace {
 
 constexpr int kDefaultMaxInner = 16;
-constexpr int kDefaultOccupancy = 4;  // 4 CTAs x 8 warps per SM (64 registers): fastest on config 2
+// Launch shape of the persistent solve: 16 warps per CTA and occupancy 4 -- 32 warps per
+// SM, the register budget (64) of 4 CTAs of 8 warps, i.e. 2 CTAs of 16 -- fastest on config 2.
+constexpr int kDefaultOccupancy = 4;
+constexpr int kDefaultBlockWarps = 16;
 constexpr float kDefaultChangeTol = 1e-6f;
 constexpr int kDefaultMaxRounds = 1 << 20;
 constexpr int kMaxRounds = 1 << 22;
@@ -337,7 +340,7 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     SolveCfg c{};
     // fields left 0: the autotuned launch shape if there is one, else the defaults
     const int inner0 = ctx->tuned_max_inner > 0 ? ctx->tuned_max_inner : kDefaultMaxInner;
-    const int warps0 = ctx->tuned_block_warps > 0 ? ctx->tuned_block_warps : 8;
+    const int warps0 = ctx->tuned_block_warps > 0 ? ctx->tuned_block_warps : kDefaultBlockWarps;
     const int occ0 = ctx->tuned_occupancy > 0 ? ctx->tuned_occupancy : kDefaultOccupancy;
     c.max_inner = (opts && opts->max_inner > 0) ? opts->max_inner : inner0;
     c.max_rounds = (opts && opts->max_rounds > 0) ? opts->max_rounds : kDefaultMaxRounds;
@@ -744,7 +747,7 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
     if (repeats == 0) repeats = 2;
     // untuned defaults while timing (an earlier tuning must not leak into the trials)
     ctx->tuned_block_warps = ctx->tuned_occupancy = ctx->tuned_max_inner = 0;
-    const int warps[] = {8, 4};
+    const int warps[] = {kDefaultBlockWarps, 8, 4};
     const int occs[] = {4, 5, 6, 3};
     const int inners[] = {16, 8, 32};
     tomo_eik_opts o{};
@@ -754,7 +757,7 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
     int rc = tomo_eik_solve(ctx, nshots, shots, windows, 0, nullptr, nullptr, &o, &st);
     if (rc != TOMO_OK) return rc;
     float best_ms = 0.f, default_ms = 0.f;
-    int trials = 0, bw = 8, bo = kDefaultOccupancy, bi = kDefaultMaxInner;
+    int trials = 0, bw = kDefaultBlockWarps, bo = kDefaultOccupancy, bi = kDefaultMaxInner;
     for (int w : warps)
         for (int oc : occs)
             for (int in : inners) {
