@@ -50,14 +50,16 @@ class EikOpts(ctypes.Structure):
     _fields_ = [("op", ctypes.c_int), ("max_inner", ctypes.c_int), ("max_rounds", ctypes.c_int),
                 ("brick", ctypes.c_int), ("block_warps", ctypes.c_int), ("occupancy", ctypes.c_int),
                 ("change_tol", ctypes.c_float), ("inner_tol", ctypes.c_float),
-                ("ieee_sqrt", ctypes.c_int), ("sweep_groups", ctypes.c_int), ("schedule", ctypes.c_int)]
+                ("ieee_sqrt", ctypes.c_int), ("sweep_groups", ctypes.c_int), ("schedule", ctypes.c_int),
+                ("time_band", ctypes.c_float)]
 
 
 class EikStats(ctypes.Structure):
     _fields_ = [("rounds", ctypes.c_longlong), ("activations", ctypes.c_longlong),
                 ("inner_iterations", ctypes.c_longlong), ("nodes_per_brick", ctypes.c_longlong),
                 ("idle_activations", ctypes.c_longlong),
-                ("setup_ms", ctypes.c_float), ("solve_ms", ctypes.c_float), ("total_ms", ctypes.c_float)]
+                ("setup_ms", ctypes.c_float), ("solve_ms", ctypes.c_float), ("total_ms", ctypes.c_float),
+                ("deferred", ctypes.c_longlong)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -294,7 +296,7 @@ class Context:
     # -- eikonal ------------------------------------------------------------------------
     def eik_solve(self, shots, windows=None, receivers=None, want_recv=True, max_inner=0, max_rounds=0,
                   block_warps=0, op=0, occupancy=0, change_tol=0.0, inner_tol=0.0, ieee_sqrt=0,
-                  sweep_groups=0, schedule=0):
+                  sweep_groups=0, schedule=0, time_band=0.0):
         """Batched solve.  shots (n,3) metres; windows (n,4) [x0,x1,y0,y1] nodes or None;
         receivers (m,3).  Returns (t_recv (n,m) float32 or None, stats dict)."""
         sp, ns, _s = _points(shots)
@@ -307,7 +309,7 @@ class Context:
             rp, nr, _r = _points(receivers)
         out = np.empty((ns, nr), np.float32) if (want_recv and nr) else None
         opts = EikOpts(op, max_inner, max_rounds, 0, block_warps, occupancy, change_tol, inner_tol, ieee_sqrt,
-                       sweep_groups, schedule)
+                       sweep_groups, schedule, time_band)
         st = EikStats()
         self._check(self.lib.tomo_eik_solve(self.h, ns, sp, wp, nr, rp,
                                             out.ctypes.data if out is not None else None,
@@ -429,7 +431,7 @@ class Context:
     def iteration(self, shots, receivers, d_tomo, windows=None, tk_order=2, tk_param=0.1, cg_iterations=30,
                   smooth=True, filter_samples=5, standard_deviation=2.0, reference_masks=True, use_graph=True,
                   max_ray_steps=0, max_cells_per_ray=0, nnz_headroom=0.0, change_tol=0.0, inner_tol=0.0,
-                  schedule=0):
+                  schedule=0, time_band=0.0):
         """One whole tomography iteration on the device (tomo_iteration); returns its stats."""
         sp, ns, _s = _points(shots)
         rp, nr, _r = _points(receivers)
@@ -440,7 +442,7 @@ class Context:
         o.jacobian = JacobianOpts(*map(float, d_tomo), tk_order, tk_param, max_ray_steps, max_cells_per_ray, 0)
         o.cg_iterations = cg_iterations
         o.update = UpdateOpts(int(smooth), filter_samples, standard_deviation, int(reference_masks))
-        o.eik = EikOpts(0, 0, 0, 0, 0, 0, change_tol, inner_tol, 0, 0, schedule)
+        o.eik = EikOpts(0, 0, 0, 0, 0, 0, change_tol, inner_tol, 0, 0, schedule, time_band)
         o.use_graph = int(use_graph)
         o.nnz_headroom = nnz_headroom
         st = IterationStats()

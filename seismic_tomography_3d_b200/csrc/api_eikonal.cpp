@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -333,6 +334,7 @@ struct SolveCfg {
     float change_tol, inner_tol;
     bool ieee_sqrt;
     bool async;  // asynchronous schedule, else rounds (default)
+    float time_band;  // rounds schedule: time-band ordering (s), 0 = off
 };
 
 SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
@@ -360,6 +362,10 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     // Rounds by default: the asynchronous schedule relaxes bricks before their upwind
     // neighbours have settled and measured 2.5x slower on config 2 (1.8x the activations).
     c.async = opts && opts->schedule == TOMO_SCHED_ASYNC;
+    // Time-band ordering: off by default.  It pays where slow paths reach bricks long
+    // before the first arrival does (1.64x on the config-5 starting model at 0.2 s) and
+    // costs where they do not (the windowed config-2 batch).
+    c.time_band = (opts && !c.async && opts->time_band > 0.f) ? opts->time_band : 0.f;
     return c;
 }
 
@@ -486,12 +492,35 @@ tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, in
     p.dy = g.dy;
     p.dz = g.dz;
     p.nz = g.nz;
+    if (c.time_band > 0.f) {  // buffers sized by band_buffers()
+        p.band = c.time_band;
+        p.keys = ctx->fim_keys.ptr;
+        p.band_min = ctx->band_min.ptr;
+    }
     return p;
+}
+
+// Key and per-shot minimum arrays of the time-band ordering, when the solve uses it.
+int band_buffers(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c)
+{
+    if (c.time_band <= 0.f) return TOMO_OK;
+    CK(ctx->fim_keys.ensure((size_t)bt.q_total));
+    CK(ctx->band_min.ensure((size_t)3 * bt.sd.size()));
+    return TOMO_OK;
+}
+
+// Every key "none" and every per-shot minimum "none" before a banded solve.
+cudaError_t band_reset(tomo_ctx *ctx, const tomo::FimLaunch &p)
+{
+    if (p.band <= 0.f) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(p.keys, 0xff, (size_t)p.list_cap * sizeof(unsigned), ctx->stream);
+    if (e != cudaSuccess) return e;
+    return cudaMemsetAsync(p.band_min, 0xff, (size_t)3 * p.nshots * sizeof(unsigned), ctx->stream);
 }
 
 // Reads the control words and counters of the last persistent solve (synchronises).
 int read_solve(tomo_ctx *ctx, unsigned &rounds, unsigned long long &act, unsigned long long &inner,
-               const SolveCfg &c, unsigned long long *idle = nullptr)
+               const SolveCfg &c, unsigned long long *idle = nullptr, unsigned long long *deferred = nullptr)
 {
     CK(cudaMemcpyAsync(ctx->pinned_ctrl, ctx->ctrl.ptr, tomo::kCtrlWords * sizeof(unsigned), cudaMemcpyDeviceToHost,
                        ctx->stream));
@@ -504,6 +533,7 @@ int read_solve(tomo_ctx *ctx, unsigned &rounds, unsigned long long &act, unsigne
     act = st[0];
     inner = st[1];
     if (idle) *idle = st[3];
+    if (deferred) *deferred = st[2];
     const unsigned derr = ctx->pinned_ctrl[tomo::kErr];
     if (derr == tomo::kDevRoundCap)
         return fail(ctx, TOMO_ERR_NOT_CONVERGED,
@@ -532,6 +562,8 @@ int eik_plan(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_wind
     if (nrec < 0 || (nrec > 0 && !receivers)) return fail(ctx, TOMO_ERR_INVALID_ARG, "bad receivers");
     if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
     if (opts && opts->op != TOMO_OP_JW) return fail(ctx, TOMO_ERR_INVALID_ARG, "the plan runs the JW operator only");
+    if (opts && !(opts->time_band >= 0.f && opts->time_band < 1e30f))
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "time_band must be a finite value >= 0");
     const SolveCfg cfg = solve_cfg(ctx, opts);
     Batch bt;
     int rc = make_batch(ctx, nshots, shots, windows, nrec, receivers, bt);
@@ -540,6 +572,8 @@ int eik_plan(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_wind
     if (rc != TOMO_OK) return rc;
     CK(cudaStreamSynchronize(ctx->stream));  // host staging of upload_batch
     keep_batch(ctx, bt, shots, nrec, receivers);
+    rc = band_buffers(ctx, bt, cfg);
+    if (rc != TOMO_OK) return rc;
     plan.p = fim_params(ctx, bt, cfg, nrec);
     plan.block_warps = cfg.block_warps;
     plan.occupancy = cfg.occupancy;
@@ -556,6 +590,7 @@ int eik_enqueue(tomo_ctx *ctx, const EikPlan &plan)
     CK(tomo::fim_init(p.T, plan.t_total, p.qflag, plan.q_total, p.ctrl, p.stats, ctx->stream));
     CK(tomo::fim_seed(p.shots, p.nshots, p.S, p.gbx, p.gbz, p.T, p.qflag, p.lists, p.local_bits, p.ctrl, ctx->stream,
                       plan.async ? 3 * (size_t)p.list_cap : 0));
+    CK(band_reset(ctx, p));
     int grid = 0;
     CK(tomo::fim_solve(p, plan.block_warps, plan.occupancy, plan.ieee_sqrt, &grid, ctx->stream, plan.async));
     return TOMO_OK;
@@ -579,6 +614,8 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
         return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown brick shape (tomo_eik_brick_shapes lists 1: 4x4x4)");
     if (opts && (opts->schedule < TOMO_SCHED_DEFAULT || opts->schedule > TOMO_SCHED_ASYNC))
         return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown work schedule");
+    if (opts && !(opts->time_band >= 0.f && opts->time_band < 1e30f))
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "time_band must be a finite value >= 0");
     const SolveCfg cfg = solve_cfg(ctx, opts);
     CK(cudaSetDevice(ctx->device));
     Batch bt;
@@ -586,6 +623,8 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     if (rc != TOMO_OK) return rc;
     ctx->have_solve = false;  // the pool is about to be overwritten
     rc = upload_batch(ctx, bt, nrec, receivers);
+    if (rc != TOMO_OK) return rc;
+    rc = band_buffers(ctx, bt, cfg);
     if (rc != TOMO_OK) return rc;
 
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
@@ -598,6 +637,7 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
         CK(tomo::fim_seed(ctx->shots_d.ptr, nshots, ctx->S.ptr, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
                           ctx->lists.ptr, bt.local_bits, ctx->ctrl.ptr, ctx->stream, cfg.async ? 3 * (size_t)bt.q_total : 0));
         const tomo::FimLaunch p = fim_params(ctx, bt, cfg, nrec);
+        CK(band_reset(ctx, p));
         int grid = 0;
         CK(cudaEventRecord(ctx->ev[3], ctx->stream));
         CK(tomo::fim_solve(p, cfg.block_warps, cfg.occupancy, cfg.ieee_sqrt, &grid, ctx->stream, cfg.async));
@@ -608,8 +648,8 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
                            ctx->stream));
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     unsigned rounds = 0;
-    unsigned long long act = 0, inner = 0, idle = 0;
-    rc = read_solve(ctx, rounds, act, inner, cfg, &idle);
+    unsigned long long act = 0, inner = 0, idle = 0, deferred = 0;
+    rc = read_solve(ctx, rounds, act, inner, cfg, &idle, &deferred);
     keep_batch(ctx, bt, shots, nrec, receivers);
     ctx->have_solve = (rc == TOMO_OK);
     if (stats) {
@@ -617,6 +657,7 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
         stats->activations = (long long)act;
         stats->inner_iterations = (long long)inner;
         stats->idle_activations = (long long)idle;
+        stats->deferred = (long long)deferred;
         stats->nodes_per_brick = tomo::kBrickNodes;
         cudaEventElapsedTime(&stats->setup_ms, ctx->ev[0], ctx->ev[3]);
         cudaEventElapsedTime(&stats->solve_ms, ctx->ev[3], ctx->ev[1]);
@@ -638,7 +679,8 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
     if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
     if (opts && opts->op != TOMO_OP_JW)
         return fail(ctx, TOMO_ERR_INVALID_ARG, "the warm-started solve runs the JW operator only");
-    const SolveCfg cfg = solve_cfg(ctx, opts);
+    SolveCfg cfg = solve_cfg(ctx, opts);
+    cfg.time_band = 0.f;  // keys start from the ceiling's pool: not used here
     CK(cudaSetDevice(ctx->device));
     Batch bt;
     int rc = make_batch(ctx, nshots, shots, windows, nrec, receivers, bt);
@@ -720,6 +762,8 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
         stats->rounds = (long long)rounds + rounds2;
         stats->activations = (long long)(act + act2);
         stats->inner_iterations = (long long)(inner + inner2);
+        stats->idle_activations = 0;
+        stats->deferred = 0;
         stats->nodes_per_brick = tomo::kBrickNodes;
         cudaEventElapsedTime(&stats->setup_ms, ev[0], ev[3]);
         cudaEventElapsedTime(&stats->solve_ms, ev[3], ev[1]);

@@ -65,6 +65,7 @@ struct tomo_ctx {
     // last eikonal solve
     tomo::DevBuf<float> T;
     tomo::DevBuf<unsigned> qflag, lists, ctrl;
+    tomo::DevBuf<unsigned> fim_keys, band_min;  // time-band ordering (per brick keys, per-shot minima)
     tomo::DevBuf<float> fsm_T;                      // TOMO_OP_NGB sweep grids (with halo)
     tomo::DevBuf<tomo::FsmShot> fsm_shots;
     tomo::DevBuf<unsigned> fsm_bar;

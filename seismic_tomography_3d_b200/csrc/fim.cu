@@ -148,7 +148,10 @@ __device__ void sample_receivers(const float *T, const ShotDesc *shots, int nsho
 
 struct WarpStats {
     unsigned long long act, inner, idle;  // idle: activations that lowered no node
+    unsigned long long deferred;          // items put off to a later round (time band)
 };
+
+constexpr unsigned kNoKey = 0xffffffffu;
 
 // Data of one work item as loaded from global memory (the face halo goes straight to the
 // warp's tile).
@@ -333,7 +336,9 @@ constexpr unsigned kPushCap = 32;
 // Queues the buffered candidates for round+1: one lane per candidate marks its brick
 // "queued for round+1" (atomicMax on the brick's flag; only the first marker of the round
 // appends it), and the survivors are appended to the next list with one atomic.
-__device__ __forceinline__ void flush_pushes(const FimLaunch &p, unsigned *pbuf, unsigned &pcnt, unsigned round)
+template <bool kBand>
+__device__ __forceinline__ void flush_pushes(const FimLaunch &p, unsigned *pbuf, const unsigned *pkey,
+                                             unsigned &pcnt, unsigned round)
 {
     const int lane = threadIdx.x & 31;
     __syncwarp();  // the buffer as the lanes wrote it
@@ -343,7 +348,12 @@ __device__ __forceinline__ void flush_pushes(const FimLaunch &p, unsigned *pbuf,
     if ((unsigned)lane < pcnt) {
         item = pbuf[lane];
         const unsigned s = item >> p.local_bits, b = item & ((1u << p.local_bits) - 1u);
-        const unsigned old = atomicMax(p.qflag + p.shots[s].qbase + b, tag);
+        const unsigned long long qi = p.shots[s].qbase + b;
+        if (kBand) {
+            const unsigned k = pkey[lane];
+            if (k != kNoKey) atomicMin(p.keys + qi, k);
+        }
+        const unsigned old = atomicMax(p.qflag + qi, tag);
         want = old < tag;
     }
     const unsigned wm = __ballot_sync(kFull, want);
@@ -359,10 +369,10 @@ __device__ __forceinline__ void flush_pushes(const FimLaunch &p, unsigned *pbuf,
 }
 
 // One activation of one (already loaded) brick by one warp.
-template <bool kFastSqrt, bool kAsync>
+template <bool kFastSqrt, bool kAsync, bool kBand = false>
 __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad &L, unsigned round, float *tile,
-                                            WarpStats &ws, unsigned *pbuf, unsigned &pcnt, unsigned *cursor,
-                                            unsigned &next)
+                                            WarpStats &ws, unsigned *pbuf, unsigned *pkey, unsigned &pcnt,
+                                            unsigned *cursor, unsigned &next)
 {
     const int lane = threadIdx.x & 31;
     const unsigned s = L.s, b = L.b;
@@ -444,6 +454,12 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     // y.  T(y) is the halo cell loaded at the start of this activation; a concurrent drop of
     // y only makes the test more permissive.
     const bool d0 = c0 < i0 - p.change_tol, d1 = c1 < i1 - p.change_tol;
+    // Key of this activation's pushes: the smallest new time among its dropped nodes.
+    unsigned key = kNoKey;
+    if (kBand) {
+        key = __reduce_min_sync(kFull, __float_as_uint(fminf(d0 ? c0 : kInf, d1 ? c1 : kInf)));
+        if (key == __float_as_uint(kInf)) key = kNoKey;
+    }
     unsigned fl = 0;  // faces: 1 z-, 2 z+, 4 x-, 8 x+, 16 y-, 32 y+
     if (z0 == 0 && ((d0 && c0 < tile[ti0 - 1]) || (d1 && c1 < tile[ti1 - 1]))) fl |= 1u;
     if (z0 == 3 && ((d0 && c0 < tile[ti0 + 1]) || (d1 && c1 < tile[ti1 + 1]))) fl |= 2u;
@@ -475,9 +491,14 @@ __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad 
     // Candidates go to the warp's push buffer; the global dedup and append happen 32 at a
     // time (flush_pushes), so most activations end without a global atomic.
     const unsigned wm = __ballot_sync(kFull, want);
-    if (want) pbuf[pcnt + __popc(wm & ((1u << lane) - 1u))] = (s << p.local_bits) | (unsigned)tgt;
+    if (want) {
+        const unsigned slot = pcnt + __popc(wm & ((1u << lane) - 1u));
+        pbuf[slot] = (s << p.local_bits) | (unsigned)tgt;
+        if (kBand) pkey[slot] = key;
+    }
     pcnt += __popc(wm);
-    if (pcnt > kPushCap - 7u) flush_pushes(p, pbuf, pcnt, round);
+    // (the banded kernel flushes once per item in its own loop)
+    if (!kBand && pcnt > kPushCap - 7u) flush_pushes<kBand>(p, pbuf, pkey, pcnt, round);
     next = __shfl_sync(kFull, nx, 0);
 }
 
@@ -493,16 +514,20 @@ __device__ __forceinline__ unsigned fetch_item(unsigned *cursor)
 constexpr int fim_regs(int minb) { return minb <= 1 ? 255 : (65536 / (minb * 256)) / 8 * 8; }
 
 // Up to 16 warps per CTA: 2 CTAs x 16 warps measured 1 % faster than 4 x 8 on the config-2
-// batch (half as many CTAs arrive at each round barrier).
-template <int MINB, bool kFastSqrt>
+// batch (half as many CTAs arrive at each round barrier).  kBand: time-band ordering
+// (FimLaunch::band > 0), a separate instance so that the plain kernel keeps its registers.
+template <int MINB, bool kFastSqrt, bool kBand>
 __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_solve(FimLaunch p)
 {
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5;
     float *tile = smem + warp * kTileNodes;
     unsigned *pbuf = reinterpret_cast<unsigned *>(smem + (blockDim.x >> 5) * kTileNodes) + warp * kPushCap;
+    // the keys of the pushes (time band) sit one push-buffer array above
+    unsigned *pkey = kBand ? pbuf + (blockDim.x >> 5) * kPushCap : nullptr;
     unsigned pcnt = 0;
-    WarpStats ws{0ull, 0ull, 0ull};
+    WarpStats ws{0ull, 0ull, 0ull, 0ull};
+    const int lane = threadIdx.x & 31;
     const unsigned nwarps = gridDim.x * (blockDim.x >> 5);
     const unsigned gwarp = blockIdx.x * (blockDim.x >> 5) + warp;
 
@@ -536,14 +561,45 @@ __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_solve(F
         // cursors on separate lines, each over a stripe of the list, are 6 % slower: the
         // one cursor is not contended enough to matter, and the stripe scan lengthens the tail.
         // A warp's first item of the round is its own index; the cursor hands out the rest.
+        // time band: per-shot minima of round - 1 (thresholds), of this round, and the array
+        // reset for round + 1 (read in round - 1)
+        if (kBand && blockIdx.x == 0) {
+            unsigned *reset = p.band_min + (size_t)((round + 1u) % 3u) * p.nshots;  // read last round
+            for (int j = threadIdx.x; j < p.nshots; j += blockDim.x) reset[j] = kNoKey;
+        }
         for (unsigned i = gwarp; i < n;) {
+            const unsigned item = __ldcg(list + i);
+            unsigned kb = kNoKey, tb = kNoKey;
+            if (kBand) {  // key and threshold loads go out with the brick's
+                const unsigned s = item >> p.local_bits;
+                kb = __ldcg(p.keys + p.shots[s].qbase + (item & ((1u << p.local_bits) - 1u)));
+                tb = __ldcg(p.band_min + (size_t)((round + 2u) % 3u) * p.nshots + s);
+            }
             BrickLoad A;
-            load_brick(p, __ldcg(list + i), A, tile);
+            load_brick(p, item, A, tile);
             unsigned next = 0;
-            relax_brick<kFastSqrt, false>(p, A, round, tile, ws, pbuf, pcnt, cursor, next);
+            bool defer = false;
+            if (kBand && kb != kNoKey) {
+                if (lane == 0) atomicMin(p.band_min + (size_t)(round % 3u) * p.nshots + A.s, kb);
+                // too far ahead of its shot's front: queued again for the next round
+                defer = tb != kNoKey && __uint_as_float(kb) > __uint_as_float(tb) + p.band;
+                if (!defer && lane == 0) p.keys[p.shots[A.s].qbase + A.b] = kNoKey;  // consumed here
+            }
+            if (kBand && defer) {
+                if (lane == 0) {
+                    pbuf[pcnt] = item;
+                    pkey[pcnt] = kNoKey;
+                }
+                pcnt += 1;
+                ws.deferred += 1;
+                next = fetch_item(cursor);
+            } else {
+                relax_brick<kFastSqrt, false, kBand>(p, A, round, tile, ws, pbuf, pkey, pcnt, cursor, next);
+            }
+            if (kBand && pcnt > kPushCap - 7u) flush_pushes<kBand>(p, pbuf, pkey, pcnt, round);
             i = nwarps + next;
         }
-        if (pcnt) flush_pushes(p, pbuf, pcnt, round);
+        if (pcnt) flush_pushes<kBand>(p, pbuf, pkey, pcnt, round);
         if (!grid_sync(p.ctrl, epoch, p.spin_limit)) { ok = false; break; }
         ++round;
     }
@@ -552,6 +608,7 @@ __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_solve(F
         atomicAdd(p.stats + 1, ws.inner);
         atomicAdd(p.stats + 3, ws.idle);
     }
+    if ((threadIdx.x & 31) == 0 && ws.deferred) atomicAdd(p.stats + 2, ws.deferred);
     if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kRounds] = round;
     if (!ok || p.nrec == 0) return;
 
@@ -608,7 +665,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_async(FimLaunch p)
         BrickLoad A;
         load_brick(p, item, A, tile);
         unsigned unused = 0, unused_next = 0;
-        relax_brick<kFastSqrt, true>(p, A, 0u, tile, ws, nullptr, unused, nullptr, unused_next);
+        relax_brick<kFastSqrt, true>(p, A, 0u, tile, ws, nullptr, nullptr, unused, nullptr, unused_next);
     }
     if (lane == 0 && ws.act) {
         atomicAdd(p.stats + 0, ws.act);
@@ -876,10 +933,14 @@ cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx,
 template <int MINB, bool kFastSqrt>
 static cudaError_t launch_solve(const FimLaunch &p, int block_warps, bool async, int *grid_out, cudaStream_t st)
 {
-    const void *fn = async ? (const void *)k_fim_async<MINB, kFastSqrt> : (const void *)k_fim_solve<MINB, kFastSqrt>;
+    const bool band = !async && p.band > 0.f;
+    const void *fn = async  ? (const void *)k_fim_async<MINB, kFastSqrt>
+                     : band ? (const void *)k_fim_solve<MINB, kFastSqrt, true>
+                            : (const void *)k_fim_solve<MINB, kFastSqrt, false>;
     if (async && block_warps > 8) block_warps = 8;  // the asynchronous kernel's CTAs hold 8 warps at most
     const int threads = 32 * block_warps;
-    const size_t smem = (size_t)block_warps * (kTileNodes * sizeof(float) + kPushCap * sizeof(unsigned));
+    // per warp: its tile, its push buffer and (time band) the pushes' keys
+    const size_t smem = (size_t)block_warps * (kTileNodes * sizeof(float) + 2 * kPushCap * sizeof(unsigned));
     int dev = 0, nsm = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;

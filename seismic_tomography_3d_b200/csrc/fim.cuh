@@ -65,6 +65,14 @@ struct FimLaunch {
     float inner_tol;      // in-brick iterations stop when no node drops by more than this
     unsigned local_bits;  // item = shot << local_bits | local brick
     unsigned long long spin_limit;
+    // Time-band ordering (band > 0, rounds schedule only).  keys[qbase + b]: the smallest
+    // new face time pushed to the brick since it was last relaxed (float bits, kNoKey =
+    // none); band_min: three rotating arrays of nshots per-shot minima of the keys met in a
+    // round.  A brick whose key exceeds its shot's minimum of the previous round by more
+    // than band waits for a later round.
+    unsigned *keys;
+    unsigned *band_min;
+    float band;
     // receivers
     int nrec;
     const float *rx, *ry, *rz;

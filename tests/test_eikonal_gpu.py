@@ -206,3 +206,40 @@ def test_async_and_round_schedules_agree(tomo, windows):
         assert st["rounds"] == 0 and st["activations"] > 0
         for i in range(len(sv.shots)):
             assert rel_err(ctx.eik_volume(i), ref[i], sv.h, float(sv.velocity.max())) < 1e-6
+
+
+@pytest.mark.parametrize("band", [0.01, 0.2])
+def test_time_band_ordering_same_fixed_point(tomo, oracle_mod, band):
+    """Time-band ordering (tomo_eik_opts.time_band) only changes when queued bricks are
+    relaxed.  On a smooth v(z) model, where a surface path reaches bricks before the
+    diving one and many bricks are put off, the solve reaches the oracle's fixed point and,
+    with every drop re-queued, the unordered solve's field."""
+    nx, ny, nz, h = 48, 44, 28, 25.0
+    v = np.ascontiguousarray(wl.gradient_model(nx, ny, nz, h, 1500.0, 1.0))
+    shots = np.array([[0.0, 0.0, 0.0], [600.0, 500.0, 0.0], [1175.0, 1075.0, 100.0]], np.float32)
+    with tomo.Context(nx, ny, nz, h) as ctx:
+        ctx.set_velocity(v)
+        _, st0 = ctx.eik_solve(shots, want_recv=False, change_tol=-1.0)
+        T0 = [ctx.eik_volume(i) for i in range(len(shots))]
+        _, st1 = ctx.eik_solve(shots, want_recv=False, change_tol=-1.0, time_band=band)
+        T1 = [ctx.eik_volume(i) for i in range(len(shots))]
+        # the bench tolerances with the band
+        ctx.eik_solve(shots, want_recv=False, change_tol=1e-5, inner_tol=1e-6, time_band=band)
+        T2 = [ctx.eik_volume(i) for i in range(len(shots))]
+    assert st0["deferred"] == 0
+    if band < 0.05:
+        assert st1["deferred"] > 0
+    for i, sh in enumerate(shots):
+        Tref = solve_oracle(oracle_mod, v, h, sh)
+        assert rel_err(T1[i], Tref, h, float(v.max())) < REL_TOL
+        assert rel_err(T2[i], Tref, h, float(v.max())) < REL_TOL
+        assert rel_err(T1[i], T0[i], h, float(v.max())) < 1e-6
+
+
+def test_time_band_rejects_bad_values(tomo):
+    sv = wl.small(5, 16, 16, 12)
+    with tomo.Context(sv.nx, sv.ny, sv.nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        for bad in (-1.0, float("nan"), float("inf")):
+            with pytest.raises(tomo.TomoError):
+                ctx.eik_solve(sv.shots, time_band=bad)
