@@ -93,7 +93,9 @@ typedef struct {
                         Same fixed point either way.  Measured with 0.2 s: 1.64x faster
                         on the config-5 starting model (v = 1500 + z, 0.38 x the brick
                         activations), 1.08x on config 3, slower on the windowed config-2
-                        batch.  Ignored by the warm-started solve and the ASYNC schedule. */
+                        batch.  0: the band tomo_eik_autotune chose on this context, if
+                        any, else off; < 0: off.  Ignored by the warm-started solve and
+                        the ASYNC schedule.                                           */
 } tomo_eik_opts;
 
 /* Work schedules of the JW solve (same fixed point, different order of brick updates).
@@ -211,12 +213,13 @@ typedef struct {
 } tomo_tune_stats;
 
 /* Autotuner of the JW solve (no counterpart in the reference, whose launch shape is fixed).
- * Solves this batch (no receivers) with every launch shape -- warps per CTA {4, 8}, CTAs
- * per SM {3, 4, 5, 6}, in-brick iteration cap {8, 16, 32}, each brick shape of
- * tomo_eik_brick_shapes -- `repeats` times each (0: 2), keeps the fastest in the context
- * and writes it to *best (may be NULL).  Later solves on this context use the tuned value
- * for every tomo_eik_opts field they leave 0.  The traveltime pool holds the last trial's
- * fields afterwards. */
+ * Solves this batch (no receivers) with every launch shape -- warps per CTA {16, 8, 4},
+ * CTAs per SM {3, 4, 5, 6}, in-brick iteration cap {8, 16, 32}, each brick shape of
+ * tomo_eik_brick_shapes -- `repeats` times each (0: 2), then, at the fastest shape, the
+ * time band at 3, 6, 9 and 12 times the slowest brick crossing (4 dx s_max; none is the
+ * shape's own time).  Keeps the fastest in the context and writes it to *best (may be
+ * NULL).  Later solves on this context use the tuned value for every tomo_eik_opts field
+ * they leave 0.  The traveltime pool holds the last trial's fields afterwards. */
 int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows,
                       int repeats, tomo_eik_opts *best, tomo_tune_stats *stats);
 

@@ -364,8 +364,11 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     c.async = opts && opts->schedule == TOMO_SCHED_ASYNC;
     // Time-band ordering: off by default.  It pays where slow paths reach bricks long
     // before the first arrival does (1.64x on the config-5 starting model at 0.2 s) and
-    // costs where they do not (the windowed config-2 batch).
-    c.time_band = (opts && !c.async && opts->time_band > 0.f) ? opts->time_band : 0.f;
+    // costs where they do not (the windowed config-2 batch).  0: the autotuned band, if
+    // the autotuner chose one; < 0: off.
+    const float band = opts ? opts->time_band : 0.f;
+    c.time_band = band > 0.f ? band : (band < 0.f ? 0.f : ctx->tuned_time_band);
+    if (c.async) c.time_band = 0.f;
     return c;
 }
 
@@ -562,8 +565,8 @@ int eik_plan(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_wind
     if (nrec < 0 || (nrec > 0 && !receivers)) return fail(ctx, TOMO_ERR_INVALID_ARG, "bad receivers");
     if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
     if (opts && opts->op != TOMO_OP_JW) return fail(ctx, TOMO_ERR_INVALID_ARG, "the plan runs the JW operator only");
-    if (opts && !(opts->time_band >= 0.f && opts->time_band < 1e30f))
-        return fail(ctx, TOMO_ERR_INVALID_ARG, "time_band must be a finite value >= 0");
+    if (opts && !(std::fabs(opts->time_band) < 1e30f))
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "time_band must be finite");
     const SolveCfg cfg = solve_cfg(ctx, opts);
     Batch bt;
     int rc = make_batch(ctx, nshots, shots, windows, nrec, receivers, bt);
@@ -614,8 +617,8 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
         return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown brick shape (tomo_eik_brick_shapes lists 1: 4x4x4)");
     if (opts && (opts->schedule < TOMO_SCHED_DEFAULT || opts->schedule > TOMO_SCHED_ASYNC))
         return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown work schedule");
-    if (opts && !(opts->time_band >= 0.f && opts->time_band < 1e30f))
-        return fail(ctx, TOMO_ERR_INVALID_ARG, "time_band must be a finite value >= 0");
+    if (opts && !(std::fabs(opts->time_band) < 1e30f))
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "time_band must be finite");
     const SolveCfg cfg = solve_cfg(ctx, opts);
     CK(cudaSetDevice(ctx->device));
     Batch bt;
@@ -791,6 +794,7 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
     if (repeats == 0) repeats = 2;
     // untuned defaults while timing (an earlier tuning must not leak into the trials)
     ctx->tuned_block_warps = ctx->tuned_occupancy = ctx->tuned_max_inner = 0;
+    ctx->tuned_time_band = 0.f;
     const int warps[] = {kDefaultBlockWarps, 8, 4};
     const int occs[] = {4, 5, 6, 3};
     const int inners[] = {16, 8, 32};
@@ -824,15 +828,50 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
                 }
                 ++trials;
             }
+    // Then the time band at the chosen shape: multiples of the slowest brick crossing,
+    // 4 h s_max (the band is model-relative; no band is the shape loop's own time).
+    o.block_warps = bw;
+    o.occupancy = bo;
+    o.max_inner = bi;
+    float bb = 0.f;
+    {
+        CK(ctx->tune_word.ensure(1));
+        CK(tomo::max_positive(ctx->slow.ptr, (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz, ctx->tune_word.ptr,
+                              ctx->stream));
+        unsigned bits = 0;
+        CK(cudaMemcpyAsync(&bits, ctx->tune_word.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        float smax = 0.f;
+        std::memcpy(&smax, &bits, sizeof(smax));
+        const float crossing = (float)tomo::kBrick * ctx->g.dx * smax;
+        for (float mult : {3.f, 6.f, 9.f, 12.f}) {
+            if (!(crossing > 0.f)) break;
+            o.time_band = mult * crossing;
+            float ms = 0.f;
+            for (int r = 0; r < repeats + 1; r++) {
+                rc = tomo_eik_solve(ctx, nshots, shots, windows, 0, nullptr, nullptr, &o, &st);
+                if (rc != TOMO_OK) return rc;
+                if (r == 0) continue;
+                ms = (r == 1) ? st.solve_ms : std::min(ms, st.solve_ms);
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                bb = o.time_band;
+            }
+            ++trials;
+        }
+    }
     ctx->tuned_block_warps = bw;
     ctx->tuned_occupancy = bo;
     ctx->tuned_max_inner = bi;
+    ctx->tuned_time_band = bb;
     if (best) {
         *best = tomo_eik_opts{};
         best->op = TOMO_OP_JW;
         best->block_warps = bw;
         best->occupancy = bo;
         best->max_inner = bi;
+        best->time_band = bb;
     }
     if (stats) {
         stats->trials = trials;

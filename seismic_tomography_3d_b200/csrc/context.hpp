@@ -66,6 +66,7 @@ struct tomo_ctx {
     tomo::DevBuf<float> T;
     tomo::DevBuf<unsigned> qflag, lists, ctrl;
     tomo::DevBuf<unsigned> fim_keys, band_min;  // time-band ordering (per brick keys, per-shot minima)
+    tomo::DevBuf<unsigned> tune_word;            // autotuner scratch (largest slowness)
     tomo::DevBuf<float> fsm_T;                      // TOMO_OP_NGB sweep grids (with halo)
     tomo::DevBuf<tomo::FsmShot> fsm_shots;
     tomo::DevBuf<unsigned> fsm_bar;
@@ -82,6 +83,7 @@ struct tomo_ctx {
     bool have_solve = false;
     // launch shape chosen by tomo_eik_autotune (0: not tuned)
     int tuned_block_warps = 0, tuned_occupancy = 0, tuned_max_inner = 0;
+    float tuned_time_band = 0.f;  // 0: none chosen (off)
 
     cudaEvent_t ev[8] = {};
     unsigned *pinned_ctrl = nullptr;  // kCtrlWords + stats

@@ -716,6 +716,18 @@ __global__ void k_velocity_to_slowness(const float *v, float *s, size_t n)
         s[i] = __fdiv_rn(1.0f, v[i]);
 }
 
+// Largest finite positive value of v (as float bits; positive floats order as unsigned).
+__global__ void k_max_positive(const float *v, size_t n, unsigned *out)
+{
+    unsigned m = 0u;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float x = v[i];
+        if (x > 0.f && x < 3.0e38f) m = max(m, __float_as_uint(x));
+    }
+    m = __reduce_max_sync(kFull, m);
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
 // Pad to the brick multiple by edge replication (Block_FIM::expand_model,
 // block_FIM.cpp:8-57, is a clamp of the index) and store brick-major.
 __global__ void k_brick_model(const float *slow, float *S, int nx, int ny, int nz, int nxx, int nyy, int nzz)
@@ -892,6 +904,14 @@ static int grid_for(size_t n, int threads)
     size_t g = (n + threads - 1) / threads;
     if (g > 148u * 32u) g = 148u * 32u;
     return g < 1 ? 1 : (int)g;
+}
+
+cudaError_t max_positive(const float *v, size_t n, unsigned *out_bits, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(out_bits, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    k_max_positive<<<grid_for(n, 256), 256, 0, st>>>(v, n, out_bits);
+    return cudaGetLastError();
 }
 
 cudaError_t velocity_to_slowness(const float *v, float *s, size_t n, cudaStream_t st)

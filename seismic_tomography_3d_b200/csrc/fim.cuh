@@ -97,6 +97,8 @@ cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, bool i
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out,
                         cudaStream_t st);
 cudaError_t velocity_to_slowness(const float *v, float *s, size_t n, cudaStream_t st);
+// *out_bits = float bits of the largest finite positive entry of v (0 if none).
+cudaError_t max_positive(const float *v, size_t n, unsigned *out_bits, cudaStream_t st);
 
 // Warm start (fim.cu): every window node of every shot starts at ceiling * scale
 // (volumes at ShotDesc::v_off) instead of INF; non-finite or non-positive entries and

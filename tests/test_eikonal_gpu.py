@@ -184,9 +184,10 @@ def test_autotune_picks_a_shape_and_keeps_results(tomo):
         ctx.eik_solve(sv.shots, windows=sv.windows)
         ref = [ctx.eik_volume(i) for i in range(len(sv.shots))]
         shape, st = ctx.eik_autotune(sv.shots, windows=sv.windows, repeats=1)
-        assert st["trials"] == 36
+        assert st["trials"] == 40  # 36 launch shapes, then 4 time bands
         assert shape["block_warps"] in (4, 8, 16) and shape["occupancy"] in (3, 4, 5, 6)
         assert shape["max_inner"] in (8, 16, 32)
+        assert shape["time_band"] >= 0.0
         assert 0 < st["best_ms"] <= st["default_ms"]
         ctx.eik_solve(sv.shots, windows=sv.windows)
         for i in range(len(sv.shots)):
@@ -236,10 +237,14 @@ def test_time_band_ordering_same_fixed_point(tomo, oracle_mod, band):
         assert rel_err(T1[i], T0[i], h, float(v.max())) < 1e-6
 
 
-def test_time_band_rejects_bad_values(tomo):
+def test_time_band_values(tomo):
+    """A negative band switches the ordering off (even after autotuning); non-finite bands
+    are rejected."""
     sv = wl.small(5, 16, 16, 12)
     with tomo.Context(sv.nx, sv.ny, sv.nz, sv.h) as ctx:
         ctx.set_velocity(sv.velocity)
-        for bad in (-1.0, float("nan"), float("inf")):
+        _, st = ctx.eik_solve(sv.shots, time_band=-1.0)
+        assert st["deferred"] == 0
+        for bad in (float("nan"), float("inf"), -float("inf")):
             with pytest.raises(tomo.TomoError):
                 ctx.eik_solve(sv.shots, time_band=bad)
