@@ -94,7 +94,8 @@ typedef struct {
                         on the config-5 starting model (v = 1500 + z, 0.38 x the brick
                         activations), 1.08x on config 3, slower on the windowed config-2
                         batch.  0: the band tomo_eik_autotune chose on this context, if
-                        any, else off; < 0: off.  Ignored by the warm-started solve and
+                        any, else off; < 0: off.  Untuned banded solves default to 8
+                        warps per CTA at occupancy 3 (80 registers).  Ignored by the warm-started solve and
                         the ASYNC schedule.                                           */
 } tomo_eik_opts;
 
@@ -217,8 +218,8 @@ typedef struct {
  * CTAs per SM {3, 4, 5, 6}, in-brick iteration cap {8, 16, 32}, each brick shape of
  * tomo_eik_brick_shapes -- `repeats` times each (0: 2), then, at the fastest shape, the
  * time band at 3, 6, 9 and 12 times the slowest brick crossing (4 dx s_max; none is the
- * shape's own time).  Keeps the fastest in the context and writes it to *best (may be
- * NULL).  Later solves on this context use the tuned value for every tomo_eik_opts field
+ * shape's own time) and, if a band wins, the warps x CTAs-per-SM shapes again with it.
+ * Keeps the fastest in the context and writes it to *best (may be NULL).  Later solves on this context use the tuned value for every tomo_eik_opts field
  * they leave 0.  The traveltime pool holds the last trial's fields afterwards. */
 int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows,
                       int repeats, tomo_eik_opts *best, tomo_tune_stats *stats);

@@ -27,6 +27,7 @@ constexpr int kDefaultMaxInner = 16;
 // SM, the register budget (64) of 4 CTAs of 8 warps, i.e. 2 CTAs of 16 -- fastest on config 2.
 constexpr int kDefaultOccupancy = 4;
 constexpr int kDefaultBlockWarps = 16;
+constexpr int kBandBlockWarps = 8, kBandOccupancy = 3;  // banded solves, untuned
 constexpr float kDefaultChangeTol = 1e-6f;
 constexpr int kDefaultMaxRounds = 1 << 20;
 constexpr int kMaxRounds = 1 << 22;
@@ -369,6 +370,13 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     const float band = opts ? opts->time_band : 0.f;
     c.time_band = band > 0.f ? band : (band < 0.f ? 0.f : ctx->tuned_time_band);
     if (c.async) c.time_band = 0.f;
+    // Banded solves carry more live state (spills at 64 registers): untuned, they run as
+    // 3 CTAs x 8 warps at 80 registers, 1.15x faster than the plain default shape on the
+    // config-5 starting model (504 vs 581 ms) and equal on config 3.
+    if (c.time_band > 0.f) {
+        if (!(opts && opts->block_warps > 0) && ctx->tuned_block_warps == 0) c.block_warps = kBandBlockWarps;
+        if (!(opts && opts->occupancy > 0) && ctx->tuned_occupancy == 0) c.occupancy = kBandOccupancy;
+    }
     return c;
 }
 
@@ -860,6 +868,30 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
             }
             ++trials;
         }
+    }
+    // With a band, the launch shapes again (the banded kernel holds more live state, so
+    // its best shape can differ: 3 x 8 warps on the config-5 starting model).
+    if (bb > 0.f) {
+        o.time_band = bb;
+        o.max_inner = bi;
+        for (int w : warps)
+            for (int oc : occs) {
+                o.block_warps = w;
+                o.occupancy = oc;
+                float ms = 0.f;
+                for (int r = 0; r < repeats + 1; r++) {
+                    rc = tomo_eik_solve(ctx, nshots, shots, windows, 0, nullptr, nullptr, &o, &st);
+                    if (rc != TOMO_OK) return rc;
+                    if (r == 0) continue;
+                    ms = (r == 1) ? st.solve_ms : std::min(ms, st.solve_ms);
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    bw = w;
+                    bo = oc;
+                }
+                ++trials;
+            }
     }
     ctx->tuned_block_warps = bw;
     ctx->tuned_occupancy = bo;
