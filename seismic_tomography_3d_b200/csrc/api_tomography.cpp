@@ -246,7 +246,7 @@ int jac_prepare(tomo_ctx *ctx, const tomo_jacobian_opts *opts, JacGeom &jg)
     CK(ctx->ray_order.ensure((size_t)nrays));
     tb = 0;
     CK(tomo::ray_order(ctx->t_recv.ptr, ctx->ray_keys.ptr, ctx->ray_keys_out.ptr, ctx->ray_iota.ptr,
-                       ctx->ray_order.ptr, (int)nrays, nullptr, &tb, ctx->stream));
+                       ctx->ray_order.ptr, (int)nrays, ctx->nrec, nullptr, &tb, ctx->stream));
     CK(ctx->order_temp.ensure(tb));
     // the sync keeps the host staging vectors alive until the copies are done
     CK(cudaStreamSynchronize(ctx->stream));
@@ -302,7 +302,7 @@ int jac_march(tomo_ctx *ctx, const JacGeom &jg)
     }
     size_t ob = ctx->order_temp.cap;
     CK(tomo::ray_order(ctx->t_recv.ptr, ctx->ray_keys.ptr, ctx->ray_keys_out.ptr, ctx->ray_iota.ptr, ctx->ray_order.ptr,
-                       (int)jg.nrays, ctx->order_temp.ptr, &ob, ctx->stream));
+                       (int)jg.nrays, ctx->nrec, ctx->order_temp.ptr, &ob, ctx->stream));
     RayLaunch rl = ray_launch(ctx, jg);
     rl.order = ctx->ray_order.ptr;
     CK(tomo::ray_march(rl, ctx->stream));

@@ -58,9 +58,10 @@ cudaError_t csr_transpose_prepare(const int *row_ptr, const int *cols, int nrows
 // CUB device-wide primitives (temp == nullptr queries *temp_bytes).
 cudaError_t scan_exclusive(const int *in, int *out, int n, void *temp, size_t *temp_bytes, cudaStream_t st);
 cudaError_t reduce_min(const float *in, float *out, size_t n, void *temp, size_t *temp_bytes, cudaStream_t st);
-// order[0..n) = ray indices by descending receiver time (temp == nullptr queries *temp_bytes)
+// order[0..n) = ray indices shot by shot (rays ray = shot * nrec + receiver), by descending
+// receiver time within a shot (temp == nullptr queries *temp_bytes)
 cudaError_t ray_order(const float *t_recv, unsigned *keys, unsigned *keys_out, int *vals, int *order, int n,
-                      void *temp, size_t *temp_bytes, cudaStream_t st);
+                      int nrec, void *temp, size_t *temp_bytes, cudaStream_t st);
 cudaError_t sort_pairs(const int *keys_in, int *keys_out, const int *vals_in, int *vals_out, long long n, int key_bits,
                        void *temp, size_t *temp_bytes, cudaStream_t st);
 cudaError_t csr_transpose_finish(const int *sorted_pos, const int *rows_of, const float *vals, const long long *sizes,
