@@ -27,6 +27,7 @@ class Eikonal_B200 : public Eikonal {
 protected:
     tomo_ctx *ctx = nullptr;
     bool batch_ready = false;
+    float time_band = 0.f;  // optional key eikonal_time_band (s): time-band ordering, 0 = off
     bool geometry_ready = false;
     std::vector<float> recv_times;  // total_shots x total_nodes, trilinear receiver times
 
