@@ -28,6 +28,11 @@ constexpr int kDefaultMaxInner = 16;
 constexpr int kDefaultOccupancy = 4;
 constexpr int kDefaultBlockWarps = 16;
 constexpr int kBandBlockWarps = 8, kBandOccupancy = 3;  // banded solves, untuned
+#ifndef TOMO_PARK_ROUNDS
+#define TOMO_PARK_ROUNDS 4
+#endif
+constexpr int kParkRounds = TOMO_PARK_ROUNDS;  // rounds a put-off brick waits (1..4)
+static_assert(kParkRounds >= 1 && kParkRounds + 2 <= tomo::kCtrlWords - tomo::kPark0, "parking lists");
 constexpr float kDefaultChangeTol = 1e-6f;
 constexpr int kDefaultMaxRounds = 1 << 20;
 constexpr int kMaxRounds = 1 << 22;
@@ -507,6 +512,9 @@ tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, in
         p.band = c.time_band;
         p.keys = ctx->fim_keys.ptr;
         p.band_min = ctx->band_min.ptr;
+        p.park = ctx->band_park.ptr;
+        p.park_cnt = ctx->ctrl.ptr + tomo::kPark0;
+        p.park_rounds = kParkRounds;
     }
     return p;
 }
@@ -517,6 +525,7 @@ int band_buffers(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c)
     if (c.time_band <= 0.f) return TOMO_OK;
     CK(ctx->fim_keys.ensure((size_t)bt.q_total));
     CK(ctx->band_min.ensure((size_t)3 * bt.sd.size()));
+    CK(ctx->band_park.ensure((size_t)(kParkRounds + 2) * bt.q_total));
     return TOMO_OK;
 }
 

@@ -368,6 +368,62 @@ __device__ __forceinline__ void flush_pushes(const FimLaunch &p, unsigned *pbuf,
     pcnt = 0;
 }
 
+// Time band: a brick put off in round r waits on that round's parking list and is tested
+// again at the start of round r + park_rounds (or earlier, when the round's list is empty),
+// instead of every round.  park_rounds + 2 lists rotate: the list merged at the start of
+// round r is next filled in round r + 2, and block 0 zeroes its count at the start of
+// round r + 1, between the two barriers -- the same rotation as the work lists.  Each
+// warp buffers kParkCap items in shared memory and appends them with one atomic.
+constexpr unsigned kParkCap = 8;
+
+__device__ __forceinline__ unsigned park_slot(const FimLaunch &p, unsigned round)
+{
+    return round % (unsigned)(p.park_rounds + 2);
+}
+
+__device__ __forceinline__ void flush_parks(const FimLaunch &p, const unsigned *kbuf, unsigned &kcnt, unsigned round)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned j = park_slot(p, round);
+    __syncwarp();  // the buffer as lane 0 wrote it
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(p.park_cnt + j, kcnt);
+    base = __shfl_sync(kFull, base, 0);
+    if ((unsigned)lane < kcnt) p.park[(size_t)j * p.list_cap + base + lane] = kbuf[lane];
+    kcnt = 0;
+}
+
+// Appends parking list j's items that still hold a key (new information not yet relaxed)
+// to the next round's list, unless a push already queued them for it; grid-strided, one
+// item per lane.
+__device__ __noinline__ void merge_parks(const FimLaunch &p, unsigned j, unsigned np, unsigned round)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned nxt = (round + 1u) % 3u;
+    const unsigned tag = round + 2u;  // "queued for round+1"
+    const unsigned *park = p.park + (size_t)j * p.list_cap;
+    const unsigned gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    for (unsigned base = gw * 32u; base < np; base += nw * 32u) {
+        const unsigned idx = base + (unsigned)lane;
+        bool want = false;
+        unsigned item = 0;
+        if (idx < np) {
+            item = __ldcg(park + idx);
+            const unsigned s = item >> p.local_bits;
+            const unsigned long long qi = p.shots[s].qbase + (item & ((1u << p.local_bits) - 1u));
+            if (__ldcg(p.keys + qi) != kNoKey) want = atomicMax(p.qflag + qi, tag) < tag;
+        }
+        const unsigned wm = __ballot_sync(kFull, want);
+        if (wm) {
+            const int leader = __ffs(wm) - 1;
+            unsigned b0 = 0;
+            if (lane == leader) b0 = atomicAdd(p.ctrl + kCnt0 + nxt, (unsigned)__popc(wm));
+            b0 = __shfl_sync(kFull, b0, leader);
+            if (want) p.lists[(size_t)nxt * p.list_cap + b0 + __popc(wm & ((1u << lane) - 1u))] = item;
+        }
+    }
+}
+
 // One activation of one (already loaded) brick by one warp.
 template <bool kFastSqrt, bool kAsync, bool kBand = false>
 __device__ __forceinline__ void relax_brick(const FimLaunch &p, const BrickLoad &L, unsigned round, float *tile,
@@ -525,7 +581,12 @@ __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_solve(F
     unsigned *pbuf = reinterpret_cast<unsigned *>(smem + (blockDim.x >> 5) * kTileNodes) + warp * kPushCap;
     // the keys of the pushes (time band) sit one push-buffer array above
     unsigned *pkey = kBand ? pbuf + (blockDim.x >> 5) * kPushCap : nullptr;
-    unsigned pcnt = 0;
+    // parked items (time band): kParkCap per warp after the keys
+    unsigned *kbuf = kBand ? reinterpret_cast<unsigned *>(smem + (blockDim.x >> 5) * kTileNodes) +
+                                 2 * (blockDim.x >> 5) * kPushCap + warp * kParkCap
+                           : nullptr;
+    unsigned pcnt = 0, kcnt = 0;
+    unsigned parked_through = 0;  // parking lists of rounds < this one are merged (time band)
     WarpStats ws{0ull, 0ull, 0ull, 0ull};
     const int lane = threadIdx.x & 31;
     const unsigned nwarps = gridDim.x * (blockDim.x >> 5);
@@ -536,7 +597,26 @@ __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_solve(F
     for (;;) {
         const unsigned cur = round % 3u;
         const unsigned n = ld_volatile(p.ctrl + kCnt0 + cur);
-        if (n == 0u) break;
+        if (kBand) {
+            // parked items due now (put off park_rounds rounds ago), or all of them when
+            // this round has nothing else; the counts read here were final at the last
+            // barrier and nobody appends to these lists this round
+            const unsigned K = (unsigned)p.park_rounds;
+            const unsigned from = parked_through, to = n == 0u ? round : (round >= K ? round - K + 1u : 0u);
+            unsigned pending = 0;
+            for (unsigned d = from; d < to; d++) {
+                const unsigned j = park_slot(p, d);
+                const unsigned np = ld_volatile(p.park_cnt + j);
+                if (np) merge_parks(p, j, np, round);
+                pending += np;
+            }
+            if (to > parked_through) parked_through = to;
+            // the list of round - K - 1: merged by now, filled again next round
+            if (blockIdx.x == 0 && threadIdx.x == 0) p.park_cnt[park_slot(p, round + 1u)] = 0u;
+            if (n == 0u && pending == 0u) break;
+        } else if (n == 0u) {
+            break;
+        }
         if ((int)round >= p.max_rounds) {
             if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(p.ctrl + kErr, 0u, (unsigned)kDevRoundCap);
             ok = false;
@@ -586,11 +666,9 @@ __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_solve(F
                 if (!defer && lane == 0) p.keys[p.shots[A.s].qbase + A.b] = kNoKey;  // consumed here
             }
             if (kBand && defer) {
-                if (lane == 0) {
-                    pbuf[pcnt] = item;
-                    pkey[pcnt] = kNoKey;
-                }
-                pcnt += 1;
+                if (lane == 0) kbuf[kcnt] = item;
+                kcnt += 1;
+                if (kcnt == kParkCap) flush_parks(p, kbuf, kcnt, round);
                 ws.deferred += 1;
                 next = fetch_item(cursor);
             } else {
@@ -600,6 +678,7 @@ __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_solve(F
             i = nwarps + next;
         }
         if (pcnt) flush_pushes<kBand>(p, pbuf, pkey, pcnt, round);
+        if (kBand && kcnt) flush_parks(p, kbuf, kcnt, round);
         if (!grid_sync(p.ctrl, epoch, p.spin_limit)) { ok = false; break; }
         ++round;
     }
@@ -960,7 +1039,8 @@ static cudaError_t launch_solve(const FimLaunch &p, int block_warps, bool async,
     if (async && block_warps > 8) block_warps = 8;  // the asynchronous kernel's CTAs hold 8 warps at most
     const int threads = 32 * block_warps;
     // per warp: its tile, its push buffer and (time band) the pushes' keys
-    const size_t smem = (size_t)block_warps * (kTileNodes * sizeof(float) + 2 * kPushCap * sizeof(unsigned));
+    const size_t smem =
+        (size_t)block_warps * (kTileNodes * sizeof(float) + (2 * kPushCap + kParkCap) * sizeof(unsigned));
     int dev = 0, nsm = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;

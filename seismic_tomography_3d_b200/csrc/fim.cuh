@@ -72,6 +72,9 @@ struct FimLaunch {
     // than band waits for a later round.
     unsigned *keys;
     unsigned *band_min;
+    unsigned *park;       // park_rounds + 2 parking lists of list_cap entries (bricks put off)
+    unsigned *park_cnt;   // their counts (control words kPark0..)
+    int park_rounds;      // rounds a put-off brick waits before it is tested again (1..4)
     float band;
     // receivers
     int nrec;
