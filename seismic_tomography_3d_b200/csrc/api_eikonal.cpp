@@ -29,10 +29,13 @@ constexpr int kDefaultOccupancy = 4;
 constexpr int kDefaultBlockWarps = 16;
 constexpr int kBandBlockWarps = 8, kBandOccupancy = 3;  // banded solves, untuned
 #ifndef TOMO_PARK_ROUNDS
-#define TOMO_PARK_ROUNDS 4
+#define TOMO_PARK_ROUNDS 6
 #endif
-constexpr int kParkRounds = TOMO_PARK_ROUNDS;  // rounds a put-off brick waits (1..4)
-static_assert(kParkRounds >= 1 && kParkRounds + 2 <= tomo::kCtrlWords - tomo::kPark0, "parking lists");
+// Rounds a put-off brick waits before it is tested again (1..14).  Config-5 starting
+// model, banded solve: 1: 503 ms, 2: 472, 4: 404, 6: 396, 8: 397; config 3: 4: 10.8,
+// 6 and 8: 10.6 ms.
+constexpr int kParkRounds = TOMO_PARK_ROUNDS;
+static_assert(kParkRounds >= 1 && kParkRounds + 2 <= 16, "parking lists");
 constexpr float kDefaultChangeTol = 1e-6f;
 constexpr int kDefaultMaxRounds = 1 << 20;
 constexpr int kMaxRounds = 1 << 22;
@@ -513,7 +516,7 @@ tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, in
         p.keys = ctx->fim_keys.ptr;
         p.band_min = ctx->band_min.ptr;
         p.park = ctx->band_park.ptr;
-        p.park_cnt = ctx->ctrl.ptr + tomo::kPark0;
+        p.park_cnt = ctx->band_pcnt.ptr;
         p.park_rounds = kParkRounds;
     }
     return p;
@@ -526,6 +529,7 @@ int band_buffers(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c)
     CK(ctx->fim_keys.ensure((size_t)bt.q_total));
     CK(ctx->band_min.ensure((size_t)3 * bt.sd.size()));
     CK(ctx->band_park.ensure((size_t)(kParkRounds + 2) * bt.q_total));
+    CK(ctx->band_pcnt.ensure(16));
     return TOMO_OK;
 }
 
@@ -534,6 +538,8 @@ cudaError_t band_reset(tomo_ctx *ctx, const tomo::FimLaunch &p)
 {
     if (p.band <= 0.f) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(p.keys, 0xff, (size_t)p.list_cap * sizeof(unsigned), ctx->stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(p.park_cnt, 0, (size_t)(p.park_rounds + 2) * sizeof(unsigned), ctx->stream);
     if (e != cudaSuccess) return e;
     return cudaMemsetAsync(p.band_min, 0xff, (size_t)3 * p.nshots * sizeof(unsigned), ctx->stream);
 }

@@ -24,7 +24,6 @@ enum CtrlSlot : int {
     kErr = 5,                         // DevErr
     kRounds = 6,                      // rounds run (written by block 0)
     kCur0 = 7, kCur1 = 8, kCur2 = 9,  // per-round fetch cursors (3-way rotation)
-    kPark0 = 10,                      // time band: parking-list counts (up to 6 lists)
     kCtrlWords = 16,
 };
 

@@ -65,8 +65,8 @@ struct tomo_ctx {
     // last eikonal solve
     tomo::DevBuf<float> T;
     tomo::DevBuf<unsigned> qflag, lists, ctrl;
-    tomo::DevBuf<unsigned> fim_keys, band_min, band_park;  // time-band ordering (per brick keys, per-shot
-                                                           // minima, parking lists)
+    tomo::DevBuf<unsigned> fim_keys, band_min, band_park, band_pcnt;  // time-band ordering (per brick keys,
+                                                                      // per-shot minima, parking lists, counts)
     tomo::DevBuf<unsigned> tune_word;            // autotuner scratch (largest slowness)
     tomo::DevBuf<float> fsm_T;                      // TOMO_OP_NGB sweep grids (with halo)
     tomo::DevBuf<tomo::FsmShot> fsm_shots;

@@ -368,8 +368,8 @@ __device__ __forceinline__ void flush_pushes(const FimLaunch &p, unsigned *pbuf,
     pcnt = 0;
 }
 
-// Time band: a brick put off in round r waits on that round's parking list and is tested
-// again at the start of round r + park_rounds (or earlier, when the round's list is empty),
+// Time band: a brick put off in round r waits on that round's parking list and is merged
+// back at the start of round r + park_rounds (or earlier, when the round's list is empty),
 // instead of every round.  park_rounds + 2 lists rotate: the list merged at the start of
 // round r is next filled in round r + 2, and block 0 zeroes its count at the start of
 // round r + 1, between the two barriers -- the same rotation as the work lists.  Each

@@ -73,8 +73,8 @@ struct FimLaunch {
     unsigned *keys;
     unsigned *band_min;
     unsigned *park;       // park_rounds + 2 parking lists of list_cap entries (bricks put off)
-    unsigned *park_cnt;   // their counts (control words kPark0..)
-    int park_rounds;      // rounds a put-off brick waits before it is tested again (1..4)
+    unsigned *park_cnt;   // their counts (zeroed before the solve)
+    int park_rounds;      // rounds a put-off brick waits before it is tested again (1..14)
     float band;
     // receivers
     int nrec;
