@@ -42,7 +42,7 @@ BYTES_PER_NODE_ACT = 12  # slowness read + traveltime read + traveltime write (f
 # inside that budget: 2.7e-5 on this batch.  The library default is the exact fixed point.
 SOLVER = dict(change_tol=1e-5, inner_tol=1e-6)
 # Full-grid solves on the smooth starting models of configs 3 and 5 add the time-band
-# ordering (0.2 s): it removes most re-activation cascades of those models (1.13x / 2.1x
+# ordering (0.2 s): it removes most re-activation cascades of those models (1.18x / 2.3x
 # faster solves); on the windowed, layered config-2 batch it costs time and stays off.
 SOLVER_BANDED = dict(SOLVER, time_band=0.2)
 

@@ -90,9 +90,9 @@ typedef struct {
                         the previous round waits for a later round, so late, too-high
                         arrivals (a slow path reaching a brick before a faster diving
                         path) do not start re-activation cascades.  0 (default): off.
-                        Same fixed point either way.  Measured with 0.2 s: 2.1x faster
-                        on the config-5 starting model (v = 1500 + z, 0.35 x the brick
-                        activations), 1.13x on config 3, slower on the windowed config-2
+                        Same fixed point either way.  Measured with 0.2 s: 2.3x faster
+                        on the config-5 starting model (v = 1500 + z, 0.34 x the brick
+                        activations), 1.18x on config 3, slower on the windowed config-2
                         batch.  0: the band tomo_eik_autotune chose on this context, if
                         any, else off; < 0: off.  Untuned banded solves default to 8
                         warps per CTA at occupancy 3 (80 registers).  Ignored by the warm-started solve and

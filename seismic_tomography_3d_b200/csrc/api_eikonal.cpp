@@ -372,7 +372,7 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     // neighbours have settled and measured 2.5x slower on config 2 (1.8x the activations).
     c.async = opts && opts->schedule == TOMO_SCHED_ASYNC;
     // Time-band ordering: off by default.  It pays where slow paths reach bricks long
-    // before the first arrival does (2.1x on the config-5 starting model at 0.2 s) and
+    // before the first arrival does (2.3x on the config-5 starting model at 0.2 s) and
     // costs where they do not (the windowed config-2 batch).  0: the autotuned band, if
     // the autotuner chose one; < 0: off.
     const float band = opts ? opts->time_band : 0.f;

