@@ -13,6 +13,10 @@
 //    chaotic relaxation converges to the same fixed point as Block_FIM's schedule.
 //  * Slowness is read from one brick-major copy of the model shared by all shots; each
 //    shot's window is a brick-aligned sub-grid of it.
+//  * Optionally (time band), pushes carry the pushing brick's new time, and a brick far
+//    ahead of its shot's front waits on a parking list: rounds then follow traveltime
+//    rather than brick-graph distance, which removes the re-activation cascades of smooth
+//    v(z) models.
 #include "common.cuh"
 #include "fim.cuh"
 
