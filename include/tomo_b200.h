@@ -97,6 +97,12 @@ typedef struct {
                         any, else off; < 0: off.  Untuned banded solves default to 8
                         warps per CTA at occupancy 3 (80 registers).  Ignored by the warm-started solve and
                         the ASYNC schedule.                                           */
+    unsigned long long spin_limit; /* polls (>= 32 ns each) a device-side wait -- the round
+                        barrier of the persistent solve, the NGB sweep barriers, the
+                        ASYNC schedule's queue waits -- makes before it gives up: the
+                        solve then ends with TOMO_ERR_TIMEOUT and the context stays usable
+                        (0: default 2^26, i.e. seconds).  Replaces the unbounded wait of
+                        block_FIM_solver's outer loop (cuda_kernel.cu:91).              */
 } tomo_eik_opts;
 
 /* Work schedules of the JW solve (same fixed point, different order of brick updates).
@@ -238,7 +244,10 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
  * 4,194,304 nodes after padding each axis to a multiple of 4; larger grids return
  * TOMO_ERR_CAPACITY.  All calls on a device share that array: calls whose GPU work
  * overlaps race and must not be issued.  The first call on a device looks up the array's
- * address with that device current; make it before any stream capture.  Errors:
+ * address with that device current; make it before any stream capture.  Later calls
+ * look the address up again unless their stream is capturing, so a call after
+ * cudaDeviceReset finds the array where the reloaded module put it.  The call blocks
+ * until its work on `stream` is done (it reads the solver's error word back).  Errors:
  * tomo_last_error(NULL). */
 int tomo_eik_solve_static(const float *slowness, int nx, int ny, int nz, float dx, float dy, float dz, float sx,
                           float sy, float sz, float *t_out, void *stream);

@@ -2,7 +2,8 @@
 // B200 classes (seismic_tomography_3d_b200/host/) compile either against this header
 // (this repository's own executables) or against the reference's own headers
 // (src/eikonal/eikonal.hpp, src/tomography/tomography.hpp) when dropped into its tree
-// with -DTOMO_B200_REFERENCE_TREE.  The shapes follow:
+// with -DTOMO_B200_REFERENCE_TREE.  Like the reference's, the classes declare no virtual
+// destructors, so both builds give them the same virtual tables.  The shapes follow:
 //   Geometry   src/geometry/geometry.hpp:8-30
 //   Eikonal    src/eikonal/eikonal.hpp:15-58
 //   Tomography src/tomography/tomography.hpp:11-56
@@ -44,11 +45,10 @@ public:
     float *z;
 
     virtual void set_geometry(std::string parameters, std::string name) = 0;
-    virtual ~Geometry() {}
 };
 
 // Regular grid of points between the SW, NW and SE corners (regular/regular.cpp).
-class Regular : public Geometry {
+class Regular final : public Geometry {
 private:
     float sw[2] = {0, 0}, nw[2] = {0, 0}, se[2] = {0, 0};
     int lines_x = 0, lines_y = 0;
@@ -61,7 +61,7 @@ public:
 };
 
 // Rings of points around a centre (circular/circular.cpp).
-class Circular : public Geometry {
+class Circular final : public Geometry {
 private:
     float cx = 0, cy = 0, arc = 0;
     std::vector<float> radii;
@@ -114,7 +114,6 @@ public:
     virtual void write_first_arrival() = 0;
 
     virtual void destroy_volumes() = 0;
-    virtual ~Eikonal() {}
 };
 
 // ---- Tomography ------------------------------------------------------------------------
@@ -160,7 +159,6 @@ public:
     virtual void model_update() = 0;
 
     virtual void export_convergency() = 0;
-    virtual ~Tomography() {}
 };
 
 #endif

@@ -38,9 +38,20 @@ _ref_eik = None
 _ref_fim = None
 
 
+def reference_src():
+    """Checkout of the reference sources, or None: $TOMO_REFERENCE_SRC, else the checkout
+    this container keeps at /root/reference.  The GPU box has neither, and uses the
+    prebuilt oracle/_ref files."""
+    for cand in (os.environ.get("TOMO_REFERENCE_SRC"), "/root/reference"):
+        if cand and os.path.exists(os.path.join(cand, "src", "eikonal", "eikonal.hpp")):
+            return cand
+    return None
+
+
 def build() -> None:
     """Compile liboracle.so (and oracle/_ref when the reference sources are present)."""
-    subprocess.run(["make", "-s", "-C", HERE, "-j8"], check=True)
+    ref = reference_src()
+    subprocess.run(["make", "-s", "-C", HERE, "-j8"] + ([f"REF={ref}"] if ref else []), check=True)
 
 
 def _load():

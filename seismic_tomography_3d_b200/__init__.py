@@ -51,7 +51,7 @@ class EikOpts(ctypes.Structure):
                 ("brick", ctypes.c_int), ("block_warps", ctypes.c_int), ("occupancy", ctypes.c_int),
                 ("change_tol", ctypes.c_float), ("inner_tol", ctypes.c_float),
                 ("ieee_sqrt", ctypes.c_int), ("sweep_groups", ctypes.c_int), ("schedule", ctypes.c_int),
-                ("time_band", ctypes.c_float)]
+                ("time_band", ctypes.c_float), ("spin_limit", ctypes.c_ulonglong)]
 
 
 class EikStats(ctypes.Structure):
@@ -296,7 +296,7 @@ class Context:
     # -- eikonal ------------------------------------------------------------------------
     def eik_solve(self, shots, windows=None, receivers=None, want_recv=True, max_inner=0, max_rounds=0,
                   block_warps=0, op=0, occupancy=0, change_tol=0.0, inner_tol=0.0, ieee_sqrt=0,
-                  sweep_groups=0, schedule=0, time_band=0.0):
+                  sweep_groups=0, schedule=0, time_band=0.0, spin_limit=0):
         """Batched solve.  shots (n,3) metres; windows (n,4) [x0,x1,y0,y1] nodes or None;
         receivers (m,3).  Returns (t_recv (n,m) float32 or None, stats dict)."""
         sp, ns, _s = _points(shots)
@@ -309,7 +309,7 @@ class Context:
             rp, nr, _r = _points(receivers)
         out = np.empty((ns, nr), np.float32) if (want_recv and nr) else None
         opts = EikOpts(op, max_inner, max_rounds, 0, block_warps, occupancy, change_tol, inner_tol, ieee_sqrt,
-                       sweep_groups, schedule, time_band)
+                       sweep_groups, schedule, time_band, spin_limit)
         st = EikStats()
         self._check(self.lib.tomo_eik_solve(self.h, ns, sp, wp, nr, rp,
                                             out.ctypes.data if out is not None else None,

@@ -39,7 +39,7 @@ static_assert(kParkRounds >= 1 && kParkRounds + 2 <= 16, "parking lists");
 constexpr float kDefaultChangeTol = 1e-6f;
 constexpr int kDefaultMaxRounds = 1 << 20;
 constexpr int kMaxRounds = 1 << 22;
-constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~ seconds of polling, then error
+constexpr unsigned long long kSpinLimit = 1ull << 26;  // default: ~ seconds of polling, then error
 // Warm-start check: a node more than this (relative) below the update of its final
 // neighbours flags its shot.  The converged FP32 field itself holds such deficits up to
 // ~2.7e-7 (rounding of the update, which is monotone only up to a few ulp), so the bar is
@@ -91,7 +91,7 @@ int upload_model(tomo_ctx *ctx, const float *host, bool is_velocity)
 // TOMO_OP_NGB: the reference's Accurate_FSM sweeps for every shot (csrc/fsm.cu), written
 // into the brick-major pool described by sd, then the receivers.
 int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point *shots, int nshots, int nrec,
-               int groups)
+               int groups, unsigned long long spin_limit)
 {
     const tomo_grid &g = ctx->g;
     std::vector<tomo::FsmShot> fs((size_t)nshots);
@@ -157,7 +157,7 @@ int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point 
     p.ngroups = ngroups;
     p.bar = ctx->fsm_bar.ptr;
     p.err = ctx->ctrl.ptr + tomo::kErr;
-    p.spin_limit = kSpinLimit;
+    p.spin_limit = spin_limit;
     p.Tb = ctx->T.ptr;
     p.desc = ctx->shots_d.ptr;
     CK(cudaEventRecord(ctx->ev[3], ctx->stream));
@@ -344,6 +344,7 @@ struct SolveCfg {
     bool ieee_sqrt;
     bool async;  // asynchronous schedule, else rounds (default)
     float time_band;  // rounds schedule: time-band ordering (s), 0 = off
+    unsigned long long spin_limit;  // polls of a device-side wait before it gives up
 };
 
 SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
@@ -378,6 +379,7 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     const float band = opts ? opts->time_band : 0.f;
     c.time_band = band > 0.f ? band : (band < 0.f ? 0.f : ctx->tuned_time_band);
     if (c.async) c.time_band = 0.f;
+    c.spin_limit = (opts && opts->spin_limit > 0) ? opts->spin_limit : kSpinLimit;
     // Banded solves carry more live state (spills at 64 registers): untuned, they run as
     // 3 CTAs x 8 warps at 80 registers, 1.15x faster than the plain default shape on the
     // config-5 starting model (504 vs 581 ms) and equal on config 3.
@@ -501,7 +503,7 @@ tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, in
     p.inner_tol = c.inner_tol;
     p.max_rounds = c.max_rounds;
     p.local_bits = bt.local_bits;
-    p.spin_limit = kSpinLimit;
+    p.spin_limit = c.spin_limit;
     p.nrec = nrec;
     p.rx = nrec ? ctx->rec.ptr : nullptr;
     p.ry = nrec ? ctx->rec.ptr + nrec : nullptr;
@@ -655,7 +657,7 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
 
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     if (opts && opts->op == TOMO_OP_NGB) {
-        rc = launch_ngb(ctx, bt.sd, shots, nshots, nrec, opts->sweep_groups);
+        rc = launch_ngb(ctx, bt.sd, shots, nshots, nrec, opts->sweep_groups, cfg.spin_limit);
         if (rc != TOMO_OK) return rc;
     } else {
         CK(tomo::fim_init(ctx->T.ptr, (size_t)bt.t_total, ctx->qflag.ptr, (size_t)bt.q_total, ctx->ctrl.ptr,

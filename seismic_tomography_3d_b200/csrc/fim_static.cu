@@ -18,7 +18,10 @@
 //    call re-initialises everything it reads, but calls whose GPU work overlaps (on
 //    different streams or host threads) race on the array and corrupt each other;
 //  * the first call on a device looks up the array's device address (cudaGetSymbolAddress)
-//    once, with that device current; make that first call before any stream capture.
+//    with that device current; make that first call before any stream capture.  Later
+//    calls look it up again unless their stream is capturing (after cudaDeviceReset the
+//    module is loaded anew and the array may sit at another address);
+//  * the call blocks: it reads the solver's error word back and synchronises the stream.
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -56,14 +59,22 @@ int fail(int code, const std::string &msg)
     return code;
 }
 
-// Device address of the array on device `dev` (looked up once per device, with it current).
-int scratch_on(int dev, unsigned char **out)
+// Device address of the array on device `dev` (current).  Looked up on the first call on a
+// device and again on every call whose stream is not capturing, since a device reset loads
+// the module anew; a capturing call uses the address of the last lookup.
+int scratch_on(int dev, cudaStream_t st, unsigned char **out)
 {
     if (dev < 0 || dev >= kMaxDevices) return fail(TOMO_ERR_NO_DEVICE, "device index out of range");
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess)
+        return fail(TOMO_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
+    if (!g_addr[dev] || cap == cudaStreamCaptureStatusNone) {
+        if (cap != cudaStreamCaptureStatusNone)
+            return fail(TOMO_ERR_STATE, "first call on this device made during a stream capture");
         void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_eik_scratch);
+        e = cudaGetSymbolAddress(&p, g_eik_scratch);
         if (e != cudaSuccess)
             return fail(TOMO_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
         g_addr[dev] = static_cast<unsigned char *>(p);
@@ -95,21 +106,28 @@ extern "C" int tomo_eik_solve_static(const float *slowness, int nx, int ny, int 
     if (!slowness || !t_out) return fail(TOMO_ERR_INVALID_ARG, "slowness and t_out must be device pointers");
     if (nx < 2 || ny < 2 || nz < 2 || !(dx > 0) || !(dy > 0) || !(dz > 0))
         return fail(TOMO_ERR_INVALID_ARG, "grid must be at least 2x2x2 with positive spacing");
-    const size_t padded = (size_t)pad4(nx) * pad4(ny) * pad4(nz);
-    if (padded > kStaticNodes)
-        return fail(TOMO_ERR_CAPACITY, "grid of " + std::to_string(padded) + " padded nodes exceeds the " +
+    // Each axis is checked before any product is formed, so that none can wrap: a padded
+    // axis is then at most 2^22 + 3, the product of two below 2^45, and the triple product
+    // is only formed once the first two are known to be at most 2^22.
+    const int lim = (int)kStaticNodes;
+    const bool axis_ok = nx <= lim && ny <= lim && nz <= lim;
+    const size_t padx = axis_ok ? (size_t)pad4(nx) : 0, pady = axis_ok ? (size_t)pad4(ny) : 0,
+                 padz = axis_ok ? (size_t)pad4(nz) : 0;
+    if (!axis_ok || padx * pady > kStaticNodes || padx * pady * padz > kStaticNodes)
+        return fail(TOMO_ERR_CAPACITY, "grid of " + std::to_string(nx) + " x " + std::to_string(ny) + " x " +
+                                           std::to_string(nz) + " nodes exceeds the " +
                                            std::to_string(kStaticNodes) +
-                                           " nodes of the allocation-free solver; use tomo_eik_solve");
+                                           " padded nodes of the allocation-free solver; use tomo_eik_solve");
     // source seed as in Block_FIM::apply_source_time (block_FIM.cpp:305-317)
     const int sidx = (int)(sx / dx), sidy = (int)(sy / dy), sidz = (int)(sz / dz);
     if (!(sx >= 0.f) || !(sy >= 0.f) || !(sz >= 0.f) || sidx >= nx || sidy >= ny || sidz >= nz)
         return fail(TOMO_ERR_INVALID_ARG, "source outside the model");
     int dev = 0;
     CKS(cudaGetDevice(&dev));
-    unsigned char *base = nullptr;
-    int rc = scratch_on(dev, &base);
-    if (rc != TOMO_OK) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned char *base = nullptr;
+    int rc = scratch_on(dev, st, &base);
+    if (rc != TOMO_OK) return rc;
 
     ShotDesc d{};
     d.wx0 = d.wy0 = 0;

@@ -58,10 +58,13 @@ __device__ __constant__ int kSgn[8][3] = {{1, 1, 1},  {-1, 1, 1},  {1, 1, -1},  
 __device__ __forceinline__ float smin(float a, float b) { return (b < a) ? b : a; }  // std::min
 __device__ __forceinline__ float smax(float a, float b) { return (a < b) ? b : a; }  // std::max
 
-// Group barrier over the blocks of one group (bounded spin; false on any error).
+// Group barrier over the blocks of one group (bounded spin; false on any error).  Every
+// thread of a block gets thread 0's reading of the error word, so a block never splits over
+// an error raised by another block while it passes the barrier.
 __device__ __forceinline__ bool group_barrier(unsigned *bar, unsigned nblocks, unsigned *err,
                                               unsigned long long spin_limit)
 {
+    __shared__ unsigned err_seen;
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned gen = ld_volatile(bar + 1);
@@ -82,9 +85,10 @@ __device__ __forceinline__ bool group_barrier(unsigned *bar, unsigned nblocks, u
             }
         }
         __threadfence();
+        err_seen = ld_volatile(err);
     }
     __syncthreads();
-    return ld_volatile(err) == 0u;
+    return err_seen == 0u;
 }
 
 struct ShotGrid {

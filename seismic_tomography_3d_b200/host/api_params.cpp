@@ -22,8 +22,10 @@ int tomo_geometry(const char *parameter_file, const char *name, int type, float 
 {
     if (!parameter_file || !name || (type != 0 && type != 1) || cap < 0) return TOMO_ERR_INVALID_ARG;
     try {
-        std::unique_ptr<Geometry> g(type == 0 ? static_cast<Geometry *>(new Regular())
-                                              : static_cast<Geometry *>(new Circular()));
+        // held as the concrete type (the reference's Geometry has no virtual destructor)
+        std::unique_ptr<Regular> reg(type == 0 ? new Regular() : nullptr);
+        std::unique_ptr<Circular> circ(type == 1 ? new Circular() : nullptr);
+        Geometry *g = reg ? static_cast<Geometry *>(reg.get()) : static_cast<Geometry *>(circ.get());
         g->set_geometry(parameter_file, name);
         const int n = g->all;
         for (int i = 0; i < n && i < cap && xyz; i++) {

@@ -34,8 +34,8 @@ void Eikonal_B200::set_parameters()
     read_binary_float(catch_parameter("vp_file", parameters), slowness, nPoints);
     for (int i = 0; i < nPoints; i++) slowness[i] = 1.0f / slowness[i];
 
-    const int shots_type = std::stoi(catch_parameter("shots_geometry_type", parameters));
-    const int nodes_type = std::stoi(catch_parameter("nodes_geometry_type", parameters));
+    shots_type = std::stoi(catch_parameter("shots_geometry_type", parameters));
+    nodes_type = std::stoi(catch_parameter("nodes_geometry_type", parameters));
     auto make = [](int t) -> Geometry * {
         if (t == 0) return new Regular();
         if (t == 1) return new Circular();
@@ -166,6 +166,13 @@ Eikonal_B200::~Eikonal_B200()
             delete[] g->y;
             delete[] g->z;
         }
-    delete shots;
-    delete nodes;
+    // as the concrete type: deleting through Geometry * would skip Circular's members
+    auto destroy = [](Geometry *g, int type) {
+        if (type == 1)
+            delete static_cast<Circular *>(g);
+        else
+            delete static_cast<Regular *>(g);
+    };
+    destroy(shots, shots_type);  // reciprocity swaps the coordinate arrays, not the objects
+    destroy(nodes, nodes_type);
 }

@@ -23,12 +23,14 @@
 #include "async_writer.hpp"
 #include "tomo_b200.h"
 
-class Eikonal_B200 : public Eikonal {
+class Eikonal_B200 final : public Eikonal {
 protected:
     tomo_ctx *ctx = nullptr;
     bool batch_ready = false;
     float time_band = 0.f;  // optional key eikonal_time_band (s): time-band ordering, 0 = off
     bool geometry_ready = false;
+    int shots_type = 0, nodes_type = 0;  // 0 Regular, 1 Circular: deleted as that type (the
+                                         // reference's Geometry has no virtual destructor)
     std::vector<float> recv_times;  // total_shots x total_nodes, trilinear receiver times
 
     void expand_model() {}  // padding to whole bricks happens on the device

@@ -161,6 +161,27 @@ def test_errors_are_status_codes(tomo):
         ctx.eik_solve([[50.0, 50.0, 0.0]], schedule=2)
 
 
+def test_barrier_wait_limit_returns_timeout(tomo, oracle_mod):
+    """tomo_eik_opts.spin_limit bounds the round barrier's wait.  With a limit of one poll
+    the blocks waiting at the first barrier (for the one warp relaxing the source brick)
+    give up: every block leaves the launch, the call returns TOMO_ERR_TIMEOUT, and the
+    context solves the batch correctly afterwards.  A bounded wait on the device, no fault:
+    the reference waits without bound (cuda_kernel.cu:91)."""
+    sv = wl.small(44, 24, 20, 12, nshots=2)
+    with tomo.Context(sv.nx, sv.ny, sv.nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        with pytest.raises(tomo.TomoError) as e:
+            ctx.eik_solve(sv.shots, spin_limit=1)
+        assert e.value.status == -5  # TOMO_ERR_TIMEOUT
+        with pytest.raises(tomo.TomoError) as e:  # no solve to read after the timeout
+            ctx.eik_volume(0)
+        assert e.value.status == -6
+        ctx.eik_solve(sv.shots)
+        for i, sh in enumerate(sv.shots):
+            Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, sh)
+            assert rel_err(ctx.eik_volume(i), Tref, sv.h, sv.velocity.max()) < REL_TOL
+
+
 @pytest.mark.slow
 def test_config1_full_size(tomo, oracle_mod):
     sv = wl.config1()

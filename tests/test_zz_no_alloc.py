@@ -71,3 +71,8 @@ def test_static_solve_rejects_oversized_grid(tomo):
     rc = solve_static(dummy.data_ptr(), 164, 164, 164, 10.0, 10.0, 10.0, 5.0, 5.0, 0.0, dummy.data_ptr(), None)
     assert rc == -9  # TOMO_ERR_CAPACITY
     assert b"exceeds" in lib.tomo_last_error(None)
+    # sizes whose padded product wraps around 2^64 (4194304^2 x 1048576 = 2^64), and one
+    # axis beyond the limit on its own: rejected before any product is formed
+    for dims in ((4194304, 4194304, 1048576), (1 << 30, 2, 2), (2, 2, 2147483647)):
+        rc = solve_static(dummy.data_ptr(), *dims, 10.0, 10.0, 10.0, 5.0, 5.0, 0.0, dummy.data_ptr(), None)
+        assert rc == -9, dims
