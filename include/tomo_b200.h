@@ -181,7 +181,8 @@ int tomo_eik_window(tomo_ctx *ctx, int shot, tomo_window *out);
 int tomo_eik_volumes(tomo_ctx *ctx, float *dst);
 
 typedef struct {
-    long long violations;              /* nodes below the update of their final neighbours   */
+    long long violations;              /* nodes below the update of their final neighbours
+                                          by more than 5e-7 (relative)                       */
     float max_deficit;                 /* largest (update - time) / update over those nodes   */
     int shots_fallback;                /* shots solved again from INF (plain FIM)            */
     long long rounds_seeded;           /* outer rounds of the warm-started launch            */
@@ -190,6 +191,7 @@ typedef struct {
     float seeded_ms;                   /* device time of the warm-started launch             */
     float verify_ms;                   /* device time of the check                           */
     float fallback_ms;                 /* device time of the fallback solves (0 if none)     */
+    long long stuck;                   /* nodes that kept their ceiling value (never lowered) */
 } tomo_seed_stats;
 
 /* Warm-started batch solve: tomo_eik_solve (JW operator), but every window node starts at
@@ -200,10 +202,15 @@ typedef struct {
  *            ceiling at that node.
  *   inflate  in [0, 1): margin that makes the prediction an upper bound
  * A ceiling below the true time would stay in the result, so every shot is checked after
- * the solve: a node (source node excepted) whose time is below the local update of its
- * final neighbours can only hold a ceiling value; such shots are solved again from INF
- * within the call (the plain solver is the fallback).  stats counts both launches;
- * seed_stats (may be NULL) splits them. */
+ * the solve.  A shot is solved again from INF within the call (the plain solver is the
+ * fallback) when any node (source node excepted) still holds its ceiling value, bit for
+ * bit -- the solve never lowered it -- or lies below the local update of its final
+ * neighbours.  Every node of a correct result is an update of its neighbours, and a
+ * ceiling below the truth always leaves nodes that kept it (the wrong node of smallest
+ * time has correct upwind neighbours), so the check catches smooth deficits of any size.
+ * A ceiling is therefore accepted only where the solve lowered every node: use inflate
+ * well above the solver's tolerances (0.02; an exact field with inflate 0 falls back).
+ * stats counts both launches; seed_stats (may be NULL) splits them. */
 int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows,
                           int nrec, const tomo_point *receivers, float *t_recv, const float *ceiling,
                           float inflate, const tomo_eik_opts *opts, tomo_eik_stats *stats,

@@ -73,7 +73,7 @@ class SeedStats(ctypes.Structure):
     _fields_ = [("violations", ctypes.c_longlong), ("max_deficit", ctypes.c_float), ("shots_fallback", ctypes.c_int),
                 ("rounds_seeded", ctypes.c_longlong), ("activations_seeded", ctypes.c_longlong),
                 ("inner_iterations_seeded", ctypes.c_longlong), ("seeded_ms", ctypes.c_float),
-                ("verify_ms", ctypes.c_float), ("fallback_ms", ctypes.c_float)]
+                ("verify_ms", ctypes.c_float), ("fallback_ms", ctypes.c_float), ("stuck", ctypes.c_longlong)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -40,12 +40,12 @@ constexpr float kDefaultChangeTol = 1e-6f;
 constexpr int kDefaultMaxRounds = 1 << 20;
 constexpr int kMaxRounds = 1 << 22;
 constexpr unsigned long long kSpinLimit = 1ull << 26;  // default: ~ seconds of polling, then error
-// Warm-start check: a node more than this (relative) below the update of its final
-// neighbours flags its shot.  The converged FP32 field itself holds such deficits up to
-// ~2.7e-7 (rounding of the update, which is monotone only up to a few ulp), so the bar is
-// 5e-7.  A ceiling stuck below the truth by more than that where it meets correct upwind
-// nodes is always caught; a deficit spread thinly along a path of n nodes can hide at most
-// n x 5e-7 relative (1e-4 at 200 nodes from the source).
+// Warm-start check, first test: a node more than this (relative) below the update of its
+// final neighbours flags its shot.  The converged FP32 field itself holds such deficits up
+// to ~2.7e-7 (rounding of the update, which is monotone only up to a few ulp), so the bar is
+// 5e-7.  A deficit spread thinly along a path of n nodes could hide n x 5e-7 from this
+// test; the second test (a node that kept its ceiling value, fim_verify) catches any
+// ceiling below the truth, smooth or not.
 constexpr float kVerifyRelTol = 5e-7f;
 
 int fail(tomo_ctx *c, int code, const std::string &msg)
@@ -716,7 +716,7 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
     ctx->have_solve = false;  // the pool is about to be overwritten
     rc = upload_batch(ctx, bt, nrec, receivers);
     if (rc != TOMO_OK) return rc;
-    CK(ctx->viol.ensure((size_t)nshots * 2));
+    CK(ctx->viol.ensure((size_t)nshots * 3));
     cudaEvent_t *ev = ctx->ev;
 
     // 1. pool from the ceiling, source seed, persistent solve (receivers after the check)
@@ -732,11 +732,12 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
     CK(tomo::fim_solve(p, cfg.block_warps, cfg.occupancy, cfg.ieee_sqrt, &grid, ctx->stream, cfg.async));
     CK(cudaEventRecord(ev[4], ctx->stream));
     // 2. check: a node below what its neighbours give came from a ceiling below the truth
-    CK(cudaMemsetAsync(ctx->viol.ptr, 0, (size_t)nshots * 2 * sizeof(unsigned long long), ctx->stream));
+    CK(cudaMemsetAsync(ctx->viol.ptr, 0, (size_t)nshots * 3 * sizeof(unsigned long long), ctx->stream));
     CK(tomo::fim_verify(ctx->T.ptr, ctx->S.ptr, ctx->shots_d.ptr, nshots, ctx->gbx, ctx->gbz, ctx->g.dx,
-                        kVerifyRelTol, cfg.ieee_sqrt, ctx->viol.ptr, ctx->stream));
+                        kVerifyRelTol, ceiling, 1.0f + inflate, ctx->g.nz, cfg.ieee_sqrt, ctx->viol.ptr,
+                        ctx->stream));
     CK(cudaEventRecord(ev[5], ctx->stream));
-    std::vector<unsigned long long> viol((size_t)nshots * 2);
+    std::vector<unsigned long long> viol((size_t)nshots * 3);
     CK(cudaMemcpyAsync(viol.data(), ctx->viol.ptr, viol.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                        ctx->stream));
     unsigned rounds = 0, rounds2 = 0;
@@ -746,15 +747,17 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
 
     // 3. fallback: shots with violations are solved again from INF (plain FIM)
     std::vector<ShotDesc> redo;
-    long long nviol = 0;
+    long long nviol = 0, nstuck = 0;
     float worst = 0.f;
     for (int s = 0; s < nshots; s++) {
-        nviol += (long long)viol[(size_t)s];
+        const unsigned long long deficit = viol[(size_t)s], stuck = viol[(size_t)2 * nshots + s];
+        nviol += (long long)deficit;
+        nstuck += (long long)stuck;
         float w;
         const unsigned bits = (unsigned)viol[(size_t)nshots + s];
         std::memcpy(&w, &bits, sizeof(w));
         worst = std::max(worst, w);
-        if (viol[(size_t)s]) redo.push_back(bt.sd[(size_t)s]);
+        if (deficit || stuck) redo.push_back(bt.sd[(size_t)s]);
     }
     const int nredo = (int)redo.size();
     CK(cudaEventRecord(ev[6], ctx->stream));
@@ -799,6 +802,7 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
     }
     if (seed_stats) {
         seed_stats->violations = nviol;
+        seed_stats->stuck = nstuck;
         seed_stats->max_deficit = worst;
         seed_stats->shots_fallback = nredo;
         seed_stats->rounds_seeded = rounds;

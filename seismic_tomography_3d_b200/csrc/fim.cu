@@ -906,22 +906,38 @@ __global__ void k_fim_ceiling(float *T, const ShotDesc *shots, int nz, const flo
     }
 }
 
+// Two tests per node (source node excepted):
+//  * stuck: the node still holds its ceiling value, bit for bit (k_fim_ceiling's product), so
+//    the solver never lowered it.  After a converged seeded solve every other node holds a
+//    Godunov update of its final neighbours, so if no node is stuck the field solves the
+//    discrete equation everywhere but at the source, i.e. it is the plain solution.  A
+//    ceiling below the truth always leaves stuck nodes: the wrong node of smallest time
+//    has correct upwind neighbours, so it cannot be an update and must hold its ceiling.
+//    This holds for smooth deficits of any size, which a per-node test cannot see.
+//  * deficit: t is below the update of its final neighbours by more than rel_tol.
 template <bool kFastSqrt>
 __global__ void k_fim_verify(const float *T, const float *S, const ShotDesc *shots, int gbx, int gbz, float h,
-                             float rel_tol, unsigned long long *viol)
+                             float rel_tol, const float *ceiling, float scale, int nz, unsigned long long *viol)
 {
     const int s = blockIdx.y;
     const ShotDesc d = shots[s];
     const int ex = d.nbx * kBrick, ey = d.nby * kBrick, ez = d.nbz * kBrick;
     const long long n = (long long)d.nbx * d.nby * d.nbz * kBrickNodes;
     const long long src = (long long)d.src_brick * kBrickNodes + d.src_node;
-    unsigned cnt = 0;
+    unsigned cnt = 0, stuck = 0;
     float worst = 0.0f;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         if (i == src) continue;
         int z, x, y;
         pool_node(d, i, z, x, y);
         const float t = __ldcg(T + d.t_off + i);
+        if (z < nz && x < d.wnx && y < d.wny) {
+            const float c = __ldg(ceiling + d.v_off + z + (long long)nz * (x + (long long)d.wnx * y));
+            if (c > 0.0f && c < kInf) {
+                const float u = c * scale;  // as k_fim_ceiling stored it
+                if (u < kInf && __float_as_uint(t) == __float_as_uint(u)) stuck++;
+            }
+        }
         // neighbours as the solver sees them: nodes of the window's brick grid, INF beyond
         const float xm = x > 0 ? brick_T(T, d, x - 1, y, z) : kInf, xp = x < ex - 1 ? brick_T(T, d, x + 1, y, z) : kInf;
         const float ym = y > 0 ? brick_T(T, d, x, y - 1, z) : kInf, yp = y < ey - 1 ? brick_T(T, d, x, y + 1, z) : kInf;
@@ -941,15 +957,23 @@ __global__ void k_fim_verify(const float *T, const float *S, const ShotDesc *sho
     worst = fmaxf(worst, __shfl_xor_sync(kFull, worst, 1));
     if ((threadIdx.x & 31) == 0 && worst > 0.0f)  // non-negative floats order as their bits
         atomicMax(viol + gridDim.y + s, (unsigned long long)__float_as_uint(worst));
-    // block reduction, one atomic per block
+    // block reductions, one atomic per block and count
     cnt = __reduce_add_sync(kFull, cnt);
-    __shared__ unsigned part[32];
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = cnt;
+    stuck = __reduce_add_sync(kFull, stuck);
+    __shared__ unsigned part[32], part_stuck[32];
+    if ((threadIdx.x & 31) == 0) {
+        part[threadIdx.x >> 5] = cnt;
+        part_stuck[threadIdx.x >> 5] = stuck;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned tot = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += part[w];
+        unsigned tot = 0, tot_stuck = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            tot += part[w];
+            tot_stuck += part_stuck[w];
+        }
         if (tot) atomicAdd(viol + s, (unsigned long long)tot);
+        if (tot_stuck) atomicAdd(viol + 2 * gridDim.y + s, (unsigned long long)tot_stuck);
     }
 }
 
@@ -1099,13 +1123,16 @@ cudaError_t fim_ceiling(float *T, const ShotDesc *shots, int nshots, int nz, con
 }
 
 cudaError_t fim_verify(const float *T, const float *S, const ShotDesc *shots, int nshots, int gbx, int gbz, float h,
-                       float rel_tol, bool ieee_sqrt, unsigned long long *viol, cudaStream_t st)
+                       float rel_tol, const float *ceiling, float scale, int nz, bool ieee_sqrt,
+                       unsigned long long *viol, cudaStream_t st)
 {
     if (nshots < 1 || nshots > 65535) return cudaErrorInvalidValue;
     if (ieee_sqrt)
-        k_fim_verify<false><<<per_shot_grid(nshots), 256, 0, st>>>(T, S, shots, gbx, gbz, h, rel_tol, viol);
+        k_fim_verify<false><<<per_shot_grid(nshots), 256, 0, st>>>(T, S, shots, gbx, gbz, h, rel_tol, ceiling, scale,
+                                                                   nz, viol);
     else
-        k_fim_verify<true><<<per_shot_grid(nshots), 256, 0, st>>>(T, S, shots, gbx, gbz, h, rel_tol, viol);
+        k_fim_verify<true><<<per_shot_grid(nshots), 256, 0, st>>>(T, S, shots, gbx, gbz, h, rel_tol, ceiling, scale,
+                                                                  nz, viol);
     return cudaGetLastError();
 }
 

@@ -108,12 +108,15 @@ cudaError_t max_positive(const float *v, size_t n, unsigned *out_bits, cudaStrea
 // padding nodes stay INF.
 cudaError_t fim_ceiling(float *T, const ShotDesc *shots, int nshots, int nz, const float *ceiling, float scale,
                         cudaStream_t st);
-// Per shot, the number of nodes (source node excepted) whose traveltime is below the
-// local update of its final neighbours by more than rel_tol (relative): values that no
-// neighbour explains, i.e. a ceiling below the true time.  viol[s] accumulates the count
-// of shot s, viol[nshots + s] the largest relative deficit (float bits, atomicMax).
+// Per shot (source node excepted): viol[s] counts the nodes whose traveltime is below the
+// local update of its final neighbours by more than rel_tol (relative), viol[nshots + s]
+// holds the largest such relative deficit (float bits, atomicMax), and viol[2 nshots + s]
+// counts the nodes that still hold their ceiling value (ceiling x scale, as fim_ceiling
+// stored it): nodes the solve never lowered.  Either count flags a ceiling below the
+// true time; the second catches smooth deficits of any size.
 cudaError_t fim_verify(const float *T, const float *S, const ShotDesc *shots, int nshots, int gbx, int gbz, float h,
-                       float rel_tol, bool ieee_sqrt, unsigned long long *viol, cudaStream_t st);
+                       float rel_tol, const float *ceiling, float scale, int nz, bool ieee_sqrt,
+                       unsigned long long *viol, cudaStream_t st);
 // Resets the pool regions (T = INF, queue flags 0) of the listed shots only.
 cudaError_t fim_reset_shots(float *T, unsigned *qflag, const ShotDesc *shots, int nshots, cudaStream_t st);
 // All shots' window volumes, back to back at ShotDesc::v_off (z fastest, then x, then y).

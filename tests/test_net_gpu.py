@@ -2,7 +2,9 @@
 
   * forward output and the gradients of every parameter (BF16 tensor-core convolutions,
     FP32 accumulation) against the FP64 oracle (oracle/unet.py, itself pinned to torch
-    autograd): loss within 3 %, each parameter tensor's gradient at cosine >= 0.98;
+    autograd), on a small odd-sized window and on the 64^3 training tile: loss within 1 %,
+    each parameter tensor's gradient within 3e-2 relative L2 error (BF16 activations carry
+    ~4e-3 relative rounding through 14 layers and back);
   * training on solver-generated fields lowers the loss;
   * the trained network's prediction, used as the ceiling of tomo_eik_solve_seeded, leaves
     the solution unchanged (the plain solve judges it) -- and the test reports what it saves.
@@ -23,7 +25,7 @@ def _dev(a):
 
 
 def _case(tomo, seed=4, nx=20, ny=24, nz=14, h=20.0):
-    """A small layered model, one source, its plain-FIM traveltimes."""
+    """A layered model, one source, its plain-FIM traveltimes."""
     sv = wl.small(seed, nx, ny, nz, h=h, nshots=1)
     with tomo.Context(nx, ny, nz, h) as ctx:
         ctx.set_velocity(sv.velocity)
@@ -33,13 +35,18 @@ def _case(tomo, seed=4, nx=20, ny=24, nz=14, h=20.0):
     return sv, slow, T
 
 
-def _cos(a, b):
-    return float(np.dot(a, b) / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-300))
+def _rel_l2(a, b):
+    return float(np.linalg.norm(a.astype(np.float64) - b) / (np.linalg.norm(b) + 1e-300))
 
 
-def test_gradients_match_oracle(tomo):
-    sv, slow, T = _case(tomo)
-    h = sv.h
+GRAD_REL = 3e-2
+LOSS_REL = 1e-2
+
+
+@pytest.mark.parametrize("shape", [(20, 24, 14, 20.0), (64, 64, 64, 12.5)], ids=["20x24x14", "64^3"])
+def test_gradients_match_oracle(tomo, shape):
+    nx, ny, nz, h = shape
+    sv, slow, T = _case(tomo, nx=nx, ny=ny, nz=nz, h=h)
     net = tomo.Net(seed=11)
     p = unet.init_params(11)
     convs, head, _ = unet.layout()
@@ -57,14 +64,19 @@ def test_gradients_match_oracle(tomo):
     f, dist, s_src, inside = unet.features(slow, win, sv.nz, sv.shots[0], h, pad)
     tgt = unet.target(T, dist, s_src, inside, h)
     loss_o, tau_o, g_o = unet.forward_backward(p, f[None], tgt[None])
-    assert abs(loss - loss_o) <= 0.03 * loss_o, (loss, loss_o)
+    errs = {}
     for i, (w, b, ci, co) in enumerate(convs):
         gw, gw_o = g[w:w + 27 * ci * co], g_o[w:w + 27 * ci * co]
         if i == 0:  # input channels 2..15 are zero: only the first two carry gradient
             gw, gw_o = gw.reshape(co, 27, ci)[..., :2].ravel(), gw_o.reshape(co, 27, ci)[..., :2].ravel()
-        assert _cos(gw, gw_o) >= 0.98, (i, _cos(gw, gw_o))
-        assert _cos(g[b:b + co], g_o[b:b + co]) >= 0.98, (i, "bias")
-    assert _cos(g[head:head + 17], g_o[head:head + 17]) >= 0.98
+        errs[f"w{i}"] = _rel_l2(gw, gw_o)
+        errs[f"b{i}"] = _rel_l2(g[b:b + co], g_o[b:b + co])
+    errs["head"] = _rel_l2(g[head:head + 17], g_o[head:head + 17])
+    worst = max(errs, key=errs.get)
+    print(f"\n{shape}: loss {loss:.6f} vs oracle {loss_o:.6f} ({abs(loss - loss_o) / loss_o:.2e}); "
+          f"worst gradient rel L2 {errs[worst]:.3e} ({worst}); median {np.median(list(errs.values())):.3e}")
+    assert abs(loss - loss_o) <= LOSS_REL * loss_o, (loss, loss_o)
+    assert errs[worst] <= GRAD_REL, errs
     # prediction = oracle tau * s_src * distance on the window
     import torch
 

@@ -3,7 +3,8 @@
 The ceiling only prunes work: with any ceiling the result must equal the plain solve.
   * a true upper bound (the plain solution inflated) gives the plain result, no fallback;
   * a ceiling below the true times is detected by the check and the shot is solved again
-    from INF, again giving the plain result;
+    from INF, again giving the plain result -- also when the deficit is smooth and grows
+    slowly over a config-2-sized window, which no per-node deficit test can see;
   * entries <= 0 / non-finite mean "no ceiling".
 Tolerance: 1e-5 relative on nodes with T >= 2h/v_max against the plain FIM (both runs
 converge to the same FP32 fixed point; the 1e-4 budget is kept with margin).
@@ -75,7 +76,7 @@ def test_ceiling_below_truth_falls_back(case):
     low[off:off + sizes[1]] *= 0.95
     torch.cuda.synchronize()
     t, st, ss = ctx.eik_solve_seeded(sv.shots, low.data_ptr(), 0.0, windows=sv.windows, receivers=sv.receivers)
-    assert ss["violations"] > 0
+    assert ss["violations"] > 0 and ss["stuck"] > 0
     assert ss["shots_fallback"] == 1
     check_equal(ctx, sv, plain)
     fin = np.isfinite(t_plain) & (t_plain < 1e5)
@@ -100,3 +101,73 @@ def test_bad_arguments(case, tomo):
         ctx.eik_solve_seeded(sv.shots, 0, 0.02, windows=sv.windows)
     with pytest.raises(tomo.TomoError):
         ctx.eik_solve_seeded(sv.shots, dev.data_ptr(), -0.5, windows=sv.windows)
+
+
+@pytest.fixture(scope="module")
+def big_case(tomo):
+    """Two full-window shots on the config-2 model (201 x 201 x 101 at 12.5 m): one at a
+    corner (paths of ~300 nodes), one inside.  Plain fields at library defaults."""
+    import torch
+
+    sv = wl.config2()
+    shots = np.array([[0.0, 0.0, 0.0], [1250.0, 1000.0, 0.0]], np.float32)
+    ctx = tomo.Context(sv.nx, sv.ny, sv.nz, sv.h)
+    ctx.set_velocity(sv.velocity)
+    ctx.eik_solve(shots, want_recv=False)
+    plain = [ctx.eik_volume(i) for i in range(len(shots))]
+    sizes = ctx.volume_sizes(len(shots), None)
+    exact = torch.empty(sum(sizes), dtype=torch.float32, device="cuda")
+    ctx.eik_volumes_to(exact.data_ptr())
+    # distance of every node from its shot, relative to the farthest node
+    y, x, z = torch.meshgrid(*(torch.arange(n, device="cuda", dtype=torch.float32) * sv.h
+                               for n in (sv.ny, sv.nx, sv.nz)), indexing="ij")
+    ramp = []
+    for sx, sy, sz in shots:
+        r = torch.sqrt((x - float(sx)) ** 2 + (y - float(sy)) ** 2 + (z - float(sz)) ** 2)
+        ramp.append((r / r.max()).reshape(-1))
+    ramp = torch.cat(ramp)
+    torch.cuda.synchronize()
+    yield sv, shots, ctx, plain, exact, ramp
+    ctx.close()
+
+
+def _seeded_equals_plain(ctx, sv, shots, plain, ceiling):
+    import torch
+
+    torch.cuda.synchronize()
+    _, _, ss = ctx.eik_solve_seeded(shots, ceiling.data_ptr(), 0.0, want_recv=False)
+    for i in range(len(shots)):
+        assert rel_err(ctx.eik_volume(i), plain[i], sv.h, float(sv.velocity.max())) < TOL
+    return ss
+
+
+@pytest.mark.parametrize("deficit", [2e-4, 1e-5])
+def test_smooth_deficit_over_config2_window_is_caught(big_case, deficit):
+    """A ceiling equal to the exact field x (1 - deficit x r / r_max): below the truth by a
+    relative amount that grows smoothly from 0 at the source to `deficit` at the far corner,
+    i.e. only ~deficit / 300 between neighbouring nodes along a path -- under the 5e-7
+    per-node deficit bar.  Every such node kept its ceiling, so the shots fall back and the
+    result is the plain field (tomo_eik_solve_seeded, the judge the INF seed of
+    block_FIM.cpp:295-369 is replaced under)."""
+    sv, shots, ctx, plain, exact, ramp = big_case
+    ss = _seeded_equals_plain(ctx, sv, shots, plain, exact * (1.0 - deficit * ramp))
+    assert ss["stuck"] > 0
+    assert ss["shots_fallback"] == len(shots)
+
+
+def test_ceiling_low_far_from_source_is_caught(big_case):
+    """An upper bound near the source that sinks below the truth beyond 40 % of the
+    distance (2 % above at the source, 3 % below at the far corner)."""
+    sv, shots, ctx, plain, exact, ramp = big_case
+    ss = _seeded_equals_plain(ctx, sv, shots, plain, exact * (1.02 - 0.05 * ramp))
+    assert ss["stuck"] > 0
+    assert ss["shots_fallback"] == len(shots)
+
+
+def test_smooth_upper_bound_is_accepted(big_case):
+    """The same smooth ramp on a ceiling that stays above the truth (x 1.02 first): every node
+    is lowered by the solve, no shot falls back, the result is the plain field."""
+    sv, shots, ctx, plain, exact, ramp = big_case
+    ss = _seeded_equals_plain(ctx, sv, shots, plain, exact * 1.02 * (1.0 - 2e-4 * ramp))
+    assert ss["stuck"] == 0 and ss["violations"] == 0
+    assert ss["shots_fallback"] == 0
