@@ -12,6 +12,16 @@ launch; 2,500 surface receivers (50x50) sampled per shot.  Synthetic seeded data
          nodes x 12 B (slowness + traveltime in + traveltime out) / its event time
   cpu_baseline  the reference's own Accurate_FSM (compiled unmodified into oracle/_ref)
          on a bounded sample of the same shots and windows, all host threads
+  accuracy  the timed setting's fields of 8 shots against the FP64 oracle (CPU leg)
+
+On one GPU the line also carries the other configurations, each bounded to seconds:
+  config1       the single 101x101x51 shot on the device (JW, NGB) and the reference's own
+                FSM and Podvin-Lecomte on 1 core and on all cores
+  tomography    config 3: one whole iteration (stage split, CGLS roofline) and the
+                reference's own tomography.exe on a 4-shot sample
+  learned_warm  config 4: the surrogate trained in-run, its prediction seeding the solve of
+                the config-2 batch, against the plain solve
+  inversion     config 5: 3 graph-replayed iterations of the 401x401x201 inversion
 
 ``--impl reference`` times the reference's CPU eikonal path (Accurate_FSM) the same way.
 Multi-GPU (torchrun): shots are independent, each rank solves its own 64-shot batch (weak
@@ -206,6 +216,218 @@ def cpu_reference_sample(sv, max_shots=None, budget_s=20.0):
     return done / wall, nthreads, desc
 
 
+def sample_shots(sv, k=8):
+    """k shots of the batch: the smallest and the largest window and k - 2 in between."""
+    areas = np.array([(w[1] - w[0]) * (w[3] - w[2]) for w in sv.windows])
+    order = np.argsort(areas, kind="stable")
+    return sorted(set(int(order[i]) for i in np.linspace(0, len(order) - 1, k).round().astype(int)))
+
+
+def oracle_accuracy(sv, idx, vols):
+    """Max relative error of the timed setting's fields (vols, shots idx) against the FP64
+    fixed point of the same operator on each cropped window (the oracle), on nodes with
+    T >= 2h/v_max; host threads."""
+    import concurrent.futures as cf
+
+    import oracle
+
+    vmax = float(sv.velocity.max())
+
+    def one(k):
+        i = idx[k]
+        x0, x1, y0, y1 = (int(a) for a in sv.windows[i])
+        slow = np.ascontiguousarray((np.float32(1.0) / sv.velocity[y0:y1, x0:x1, :]).astype(np.float32))
+        src = (float(np.float32(sv.shots[i][0]) - np.float32(x0) * np.float32(sv.h)),
+               float(np.float32(sv.shots[i][1]) - np.float32(y0) * np.float32(sv.h)), float(sv.shots[i][2]))
+        Tref, _ = oracle.fim_jw(slow, sv.h, src)
+        m = Tref >= 2.0 * sv.h / vmax
+        return float(np.max(np.abs(vols[k][m] - Tref[m]) / Tref[m])), int(m.sum())
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(min(len(idx), os.cpu_count() or 1)) as ex:
+        res = list(ex.map(one, range(len(idx))))
+    return {"max_rel_err_vs_fp64_oracle": max(r[0] for r in res), "per_shot": [r[0] for r in res],
+            "shots_checked": [int(i) for i in idx], "nodes_checked": sum(r[1] for r in res), "budget": 1e-4,
+            "oracle": "FP64 fixed point of the Block_FIM operator on each shot's cropped window (oracle/tomo_oracle.c)",
+            "oracle_s": time.perf_counter() - t0}
+
+
+def config1_cpu():
+    """Config 1 on the host cores: the reference's own Accurate_FSM (NGB operator) and
+    Classic (Podvin-Lecomte), compiled unmodified into oracle/_ref, on 1 core (the config-1
+    shot) and on every core (one seeded surface shot per thread, solved in parallel)."""
+    import oracle
+
+    from seismic_tomography_3d_b200 import workloads as wl
+
+    sv = wl.config1()
+    n = os.cpu_count() or 1
+    rng = np.random.default_rng(11)
+    many = wl.surface_nodes(rng, sv.nx, sv.ny, sv.h, n)
+    out = {"workload": "config1: 101x101x51 @25 m, v(z) = 1500 + 0.6 z + two 10 % anomalies, surface shots",
+           "kind": "reference", "cores_all": n}
+    for name, kind, reps in (("fsm", oracle.REF_FSM, 3), ("podvin_lecomte", oracle.REF_CLASSIC, 1)):
+        one = []
+        for _ in range(reps):
+            _, secs = oracle.ref_solve(kind, sv.velocity, sv.h, sv.shots, nthreads=1, want_T=False)
+            one.append(float(secs[0]))
+        t0 = time.perf_counter()
+        oracle.ref_solve(kind, sv.velocity, sv.h, many, nthreads=n, want_T=False)
+        wall = time.perf_counter() - t0
+        out[name] = {"s_per_shot_1core": statistics.median(one), "shots_per_s_1core": 1.0 / statistics.median(one),
+                     "shots_per_s_all_cores": n / wall, "all_cores_wall_s": wall}
+    return out
+
+
+def config1_gpu(steps=10, warmup=3):
+    """Config 1 on the device: the single shot with its 200 receivers, JW (Block_FIM's
+    operator) and NGB (Accurate_FSM's, bit for bit); device time per solve and the same
+    call end to end with the host velocity upload and receiver download."""
+    import torch
+
+    import seismic_tomography_3d_b200 as tomo
+    from seismic_tomography_3d_b200 import workloads as wl
+
+    sv = wl.config1()
+    ctx = tomo.Context(sv.nx, sv.ny, sv.nz, sv.h)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    vel_pinned = torch.from_numpy(sv.velocity.copy()).pin_memory()
+    ctx.set_velocity(sv.velocity)
+    out = {"workload": "config1: 101x101x51 @25 m, 1 shot x 200 receivers (library default tolerances)"}
+    for name, op in (("jw", 0), ("ngb", 1)):
+        for _ in range(warmup):
+            ctx.eik_solve(sv.shots, receivers=sv.receivers, op=op)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False, op=op)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        e0.record(stream)
+        for _ in range(steps):
+            assert ctx.lib.tomo_set_velocity(ctx.h, vel_pinned.data_ptr()) == 0
+            ctx.eik_solve(sv.shots, receivers=sv.receivers, op=op)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / steps
+        out[name] = {"ms_per_shot": ms, "shots_per_s": 1000.0 / ms, "e2e_ms_per_shot": e2e_ms}
+    ctx.close()
+    return out
+
+
+def _regular_points(n_x, n_y, x0, x1, y0, y1, z):
+    """Points of the reference's Regular geometry in its order (regular.cpp:82-104):
+    point k + j * n_y is (x_j, y_k)."""
+    xs = np.linspace(x0, x1, n_x, dtype=np.float32) if n_x > 1 else np.array([x0], np.float32)
+    ys = np.linspace(y0, y1, n_y, dtype=np.float32) if n_y > 1 else np.array([y0], np.float32)
+    pts = np.zeros((n_x * n_y, 3), np.float32)
+    for k in range(n_y):
+        for j in range(n_x):
+            pts[k + j * n_y] = (xs[j], ys[k], z)
+    return pts
+
+
+def reference_tomography_exe(timeout_s=240):
+    """The reference's own tomography.exe (Least_squares with the FSM forward model, serial),
+    compiled unmodified into oracle/_ref, on a bounded sample of config 3: the config-3 true
+    and starting models (201x201x101 at 12.5 m), 4 shots (2x2) x 2,500 receivers (the
+    config-3 50x50 grid), 50 m cells, lambda 0.1, order 2, smoothing; picks from the
+    reference FSM on the true model.  50 m cells (4 h) rather than config 3's 51 m: the
+    reference ray tracer loops forever when a cell face splits the source node's box,
+    which 51 m cells do.  One iteration = wall time with max_iteration = 1 minus the time
+    with max_iteration = 0 (the loop of tomography_main.cpp:19-30 forward-models once more
+    before it stops)."""
+    import tempfile
+
+    import oracle
+
+    from seismic_tomography_3d_b200 import workloads as wl
+
+    exe = oracle.ref_tomography_exe()
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/tomography.exe not built"}
+    sv, start, inv = wl.config3()
+    h, nx, ny, nz = sv.h, sv.nx, sv.ny, sv.nz
+    lo, hi = 41 * h, 161 * h  # source nodes off the 50 m cell faces
+    shots = _regular_points(2, 2, lo, hi, lo, hi, 0.0)
+    nodes = _regular_points(50, 50, 25.0, 2475.0, 25.0, 2475.0, 0.0)
+    Tt, _ = oracle.ref_solve(oracle.REF_FSM, sv.velocity, h, shots, nthreads=4)
+    dobs = np.stack([oracle.first_arrival(Tt[i], h, *nodes.T) for i in range(len(shots))])
+    del Tt
+    times = {}
+    with tempfile.TemporaryDirectory() as d:
+        for sub in ("run", "picks", "fa", "conv", "models", "geom", "outputs/illumination"):
+            os.makedirs(os.path.join(d, sub), exist_ok=True)
+        np.ascontiguousarray(start).tofile(os.path.join(d, "start.bin"))
+        for i in range(len(shots)):
+            dobs[i].astype(np.float32).tofile(os.path.join(d, "picks", f"obsData_{len(nodes)}_samples_shot_{i + 1}.bin"))
+        for max_it in (0, 1):
+            par = f"""x_samples = {nx}
+y_samples = {ny}
+z_samples = {nz}
+x_spacing = {h}
+y_spacing = {h}
+z_spacing = {h}
+vp_file = {d}/start.bin
+reciprocity = False
+shots_geometry_type = 0
+nodes_geometry_type = 0
+shots_elevation = 0
+nodes_elevation = 0
+shots_topography = False
+nodes_topography = False
+shots_topography_file = none
+nodes_topography_file = none
+shots_output_file = {d}/geom/shots.txt
+nodes_output_file = {d}/geom/nodes.txt
+shots_n_xline = 2
+shots_n_yline = 2
+shots_SW = {lo}, {lo}
+shots_NW = {lo}, {hi}
+shots_SE = {hi}, {lo}
+nodes_n_xline = 50
+nodes_n_yline = 50
+nodes_SW = 25.0, 25.0
+nodes_NW = 25.0, 2475.0
+nodes_SE = 2475.0, 25.0
+eikonal_type = 2
+export_time_volume = False
+export_first_arrival = True
+time_volume_folder = {d}/fa/
+first_arrival_folder = {d}/fa/
+tomography_type = 0
+max_iteration = {max_it}
+dx_tomo = 50.0
+dy_tomo = 50.0
+dz_tomo = 50.0
+tk_order = {inv['tk_order']}
+tk_param = {inv['tk_param']}
+smooth = True
+filter_samples = {inv['filter_samples']}
+standard_deviation = {inv['standard_deviation']}
+dobs_folder = {d}/picks/
+convergency_folder = {d}/conv/
+estimated_models_folder = {d}/models/
+"""
+            pf = os.path.join(d, f"params{max_it}.txt")
+            with open(pf, "w") as f:
+                f.write(par)
+            t0 = time.perf_counter()
+            try:
+                subprocess.run([exe, pf], cwd=os.path.join(d, "run"), check=True, stdout=subprocess.DEVNULL,
+                               timeout=timeout_s)
+            except (subprocess.TimeoutExpired, subprocess.CalledProcessError) as e:
+                return {"unavailable": f"reference tomography.exe did not finish: {type(e).__name__}"}
+            times[max_it] = time.perf_counter() - t0
+    it_s = times[1] - times[0]
+    return {"kind": "reference", "cores": 1, "iteration_s": it_s, "run_s_max_iteration_0": times[0],
+            "run_s_max_iteration_1": times[1], "shots": len(shots), "receivers": len(nodes),
+            "sample": "config-3 models, 4 shots (2x2) x 2,500 receivers, 50 m cells, 10 CGLS iterations "
+                      "(the reference's count), FSM forward model, serial"}
+
+
 def run_reference(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -297,6 +519,10 @@ def run_ours(args):
     e2e_ms = e0.elapsed_time(e1) / args.steps
     e2e_ms = max_over_ranks(e2e_ms, dist, 'cuda')
     e2e_value = world * ns / (e2e_ms / 1000.0)
+    # fields of the timed setting (the last e2e solve) for the oracle check of the CPU leg
+    cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
+    acc_idx = sample_shots(sv) if cpu_leg else []
+    acc_vols = [ctx.eik_volume(i) for i in acc_idx]
 
     # ---- roofline of the dominant kernel -----------------------------------------------
     act = statistics.mean(s["activations"] for s in stats)
@@ -317,8 +543,8 @@ def run_ours(args):
                 if ln.startswith("dram_bytes_per_activation:"):
                     traffic = float(ln.split(":")[1]) * act
 
-    # ---- accuracy of the timed setting against the fully converged field ----------------
-    accuracy = solver_accuracy(ctx, sv)
+    # ---- the timed setting against the fully converged field of the same solver ---------
+    accuracy_conv = solver_accuracy(ctx, sv)
 
     # ---- the NGB operator: the reference's own Accurate_FSM sweeps, bit-exact ------------
     ngb_steps = max(1, min(args.steps, 5))
@@ -358,19 +584,33 @@ def run_ours(args):
             "gpu_launches": 3 * args.steps,
             "solver": {"rounds": stats[-1]["rounds"], "activations": stats[-1]["activations"],
                        "inner_iterations": stats[-1]["inner_iterations"], **SOLVER},
-            "accuracy": accuracy,
+            "accuracy_vs_converged": accuracy_conv,
             "ngb_fsm": {"value": world * ns / (ngb_ms / 1000.0), "unit": UNIT, "ms_per_step": ngb_ms,
                         "steps": ngb_steps,
                         "what": "TOMO_OP_NGB: the reference Accurate_FSM's 8+8 sweeps on the same batch, "
                                 "bit-exact with the reference CPU solver (the cpu_baseline's algorithm)"},
             "warm_start": warm}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    ctx.close()
+    del stream
+    torch.cuda.empty_cache()
+    # ---- the other configurations (one GPU only; each bounded to seconds) ----------------
+    if world == 1 and not args.headline_only:
+        line["config1"] = {"gpu": config1_gpu()}
+        line["tomography"] = tomography_object(args, steps=5, warmup=3)
+        line["learned_warm"] = learned_warm_object(args.warm_fields, args.warm_epochs)
+        if not args.no_inversion:
+            line["inversion"] = inversion_object(args, iterations=3)
+    # ---- CPU leg: the reference on the host cores, and the oracle as the checker ----------
+    if cpu_leg:
         rate, cores, desc = cpu_reference_sample(sv, max_shots=min(ns, max(8, 2 * (os.cpu_count() or 1))),
                                                  budget_s=25.0)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
+        line["accuracy"] = oracle_accuracy(sv, acc_idx, acc_vols)
+        if not args.headline_only:
+            line["config1"]["cpu"] = config1_cpu()
+            line["tomography"]["reference_tomography_exe"] = reference_tomography_exe()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ctx.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -438,16 +678,25 @@ def warm_start_bound(ctx, sv, stream, steps, barrier, dist, world, inflate=0.02)
 
 
 def run_inversion(args):
+    """Config 5 on its own JSON line (not the headline metric); see inversion_object."""
+    print(json.dumps(inversion_object(args)), flush=True)
+    return 0
+
+
+def inversion_object(args, iterations=None):
     """Config 5: the large device-resident inversion -- 401x401x201 nodes at 10 m (32.3 M),
-    256 shots x 10,000 receivers, 50 m inversion cells, 5 iterations of eikonal -> rays ->
-    CGLS (30) -> model update with every field, matrix and vector kept in HBM.  Prints its
-    own JSON line (not the headline metric)."""
+    256 shots x 10,000 receivers, 50 m inversion cells, `iterations` (default 5) iterations
+    of eikonal -> rays -> CGLS (30) -> model update with every field, matrix and vector kept
+    in HBM.  Returns its JSON object."""
     import torch
 
     import seismic_tomography_3d_b200 as tomo
     from seismic_tomography_3d_b200 import workloads as wl
 
+    t_wall = time.perf_counter()
     sv, start, inv = wl.config5_inversion()
+    if iterations:
+        inv = dict(inv, iterations=iterations)
     rng = np.random.default_rng(5)
     ctx = tomo.Context(sv.nx, sv.ny, sv.nz, sv.h)
     stream = torch.cuda.ExternalStream(ctx.stream)
@@ -530,26 +779,33 @@ def run_inversion(args):
                                    "full windows, 50 m cells (81x81x41), tk order 2 lambda 0.1, 30 CGLS, 5 iterations",
                        "eikonal_tolerances_s": SOLVER_BANDED,
                        "start": "v(z) = 1500 + 1.0 z", "picks": "plain FIM on the true model + N(0, 2 ms)"},
-            "data": "synthetic (seeded config-5 model, shots, receivers)"}
-    print(json.dumps(line), flush=True)
+            "data": "synthetic (seeded config-5 model, shots, receivers)",
+            "wall_s": time.perf_counter() - t_wall}
     ctx.close()
-    return 0
+    return line
 
 
 def run_warm_start(args):
-    """Config 4: the learned warm start end to end -- solver-generated training fields on
-    seeded random models, the U-Net trained on the device, then used on the config-2 batch:
-    prediction -> ceiling (x 1.02) -> warm-started FIM, against the plain FIM.  Prints its own
-    JSON line (not the headline metric)."""
+    """Config 4 on its own JSON line (not the headline metric); see learned_warm_object."""
+    print(json.dumps(learned_warm_object(args.fields, args.epochs)), flush=True)
+    return 0
+
+
+def learned_warm_object(fields, epochs):
+    """Config 4: the learned warm start end to end -- `fields` solver-generated training
+    fields on seeded random models, the U-Net trained on the device for `epochs`, then used
+    on the config-2 batch: prediction -> ceiling (x 1.02) -> warm-started FIM (solve at the
+    timed tolerances, check, fallback), against the plain FIM at the same tolerances.
+    Returns its JSON object."""
     import torch
 
     import seismic_tomography_3d_b200 as tomo
     from seismic_tomography_3d_b200 import surrogate
 
     t0 = time.perf_counter()
-    ds = surrogate.make_dataset(nfields=args.fields, tile=64, nz=64, h=12.5)
+    ds = surrogate.make_dataset(nfields=fields, tile=64, nz=64, h=12.5)
     net = tomo.Net(seed=0)
-    summ = surrogate.train(net, ds, epochs=args.epochs, batch=8, lr=1e-3)
+    summ = surrogate.train(net, ds, epochs=epochs, batch=8, lr=1e-3)
     gen_s, gen_solve_ms = ds.gen_s, ds.solve_ms
     del ds
     torch.cuda.empty_cache()
@@ -558,8 +814,9 @@ def run_warm_start(args):
     ctx = tomo.Context(sv.nx, sv.ny, sv.nz, sv.h)
     ctx.set_velocity(sv.velocity)
     for _ in range(2):
-        _, st_plain = ctx.eik_solve(sv.shots, windows=sv.windows)
-    plain_ms = statistics.median(ctx.eik_solve(sv.shots, windows=sv.windows)[1]["total_ms"] for _ in range(5))
+        _, st_plain = ctx.eik_solve(sv.shots, windows=sv.windows, **SOLVER)
+    plain_ms = statistics.median(ctx.eik_solve(sv.shots, windows=sv.windows, **SOLVER)[1]["total_ms"]
+                                 for _ in range(5))
     sizes = ctx.volume_sizes(ns, sv.windows)
     exact = torch.empty(sum(sizes), dtype=torch.float32, device="cuda")
     ctx.eik_volumes_to(exact.data_ptr())
@@ -567,7 +824,7 @@ def run_warm_start(args):
     pred, infer_ms = surrogate.predict_ceiling(net, ctx, sv.shots, sv.windows)
     m = (exact >= 2.0 * sv.h / float(sv.velocity.max())) & (pred > 0)
     rel = ((pred - exact) / exact)[m]
-    runs = [ctx.eik_solve_seeded(sv.shots, pred.data_ptr(), 0.02, windows=sv.windows) for _ in range(3)]
+    runs = [ctx.eik_solve_seeded(sv.shots, pred.data_ptr(), 0.02, windows=sv.windows, **SOLVER) for _ in range(3)]
     _, st_w, ss_w = runs[-1]
     warm_ms = statistics.median(r[1]["total_ms"] for r in runs)
     out = torch.empty_like(exact)
@@ -581,8 +838,9 @@ def run_warm_start(args):
             "warm": {"ms_per_batch_solve": warm_ms, "ms_inference": infer_ms,
                      "activations": st_w["activations"], "inner_iterations": st_w["inner_iterations"],
                      "activations_seeded_launch": ss_w["activations_seeded"], "shots_fallback": ss_w["shots_fallback"],
-                     "violations": ss_w["violations"], "max_rel_err_vs_plain": err},
+                     "violations": ss_w["violations"], "stuck": ss_w["stuck"], "max_rel_err_vs_plain": err},
             "speedup_vs_plain": plain_ms / (warm_ms + infer_ms),
+            "tolerances_s": SOLVER,
             "predictor_rel_err": {"median_abs": float(rel.abs().median()), "p99_abs": float(rel.abs().quantile(0.99))
                                   if rel.numel() < 16_000_000 else None,
                                   "frac_below_truth_by_2pct": float((rel < -0.02).float().mean())},
@@ -591,16 +849,24 @@ def run_warm_start(args):
                      "models": "seeded random: 3-6 dipping layers 1500-4500 m/s, 0-12 Gaussian anomalies +-15 %",
                      "generation_s": gen_s, "generation_solve_ms": gen_solve_ms},
             "wall_s": time.perf_counter() - t0}
-    print(json.dumps(line), flush=True)
     net.close()
     ctx.close()
-    return 0
+    del exact, pred, out
+    torch.cuda.empty_cache()
+    return line
 
 
 def run_tomography(args):
+    """Config 3 on its own JSON line (not the headline metric); see tomography_object."""
+    print(json.dumps(tomography_object(args, args.steps, args.warmup)), flush=True)
+    return 0
+
+
+def tomography_object(args, steps, warmup):
     """Config 3: one full tomography iteration on the device (64 shots x 2,500 receivers,
     201x201x101 at 12.5 m, 50x50x25 cells, Tikhonov order 2, lambda 0.1, 30 CGLS
-    iterations).  Prints its own JSON line (not the headline metric)."""
+    iterations), warmup + steps times from the same starting model.  Returns its JSON
+    object."""
     import torch
 
     import seismic_tomography_3d_b200 as tomo
@@ -618,7 +884,7 @@ def run_tomography(args):
     # the starting model is uploaded every iteration (from pinned host memory, as a caller
     # that keeps its model in a pinned buffer would), so each iteration starts alike
     start_pinned = torch.from_numpy(np.ascontiguousarray(start)).pin_memory()
-    for it in range(args.warmup + args.steps):
+    for it in range(warmup + steps):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         ev[0].record(stream)
         assert ctx.lib.tomo_set_velocity(ctx.h, start_pinned.data_ptr()) == 0
@@ -632,7 +898,7 @@ def run_tomography(args):
         ctx.model_update(inv["smooth"], inv["filter_samples"], inv["standard_deviation"], want_velocity=False)
         ev[4].record(stream)
         torch.cuda.synchronize()
-        if it >= args.warmup:
+        if it >= warmup:
             for k, (a, b) in zip(("eikonal", "jacobian", "cgls", "update"), zip(ev[:4], ev[1:])):
                 timings[k].append(a.elapsed_time(b))
             timings["total"].append(ev[0].elapsed_time(ev[4]))
@@ -644,7 +910,7 @@ def run_tomography(args):
     cg_ms_it = c["ms"] / max(c["iterations"], 1)
     peak, peak_kind = peaks()
     line = {"metric": "tomography iteration time (config 3)", "value": med["total"], "unit": "ms",
-            "higher_is_better": False, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": False, "steps": steps, "warmup": warmup,
             "breakdown_ms": med, "shots_per_s_eikonal": len(sv.shots) / (med["eikonal"] / 1000.0),
             "jacobian": {k: j[k] for k in ("rows", "cols", "nnz_rays", "nnz", "rays", "rays_ok", "rays_stalled",
                                            "rays_capped", "rays_nonfinite", "rays_outside", "ray_steps")},
@@ -656,9 +922,8 @@ def run_tomography(args):
                                   "peak_kind": peak_kind, "alg_bytes_per_iteration": cg_bytes}},
             "eikonal_tolerances_s": SOLVER_BANDED,
             "data": "synthetic (seeded config-3 model, 64 shots x 2500 receivers, picks + N(0, 2 ms))"}
-    print(json.dumps(line), flush=True)
     ctx.close()
-    return 0
+    return line
 
 
 def run_jacobian(args):
@@ -720,6 +985,12 @@ def main():
                     help="run the config-4 learned warm start instead (separate JSON line)")
     ap.add_argument("--fields", type=int, default=20000, help="training fields (--warm-start)")
     ap.add_argument("--epochs", type=int, default=3, help="training epochs (--warm-start)")
+    ap.add_argument("--warm-fields", type=int, default=4000,
+                    help="training fields of the default line's learned_warm object")
+    ap.add_argument("--warm-epochs", type=int, default=2, help="its training epochs")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="the config-2 headline alone (no config1/tomography/learned_warm/inversion objects)")
+    ap.add_argument("--no-inversion", action="store_true", help="skip the config-5 inversion object")
     args = ap.parse_args()
     if args.warm_start:
         return run_warm_start(args)

@@ -125,14 +125,60 @@ int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point 
         f.t_off = total;
         total += (long long)(g.nz + 2) * (d.wnx + 2) * (d.wny + 2);
     }
+    // Schedule: tile by tile (fsm_solve_tiled) unless a source lies on a far face of its
+    // window, where the reference's reads cross column edges and only the plane schedule
+    // reproduces them; sweep_groups > 0 asks for the plane schedule with that many groups.
+    const int nzz = g.nz + 2;
+    bool tiled = groups <= 0;
+    for (const tomo::FsmShot &f : fs)
+        tiled = tiled && f.sidz <= nzz - 3 && f.sidx <= f.wnx - 1 && f.sidy <= f.wny - 1;
     int ngroups = groups > 0 ? groups : 4;  // 4 groups: fastest of 1..16 on the 64-shot batch
     if (ngroups > nshots) ngroups = nshots;
+    if (tiled) ngroups = 1;
+    std::vector<int> tab;
+    int tab_base[16] = {}, tab_nd[16] = {};
+    long long nflags = 0;
+    if (tiled) {
+        auto cdiv = [](int a, int b) { return (a + b - 1) / b; };
+        for (tomo::FsmShot &f : fs) {
+            f.flag_off = nflags;
+            nflags += (long long)cdiv(nzz - 1, tomo::kFsmTZ) * cdiv(f.wnx + 1, tomo::kFsmTX) *
+                      cdiv(f.wny + 1, tomo::kFsmTY);
+        }
+        // per sweep: first tile of (tile diagonal d, shot s), d-major, and the tile count
+        std::vector<int> A((size_t)nshots), B((size_t)nshots), C((size_t)nshots);
+        for (int q = 0; q < 16; q++) {
+            int nd = 0;
+            for (int s = 0; s < nshots; s++) {
+                const tomo::FsmShot &f = fs[(size_t)s];
+                A[(size_t)s] = cdiv(tomo::fsm_sweep_range(q, tomo::fsm_sign_z(q), nzz, f.sidz).L, tomo::kFsmTZ);
+                B[(size_t)s] = cdiv(tomo::fsm_sweep_range(q, tomo::fsm_sign_x(q), f.wnx + 2, f.sidx).L, tomo::kFsmTX);
+                C[(size_t)s] = cdiv(tomo::fsm_sweep_range(q, tomo::fsm_sign_y(q), f.wny + 2, f.sidy).L, tomo::kFsmTY);
+                nd = std::max(nd, A[(size_t)s] + B[(size_t)s] + C[(size_t)s] - 2);
+            }
+            tab_base[q] = (int)tab.size();
+            tab_nd[q] = nd;
+            long long run = 0;
+            for (int dg = 0; dg < nd; dg++)
+                for (int s = 0; s < nshots; s++) {
+                    tab.push_back((int)run);
+                    run += tomo::fsm_diag_count(dg, A[(size_t)s], B[(size_t)s], C[(size_t)s]);
+                }
+            if (run >= (1ll << 31)) return fail(ctx, TOMO_ERR_CAPACITY, "too many sweep tiles for one NGB batch");
+            tab.push_back((int)run);
+        }
+        CK(ctx->fsm_tab.ensure(tab.size()));
+        CK(ctx->fsm_flags.ensure((size_t)nflags));
+        CK(cudaMemcpyAsync(ctx->fsm_tab.ptr, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(cudaMemsetAsync(ctx->fsm_flags.ptr, 0, (size_t)nflags * sizeof(unsigned), ctx->stream));
+    }
     CK(ctx->fsm_T.ensure((size_t)total));
     CK(ctx->fsm_shots.ensure((size_t)nshots));
-    CK(ctx->fsm_bar.ensure((size_t)2 * ngroups));
+    CK(ctx->fsm_bar.ensure((size_t)2 * ngroups + 16));
     CK(cudaMemcpyAsync(ctx->fsm_shots.ptr, fs.data(), fs.size() * sizeof(tomo::FsmShot), cudaMemcpyHostToDevice,
                        ctx->stream));
-    CK(cudaMemsetAsync(ctx->fsm_bar.ptr, 0, 2 * ngroups * sizeof(unsigned), ctx->stream));
+    CK(cudaMemsetAsync(ctx->fsm_bar.ptr, 0, (2 * ngroups + 16) * sizeof(unsigned), ctx->stream));
     CK(cudaMemsetAsync(ctx->ctrl.ptr, 0, tomo::kCtrlWords * sizeof(unsigned), ctx->stream));
     CK(cudaMemsetAsync(ctx->stats.ptr, 0, 2 * sizeof(unsigned long long), ctx->stream));
     tomo::FsmLaunch p{};
@@ -160,9 +206,19 @@ int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point 
     p.spin_limit = spin_limit;
     p.Tb = ctx->T.ptr;
     p.desc = ctx->shots_d.ptr;
+    if (tiled) {
+        p.tab = ctx->fsm_tab.ptr;
+        std::memcpy(p.tab_base, tab_base, sizeof(tab_base));
+        std::memcpy(p.tab_nd, tab_nd, sizeof(tab_nd));
+        p.flags = ctx->fsm_flags.ptr;
+        p.cursors = ctx->fsm_bar.ptr + 2;
+    }
     CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     int grid = 0;
-    CK(tomo::fsm_solve(p, &grid, ctx->stream));
+    if (tiled)
+        CK(tomo::fsm_solve_tiled(p, &grid, ctx->stream));
+    else
+        CK(tomo::fsm_solve(p, &grid, ctx->stream));
     if (nrec > 0)
         CK(tomo::receivers_sample(ctx->T.ptr, ctx->shots_d.ptr, nshots, ctx->rec.ptr, ctx->rec.ptr + nrec,
                                   ctx->rec.ptr + 2 * nrec, nrec, g.dx, g.dy, g.dz, g.nz, ctx->t_recv.ptr, ctx->stream));

@@ -70,7 +70,9 @@ struct tomo_ctx {
     tomo::DevBuf<unsigned> tune_word;            // autotuner scratch (largest slowness)
     tomo::DevBuf<float> fsm_T;                      // TOMO_OP_NGB sweep grids (with halo)
     tomo::DevBuf<tomo::FsmShot> fsm_shots;
-    tomo::DevBuf<unsigned> fsm_bar;
+    tomo::DevBuf<unsigned> fsm_bar;                 // barrier words (+ the tiled schedule's cursors)
+    tomo::DevBuf<int> fsm_tab;                      // tiled schedule: tile-diagonal tables
+    tomo::DevBuf<unsigned> fsm_flags;               // tiled schedule: per-tile sweep flags
     tomo::DevBuf<unsigned long long> stats;
     tomo::DevBuf<tomo::ShotDesc> shots_d;
     tomo::DevBuf<tomo::ShotDesc> shots_redo;        // warm start: shots solved again from INF

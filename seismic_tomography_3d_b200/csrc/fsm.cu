@@ -18,39 +18,6 @@ namespace tomo {
 
 namespace {
 
-struct Range {
-    int i0, di, L;
-};
-
-// Sweep q (0..7 source-anchored, 8..15 full) of axis with sign s (+1 ascending), halo extent
-// n and source index sid (accurate_FSM.cpp:267-511).
-__device__ __forceinline__ Range sweep_range(int q, int s, int n, int sid)
-{
-    Range r;
-    if (q < 8) {
-        if (s > 0) {
-            r.i0 = max(1, sid);
-            r.di = 1;
-            r.L = n - r.i0;
-        } else {
-            r.i0 = sid + 1;
-            r.di = -1;
-            r.L = sid + 2;
-        }
-    } else {
-        if (s > 0) {
-            r.i0 = 1;
-            r.di = 1;
-            r.L = n - 1;
-        } else {
-            r.i0 = n - 2;
-            r.di = -1;
-            r.L = n - 1;
-        }
-    }
-    return r;
-}
-
 // octant signs (z, x, y) of the 8 sweeps, in the reference's order
 __device__ __constant__ int kSgn[8][3] = {{1, 1, 1},  {-1, 1, 1},  {1, 1, -1},  {-1, 1, -1},
                                           {1, -1, 1}, {-1, -1, 1}, {1, -1, -1}, {-1, -1, -1}};
@@ -114,49 +81,65 @@ __device__ __forceinline__ float sget(const FsmLaunch &p, const ShotGrid &g, int
     return __ldg(p.slow + z + (long long)x * p.nz + (long long)y * p.nx * p.nz);
 }
 
-// Accurate_FSM::inner_sweep (accurate_FSM.cpp:159-265), same operations in the same order.
-__device__ float ngb_update(const FsmLaunch &p, const ShotGrid &g, int i, int j, int k, int sgntz, int sgntx, int sgnty)
+// Traveltimes and slowness of one shot's halo grid as the sweep reads them, from global
+// memory with the reference's flattened indexing (the plane schedule).
+struct GlobalAcc {
+    const FsmLaunch &p;
+    const ShotGrid &g;
+    __device__ __forceinline__ float t(int i, int j, int k) const
+    {
+        return tget(g, i + j * (long long)g.nzz + k * ((long long)g.nxx * g.nzz));
+    }
+    __device__ __forceinline__ float self(int i, int j, int k) const
+    {
+        return __ldcg(g.T + i + j * (long long)g.nzz + k * ((long long)g.nxx * g.nzz));
+    }
+    __device__ __forceinline__ float s(int i, int j, int k) const { return sget(p, g, i, j, k); }
+};
+
+// Accurate_FSM::inner_sweep (accurate_FSM.cpp:159-265), same operations in the same order,
+// on the values the accessor returns (global memory or a shared-memory tile).
+template <class Acc>
+__device__ __forceinline__ float ngb_update(const FsmLaunch &p, const Acc &A, int nxx, int nyy, int nzz, int i, int j,
+                                            int k, int sgntz, int sgntx, int sgnty)
 {
-    const int nxx = g.nxx, nyy = g.nyy, nzz = g.nzz;
-    const long long sx = nzz, sy = (long long)nxx * nzz;
     const int sgnvz = sgntz == 1, sgnvx = sgntx == 1, sgnvy = sgnty == 1;
     const int i1 = i - sgnvz, j1 = j - sgnvx, k1 = k - sgnvy;
-    const float tv = tget(g, (i - sgntz) + j * sx + k * sy);
-    const float te = tget(g, i + (j - sgntx) * sx + k * sy);
-    const float tn = tget(g, i + j * sx + (k - sgnty) * sy);
-    const float tev = tget(g, (i - sgntz) + (j - sgntx) * sx + k * sy);
-    const float ten = tget(g, i + (j - sgntx) * sx + (k - sgnty) * sy);
-    const float tnv = tget(g, (i - sgntz) + j * sx + (k - sgnty) * sy);
-    const float tnve = tget(g, (i - sgntz) + (j - sgntx) * sx + (k - sgnty) * sy);
-    const long long ijk = i + j * sx + k * sy;
+    const float tv = A.t(i - sgntz, j, k);
+    const float te = A.t(i, j - sgntx, k);
+    const float tn = A.t(i, j, k - sgnty);
+    const float tev = A.t(i - sgntz, j - sgntx, k);
+    const float ten = A.t(i, j - sgntx, k - sgnty);
+    const float tnv = A.t(i - sgntz, j, k - sgnty);
+    const float tnve = A.t(i - sgntz, j - sgntx, k - sgnty);
     const int jm = max(j - 1, 1), jp = min(j, nxx - 1), km = max(k - 1, 1), kp = min(k, nyy - 1);
     const int im = max(i - 1, 1), ip = min(i, nzz - 1);
     const float dz2i = p.dz2i, dx2i = p.dx2i, dy2i = p.dy2i;
 
-    const float t1D1 = tv + p.dz * smin(sget(p, g, i1, jm, km),
-                                        smin(sget(p, g, i1, jm, kp), smin(sget(p, g, i1, jp, km), sget(p, g, i1, jp, kp))));
-    const float t1D2 = te + p.dx * smin(sget(p, g, im, j1, km),
-                                        smin(sget(p, g, ip, j1, km), smin(sget(p, g, im, j1, kp), sget(p, g, ip, j1, kp))));
-    const float t1D3 = tn + p.dy * smin(sget(p, g, im, jm, k1),
-                                        smin(sget(p, g, im, jp, k1), smin(sget(p, g, ip, jm, k1), sget(p, g, ip, jp, k1))));
+    const float t1D1 = tv + p.dz * smin(A.s(i1, jm, km),
+                                        smin(A.s(i1, jm, kp), smin(A.s(i1, jp, km), A.s(i1, jp, kp))));
+    const float t1D2 = te + p.dx * smin(A.s(im, j1, km),
+                                        smin(A.s(ip, j1, km), smin(A.s(im, j1, kp), A.s(ip, j1, kp))));
+    const float t1D3 = tn + p.dy * smin(A.s(im, jm, k1),
+                                        smin(A.s(im, jp, k1), smin(A.s(ip, jm, k1), A.s(ip, jp, k1))));
     const float t1D = smin(t1D1, smin(t1D2, t1D3));
 
     float t2D1 = 1e6f, t2D2 = 1e6f, t2D3 = 1e6f, ta, tb, tc, Sref;
-    Sref = smin(sget(p, g, i1, j1, km), sget(p, g, i1, j1, kp));
+    Sref = smin(A.s(i1, j1, km), A.s(i1, j1, kp));
     if ((tv < te + p.dx * Sref) && (te < tv + p.dz * Sref)) {
         ta = tev + te - tv;
         tb = tev - te + tv;
         t2D1 = ((tb * dz2i + ta * dx2i) + sqrtf(4.0f * Sref * Sref * (dz2i + dx2i) - dz2i * dx2i * (ta - tb) * (ta - tb))) /
                (dz2i + dx2i);
     }
-    Sref = smin(sget(p, g, i1, jm, k1), sget(p, g, i1, jp, k1));
+    Sref = smin(A.s(i1, jm, k1), A.s(i1, jp, k1));
     if ((tv < tn + p.dy * Sref) && (tn < tv + p.dz * Sref)) {
         ta = tv - tn + tnv;
         tb = tn - tv + tnv;
         t2D2 = ((ta * dz2i + tb * dy2i) + sqrtf(4.0f * Sref * Sref * (dz2i + dy2i) - dz2i * dy2i * (ta - tb) * (ta - tb))) /
                (dz2i + dy2i);
     }
-    Sref = smin(sget(p, g, im, j1, k1), sget(p, g, ip, j1, k1));
+    Sref = smin(A.s(im, j1, k1), A.s(ip, j1, k1));
     if ((te < tn + p.dy * Sref) && (tn < te + p.dx * Sref)) {
         ta = te - tn + ten;
         tb = tn - te + ten;
@@ -166,7 +149,7 @@ __device__ float ngb_update(const FsmLaunch &p, const ShotGrid &g, int i, int j,
     const float t2D = smin(t2D1, smin(t2D2, t2D3));
 
     float t3D = 1e6f;
-    Sref = sget(p, g, i1, j1, k1);
+    Sref = A.s(i1, j1, k1);
     ta = te - 0.5f * tn + 0.5f * ten - 0.5f * tv + 0.5f * tev - tnv + tnve;
     tb = tv - 0.5f * tn + 0.5f * tnv - 0.5f * te + 0.5f * tev - ten + tnve;
     tc = tn - 0.5f * te + 0.5f * ten - 0.5f * tv + 0.5f * tnv - tev + tnve;
@@ -178,7 +161,7 @@ __device__ float ngb_update(const FsmLaunch &p, const ShotGrid &g, int i, int j,
             t3D = (t1 + sqrtf(t2 - t3)) / p.dsum;
         }
     }
-    return smin(__ldcg(g.T + ijk), smin(t1D, smin(t2D, t3D)));
+    return smin(A.self(i, j, k), smin(t1D, smin(t2D, t3D)));
 }
 
 }  // namespace
@@ -222,8 +205,8 @@ __global__ void __launch_bounds__(256, 3) k_fsm_sweeps(FsmLaunch p)
         int W = 0;
         for (int m = 0; m < ns; m++) {
             const FsmShot &s = p.shots[grp + m * G];
-            const Range rz = sweep_range(q, sgz, nzz, s.sidz), rx = sweep_range(q, sgx, s.wnx + 2, s.sidx),
-                        ry = sweep_range(q, sgy, s.wny + 2, s.sidy);
+            const FsmRange rz = fsm_sweep_range(q, sgz, nzz, s.sidz), rx = fsm_sweep_range(q, sgx, s.wnx + 2, s.sidx),
+                           ry = fsm_sweep_range(q, sgy, s.wny + 2, s.sidy);
             W = max(W, rz.L + rx.L + ry.L - 2);
         }
         for (int w = 0; w < W; w++) {
@@ -231,8 +214,8 @@ __global__ void __launch_bounds__(256, 3) k_fsm_sweeps(FsmLaunch p)
             for (long long row = gwarp; row < (long long)ns * nzz; row += nwarps) {
                 const int m = (int)(row / nzz), c = (int)(row % nzz);
                 const FsmShot &s = p.shots[grp + m * G];
-                const Range rz = sweep_range(q, sgz, nzz, s.sidz), rx = sweep_range(q, sgx, s.wnx + 2, s.sidx),
-                            ry = sweep_range(q, sgy, s.wny + 2, s.sidy);
+                const FsmRange rz = fsm_sweep_range(q, sgz, nzz, s.sidz), rx = fsm_sweep_range(q, sgx, s.wnx + 2, s.sidx),
+                               ry = fsm_sweep_range(q, sgy, s.wny + 2, s.sidy);
                 if (c >= rz.L) continue;
                 const int t = w - c;
                 const int a_lo = max(0, t - (ry.L - 1)), a_hi = min(rx.L - 1, t);
@@ -241,7 +224,7 @@ __global__ void __launch_bounds__(256, 3) k_fsm_sweeps(FsmLaunch p)
                 const int i = rz.i0 + rz.di * c;
                 for (int a = a_lo + lane; a <= a_hi; a += 32) {
                     const int j = rx.i0 + rx.di * a, k = ry.i0 + ry.di * (t - a);
-                    const float v = ngb_update(p, g, i, j, k, sgz, sgx, sgy);
+                    const float v = ngb_update(p, GlobalAcc{p, g}, g.nxx, g.nyy, g.nzz, i, j, k, sgz, sgx, sgy);
                     __stcg(g.T + i + (long long)j * nzz + (long long)k * g.nxx * nzz, v);
                 }
             }
@@ -287,6 +270,266 @@ cudaError_t fsm_solve(const FsmLaunch &p, int *grid_out, cudaStream_t st)
     FsmLaunch pp = p;
     void *args[] = {&pp};
     return cudaLaunchCooperativeKernel((const void *)k_fsm_sweeps, dim3(grid), dim3(256), args, 0, st);
+}
+
+// -------------------------------------------------------------------------------------
+// Tiled schedule.  One sweep is a Gauss-Seidel pass whose node updates depend only on the
+// upwind neighbours of the sweep's octant.  The sweep's node box (sweep order z, x, y) is
+// cut into kFsmTZ x kFsmTX x kFsmTY tiles; a tile depends only on the (up to 7) tiles
+// below it on some axes, so tiles are handed out in the order of their tile diagonal
+// tc + ta + tb.  One warp relaxes one tile in shared memory, diagonal plane by diagonal
+// plane (the nodes of a plane are independent), after waiting for its upwind tiles' flags;
+// every tile it waits on was handed out before its own and every CTA is resident, so the
+// waits end.  Each node sees exactly the values it sees in the sequential loop, and the
+// update is the same function, so the result is the plane schedule's bit for bit -- with
+// one grid barrier per sweep instead of one per diagonal plane.  Every source must lie off
+// the far faces of its window (halo index sid <= n - 3), so that no read leaves the grid
+// (the reference's flattened reads would otherwise cross a column edge).
+// -------------------------------------------------------------------------------------
+namespace {
+
+constexpr int kHZ = kFsmTZ + 1, kHX = kFsmTX + 1, kHY = kFsmTY + 1;
+constexpr int kHN = kHZ * kHX * kHY;  // a tile plus one upwind layer per axis
+// Slowness arguments of the operator span one index below to one above the tile's own
+// (at halo index 0 it reads index 1: max(i - 1, 1))
+constexpr int kSZ = kFsmTZ + 2, kSX = kFsmTX + 2, kSY = kFsmTY + 2;
+constexpr int kSN = kSZ * kSX * kSY;
+constexpr int kTileN = kFsmTZ * kFsmTX * kFsmTY;
+constexpr int kNPlanes = kFsmTZ + kFsmTX + kFsmTY - 2;
+static_assert(kFsmTZ <= 16 && kFsmTX <= 8 && kFsmTY <= 8, "plane table packs (c, a, b) in 4 + 3 + 3 bits");
+
+// A tile staged in shared memory: the traveltimes of the tile and its upwind layer (halo
+// index origin tz, tx, ty) and the slowness of the halo indices the operator reads, one
+// below the tile's lowest index to one above its highest (origin sz, sx, sy).
+struct TileAcc {
+    const float *T, *S;
+    int tz, tx, ty, sz, sx, sy;
+    __device__ __forceinline__ float t(int i, int j, int k) const
+    {
+        return T[(i - tz) + kHZ * ((j - tx) + kHX * (k - ty))];
+    }
+    __device__ __forceinline__ float self(int i, int j, int k) const { return t(i, j, k); }
+    __device__ __forceinline__ float s(int i, int j, int k) const
+    {
+        return S[(i - sz) + kSZ * ((j - sx) + kSX * (k - sy))];
+    }
+};
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// Lowest halo index of the tile's own nodes on one axis (l0: the tile's first local index).
+__device__ __forceinline__ int tile_lo(const FsmRange &r, int l0, int T)
+{
+    return r.di > 0 ? r.i0 + l0 : r.i0 - (l0 + T - 1);
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
+{
+    extern __shared__ float smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    float *Ts = smem + warp * (kHN + kSN), *Ss = Ts + kHN;
+    unsigned short *plane = reinterpret_cast<unsigned short *>(smem + wpb * (kHN + kSN));
+    int *pstart = reinterpret_cast<int *>(plane + kTileN);
+    // the tile's nodes (c, a, b) ordered by diagonal plane c + a + b
+    if (threadIdx.x < kNPlanes) {
+        const int w = threadIdx.x;
+        int m = 0;
+        for (int v = 0; v < w; v++)
+            m += (int)fsm_diag_count(v, kFsmTZ, kFsmTX, kFsmTY);
+        pstart[w] = m;
+        for (int b = 0; b < kFsmTY; b++)
+            for (int a = 0; a < kFsmTX; a++) {
+                const int c = w - a - b;
+                if (c >= 0 && c < kFsmTZ) plane[m++] = (unsigned short)(c | (a << 4) | (b << 7));
+            }
+        if (w == kNPlanes - 1) pstart[kNPlanes] = m;
+    }
+    const long long gthread = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nthreads = (long long)gridDim.x * blockDim.x;
+    const int nzz = p.nz + 2;
+
+    // T = 1e6 on the shots' halo grids, then the 27 analytic seeds (accurate_FSM.cpp:591-630)
+    for (int m = 0; m < p.nshots; m++) {
+        const FsmShot &s = p.shots[m];
+        const long long n = (long long)nzz * (s.wnx + 2) * (s.wny + 2);
+        for (long long q = gthread; q < n; q += nthreads) __stcg(p.T + s.t_off + q, 1e6f);
+    }
+    if (!group_barrier(p.bar, gridDim.x, p.err, p.spin_limit)) return;
+    for (long long q = gthread; q < (long long)p.nshots * 27; q += nthreads) {
+        const FsmShot &s = p.shots[(int)(q / 27)];
+        const int e = (int)(q % 27), oz = e % 3 - 1, ox = (e / 3) % 3 - 1, oy = e / 9 - 1;
+        const int nxx = s.wnx + 2;
+        const long long sid = s.sidz + (long long)s.sidx * nzz + (long long)s.sidy * nxx * nzz;
+        ShotGrid g{&s, p.T + s.t_off, 0, nxx, s.wny + 2, nzz};
+        const float S0 = sget(p, g, s.sidz, s.sidx, s.sidy);
+        __stcg(p.T + s.t_off + sid + oz + (long long)ox * nzz + (long long)oy * nxx * nzz, S0 * s.seed_dist[e]);
+    }
+    if (!group_barrier(p.bar, gridDim.x, p.err, p.spin_limit)) return;
+
+    const int S = p.nshots;
+    for (int q = 0; q < 16; q++) {
+        const int sgz = fsm_sign_z(q), sgx = fsm_sign_x(q), sgy = fsm_sign_y(q);
+        const int *tab = p.tab + p.tab_base[q];
+        const int nd = p.tab_nd[q];
+        const int total = tab[nd * S];
+        for (;;) {
+            int item = 0;
+            if (lane == 0) item = ld_volatile(p.err) != 0u ? total : (int)atomicAdd(p.cursors + q, 1u);
+            item = __shfl_sync(kFull, item, 0);
+            if (item >= total) break;
+            // (diagonal, shot): the last table entry <= item (tab[lo] <= item < tab[hi])
+            int lo = 0, hi = nd * S;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (__ldg(tab + mid) <= item)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const int d = lo / S, si = lo % S;
+            int r = item - __ldg(tab + lo);
+            const FsmShot &sh = p.shots[si];
+            const int nxx = sh.wnx + 2, nyy = sh.wny + 2;
+            const FsmRange rz = fsm_sweep_range(q, sgz, nzz, sh.sidz), rx = fsm_sweep_range(q, sgx, nxx, sh.sidx),
+                           ry = fsm_sweep_range(q, sgy, nyy, sh.sidy);
+            const int A = cdiv(rz.L, kFsmTZ), B = cdiv(rx.L, kFsmTX), C = cdiv(ry.L, kFsmTY);
+            // the r-th tile (tc, ta, tb) of diagonal d, tb ascending, then ta
+            int tc = 0, ta = 0, tb = max(0, d - (A - 1) - (B - 1));
+            for (; tb <= min(C - 1, d); tb++) {
+                const int e = d - tb, alo = max(0, e - (A - 1)), ahi = min(B - 1, e);
+                if (r <= ahi - alo) {
+                    ta = alo + r;
+                    tc = e - ta;
+                    break;
+                }
+                r -= ahi - alo + 1;
+            }
+            // wait for the upwind tiles of this sweep (lanes 0-6: one each)
+            const int fa = cdiv(nzz - 1, kFsmTZ), fb = cdiv(nxx - 1, kFsmTX);
+            unsigned *flags = p.flags + sh.flag_off;
+            bool gave_up = false;
+            if (lane < 7) {
+                const int dc = (lane + 1) & 1, da = ((lane + 1) >> 1) & 1, db = (lane + 1) >> 2;
+                if (tc >= dc && ta >= da && tb >= db) {
+                    const unsigned *f = flags + (tc - dc) + fa * ((ta - da) + fb * (tb - db));
+                    unsigned long long spins = 0;
+                    while (ld_acquire(f) != (unsigned)(q + 1)) {
+                        if (++spins > p.spin_limit || ld_volatile(p.err) != 0u) {
+                            atomicCAS(p.err, 0u, (unsigned)kDevBarrierTimeout);
+                            gave_up = true;
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                }
+            }
+            if (__any_sync(kFull, gave_up)) break;  // the whole warp leaves the sweep
+            __syncwarp();  // the upwind tiles' stores, acquired by lanes 0-6, for every lane
+            // stage the tile: traveltimes of the tile and its upwind layer, slowness
+            const int gz = tile_lo(rz, tc * kFsmTZ, kFsmTZ), gx = tile_lo(rx, ta * kFsmTX, kFsmTX),
+                      gy = tile_lo(ry, tb * kFsmTY, kFsmTY);
+            const TileAcc acc{Ts, Ss, rz.di > 0 ? gz - 1 : gz, rx.di > 0 ? gx - 1 : gx, ry.di > 0 ? gy - 1 : gy,
+                              gz - 1, gx - 1, gy - 1};
+            const float *T = p.T + sh.t_off;
+            ShotGrid g{&sh, p.T + sh.t_off, 0, nxx, nyy, nzz};
+            for (int m = lane; m < kHN; m += 32) {
+                const int ci = m % kHZ, cj = (m / kHZ) % kHX, ck = m / (kHZ * kHX);
+                const int i = acc.tz + ci, j = acc.tx + cj, k = acc.ty + ck;
+                Ts[m] = (i >= 0 && i < nzz && j >= 0 && j < nxx && k >= 0 && k < nyy)
+                            ? __ldcg(T + i + (long long)j * nzz + (long long)k * nxx * nzz)
+                            : 1e6f;
+            }
+            for (int m = lane; m < kSN; m += 32) {  // sget clamps every index into the window
+                const int ci = m % kSZ, cj = (m / kSZ) % kSX, ck = m / (kSZ * kSX);
+                Ss[m] = sget(p, g, acc.sz + ci, acc.sx + cj, acc.sy + ck);
+            }
+            __syncwarp();
+            for (int w = 0; w < kNPlanes; w++) {
+                for (int m = pstart[w] + lane; m < pstart[w + 1]; m += 32) {
+                    const unsigned e = plane[m];
+                    const int lc = tc * kFsmTZ + (int)(e & 15u), la = ta * kFsmTX + (int)((e >> 4) & 7u),
+                              lb = tb * kFsmTY + (int)(e >> 7);
+                    if (lc < rz.L && la < rx.L && lb < ry.L) {
+                        const int i = rz.i0 + rz.di * lc, j = rx.i0 + rx.di * la, k = ry.i0 + ry.di * lb;
+                        const float v = ngb_update(p, acc, nxx, nyy, nzz, i, j, k, sgz, sgx, sgy);
+                        Ts[(i - acc.tz) + kHZ * ((j - acc.tx) + kHX * (k - acc.ty))] = v;
+                    }
+                }
+                __syncwarp();
+            }
+            // the tile's nodes back to global memory, then its flag
+            float *Tw = p.T + sh.t_off;
+            for (int m = lane; m < kTileN; m += 32) {
+                const int c = m % kFsmTZ, a = (m / kFsmTZ) % kFsmTX, b = m / (kFsmTZ * kFsmTX);
+                const int lc = tc * kFsmTZ + c, la = ta * kFsmTX + a, lb = tb * kFsmTY + b;
+                if (lc < rz.L && la < rx.L && lb < ry.L) {
+                    const int i = rz.i0 + rz.di * lc, j = rx.i0 + rx.di * la, k = ry.i0 + ry.di * lb;
+                    __stcg(Tw + i + (long long)j * nzz + (long long)k * nxx * nzz,
+                           Ts[(i - acc.tz) + kHZ * ((j - acc.tx) + kHX * (k - acc.ty))]);
+                }
+            }
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) st_release(flags + tc + fa * (ta + fb * tb), (unsigned)(q + 1));
+        }
+        if (!group_barrier(p.bar, gridDim.x, p.err, p.spin_limit)) return;
+    }
+
+    // reduce_model (accurate_FSM.cpp:62-72) into the brick-major pool of the shot
+    for (int m = 0; m < p.nshots; m++) {
+        const FsmShot &s = p.shots[m];
+        const ShotDesc &d = p.desc[m];
+        const long long n = (long long)d.nbx * d.nby * d.nbz * kBrickNodes;
+        const int nxx = s.wnx + 2;
+        for (long long e = gthread; e < n; e += nthreads) {
+            const long long b = e / kBrickNodes;
+            const int node = (int)(e % kBrickNodes);
+            const int bz = (int)(b % d.nbz);
+            const long long tq = b / d.nbz;
+            const int bx = (int)(tq % d.nbx), by = (int)(tq / d.nbx);
+            const int z = bz * 4 + (node & 3), x = bx * 4 + ((node >> 2) & 3), y = by * 4 + (node >> 4);
+            float v = kInf;
+            if (z < p.nz && x < s.wnx && y < s.wny)
+                v = __ldcg(p.T + s.t_off + (z + 1) + (long long)(x + 1) * nzz + (long long)(y + 1) * nxx * nzz);
+            p.Tb[d.t_off + e] = v;
+        }
+    }
+}
+
+cudaError_t fsm_solve_tiled(const FsmLaunch &p, int *grid_out, cudaStream_t st)
+{
+    constexpr int threads = 256;
+    const size_t smem = (size_t)(threads / 32) * (kHN + kSN) * sizeof(float) + kTileN * sizeof(unsigned short) +
+                        (kNPlanes + 1) * sizeof(int);
+    cudaError_t e = cudaFuncSetAttribute(k_fsm_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 0, per_sm = 0;
+    e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fsm_tiled, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const int grid = nsm * per_sm;
+    if (grid_out) *grid_out = grid;
+    FsmLaunch pp = p;
+    void *args[] = {&pp};
+    return cudaLaunchCooperativeKernel((const void *)k_fsm_tiled, dim3(grid), dim3(threads), args, smem, st);
 }
 
 }  // namespace tomo

@@ -19,6 +19,8 @@ NGB = 1
 
 
 def test_matches_reference_fsm_golden(tomo):
+    """Default schedule (tiled where every source lies off its window's far faces, plane
+    otherwise) against the reference's own FSM volumes."""
     g = np.load(os.path.join(HERE, "golden", "eik_ref.npz"))
     for seed, nx, ny, nz, h, shots in mg.EIK_CASES:
         v, sh = g[f"v_{seed}"], g[f"shots_{seed}"]
@@ -41,8 +43,10 @@ def test_matches_oracle_on_config1_and_receivers(tomo, oracle_mod):
     np.testing.assert_array_equal(t_recv[0], oracle_mod.first_arrival(T_ref, sv.h, *sv.receivers.T))
 
 
-@pytest.mark.parametrize("groups", [1, 3])
+@pytest.mark.parametrize("groups", [0, 1, 3])
 def test_windowed_batch_matches_cropped_oracle(tomo, oracle_mod, groups):
+    """groups 0: the tile-wavefront schedule (default); 1, 3: the plane schedule with that
+    many independent block groups.  Both reproduce the sequential sweeps bit for bit."""
     nx, ny, nz = 37, 30, 14
     sv = wl.small(11, nx, ny, nz, nshots=6, windows=True)
     s = (np.float32(1.0) / sv.velocity).astype(np.float32)
@@ -73,3 +77,4 @@ def test_ngb_batch_feeds_ray_tracing(tomo, oracle_mod):
         rt = oracle_mod.raytrace(vols[i], h, sv.shots[i], *sv.receivers.T, (100.0,) * 3, nt, max_steps=6000)
         got.append(rt["cols"])
     np.testing.assert_array_equal(cols[:st["nnz_rays"]], np.concatenate(got))
+
