@@ -458,6 +458,8 @@ def run_reference(args):
 def run_ours(args):
     import torch
 
+    SOLVER_RUN = dict(SOLVER)  # the headline's options: timed tolerances (+ --brick)
+
     import seismic_tomography_3d_b200 as tomo
 
     rank, world, local = rank_info()
@@ -476,9 +478,16 @@ def run_ours(args):
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
     vel_pinned = torch.from_numpy(sv.velocity.copy()).pin_memory()
     ctx.set_velocity(sv.velocity)
+    # launch shape and brick shape tuned on this batch (setup, untimed); later solves use them
+    tuned = None
+    if args.brick:  # a fixed brick shape (profiling), default launch shape
+        SOLVER_RUN.update(brick=args.brick)
+    elif not args.no_autotune:
+        shape, tst = ctx.eik_autotune(sv.shots, windows=sv.windows, repeats=2)
+        tuned = dict(shape, trials=tst["trials"], best_ms=tst["best_ms"], default_ms=tst["default_ms"])
 
     def step_resident():
-        _, st = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=False, **SOLVER)
+        _, st = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=False, **SOLVER_RUN)
         return st
 
     def barrier():
@@ -513,7 +522,7 @@ def run_ours(args):
     for _ in range(args.steps):
         tomo_rc = lib.tomo_set_velocity(ctx.h, vel_pinned.data_ptr())
         assert tomo_rc == 0
-        t_out, _ = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=True, **SOLVER)
+        t_out, _ = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=True, **SOLVER_RUN)
     e1.record(stream)
     barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
@@ -533,10 +542,12 @@ def run_ours(args):
     # compulsory traffic of the batch whatever the algorithm: slowness read + traveltime
     # written once per window node (8 B/node)
     compulsory = 8.0 * sum(ctx.volume_sizes(ns, sv.windows))
-    # DRAM bytes per brick activation from the committed ncu summary (one capture of a
-    # 16-shot launch of the same workload), scaled to this launch's activations
+    # DRAM bytes per brick activation from the committed ncu summary of the kernel that ran
+    # (one capture of a 16-shot launch of the same workload), scaled to this launch's
+    # activations
+    kernel = "k_fim_solve8" if stats[0]["nodes_per_brick"] == 512 else "k_fim_solve"
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "k_fim_solve_config2.md")
+    tpath = os.path.join(ROOT, "profiles", f"{kernel}_config2.md")
     if os.path.exists(tpath):
         with open(tpath) as f:
             for ln in f:
@@ -544,7 +555,7 @@ def run_ours(args):
                     traffic = float(ln.split(":")[1]) * act
 
     # ---- the timed setting against the fully converged field of the same solver ---------
-    accuracy_conv = solver_accuracy(ctx, sv)
+    accuracy_conv = solver_accuracy(ctx, sv, SOLVER_RUN)
 
     # ---- the NGB operator: the reference's own Accurate_FSM sweeps, bit-exact ------------
     ngb_steps = max(1, min(args.steps, 5))
@@ -567,7 +578,7 @@ def run_ours(args):
             "data": "synthetic (seeded config-2 model, shots, windows, receivers)",
             "config": {"workload": "config2: 64 shots/GPU, 201x201x101 @12.5 m, brick-aligned windows "
                                    "60-100 % lateral, 2500 receivers, plain FIM (JW operator)",
-                       "tolerances_s": SOLVER,
+                       "tolerances_s": SOLVER, "autotuned_shape": tuned,
                        "shots_per_gpu": ns, "grid": [sv.nx, sv.ny, sv.nz], "h_m": sv.h,
                        "l2": "traveltime pool 1.1 GB > 126 MB L2 (inputs larger than L2)",
                        "parallelism": f"shot-sharded x{world}"},
@@ -576,7 +587,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": int(t_out.nbytes) if t_out is not None else 0},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_fim_solve", "kernel_ms": kern_ms,
+                         "kernel": kernel, "kernel_ms": kern_ms,
                          "alg_bytes_per_launch": alg_bytes, "activations_per_launch": act,
                          "compulsory_bytes_per_launch": compulsory,
                          "compulsory_frac": compulsory / (kern_ms / 1000.0) / 1e9 / peak},
@@ -617,9 +628,9 @@ def run_ours(args):
     return 0
 
 
-def solver_accuracy(ctx, sv):
-    """Max relative error of the timed setting against the fully converged field (any face
-    drop re-queues, exact in-brick convergence) on nodes with T >= 2h/v_max."""
+def solver_accuracy(ctx, sv, solver):
+    """Max relative error of the timed setting (solver options) against the fully converged
+    field (any face drop re-queues, exact in-brick convergence) on nodes with T >= 2h/v_max."""
     import torch
 
     ns = len(sv.shots)
@@ -628,7 +639,7 @@ def solver_accuracy(ctx, sv):
     out = torch.empty_like(ref)
     ctx.eik_solve(sv.shots, windows=sv.windows, want_recv=False, change_tol=-1.0)
     ctx.eik_volumes_to(ref.data_ptr())
-    ctx.eik_solve(sv.shots, windows=sv.windows, want_recv=False, **SOLVER)
+    ctx.eik_solve(sv.shots, windows=sv.windows, want_recv=False, **solver)
     ctx.eik_volumes_to(out.data_ptr())
     torch.cuda.synchronize()
     m = ref >= 2.0 * sv.h / float(sv.velocity.max())
@@ -991,6 +1002,10 @@ def main():
     ap.add_argument("--headline-only", action="store_true",
                     help="the config-2 headline alone (no config1/tomography/learned_warm/inversion objects)")
     ap.add_argument("--no-inversion", action="store_true", help="skip the config-5 inversion object")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="headline solve with the built-in default shape instead of the autotuned one")
+    ap.add_argument("--brick", type=int, default=0, choices=[0, 1, 2],
+                    help="headline solve with this brick shape (1: 4x4x4, 2: 8x8x8), untuned (profiling)")
     args = ap.parse_args()
     if args.warm_start:
         return run_warm_start(args)

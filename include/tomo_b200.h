@@ -69,7 +69,10 @@ typedef struct {
     int op;          /* TOMO_OP_*                                                     */
     int max_inner;   /* cap of in-brick iterations per activation (0: default 16)     */
     int max_rounds;  /* cap of outer rounds (0: default 1<<20)                        */
-    int brick;       /* brick shape: 0 or 1 = 4x4x4, the one shape of tomo_eik_brick_shapes */
+    int brick;       /* brick shape of the JW solve: TOMO_BRICK_4 (4x4x4, one warp per
+                        brick) or TOMO_BRICK_8 (8x8x8, one CTA of 8 warps per brick, each
+                        warp on one of its 4x4x4 sub-bricks; rounds schedule, no time band);
+                        0: the autotuned shape, if any, else 4x4x4                     */
     int block_warps; /* warps per CTA of the persistent kernel, 1-16 (0: default 16;
                         the asynchronous schedule uses at most 8)                     */
     int occupancy;   /* register budget of the kernel, in CTAs of 8 warps per SM, 1..6
@@ -104,6 +107,10 @@ typedef struct {
                         (0: default 2^26, i.e. seconds).  Replaces the unbounded wait of
                         block_FIM_solver's outer loop (cuda_kernel.cu:91).              */
 } tomo_eik_opts;
+
+/* Brick shapes of the JW solve (tomo_eik_opts.brick; tomo_eik_brick_shapes lists them). */
+#define TOMO_BRICK_4 1
+#define TOMO_BRICK_8 2
 
 /* Work schedules of the JW solve (same fixed point, different order of brick updates).
  * ROUNDS (default): bricks queued during a round are relaxed in the next one, rounds
@@ -216,8 +223,8 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
                           float inflate, const tomo_eik_opts *opts, tomo_eik_stats *stats,
                           tomo_seed_stats *seed_stats);
 
-/* Brick shapes the solver supports: writes up to `cap` triples (bx,by,bz) of nodes and
- * returns how many there are. */
+/* Brick shapes the solver supports, in TOMO_BRICK_* order (4x4x4, 8x8x8): writes up to
+ * `cap` triples (bx,by,bz) of nodes and returns how many there are. */
 int tomo_eik_brick_shapes(int *xyz_triples, int cap);
 
 typedef struct {
@@ -227,11 +234,12 @@ typedef struct {
 } tomo_tune_stats;
 
 /* Autotuner of the JW solve (no counterpart in the reference, whose launch shape is fixed).
- * Solves this batch (no receivers) with every launch shape -- warps per CTA {16, 8, 4},
- * CTAs per SM {3, 4, 5, 6}, in-brick iteration cap {8, 16, 32}, each brick shape of
- * tomo_eik_brick_shapes -- `repeats` times each (0: 2), then, at the fastest shape, the
- * time band at 3, 6, 9 and 12 times the slowest brick crossing (4 dx s_max; none is the
- * shape's own time) and, if a band wins, the warps x CTAs-per-SM shapes again with it.
+ * Solves this batch (no receivers) with every launch shape -- 4x4x4 bricks: warps per CTA
+ * {16, 8, 4} x CTAs per SM {3, 4, 5, 6} x in-brick iteration cap {8, 16, 32}; 8x8x8 bricks:
+ * CTAs of 8 warps per SM {2, 3, 4, 5} x cap {16, 32} -- `repeats` times each (0: 2), then,
+ * at the fastest 4x4x4 shape, the time band at 3, 6, 9 and 12 times the slowest brick
+ * crossing (4 dx s_max; none is the shape's own time) and, if a band wins, the warps x
+ * CTAs-per-SM shapes again with it.
  * Keeps the fastest in the context and writes it to *best (may be NULL).  Later solves on this context use the tuned value for every tomo_eik_opts field
  * they leave 0.  The traveltime pool holds the last trial's fields afterwards. */
 int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows,

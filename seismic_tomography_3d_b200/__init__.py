@@ -296,7 +296,7 @@ class Context:
     # -- eikonal ------------------------------------------------------------------------
     def eik_solve(self, shots, windows=None, receivers=None, want_recv=True, max_inner=0, max_rounds=0,
                   block_warps=0, op=0, occupancy=0, change_tol=0.0, inner_tol=0.0, ieee_sqrt=0,
-                  sweep_groups=0, schedule=0, time_band=0.0, spin_limit=0):
+                  sweep_groups=0, schedule=0, time_band=0.0, spin_limit=0, brick=0):
         """Batched solve.  shots (n,3) metres; windows (n,4) [x0,x1,y0,y1] nodes or None;
         receivers (m,3).  Returns (t_recv (n,m) float32 or None, stats dict)."""
         sp, ns, _s = _points(shots)
@@ -308,7 +308,7 @@ class Context:
         if receivers is not None and len(receivers):
             rp, nr, _r = _points(receivers)
         out = np.empty((ns, nr), np.float32) if (want_recv and nr) else None
-        opts = EikOpts(op, max_inner, max_rounds, 0, block_warps, occupancy, change_tol, inner_tol, ieee_sqrt,
+        opts = EikOpts(op, max_inner, max_rounds, brick, block_warps, occupancy, change_tol, inner_tol, ieee_sqrt,
                        sweep_groups, schedule, time_band, spin_limit)
         st = EikStats()
         self._check(self.lib.tomo_eik_solve(self.h, ns, sp, wp, nr, rp,
@@ -348,8 +348,8 @@ class Context:
             wp, _w = _windows(windows)
         best, st = EikOpts(), TuneStats()
         self._check(self.lib.tomo_eik_autotune(self.h, ns, sp, wp, repeats, ctypes.byref(best), ctypes.byref(st)))
-        shape = {"block_warps": best.block_warps, "occupancy": best.occupancy, "max_inner": best.max_inner,
-                 "time_band": best.time_band}
+        shape = {"brick": best.brick, "block_warps": best.block_warps, "occupancy": best.occupancy,
+                 "max_inner": best.max_inner, "time_band": best.time_band}
         return shape, {f: getattr(st, f) for f, _ in st._fields_}
 
     def volume_sizes(self, nshots, windows=None):

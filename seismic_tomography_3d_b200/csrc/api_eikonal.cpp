@@ -330,6 +330,7 @@ int tomo_ctx_destroy(tomo_ctx *ctx)
     ctx->scratch_v.release();
     ctx->T.release();
     ctx->qflag.release();
+    ctx->qflag8.release();
     ctx->lists.release();
     ctx->ctrl.release();
     ctx->stats.release();
@@ -383,10 +384,9 @@ int tomo_get_slowness(tomo_ctx *ctx, float *out)
 
 int tomo_eik_brick_shapes(int *xyz, int cap)
 {
-    if (xyz && cap >= 1) {
-        xyz[0] = xyz[1] = xyz[2] = tomo::kBrick;
-    }
-    return 1;
+    const int edge[2] = {tomo::kBrick, 2 * tomo::kBrick};  // TOMO_BRICK_4, TOMO_BRICK_8
+    for (int i = 0; i < 2 && xyz && i < cap; i++) xyz[3 * i] = xyz[3 * i + 1] = xyz[3 * i + 2] = edge[i];
+    return 2;
 }
 
 }  // extern "C"
@@ -401,6 +401,7 @@ struct SolveCfg {
     bool async;  // asynchronous schedule, else rounds (default)
     float time_band;  // rounds schedule: time-band ordering (s), 0 = off
     unsigned long long spin_limit;  // polls of a device-side wait before it gives up
+    bool brick8;      // 8^3 bricks (one CTA per 2 x 2 x 2 group of storage bricks)
 };
 
 SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
@@ -436,6 +437,11 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     c.time_band = band > 0.f ? band : (band < 0.f ? 0.f : ctx->tuned_time_band);
     if (c.async) c.time_band = 0.f;
     c.spin_limit = (opts && opts->spin_limit > 0) ? opts->spin_limit : kSpinLimit;
+    // Brick shape: 4^3 unless asked for (or tuned to) 8^3.  The 8^3 kernel runs the rounds
+    // schedule without the time band.
+    const int brick = (opts && opts->brick > 0) ? opts->brick : ctx->tuned_brick;
+    c.brick8 = brick == TOMO_BRICK_8 && !c.async;
+    if (c.brick8) c.time_band = 0.f;
     // Banded solves carry more live state (spills at 64 registers): untuned, they run as
     // 3 CTAs x 8 warps at 80 registers, 1.15x faster than the plain default shape on the
     // config-5 starting model (504 vs 581 ms) and equal on config 3.
@@ -452,6 +458,7 @@ struct Batch {
     long long t_total = 0;            // traveltime pool (floats)
     long long v_total = 0;            // all window volumes back to back (floats)
     unsigned long long q_total = 0;   // bricks
+    unsigned long long q_total8 = 0;  // 8^3 groups
     unsigned local_bits = 1;
 };
 
@@ -495,6 +502,9 @@ int make_batch(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_wi
         d.t_off = bt.t_total;
         d.qbase = bt.q_total;
         d.v_off = bt.v_total;
+        tomo::set_brick8(d);
+        d.qbase8 = bt.q_total8;
+        bt.q_total8 += (unsigned long long)d.gbz8 * d.gbx8 * d.gby8;
         bt.t_total += nb * tomo::kBrickNodes;
         bt.q_total += (unsigned long long)nb;
         bt.v_total += (long long)g.nz * d.wnx * d.wny;
@@ -520,6 +530,7 @@ int upload_batch(tomo_ctx *ctx, const Batch &bt, int nrec, const tomo_point *rec
     const int nshots = (int)bt.sd.size();
     CK(ctx->T.ensure((size_t)bt.t_total));
     CK(ctx->qflag.ensure((size_t)bt.q_total));
+    CK(ctx->qflag8.ensure((size_t)bt.q_total8));
     CK(ctx->lists.ensure((size_t)bt.q_total * 3));
     CK(ctx->shots_d.ensure((size_t)nshots));
     if (nrec > 0) {
@@ -546,9 +557,9 @@ tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, in
     p.T = ctx->T.ptr;
     p.shots = ctx->shots_d.ptr;
     p.nshots = (int)bt.sd.size();
-    p.qflag = ctx->qflag.ptr;
+    p.qflag = c.brick8 ? ctx->qflag8.ptr : ctx->qflag.ptr;
     p.lists = ctx->lists.ptr;
-    p.list_cap = (unsigned)bt.q_total;
+    p.list_cap = (unsigned)(c.brick8 ? bt.q_total8 : bt.q_total);
     p.ctrl = ctx->ctrl.ptr;
     p.stats = ctx->stats.ptr;
     p.gbx = ctx->gbx;
@@ -600,6 +611,30 @@ cudaError_t band_reset(tomo_ctx *ctx, const tomo::FimLaunch &p)
     e = cudaMemsetAsync(p.park_cnt, 0, (size_t)(p.park_rounds + 2) * sizeof(unsigned), ctx->stream);
     if (e != cudaSuccess) return e;
     return cudaMemsetAsync(p.band_min, 0xff, (size_t)3 * p.nshots * sizeof(unsigned), ctx->stream);
+}
+
+// Enqueues the pool reset, the source seeds and the persistent JW solve of a batch (4^3 or
+// 8^3 bricks, rounds or asynchronous schedule); ev_solve (may be null) is recorded just
+// before the persistent launch.
+int enqueue_fim(tomo_ctx *ctx, const tomo::FimLaunch &p, size_t t_total, size_t q_total, const SolveCfg &c,
+                cudaEvent_t ev_solve)
+{
+    int grid = 0;
+    if (c.brick8) {
+        CK(tomo::fim_init(p.T, t_total, p.qflag, (size_t)p.list_cap, p.ctrl, p.stats, ctx->stream));
+        CK(tomo::fim_seed8(p.shots, p.nshots, p.S, p.gbx, p.gbz, p.T, p.qflag, p.lists, p.local_bits, p.ctrl,
+                           ctx->stream));
+        if (ev_solve) CK(cudaEventRecord(ev_solve, ctx->stream));
+        CK(tomo::fim_solve8(p, c.occupancy, c.ieee_sqrt, &grid, ctx->stream));
+        return TOMO_OK;
+    }
+    CK(tomo::fim_init(p.T, t_total, p.qflag, q_total, p.ctrl, p.stats, ctx->stream));
+    CK(tomo::fim_seed(p.shots, p.nshots, p.S, p.gbx, p.gbz, p.T, p.qflag, p.lists, p.local_bits, p.ctrl, ctx->stream,
+                      c.async ? 3 * (size_t)p.list_cap : 0));
+    CK(band_reset(ctx, p));
+    if (ev_solve) CK(cudaEventRecord(ev_solve, ctx->stream));
+    CK(tomo::fim_solve(p, c.block_warps, c.occupancy, c.ieee_sqrt, &grid, ctx->stream, c.async));
+    return TOMO_OK;
 }
 
 // Reads the control words and counters of the last persistent solve (synchronises).
@@ -663,6 +698,7 @@ int eik_plan(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_wind
     plan.occupancy = cfg.occupancy;
     plan.ieee_sqrt = cfg.ieee_sqrt;
     plan.async = cfg.async;
+    plan.brick8 = cfg.brick8;
     plan.t_total = (size_t)bt.t_total;
     plan.q_total = (size_t)bt.q_total;
     return TOMO_OK;
@@ -670,14 +706,13 @@ int eik_plan(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_wind
 
 int eik_enqueue(tomo_ctx *ctx, const EikPlan &plan)
 {
-    const FimLaunch &p = plan.p;
-    CK(tomo::fim_init(p.T, plan.t_total, p.qflag, plan.q_total, p.ctrl, p.stats, ctx->stream));
-    CK(tomo::fim_seed(p.shots, p.nshots, p.S, p.gbx, p.gbz, p.T, p.qflag, p.lists, p.local_bits, p.ctrl, ctx->stream,
-                      plan.async ? 3 * (size_t)p.list_cap : 0));
-    CK(band_reset(ctx, p));
-    int grid = 0;
-    CK(tomo::fim_solve(p, plan.block_warps, plan.occupancy, plan.ieee_sqrt, &grid, ctx->stream, plan.async));
-    return TOMO_OK;
+    SolveCfg c{};
+    c.block_warps = plan.block_warps;
+    c.occupancy = plan.occupancy;
+    c.ieee_sqrt = plan.ieee_sqrt;
+    c.async = plan.async;
+    c.brick8 = plan.brick8;
+    return enqueue_fim(ctx, plan.p, plan.t_total, plan.q_total, c, nullptr);
 }
 
 }  // namespace tomo
@@ -694,8 +729,10 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
     if (!ctx->have_model) return fail(ctx, TOMO_ERR_STATE, "no model set (tomo_set_velocity / tomo_set_slowness)");
     if (opts && opts->op != TOMO_OP_JW && opts->op != TOMO_OP_NGB)
         return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown eikonal operator");
-    if (opts && (opts->brick < 0 || opts->brick > 1))
-        return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown brick shape (tomo_eik_brick_shapes lists 1: 4x4x4)");
+    if (opts && (opts->brick < 0 || opts->brick > TOMO_BRICK_8))
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown brick shape (TOMO_BRICK_4 or TOMO_BRICK_8)");
+    if (opts && opts->brick == TOMO_BRICK_8 && opts->schedule == TOMO_SCHED_ASYNC)
+        return fail(ctx, TOMO_ERR_INVALID_ARG, "8x8x8 bricks run the rounds schedule only");
     if (opts && (opts->schedule < TOMO_SCHED_DEFAULT || opts->schedule > TOMO_SCHED_ASYNC))
         return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown work schedule");
     if (opts && !(std::fabs(opts->time_band) < 1e30f))
@@ -716,15 +753,9 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
         rc = launch_ngb(ctx, bt.sd, shots, nshots, nrec, opts->sweep_groups, cfg.spin_limit);
         if (rc != TOMO_OK) return rc;
     } else {
-        CK(tomo::fim_init(ctx->T.ptr, (size_t)bt.t_total, ctx->qflag.ptr, (size_t)bt.q_total, ctx->ctrl.ptr,
-                          ctx->stats.ptr, ctx->stream));
-        CK(tomo::fim_seed(ctx->shots_d.ptr, nshots, ctx->S.ptr, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
-                          ctx->lists.ptr, bt.local_bits, ctx->ctrl.ptr, ctx->stream, cfg.async ? 3 * (size_t)bt.q_total : 0));
         const tomo::FimLaunch p = fim_params(ctx, bt, cfg, nrec);
-        CK(band_reset(ctx, p));
-        int grid = 0;
-        CK(cudaEventRecord(ctx->ev[3], ctx->stream));
-        CK(tomo::fim_solve(p, cfg.block_warps, cfg.occupancy, cfg.ieee_sqrt, &grid, ctx->stream, cfg.async));
+        rc = enqueue_fim(ctx, p, (size_t)bt.t_total, (size_t)bt.q_total, cfg, ctx->ev[3]);
+        if (rc != TOMO_OK) return rc;
     }
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     if (t_recv && nrec > 0)
@@ -742,7 +773,7 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
         stats->inner_iterations = (long long)inner;
         stats->idle_activations = (long long)idle;
         stats->deferred = (long long)deferred;
-        stats->nodes_per_brick = tomo::kBrickNodes;
+        stats->nodes_per_brick = cfg.brick8 ? 8 * tomo::kBrickNodes : tomo::kBrickNodes;
         cudaEventElapsedTime(&stats->setup_ms, ctx->ev[0], ctx->ev[3]);
         cudaEventElapsedTime(&stats->solve_ms, ctx->ev[3], ctx->ev[1]);
         cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[2]);
@@ -765,6 +796,7 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
         return fail(ctx, TOMO_ERR_INVALID_ARG, "the warm-started solve runs the JW operator only");
     SolveCfg cfg = solve_cfg(ctx, opts);
     cfg.time_band = 0.f;  // keys start from the ceiling's pool: not used here
+    cfg.brick8 = false;   // the warm-started solve and its fallback run 4^3 bricks
     CK(cudaSetDevice(ctx->device));
     Batch bt;
     int rc = make_batch(ctx, nshots, shots, windows, nrec, receivers, bt);
@@ -879,12 +911,14 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
     if (repeats == 0) repeats = 2;
     // untuned defaults while timing (an earlier tuning must not leak into the trials)
     ctx->tuned_block_warps = ctx->tuned_occupancy = ctx->tuned_max_inner = 0;
+    ctx->tuned_brick = 0;
     ctx->tuned_time_band = 0.f;
     const int warps[] = {kDefaultBlockWarps, 8, 4};
     const int occs[] = {4, 5, 6, 3};
     const int inners[] = {16, 8, 32};
     tomo_eik_opts o{};
     o.op = TOMO_OP_JW;
+    o.brick = TOMO_BRICK_4;
     tomo_eik_stats st{};
     // warm-up (first launch of each kernel variant pays for module loading)
     int rc = tomo_eik_solve(ctx, nshots, shots, windows, 0, nullptr, nullptr, &o, &st);
@@ -913,7 +947,34 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
                 }
                 ++trials;
             }
-    // Then the time band at the chosen shape: multiples of the slowest brick crossing,
+    // 8^3 bricks: one CTA of 8 warps per brick, CTAs per SM {2, 3, 4, 5} (register
+    // budgets 128/80/64/48), in-brick cap {16, 32}.
+    int bbrick = TOMO_BRICK_4, bo8 = 0, bi8 = 0;
+    float best8 = 0.f;
+    {
+        tomo_eik_opts o8{};
+        o8.op = TOMO_OP_JW;
+        o8.brick = TOMO_BRICK_8;
+        for (int oc : {4, 3, 5, 2})
+            for (int in : {16, 32}) {
+                o8.occupancy = oc;
+                o8.max_inner = in;
+                float ms = 0.f;
+                for (int r = 0; r < repeats + 1; r++) {
+                    rc = tomo_eik_solve(ctx, nshots, shots, windows, 0, nullptr, nullptr, &o8, &st);
+                    if (rc != TOMO_OK) return rc;
+                    if (r == 0) continue;
+                    ms = (r == 1) ? st.solve_ms : std::min(ms, st.solve_ms);
+                }
+                if (bo8 == 0 || ms < best8) {
+                    best8 = ms;
+                    bo8 = oc;
+                    bi8 = in;
+                }
+                ++trials;
+            }
+    }
+    // Then the time band at the chosen 4^3 shape: multiples of the slowest brick crossing,
     // 4 h s_max (the band is model-relative; no band is the shape loop's own time).
     o.block_warps = bw;
     o.occupancy = bo;
@@ -970,6 +1031,14 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
                 ++trials;
             }
     }
+    if (best8 < best_ms) {  // the 8^3 shape beats every 4^3 one (with or without a band)
+        bbrick = TOMO_BRICK_8;
+        best_ms = best8;
+        bo = bo8;
+        bi = bi8;
+        bb = 0.f;
+    }
+    ctx->tuned_brick = bbrick;
     ctx->tuned_block_warps = bw;
     ctx->tuned_occupancy = bo;
     ctx->tuned_max_inner = bi;
@@ -977,6 +1046,7 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
     if (best) {
         *best = tomo_eik_opts{};
         best->op = TOMO_OP_JW;
+        best->brick = bbrick;
         best->block_warps = bw;
         best->occupancy = bo;
         best->max_inner = bi;

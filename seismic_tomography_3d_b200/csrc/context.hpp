@@ -65,6 +65,7 @@ struct tomo_ctx {
     // last eikonal solve
     tomo::DevBuf<float> T;
     tomo::DevBuf<unsigned> qflag, lists, ctrl;
+    tomo::DevBuf<unsigned> qflag8;  // queue flags of the 8^3 groups (TOMO_BRICK_8 solves)
     tomo::DevBuf<unsigned> fim_keys, band_min, band_park, band_pcnt;  // time-band ordering (per brick keys,
                                                                       // per-shot minima, parking lists, counts)
     tomo::DevBuf<unsigned> tune_word;            // autotuner scratch (largest slowness)
@@ -86,6 +87,7 @@ struct tomo_ctx {
     bool have_solve = false;
     // launch shape chosen by tomo_eik_autotune (0: not tuned)
     int tuned_block_warps = 0, tuned_occupancy = 0, tuned_max_inner = 0;
+    int tuned_brick = 0;          // 0: none chosen (4^3); TOMO_BRICK_4 / TOMO_BRICK_8
     float tuned_time_band = 0.f;  // 0: none chosen (off)
 
     cudaEvent_t ev[8] = {};

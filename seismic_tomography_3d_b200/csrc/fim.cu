@@ -774,6 +774,273 @@ __global__ void __launch_bounds__(256, MINB) k_fim_async(FimLaunch p)
     sample_receivers(p.T, p.shots, p.nshots, p.rx, p.ry, p.rz, p.nrec, p.dx, p.dy, p.dz, p.nz, p.t_recv);
 }
 
+// -------------------------------------------------------------------------------------
+// 8^3 bricks.  A work item is a 2 x 2 x 2 group of the 4^3 storage bricks (so every other
+// reader of the traveltime pool is unchanged), relaxed by one CTA of 8 warps: warp w owns
+// the group's brick (w & 1, (w >> 1) & 1, w >> 2) in (z, x, y), two y-adjacent nodes per
+// lane as in the 4^3 kernel, and the group's 10^3 tile (the 8^3 nodes and the one-node
+// halo of its six faces) sits in shared memory.  The red-black phases are separated by
+// __syncthreads_or, which is both the barrier and the convergence vote.  Halo, face tests
+// and re-queueing are per group: a dropped node on an outer face below the neighbouring
+// halo cell queues the neighbouring group.  Groups at the far edges of a window where a
+// brick count is odd are partial; their missing bricks stay INF and are never relaxed.
+// Rounds, lists, cursors and the grid barrier are those of the 4^3 kernel.
+// -------------------------------------------------------------------------------------
+constexpr int kT8X = 12;         // tile strides, z fastest: 10 z padded to 12, then 10 x
+constexpr int kT8Y = kT8X * 10;  // the lane pattern of a phase falls in 32 distinct banks
+constexpr int kT8N = kT8Y * 10;
+constexpr unsigned kPushCap8 = 64;
+
+__device__ __forceinline__ int t8(int z, int x, int y) { return (z + 1) + kT8X * (x + 1) + kT8Y * (y + 1); }
+
+__device__ __forceinline__ void group_coords(const ShotDesc &d, unsigned g, int &gz, int &gx, int &gy)
+{
+    const unsigned tq = (unsigned)(((unsigned long long)g * d.div8z_m) >> d.div8z_sh);  // g / gbz8
+    gz = (int)(g - tq * (unsigned)d.gbz8);
+    const unsigned q2 = (unsigned)(((unsigned long long)tq * d.div8x_m) >> d.div8x_sh);  // / gbx8
+    gx = (int)(tq - q2 * (unsigned)d.gbx8);
+    gy = (int)q2;
+}
+
+// Warp 0: queues the buffered groups for round + 1 (de-duplicated by the groups' queue flags).
+__device__ __forceinline__ void flush_pushes8(const FimLaunch &p, const unsigned *pbuf, unsigned cnt, unsigned round)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned tag = round + 2u;  // "queued for round+1", offset by one so 0 = never
+    const unsigned nxt = (round + 1u) % 3u;
+    for (unsigned base = 0; base < cnt; base += 32u) {
+        bool want = false;
+        unsigned item = 0;
+        if (base + (unsigned)lane < cnt) {
+            item = pbuf[base + lane];
+            const unsigned s = item >> p.local_bits, g = item & ((1u << p.local_bits) - 1u);
+            want = atomicMax(p.qflag + p.shots[s].qbase8 + g, tag) < tag;
+        }
+        const unsigned wm = __ballot_sync(kFull, want);
+        if (wm) {
+            const int leader = __ffs(wm) - 1;
+            unsigned b0 = 0;
+            if (lane == leader) b0 = atomicAdd(p.ctrl + kCnt0 + nxt, (unsigned)__popc(wm));
+            b0 = __shfl_sync(kFull, b0, leader);
+            if (want) p.lists[(size_t)nxt * p.list_cap + b0 + __popc(wm & ((1u << lane) - 1u))] = item;
+        }
+    }
+}
+
+template <int MINB, bool kFastSqrt>
+__global__ void __launch_bounds__(256) __maxnreg__(fim_regs(MINB)) k_fim_solve8(FimLaunch p)
+{
+    __shared__ float tile[kT8N];
+    __shared__ unsigned pbuf[kPushCap8];
+    __shared__ unsigned s_face, s_next, s_pcnt;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wz = warp & 1, wx = (warp >> 1) & 1, wy = warp >> 2;
+    const int z0 = 4 * wz + (lane & 3), x0 = 4 * wx + ((lane >> 2) & 3), y0 = 4 * wy + 2 * (lane >> 4);
+    const int ti0 = t8(z0, x0, y0), ti1 = ti0 + kT8Y;  // the lane's nodes (y, y + 1)
+    const int n0 = lane_node(lane);
+    // red: z + x + y even (y0 is even); the lane's two nodes have opposite colours
+    const bool red0 = ((z0 + x0) & 1) == 0;
+    const int tA = red0 ? ti0 : ti1, tB = red0 ? ti1 : ti0;
+    const int yA = red0 ? -kT8Y : kT8Y;
+    unsigned long long act = 0, inner = 0, idle = 0;
+    if (threadIdx.x == 0) s_pcnt = 0;
+    unsigned round = 0, epoch = 0;
+    bool ok = true;
+    for (;;) {
+        const unsigned cur = round % 3u;
+        const unsigned n = ld_volatile(p.ctrl + kCnt0 + cur);
+        if (n == 0u) break;
+        if ((int)round >= p.max_rounds) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(p.ctrl + kErr, 0u, (unsigned)kDevRoundCap);
+            ok = false;
+            break;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            p.ctrl[kCnt0 + (round + 2u) % 3u] = 0u;
+            p.ctrl[kCur0 + (round + 2u) % 3u] = 0u;
+        }
+        const unsigned *list = p.lists + (size_t)cur * p.list_cap;
+        unsigned *cursor = p.ctrl + kCur0 + cur;
+        for (unsigned i = blockIdx.x; i < n;) {
+            const unsigned item = __ldcg(list + i);
+            const unsigned s = item >> p.local_bits, g = item & ((1u << p.local_bits) - 1u);
+            const ShotDesc &d = p.shots[s];
+            int gz, gx, gy;
+            group_coords(d, g, gz, gx, gy);
+            const int bz = 2 * gz + wz, bx = 2 * gx + wx, by = 2 * gy + wy;
+            const bool present = bz < d.nbz && bx < d.nbx && by < d.nby;
+            const long long b = bz + (long long)d.nbz * (bx + (long long)d.nbx * by);
+            float *Tb = p.T + d.t_off + b * kBrickNodes;
+            float s0 = 0.f, s1 = 0.f, i0 = kInf, i1 = kInf;
+            if (present) {
+                const long long gb =
+                    bz + (long long)p.gbz * ((bx + (d.wx0 >> 2)) + (long long)p.gbx * (by + (d.wy0 >> 2)));
+                s0 = __ldg(p.S + gb * kBrickNodes + n0);
+                s1 = __ldg(p.S + gb * kBrickNodes + n0 + 16);
+                i0 = __ldcg(Tb + n0);
+                i1 = __ldcg(Tb + n0 + 16);
+            }
+            tile[ti0] = i0;
+            tile[ti1] = i1;
+            // outer-face halo next to this warp's brick: slot 0 -- lanes 0-15 axis z, 16-31
+            // axis x; slot 1 -- lanes 0-15 axis y (one face node each)
+#pragma unroll
+            for (int slot = 0; slot < 2; slot++) {
+                const int q = slot == 0 ? (lane >> 4) : 2;
+                if (slot == 1 && lane >= 16) break;
+                const int j = lane & 15, u = j & 3, v = j >> 2;
+                const bool lower = (q == 0 ? wz : q == 1 ? wx : wy) == 0;
+                int node, ti;
+                long long nb = -1;
+                if (q == 0) {
+                    node = (lower ? 3 : 0) + 4 * u + 16 * v;
+                    ti = t8(lower ? -1 : 8, 4 * wx + u, 4 * wy + v);
+                    if (present && (lower ? bz > 0 : bz < d.nbz - 1)) nb = b + (lower ? -1 : 1);
+                } else if (q == 1) {
+                    node = u + (lower ? 12 : 0) + 16 * v;
+                    ti = t8(4 * wz + u, lower ? -1 : 8, 4 * wy + v);
+                    if (present && (lower ? bx > 0 : bx < d.nbx - 1)) nb = b + (lower ? -d.nbz : d.nbz);
+                } else {
+                    node = u + 4 * v + (lower ? 48 : 0);
+                    ti = t8(4 * wz + u, 4 * wx + v, lower ? -1 : 8);
+                    const long long sy = (long long)d.nbz * d.nbx;
+                    if (present && (lower ? by > 0 : by < d.nby - 1)) nb = b + (lower ? -sy : sy);
+                }
+                tile[ti] = nb >= 0 ? __ldcg(p.T + d.t_off + nb * kBrickNodes + node) : kInf;
+            }
+            if (threadIdx.x == 0) s_face = 0u;
+            __syncthreads();  // the tile
+
+            float cA = red0 ? i0 : i1, cB = red0 ? i1 : i0;
+            const NodeConst kA = node_const(p.h, red0 ? s0 : s1), kB = node_const(p.h, red0 ? s1 : s0);
+            bool more = true;
+            int it = 0;
+            for (; it < p.max_inner; ++it) {
+                bool chA = false;
+                if (present) {
+                    const float aA = fminf(tile[tA - kT8X], tile[tA + kT8X]);
+                    const float gA = fminf(tile[tA - 1], tile[tA + 1]);
+                    const float bA = fminf(tile[tA + yA], cB);
+                    const float nA = fminf(cA, godunov_jw<kFastSqrt, false>(aA, bA, gA, kA));
+                    tile[tA] = nA;
+                    chA = nA < cA - p.inner_tol;
+                    cA = nA;
+                }
+                if (!__syncthreads_or(chA) && it > 0) {
+                    more = false;
+                    ++it;
+                    break;
+                }
+                bool chB = false;
+                if (present) {
+                    const float aB = fminf(tile[tB - kT8X], tile[tB + kT8X]);
+                    const float gB = fminf(tile[tB - 1], tile[tB + 1]);
+                    const float bB = fminf(tile[tB - yA], cA);
+                    const float nB = fminf(cB, godunov_jw<kFastSqrt, false>(aB, bB, gB, kB));
+                    tile[tB] = nB;
+                    chB = nB < cB - p.inner_tol;
+                    cB = nB;
+                }
+                if (!__syncthreads_or(chB)) {
+                    more = false;
+                    ++it;
+                    break;
+                }
+            }
+            // the next item's cursor atomic overlaps the epilogue
+            if (threadIdx.x == 0) s_next = atomicAdd(cursor, 1u);
+            const float c0 = red0 ? cA : cB, c1 = red0 ? cB : cA;
+            const bool drop = present && ((c0 < i0) | (c1 < i1));
+            if (present && __any_sync(kFull, drop)) {
+                __stcg(Tb + n0, c0);
+                __stcg(Tb + n0 + 16, c1);
+            }
+            // outer faces of the group (1 z-, 2 z+, 4 x-, 8 x+, 16 y-, 32 y+): a node that
+            // dropped by more than change_tol below the neighbouring halo cell
+            const bool d0 = present && c0 < i0 - p.change_tol, d1 = present && c1 < i1 - p.change_tol;
+            unsigned fl = 0;
+            if (z0 == 0 && ((d0 && c0 < tile[ti0 - 1]) || (d1 && c1 < tile[ti1 - 1]))) fl |= 1u;
+            if (z0 == 7 && ((d0 && c0 < tile[ti0 + 1]) || (d1 && c1 < tile[ti1 + 1]))) fl |= 2u;
+            if (x0 == 0 && ((d0 && c0 < tile[ti0 - kT8X]) || (d1 && c1 < tile[ti1 - kT8X]))) fl |= 4u;
+            if (x0 == 7 && ((d0 && c0 < tile[ti0 + kT8X]) || (d1 && c1 < tile[ti1 + kT8X]))) fl |= 8u;
+            if (y0 == 0 && d0 && c0 < tile[ti0 - kT8Y]) fl |= 16u;
+            if (y0 == 6 && d1 && c1 < tile[ti1 + kT8Y]) fl |= 32u;
+            fl = __reduce_or_sync(kFull, fl);
+            if (lane == 0 && fl) atomicOr(&s_face, fl);
+            const int any_drop = __syncthreads_or(drop);  // also publishes s_face and s_next
+            if (warp == 0) {
+                bool want = false;
+                unsigned tgt = g;
+                if (lane < 6) {
+                    const int axis = lane >> 1;
+                    const bool up = lane & 1;
+                    const int c = axis == 0 ? gz : (axis == 1 ? gx : gy);
+                    const int nmax = axis == 0 ? d.gbz8 : (axis == 1 ? d.gbx8 : d.gby8);
+                    const unsigned stride = axis == 0 ? 1u : (axis == 1 ? (unsigned)d.gbz8 : (unsigned)(d.gbz8 * d.gbx8));
+                    want = ((s_face >> lane) & 1u) && (up ? c < nmax - 1 : c > 0);
+                    tgt = up ? g + stride : g - stride;
+                } else if (lane == 6) {
+                    want = more;
+                }
+                const unsigned wm = __ballot_sync(kFull, want);
+                unsigned pc = s_pcnt;
+                if (want) pbuf[pc + __popc(wm & ((1u << lane) - 1u))] = (s << p.local_bits) | tgt;
+                pc += __popc(wm);
+                __syncwarp();
+                if (pc > kPushCap8 - 7u) {
+                    flush_pushes8(p, pbuf, pc, round);
+                    pc = 0;
+                }
+                if (lane == 0) {
+                    s_pcnt = pc;
+                    act += 1;
+                    inner += (unsigned long long)it;
+                    if (!any_drop) idle += 1;
+                }
+                __syncwarp();
+            }
+            const unsigned next = s_next;
+            __syncthreads();  // the tile, s_face and s_next are reused by the next item
+            i = gridDim.x + next;
+        }
+        if (warp == 0) {
+            const unsigned pc = s_pcnt;
+            if (pc) flush_pushes8(p, pbuf, pc, round);
+            __syncwarp();
+            if (lane == 0) s_pcnt = 0;
+        }
+        if (!grid_sync(p.ctrl, epoch, p.spin_limit)) {
+            ok = false;
+            break;
+        }
+        ++round;
+    }
+    if (threadIdx.x == 0 && act) {
+        atomicAdd(p.stats + 0, act);
+        atomicAdd(p.stats + 1, inner);
+        atomicAdd(p.stats + 3, idle);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kRounds] = round;
+    if (!ok || p.nrec == 0) return;
+    sample_receivers(p.T, p.shots, p.nshots, p.rx, p.ry, p.rz, p.nrec, p.dx, p.dy, p.dz, p.nz, p.t_recv);
+}
+
+__global__ void k_fim_seed8(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
+                            unsigned *qflag8, unsigned *lists, unsigned local_bits, unsigned *ctrl)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nshots) {
+        const ShotDesc d = shots[s];
+        const int bz = d.src_brick % d.nbz, t = d.src_brick / d.nbz;
+        const int bx = t % d.nbx, by = t / d.nbx;
+        const long long gb = bz + (long long)gbz * ((bx + (d.wx0 >> 2)) + (long long)gbx * (by + (d.wy0 >> 2)));
+        T[d.t_off + (long long)d.src_brick * kBrickNodes + d.src_node] = __fmul_rn(S[gb * kBrickNodes + d.src_node], d.src_dist);
+        qflag8[d.qbase8 + d.src_brick8] = 1u;
+        lists[s] = ((unsigned)s << local_bits) | (unsigned)d.src_brick8;
+    }
+    if (s == 0) ctrl[kCnt0] = (unsigned)nshots;
+}
+
 __global__ void k_receivers(const float *T, const ShotDesc *shots, int nshots, const float *rx, const float *ry,
                             const float *rz, int nrec, float dx, float dy, float dz, int nz, float *t_recv)
 {
@@ -1104,6 +1371,49 @@ cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, bool i
     if (block_warps < 1 || block_warps > 16) block_warps = 16;
     return ieee_sqrt ? solve_occ<false>(p, block_warps, occupancy, async, grid_out, st)
                      : solve_occ<true>(p, block_warps, occupancy, async, grid_out, st);
+}
+
+template <int MINB, bool kFastSqrt>
+static cudaError_t launch_solve8(const FimLaunch &p, int *grid_out, cudaStream_t st)
+{
+    const void *fn = (const void *)k_fim_solve8<MINB, kFastSqrt>;
+    int dev = 0, nsm = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const int grid = nsm * per_sm;
+    if (grid_out) *grid_out = grid;
+    FimLaunch pp = p;
+    void *args[] = {&pp};
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(256), args, 0, st);
+}
+
+template <bool kFastSqrt>
+static cudaError_t solve8_occ(const FimLaunch &p, int occupancy, int *grid_out, cudaStream_t st)
+{
+    switch (occupancy) {
+    case 2: return launch_solve8<2, kFastSqrt>(p, grid_out, st);
+    case 3: return launch_solve8<3, kFastSqrt>(p, grid_out, st);
+    case 5: return launch_solve8<5, kFastSqrt>(p, grid_out, st);
+    case 6: return launch_solve8<6, kFastSqrt>(p, grid_out, st);
+    default: return launch_solve8<4, kFastSqrt>(p, grid_out, st);
+    }
+}
+
+cudaError_t fim_solve8(const FimLaunch &p, int occupancy, bool ieee_sqrt, int *grid_out, cudaStream_t st)
+{
+    return ieee_sqrt ? solve8_occ<false>(p, occupancy, grid_out, st) : solve8_occ<true>(p, occupancy, grid_out, st);
+}
+
+cudaError_t fim_seed8(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T, unsigned *qflag8,
+                      unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st)
+{
+    k_fim_seed8<<<(nshots + 127) / 128, 128, 0, st>>>(shots, nshots, S, gbx, gbz, T, qflag8, lists, local_bits, ctrl);
+    return cudaGetLastError();
 }
 
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out, cudaStream_t st)

@@ -26,6 +26,14 @@ struct ShotDesc {
     // (n * m) >> sh, exact for every n below 2^local_bits (set by set_brick_division).
     unsigned long long divz_m, divx_m;
     unsigned divz_sh, divx_sh;
+    // 8^3 bricks (TOMO_BRICK_8): 2 x 2 x 2 groups of the 4^3 storage bricks, the last ones
+    // partial where nbz, nbx or nby is odd.  Their grid, the group holding the source, the
+    // offset of the shot's groups in the group queue flags, and the division constants.
+    int gbz8, gbx8, gby8;
+    int src_brick8;
+    unsigned long long qbase8;
+    unsigned long long div8z_m, div8x_m;
+    unsigned div8z_sh, div8x_sh;
 };
 
 // Multiply-shift constants for an exact n / d over 0 <= n < 2^nbits (nbits <= 31): with
@@ -40,11 +48,25 @@ inline void fastdiv_consts(unsigned d, unsigned nbits, unsigned long long &m, un
     m = ((1ull << sh) + d - 1) / d;
 }
 
-// Fills a descriptor's division constants once nbz, nbx and the batch's local_bits are set.
+// Fills a descriptor's division constants once nbz, nbx (and the 8^3 grid) and the batch's
+// local_bits are set.
 inline void set_brick_division(ShotDesc &d, unsigned local_bits)
 {
     fastdiv_consts((unsigned)d.nbz, local_bits, d.divz_m, d.divz_sh);
     fastdiv_consts((unsigned)d.nbx, local_bits, d.divx_m, d.divx_sh);
+    fastdiv_consts((unsigned)(d.gbz8 > 0 ? d.gbz8 : 1), local_bits, d.div8z_m, d.div8z_sh);
+    fastdiv_consts((unsigned)(d.gbx8 > 0 ? d.gbx8 : 1), local_bits, d.div8x_m, d.div8x_sh);
+}
+
+// The 8^3 group grid of a shot and the group holding its source brick.
+inline void set_brick8(ShotDesc &d)
+{
+    d.gbz8 = (d.nbz + 1) / 2;
+    d.gbx8 = (d.nbx + 1) / 2;
+    d.gby8 = (d.nby + 1) / 2;
+    const int bz = d.src_brick % d.nbz, t = d.src_brick / d.nbz;
+    const int bx = t % d.nbx, by = t / d.nbx;
+    d.src_brick8 = (bz >> 1) + d.gbz8 * ((bx >> 1) + d.gbx8 * (by >> 1));
 }
 
 struct FimLaunch {
@@ -97,6 +119,11 @@ cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx,
 // async: the asynchronous schedule (seeded with ring_cap = list_cap), else rounds.
 cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, bool ieee_sqrt, int *grid_out,
                       cudaStream_t st, bool async = false);
+// 8^3 bricks, rounds schedule: work items are (shot, 8^3 group); p.qflag / p.list_cap are
+// the group queue flags and count; seeded by fim_seed8.  One CTA of 8 warps per group.
+cudaError_t fim_solve8(const FimLaunch &p, int occupancy, bool ieee_sqrt, int *grid_out, cudaStream_t st);
+cudaError_t fim_seed8(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
+                      unsigned *qflag8, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st);
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out,
                         cudaStream_t st);
 cudaError_t velocity_to_slowness(const float *v, float *s, size_t n, cudaStream_t st);

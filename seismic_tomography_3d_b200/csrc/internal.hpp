@@ -34,7 +34,7 @@ int update_enqueue_v(tomo_ctx *ctx, const tomo_update_opts *opts, float *velocit
 struct EikPlan {
     FimLaunch p;
     int block_warps, occupancy;
-    bool ieee_sqrt, async;
+    bool ieee_sqrt, async, brick8;
     size_t t_total, q_total;
 };
 int eik_plan(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_window *windows, int nrec,

@@ -33,13 +33,20 @@ def solve_oracle(oracle_mod, v, h, shot, window=None):
     return T
 
 
+BRICKS = {"4^3": 1, "8^3": 2}  # TOMO_BRICK_4, TOMO_BRICK_8
+
+
+@pytest.mark.parametrize("brick", sorted(BRICKS))
 @pytest.mark.parametrize("dims", [(13, 11, 9), (16, 16, 16), (21, 17, 10), (33, 29, 18)])
-def test_single_shot_matches_oracle(tomo, oracle_mod, dims):
+def test_single_shot_matches_oracle(tomo, oracle_mod, dims, brick):
+    """Both brick shapes; odd brick counts (13 x 11 x 9 pads to 4 x 3 x 3 bricks) leave
+    partial 8^3 groups at the far edges."""
     nx, ny, nz = dims
     sv = wl.small(sum(dims), nx, ny, nz, nshots=1)
     with tomo.Context(nx, ny, nz, sv.h) as ctx:
         ctx.set_velocity(sv.velocity)
-        ctx.eik_solve(sv.shots)
+        _, st = ctx.eik_solve(sv.shots, brick=BRICKS[brick])
+        assert st["nodes_per_brick"] == (64 if brick == "4^3" else 512)
         T = ctx.eik_volume(0)
     Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, sv.shots[0])
     assert T.shape == Tref.shape
@@ -121,6 +128,26 @@ def test_receivers_bit_exact_vs_oracle_trilinear(tomo, oracle_mod):
             T = ctx.eik_volume(i)
             ref = oracle_mod.first_arrival(T, sv.h, rec[:, 0], rec[:, 1], rec[:, 2])
             np.testing.assert_array_equal(t_recv[i], ref)
+
+
+@pytest.mark.parametrize("tol", [{}, dict(change_tol=1e-5, inner_tol=1e-6)], ids=["default", "timed"])
+def test_brick8_windowed_batch_matches_oracle(tomo, oracle_mod, tol):
+    """8^3 bricks on a windowed batch (windows of any brick-aligned origin, so groups start
+    at odd bricks of the model) with receivers: every shot against the oracle on its cropped
+    window, and the receiver times against the 4^3 solve's at the same tolerances."""
+    sv = wl.small(57, 52, 44, 26, nshots=6, windows=True, nrec=24)
+    with tomo.Context(sv.nx, sv.ny, sv.nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        t4, _ = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, brick=1, **tol)
+        t8, st = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, brick=2, **tol)
+        assert st["activations"] > 0 and st["nodes_per_brick"] == 512
+        for i, sh in enumerate(sv.shots):
+            Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, sh, sv.windows[i])
+            assert rel_err(ctx.eik_volume(i), Tref, sv.h, sv.velocity.max()) < REL_TOL
+    fin = t4 < 1e5
+    assert np.array_equal(fin, t8 < 1e5)
+    m = fin & (t4 >= 2.0 * sv.h / float(sv.velocity.max()))
+    np.testing.assert_allclose(t8[m], t4[m], rtol=REL_TOL)
 
 
 def test_repeat_runs_agree(tomo):
@@ -205,9 +232,11 @@ def test_autotune_picks_a_shape_and_keeps_results(tomo):
         ctx.eik_solve(sv.shots, windows=sv.windows)
         ref = [ctx.eik_volume(i) for i in range(len(sv.shots))]
         shape, st = ctx.eik_autotune(sv.shots, windows=sv.windows, repeats=1)
-        # 36 launch shapes, 4 time bands, and the 12 warps x occupancy shapes again if a band won
-        assert st["trials"] == (52 if shape["time_band"] > 0 else 40)
-        assert shape["block_warps"] in (4, 8, 16) and shape["occupancy"] in (3, 4, 5, 6)
+        # 36 + 8 launch shapes (4^3, 8^3), 4 time bands, and the 12 warps x occupancy shapes
+        # again if a band won
+        assert st["trials"] in (48, 60)
+        assert shape["brick"] in (1, 2)
+        assert shape["block_warps"] in (4, 8, 16) and shape["occupancy"] in (2, 3, 4, 5, 6)
         assert shape["max_inner"] in (8, 16, 32)
         assert shape["time_band"] >= 0.0
         assert 0 < st["best_ms"] <= st["default_ms"]
