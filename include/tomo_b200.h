@@ -83,8 +83,14 @@ typedef struct {
     float inner_tol; /* in-brick relaxation stops when no node drops by more than this
                         (s).  <= 0: exact (default)                                  */
     int ieee_sqrt;   /* 1: IEEE sqrtf in the local update; 0 (default): sqrt.approx  */
-    int sweep_groups;/* TOMO_OP_NGB: independent block groups sweeping their own shots
-                        (0: default)                                                  */
+    int sweep_groups;/* TOMO_OP_NGB schedule.  0 (default): tile wavefront -- one warp
+                        per 16x8x8 tile of a sweep in shared memory, tiles in diagonal
+                        order behind their upwind tiles, one grid barrier per sweep;
+                        batches with a source on the last node of its window along an
+                        axis take the plane schedule.  > 0: the diagonal-plane schedule
+                        (a barrier per plane) with that many independent block groups
+                        sweeping their own shots.  Both are bit-exact with the reference
+                        where every source lies off the far faces of its window.        */
     int schedule;    /* TOMO_OP_JW work schedule: TOMO_SCHED_DEFAULT, TOMO_SCHED_ROUNDS,
                         TOMO_SCHED_ASYNC                                              */
     float time_band; /* ROUNDS schedule, time-band ordering (s).  Every push carries the

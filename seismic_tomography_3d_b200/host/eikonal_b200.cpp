@@ -62,6 +62,16 @@ void Eikonal_B200::set_parameters()
     // about 0.2 s; absent or empty keeps it off.
     const std::string band = catch_parameter("eikonal_time_band", parameters);
     time_band = band.empty() ? 0.f : std::stof(band);
+    // Optional: the local operator.  "fim" (default) is Block_FIM's Jeong-Whitaker update;
+    // "fsm" runs Accurate_FSM's Noble-Gesret-Belayouni sweeps on the device, bit for bit,
+    // and names the outputs as Accurate_FSM does (fsm_*), so that its results can stand in
+    // for those of the reference's eikonal_type = 2.
+    const std::string op = catch_parameter("eikonal_operator", parameters);
+    if (op == "fsm")
+        ngb = true;
+    else if (!op.empty() && op != "fim")
+        throw std::invalid_argument("eikonal_operator must be fim or fsm");
+    if (ngb) name = "fsm";
 
     export_time_volume = str2bool(catch_parameter("export_time_volume", parameters));
     export_first_arrival = str2bool(catch_parameter("export_first_arrival", parameters));
@@ -99,7 +109,9 @@ void Eikonal_B200::info_message()
     std::cout << "Shot " << shot_id + 1 << " of " << total_shots << "\n";
     std::cout << "Position (x,y,z) = (" << shots->x[shot_id] << ", " << shots->y[shot_id] << ", " << shots->z[shot_id]
               << ") m\n\n";
-    std::cout << "Solving eikonal equation with the Jeong & Whitaker (2008) formulation, batched on B200\n\n";
+    std::cout << (ngb ? "Solving eikonal equation with the Noble, Gesret and Belayouni (2014) formulation, "
+                        "batched on B200\n\n"
+                      : "Solving eikonal equation with the Jeong & Whitaker (2008) formulation, batched on B200\n\n");
 }
 
 void Eikonal_B200::solve_batch()
@@ -108,7 +120,8 @@ void Eikonal_B200::solve_batch()
     for (int i = 0; i < total_shots; i++) sp[(size_t)i] = tomo_point{shots->x[i], shots->y[i], shots->z[i]};
     for (int i = 0; i < total_nodes; i++) rp[(size_t)i] = tomo_point{nodes->x[i], nodes->y[i], nodes->z[i]};
     recv_times.assign((size_t)total_shots * total_nodes, 0.0f);
-    tomo_eik_opts opts{};  // defaults (JW operator), plus the optional time band
+    tomo_eik_opts opts{};  // defaults, plus the optional operator and time band
+    opts.op = ngb ? TOMO_OP_NGB : TOMO_OP_JW;
     opts.time_band = time_band;
     check(tomo_eik_solve(ctx, total_shots, sp.data(), nullptr, total_nodes, rp.data(), recv_times.data(), &opts,
                          nullptr),

@@ -28,6 +28,7 @@ protected:
     tomo_ctx *ctx = nullptr;
     bool batch_ready = false;
     float time_band = 0.f;  // optional key eikonal_time_band (s): time-band ordering, 0 = off
+    bool ngb = false;       // optional key eikonal_operator = fsm: Accurate_FSM's operator
     bool geometry_ready = false;
     int shots_type = 0, nodes_type = 0;  // 0 Regular, 1 Circular: deleted as that type (the
                                          // reference's Geometry has no virtual destructor)

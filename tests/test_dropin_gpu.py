@@ -124,6 +124,37 @@ def test_eikonal_and_tomography_executables(tomo, tmp_path):
     assert il.size == nx * ny * nz and il.sum() > 0
 
 
+def test_tomography_executable_matches_reference_run(tomo, tmp_path):
+    """tomography_b200 with eikonal_operator = fsm (Accurate_FSM's operator, bit for bit on
+    the device) on the inputs of the golden reference run (tomo_ref.npz: the reference's own
+    tomography.exe, eikonal_type 2, one iteration; the picks are the reference FSM's): the
+    recovered model against the reference's fsm_model_iteration_1.bin within the 0.5 % RMS
+    bound (the CGLS here reduces in FP64 where the reference accumulates in FP32), and the
+    convergence file against the reference's."""
+    g = np.load(os.path.join(HERE, "golden", "tomo_ref.npz"))
+    t = mg.TOMO
+    d = str(tmp_path)
+    for sub in ("tt", "fa", "picks", "conv", "models", "run", "outputs/illumination"):
+        os.makedirs(os.path.join(d, sub), exist_ok=True)
+    g["start_v"].tofile(os.path.join(d, "start.bin"))
+    nodes = g["nodes"]
+    for i in range(len(g["shots"])):
+        g["dobs"][i].astype(np.float32).tofile(os.path.join(d, "picks", f"obsData_{len(nodes)}_samples_shot_{i + 1}.bin"))
+    params = write_params(d, t, extra="eikonal_operator = fsm\n")
+    exe = os.path.join(os.path.dirname(tomo.LIB_PATH), "tomography_b200")
+    r = subprocess.run([exe, params], cwd=os.path.join(d, "run"), capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    nz, nx, ny = t["nz"], t["nx"], t["ny"]
+    model = np.fromfile(os.path.join(d, "models", "fsm_model_iteration_1.bin"), np.float32).reshape(ny, nx, nz)
+    ref = g["model_iter1"].astype(np.float64)
+    rms = float(np.sqrt(np.mean(((model - ref) / ref) ** 2)))
+    upd = float(np.linalg.norm(model - ref) / np.linalg.norm(ref - g["start_v"]))
+    print(f"\ndrop-in vs reference tomography.exe: model RMS rel {rms:.2e}, update rel L2 {upd:.2e}")
+    assert rms <= 5e-3
+    conv = np.loadtxt(os.path.join(d, "conv", "fsm_convergency.txt"))
+    np.testing.assert_allclose(conv, g["convergency"], rtol=1e-4)
+
+
 def test_wrong_eikonal_type_is_an_error(tomo, tmp_path):
     t = mg.TOMO
     p = write_params(str(tmp_path), t).replace("", "")
