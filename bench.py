@@ -856,7 +856,7 @@ def learned_warm_object(fields, epochs):
                                   if rel.numel() < 16_000_000 else None,
                                   "frac_below_truth_by_2pct": float((rel < -0.02).float().mean())},
             "training": {k: v for k, v in summ.items() if k != "history"}, "history": summ["history"],
-            "data": {"fields": args.fields, "tile": [64, 64, 64], "h_m": 12.5,
+            "data": {"fields": fields, "epochs": epochs, "tile": [64, 64, 64], "h_m": 12.5,
                      "models": "seeded random: 3-6 dipping layers 1500-4500 m/s, 0-12 Gaussian anomalies +-15 %",
                      "generation_s": gen_s, "generation_solve_ms": gen_solve_ms},
             "wall_s": time.perf_counter() - t0}
