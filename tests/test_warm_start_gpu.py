@@ -71,11 +71,12 @@ def test_ceiling_below_truth_falls_back(case):
 
     sv, ctx, plain, t_plain, _, dev, sizes = case
     low = dev.clone()
-    # shot 1's ceiling 5 % below the truth: must be detected and solved again from INF
+    # shot 1's ceiling 5 % below the truth (3 % after the 2 % inflation): detected and solved
+    # again from INF; shots 0 and 2 (exact fields x 1.02, upper bounds) are accepted
     off = sizes[0]
     low[off:off + sizes[1]] *= 0.95
     torch.cuda.synchronize()
-    t, st, ss = ctx.eik_solve_seeded(sv.shots, low.data_ptr(), 0.0, windows=sv.windows, receivers=sv.receivers)
+    t, st, ss = ctx.eik_solve_seeded(sv.shots, low.data_ptr(), 0.02, windows=sv.windows, receivers=sv.receivers)
     assert ss["violations"] > 0 and ss["stuck"] > 0
     assert ss["shots_fallback"] == 1
     check_equal(ctx, sv, plain)
