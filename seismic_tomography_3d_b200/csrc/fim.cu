@@ -833,8 +833,6 @@ __global__ void __launch_bounds__(256) __maxnreg__(fim_regs(MINB)) k_fim_solve8(
     __shared__ float tile[kT8N];
     __shared__ unsigned pbuf[kPushCap8];
     __shared__ unsigned s_face, s_next, s_pcnt;
-    // per warp (sub-brick): did its last red (A) / black (B) phase change a node
-    __shared__ unsigned char s_chgA[8], s_chgB[8];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wz = warp & 1, wx = (warp >> 1) & 1, wy = warp >> 2;
     const int z0 = 4 * wz + (lane & 3), x0 = 4 * wx + ((lane >> 2) & 3), y0 = 4 * wy + 2 * (lane >> 4);
@@ -915,47 +913,34 @@ __global__ void __launch_bounds__(256) __maxnreg__(fim_regs(MINB)) k_fim_solve8(
 
             float cA = red0 ? i0 : i1, cB = red0 ? i1 : i0;
             const NodeConst kA = node_const(p.h, red0 ? s0 : s1), kB = node_const(p.h, red0 ? s1 : s0);
-            // After the first full iteration a sub-brick relaxes a phase only if its own
-            // other-colour nodes or those of its three neighbours in the group (warps w ^ 1,
-            // w ^ 2, w ^ 4) changed in the previous phase: the outer halo is fixed during the
-            // activation, so otherwise the phase would reproduce its values.  Idle warps
-            // leave the SM's issue slots to other CTAs while the front crosses the group.
             bool more = true;
             int it = 0;
             for (; it < p.max_inner; ++it) {
-                bool chA = false, anyA = false;
-                if (present && (it == 0 || (s_chgB[warp] | s_chgB[warp ^ 1] | s_chgB[warp ^ 2] | s_chgB[warp ^ 4]))) {
+                bool chA = false;
+                if (present) {
                     const float aA = fminf(tile[tA - kT8X], tile[tA + kT8X]);
                     const float gA = fminf(tile[tA - 1], tile[tA + 1]);
                     const float bA = fminf(tile[tA + yA], cB);
                     const float nA = fminf(cA, godunov_jw<kFastSqrt, false>(aA, bA, gA, kA));
                     tile[tA] = nA;
                     chA = nA < cA - p.inner_tol;
-                    anyA = nA < cA;
                     cA = nA;
                 }
-                // the activity flag records any change (one below inner_tol still changes the
-                // inputs of the neighbours); the convergence vote uses the tolerance
-                const bool wA = __any_sync(kFull, anyA);
-                if (lane == 0) s_chgA[warp] = wA;
                 if (!__syncthreads_or(chA) && it > 0) {
                     more = false;
                     ++it;
                     break;
                 }
-                bool chB = false, anyB = false;
-                if (present && (it == 0 || (s_chgA[warp] | s_chgA[warp ^ 1] | s_chgA[warp ^ 2] | s_chgA[warp ^ 4]))) {
+                bool chB = false;
+                if (present) {
                     const float aB = fminf(tile[tB - kT8X], tile[tB + kT8X]);
                     const float gB = fminf(tile[tB - 1], tile[tB + 1]);
                     const float bB = fminf(tile[tB - yA], cA);
                     const float nB = fminf(cB, godunov_jw<kFastSqrt, false>(aB, bB, gB, kB));
                     tile[tB] = nB;
                     chB = nB < cB - p.inner_tol;
-                    anyB = nB < cB;
                     cB = nB;
                 }
-                const bool wB = __any_sync(kFull, anyB);
-                if (lane == 0) s_chgB[warp] = wB;
                 if (!__syncthreads_or(chB)) {
                     more = false;
                     ++it;

@@ -97,49 +97,41 @@ struct GlobalAcc {
     __device__ __forceinline__ float s(int i, int j, int k) const { return sget(p, g, i, j, k); }
 };
 
-// Accurate_FSM::inner_sweep (accurate_FSM.cpp:159-265), same operations in the same order,
-// on the values the accessor returns (global memory or a shared-memory tile).
-template <class Acc>
-__device__ __forceinline__ float ngb_update(const FsmLaunch &p, const Acc &A, int nxx, int nyy, int nzz, int i, int j,
-                                            int k, int sgntz, int sgntx, int sgnty)
-{
-    const int sgnvz = sgntz == 1, sgnvx = sgntx == 1, sgnvy = sgnty == 1;
-    const int i1 = i - sgnvz, j1 = j - sgnvx, k1 = k - sgnvy;
-    const float tv = A.t(i - sgntz, j, k);
-    const float te = A.t(i, j - sgntx, k);
-    const float tn = A.t(i, j, k - sgnty);
-    const float tev = A.t(i - sgntz, j - sgntx, k);
-    const float ten = A.t(i, j - sgntx, k - sgnty);
-    const float tnv = A.t(i - sgntz, j, k - sgnty);
-    const float tnve = A.t(i - sgntz, j - sgntx, k - sgnty);
-    const int jm = max(j - 1, 1), jp = min(j, nxx - 1), km = max(k - 1, 1), kp = min(k, nyy - 1);
-    const int im = max(i - 1, 1), ip = min(i, nzz - 1);
-    const float dz2i = p.dz2i, dx2i = p.dx2i, dy2i = p.dy2i;
+// Inputs of one node update: the node's own value, its upwind traveltimes, and the
+// slowness minima the operator uses -- m1..m3 (the 1D candidates), r1..r3 (the 2D
+// candidates) and r0 (the 3D candidate).
+struct NgbIn {
+    float self, tv, te, tn, tev, ten, tnv, tnve;
+    float m1, m2, m3, r1, r2, r3, r0;
+};
 
-    const float t1D1 = tv + p.dz * smin(A.s(i1, jm, km),
-                                        smin(A.s(i1, jm, kp), smin(A.s(i1, jp, km), A.s(i1, jp, kp))));
-    const float t1D2 = te + p.dx * smin(A.s(im, j1, km),
-                                        smin(A.s(ip, j1, km), smin(A.s(im, j1, kp), A.s(ip, j1, kp))));
-    const float t1D3 = tn + p.dy * smin(A.s(im, jm, k1),
-                                        smin(A.s(im, jp, k1), smin(A.s(ip, jm, k1), A.s(ip, jp, k1))));
+// Accurate_FSM::inner_sweep (accurate_FSM.cpp:159-265) from the minima on: the same
+// operations in the same order (this file is compiled with -fmad=false).
+__device__ __forceinline__ float ngb_core(const FsmLaunch &p, const NgbIn &v)
+{
+    const float tv = v.tv, te = v.te, tn = v.tn, tev = v.tev, ten = v.ten, tnv = v.tnv, tnve = v.tnve;
+    const float dz2i = p.dz2i, dx2i = p.dx2i, dy2i = p.dy2i;
+    const float t1D1 = tv + p.dz * v.m1;
+    const float t1D2 = te + p.dx * v.m2;
+    const float t1D3 = tn + p.dy * v.m3;
     const float t1D = smin(t1D1, smin(t1D2, t1D3));
 
     float t2D1 = 1e6f, t2D2 = 1e6f, t2D3 = 1e6f, ta, tb, tc, Sref;
-    Sref = smin(A.s(i1, j1, km), A.s(i1, j1, kp));
+    Sref = v.r1;
     if ((tv < te + p.dx * Sref) && (te < tv + p.dz * Sref)) {
         ta = tev + te - tv;
         tb = tev - te + tv;
         t2D1 = ((tb * dz2i + ta * dx2i) + sqrtf(4.0f * Sref * Sref * (dz2i + dx2i) - dz2i * dx2i * (ta - tb) * (ta - tb))) /
                (dz2i + dx2i);
     }
-    Sref = smin(A.s(i1, jm, k1), A.s(i1, jp, k1));
+    Sref = v.r2;
     if ((tv < tn + p.dy * Sref) && (tn < tv + p.dz * Sref)) {
         ta = tv - tn + tnv;
         tb = tn - tv + tnv;
         t2D2 = ((ta * dz2i + tb * dy2i) + sqrtf(4.0f * Sref * Sref * (dz2i + dy2i) - dz2i * dy2i * (ta - tb) * (ta - tb))) /
                (dz2i + dy2i);
     }
-    Sref = smin(A.s(im, j1, k1), A.s(ip, j1, k1));
+    Sref = v.r3;
     if ((te < tn + p.dy * Sref) && (tn < te + p.dx * Sref)) {
         ta = te - tn + ten;
         tb = tn - te + ten;
@@ -149,7 +141,7 @@ __device__ __forceinline__ float ngb_update(const FsmLaunch &p, const Acc &A, in
     const float t2D = smin(t2D1, smin(t2D2, t2D3));
 
     float t3D = 1e6f;
-    Sref = A.s(i1, j1, k1);
+    Sref = v.r0;
     ta = te - 0.5f * tn + 0.5f * ten - 0.5f * tv + 0.5f * tev - tnv + tnve;
     tb = tv - 0.5f * tn + 0.5f * tnv - 0.5f * te + 0.5f * tev - ten + tnve;
     tc = tn - 0.5f * te + 0.5f * ten - 0.5f * tv + 0.5f * tnv - tev + tnve;
@@ -161,7 +153,36 @@ __device__ __forceinline__ float ngb_update(const FsmLaunch &p, const Acc &A, in
             t3D = (t1 + sqrtf(t2 - t3)) / p.dsum;
         }
     }
-    return smin(A.self(i, j, k), smin(t1D, smin(t2D, t3D)));
+    return smin(v.self, smin(t1D, smin(t2D, t3D)));
+}
+
+// The update with the reference's own neighbour indices and minima, read through the
+// accessor with the reference's flattened indexing (the plane schedule).
+template <class Acc>
+__device__ __forceinline__ float ngb_update(const FsmLaunch &p, const Acc &A, int nxx, int nyy, int nzz, int i, int j,
+                                            int k, int sgntz, int sgntx, int sgnty)
+{
+    const int sgnvz = sgntz == 1, sgnvx = sgntx == 1, sgnvy = sgnty == 1;
+    const int i1 = i - sgnvz, j1 = j - sgnvx, k1 = k - sgnvy;
+    const int jm = max(j - 1, 1), jp = min(j, nxx - 1), km = max(k - 1, 1), kp = min(k, nyy - 1);
+    const int im = max(i - 1, 1), ip = min(i, nzz - 1);
+    NgbIn v;
+    v.self = A.self(i, j, k);
+    v.tv = A.t(i - sgntz, j, k);
+    v.te = A.t(i, j - sgntx, k);
+    v.tn = A.t(i, j, k - sgnty);
+    v.tev = A.t(i - sgntz, j - sgntx, k);
+    v.ten = A.t(i, j - sgntx, k - sgnty);
+    v.tnv = A.t(i - sgntz, j, k - sgnty);
+    v.tnve = A.t(i - sgntz, j - sgntx, k - sgnty);
+    v.m1 = smin(A.s(i1, jm, km), smin(A.s(i1, jm, kp), smin(A.s(i1, jp, km), A.s(i1, jp, kp))));
+    v.m2 = smin(A.s(im, j1, km), smin(A.s(ip, j1, km), smin(A.s(im, j1, kp), A.s(ip, j1, kp))));
+    v.m3 = smin(A.s(im, jm, k1), smin(A.s(im, jp, k1), smin(A.s(ip, jm, k1), A.s(ip, jp, k1))));
+    v.r1 = smin(A.s(i1, j1, km), A.s(i1, j1, kp));
+    v.r2 = smin(A.s(i1, jm, k1), A.s(i1, jp, k1));
+    v.r3 = smin(A.s(im, j1, k1), A.s(ip, j1, k1));
+    v.r0 = A.s(i1, j1, k1);
+    return ngb_core(p, v);
 }
 
 }  // namespace
@@ -288,32 +309,50 @@ cudaError_t fsm_solve(const FsmLaunch &p, int *grid_out, cudaStream_t st)
 // -------------------------------------------------------------------------------------
 namespace {
 
-constexpr int kHZ = kFsmTZ + 1, kHX = kFsmTX + 1, kHY = kFsmTY + 1;
-constexpr int kHN = kHZ * kHX * kHY;  // a tile plus one upwind layer per axis
-// Slowness arguments of the operator span one index below to one above the tile's own
-// (at halo index 0 it reads index 1: max(i - 1, 1))
-constexpr int kSZ = kFsmTZ + 2, kSX = kFsmTX + 2, kSY = kFsmTY + 2;
-constexpr int kSN = kSZ * kSX * kSY;
+constexpr int kHZ = kFsmTZ + 1, kHX = kFsmTX + 1, kHY = kFsmTY + 1;  // a tile + one layer per axis
+// Strides of the staged arrays (z, then x; words): padded from 17 x 9 so that the lanes of a
+// diagonal-plane pass, which differ by (+-19 -+ 1) a + (+-190 -+ 1) b words, fall in
+// distinct banks (a search over the plane order and the 8 sweep signs: 548 shared-memory
+// wavefronts per tile instead of 1,280).
+constexpr int kPZ = 19, kPX = 10;
+constexpr int kHN = kPZ * kPX * kHY;
 constexpr int kTileN = kFsmTZ * kFsmTX * kFsmTY;
 constexpr int kNPlanes = kFsmTZ + kFsmTX + kFsmTY - 2;
 static_assert(kFsmTZ <= 16 && kFsmTX <= 8 && kFsmTY <= 8, "plane table packs (c, a, b) in 4 + 3 + 3 bits");
+static_assert(kPZ >= kHZ && kPX >= kHX, "padded strides");
 
-// A tile staged in shared memory: the traveltimes of the tile and its upwind layer (halo
-// index origin tz, tx, ty) and the slowness of the halo indices the operator reads, one
-// below the tile's lowest index to one above its highest (origin sz, sx, sy).
-struct TileAcc {
-    const float *T, *S;
-    int tz, tx, ty, sz, sx, sy;
-    __device__ __forceinline__ float t(int i, int j, int k) const
-    {
-        return T[(i - tz) + kHZ * ((j - tx) + kHX * (k - ty))];
-    }
-    __device__ __forceinline__ float self(int i, int j, int k) const { return t(i, j, k); }
-    __device__ __forceinline__ float s(int i, int j, int k) const
-    {
-        return S[(i - sz) + kSZ * ((j - sx) + kSX * (k - sy))];
-    }
-};
+// The update on a tile staged in shared memory.  sget clamps every index into the window,
+// so the slowness at halo indices -1, 0 and 1 of an axis is one value, and the operator's
+// max(i - 1, 1) and min(i, n - 1) read the values at i - 1 and i: every minimum comes from
+// the node's 2 x 2 x 2 cell cube (halo indices i-1..i, j-1..j, k-1..k).  A minimum of
+// floats is exact and independent of its order, so each has the reference's value, and
+// ngb_core does the rest of the reference's arithmetic.
+//   Tt + tb: the node in the traveltime tile; oz, ox, oy: word offsets of one step against
+//   the sweep along z, x, y;  St + sb: cell (i-1, j-1, k-1) in the slowness tile;
+//   cz, cx, cy: 1 - sgnv of each axis (the cube index of i1, j1, k1).
+__device__ __forceinline__ float ngb_update_tile(const FsmLaunch &p, const float *Tt, int tb, int oz, int ox, int oy,
+                                                 const float *St, int sb, int cz, int cx, int cy)
+{
+    const float *c = St + sb;
+    auto C = [&](int dz, int dx, int dy) { return c[dz + kPZ * dx + kPZ * kPX * dy]; };
+    NgbIn v;
+    v.self = Tt[tb];
+    v.tv = Tt[tb - oz];
+    v.te = Tt[tb - ox];
+    v.tn = Tt[tb - oy];
+    v.tev = Tt[tb - oz - ox];
+    v.ten = Tt[tb - ox - oy];
+    v.tnv = Tt[tb - oz - oy];
+    v.tnve = Tt[tb - oz - ox - oy];
+    v.m1 = smin(C(cz, 0, 0), smin(C(cz, 0, 1), smin(C(cz, 1, 0), C(cz, 1, 1))));
+    v.m2 = smin(C(0, cx, 0), smin(C(1, cx, 0), smin(C(0, cx, 1), C(1, cx, 1))));
+    v.m3 = smin(C(0, 0, cy), smin(C(0, 1, cy), smin(C(1, 0, cy), C(1, 1, cy))));
+    v.r1 = smin(C(cz, cx, 0), C(cz, cx, 1));
+    v.r2 = smin(C(cz, 0, cy), C(cz, 1, cy));
+    v.r3 = smin(C(0, cx, cy), C(1, cx, cy));
+    v.r0 = C(cz, cx, cy);
+    return ngb_core(p, v);
+}
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
 {
@@ -341,8 +380,8 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
 {
     extern __shared__ float smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-    float *Ts = smem + warp * (kHN + kSN), *Ss = Ts + kHN;
-    unsigned short *plane = reinterpret_cast<unsigned short *>(smem + wpb * (kHN + kSN));
+    float *Ts = smem + warp * 2 * kHN, *Ss = Ts + kHN;
+    unsigned short *plane = reinterpret_cast<unsigned short *>(smem + wpb * 2 * kHN);
     int *pstart = reinterpret_cast<int *>(plane + kTileN);
     // the tile's nodes (c, a, b) ordered by diagonal plane c + a + b
     if (threadIdx.x < kNPlanes) {
@@ -439,25 +478,26 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
             }
             if (__any_sync(kFull, gave_up)) break;  // the whole warp leaves the sweep
             __syncwarp();  // the upwind tiles' stores, acquired by lanes 0-6, for every lane
-            // stage the tile: traveltimes of the tile and its upwind layer, slowness
+            // stage the tile: traveltimes of the tile and its upwind layer (halo index
+            // origin tz..), slowness of the halo indices one below the tile's lowest to its
+            // highest (origin gz - 1..)
             const int gz = tile_lo(rz, tc * kFsmTZ, kFsmTZ), gx = tile_lo(rx, ta * kFsmTX, kFsmTX),
                       gy = tile_lo(ry, tb * kFsmTY, kFsmTY);
-            const TileAcc acc{Ts, Ss, rz.di > 0 ? gz - 1 : gz, rx.di > 0 ? gx - 1 : gx, ry.di > 0 ? gy - 1 : gy,
-                              gz - 1, gx - 1, gy - 1};
+            const int tz = rz.di > 0 ? gz - 1 : gz, tx = rx.di > 0 ? gx - 1 : gx, ty = ry.di > 0 ? gy - 1 : gy;
             const float *T = p.T + sh.t_off;
             ShotGrid g{&sh, p.T + sh.t_off, 0, nxx, nyy, nzz};
-            for (int m = lane; m < kHN; m += 32) {
+            for (int m = lane; m < kHZ * kHX * kHY; m += 32) {
                 const int ci = m % kHZ, cj = (m / kHZ) % kHX, ck = m / (kHZ * kHX);
-                const int i = acc.tz + ci, j = acc.tx + cj, k = acc.ty + ck;
-                Ts[m] = (i >= 0 && i < nzz && j >= 0 && j < nxx && k >= 0 && k < nyy)
-                            ? __ldcg(T + i + (long long)j * nzz + (long long)k * nxx * nzz)
-                            : 1e6f;
-            }
-            for (int m = lane; m < kSN; m += 32) {  // sget clamps every index into the window
-                const int ci = m % kSZ, cj = (m / kSZ) % kSX, ck = m / (kSZ * kSX);
-                Ss[m] = sget(p, g, acc.sz + ci, acc.sx + cj, acc.sy + ck);
+                const int i = tz + ci, j = tx + cj, k = ty + ck;
+                Ts[ci + kPZ * (cj + kPX * ck)] = (i >= 0 && i < nzz && j >= 0 && j < nxx && k >= 0 && k < nyy)
+                                                     ? __ldcg(T + i + (long long)j * nzz + (long long)k * nxx * nzz)
+                                                     : 1e6f;
+                Ss[ci + kPZ * (cj + kPX * ck)] = sget(p, g, gz - 1 + ci, gx - 1 + cj, gy - 1 + ck);
             }
             __syncwarp();
+            // one step against the sweep, per axis, in the tile's words
+            const int oz = sgz, ox = sgx * kPZ, oy = sgy * kPZ * kPX;
+            const int cz = sgz == 1 ? 0 : 1, cx = sgx == 1 ? 0 : 1, cy = sgy == 1 ? 0 : 1;
             for (int w = 0; w < kNPlanes; w++) {
                 for (int m = pstart[w] + lane; m < pstart[w + 1]; m += 32) {
                     const unsigned e = plane[m];
@@ -465,8 +505,9 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
                               lb = tb * kFsmTY + (int)(e >> 7);
                     if (lc < rz.L && la < rx.L && lb < ry.L) {
                         const int i = rz.i0 + rz.di * lc, j = rx.i0 + rx.di * la, k = ry.i0 + ry.di * lb;
-                        const float v = ngb_update(p, acc, nxx, nyy, nzz, i, j, k, sgz, sgx, sgy);
-                        Ts[(i - acc.tz) + kHZ * ((j - acc.tx) + kHX * (k - acc.ty))] = v;
+                        const int tn = (i - tz) + kPZ * ((j - tx) + kPX * (k - ty));
+                        const int sn = (i - gz) + kPZ * ((j - gx) + kPX * (k - gy));  // cell (i-1, j-1, k-1)
+                        Ts[tn] = ngb_update_tile(p, Ts, tn, oz, ox, oy, Ss, sn, cz, cx, cy);
                     }
                 }
                 __syncwarp();
@@ -479,7 +520,7 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
                 if (lc < rz.L && la < rx.L && lb < ry.L) {
                     const int i = rz.i0 + rz.di * lc, j = rx.i0 + rx.di * la, k = ry.i0 + ry.di * lb;
                     __stcg(Tw + i + (long long)j * nzz + (long long)k * nxx * nzz,
-                           Ts[(i - acc.tz) + kHZ * ((j - acc.tx) + kHX * (k - acc.ty))]);
+                           Ts[(i - tz) + kPZ * ((j - tx) + kPX * (k - ty))]);
                 }
             }
             __threadfence();
@@ -513,7 +554,7 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
 cudaError_t fsm_solve_tiled(const FsmLaunch &p, int *grid_out, cudaStream_t st)
 {
     constexpr int threads = 256;
-    const size_t smem = (size_t)(threads / 32) * (kHN + kSN) * sizeof(float) + kTileN * sizeof(unsigned short) +
+    const size_t smem = (size_t)(threads / 32) * 2 * kHN * sizeof(float) + kTileN * sizeof(unsigned short) +
                         (kNPlanes + 1) * sizeof(int);
     cudaError_t e = cudaFuncSetAttribute(k_fsm_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
