@@ -802,12 +802,13 @@ def run_warm_start(args):
     return 0
 
 
-def learned_warm_object(fields, epochs):
+def learned_warm_object(fields, epochs, strides=(1, 4, 8)):
     """Config 4: the learned warm start end to end -- `fields` solver-generated training
     fields on seeded random models, the U-Net trained on the device for `epochs`, then used
-    on the config-2 batch: prediction -> ceiling (x 1.02) -> warm-started FIM (solve at the
-    timed tolerances, check, fallback), against the plain FIM at the same tolerances.
-    Returns its JSON object."""
+    on the config-2 batch: prediction (full resolution, and on every 4th and 8th node with
+    tau interpolated back) -> ceiling (x 1.02) -> warm-started FIM (solve at the timed
+    tolerances, check, fallback), against the plain FIM at the same tolerances.  Returns
+    its JSON object; `value` is the best of the strides."""
     import torch
 
     import seismic_tomography_3d_b200 as tomo
@@ -831,30 +832,43 @@ def learned_warm_object(fields, epochs):
     sizes = ctx.volume_sizes(ns, sv.windows)
     exact = torch.empty(sum(sizes), dtype=torch.float32, device="cuda")
     ctx.eik_volumes_to(exact.data_ptr())
-    pred, infer_ms = surrogate.predict_ceiling(net, ctx, sv.shots, sv.windows)
-    pred, infer_ms = surrogate.predict_ceiling(net, ctx, sv.shots, sv.windows)
-    m = (exact >= 2.0 * sv.h / float(sv.velocity.max())) & (pred > 0)
-    rel = ((pred - exact) / exact)[m]
-    runs = [ctx.eik_solve_seeded(sv.shots, pred.data_ptr(), 0.02, windows=sv.windows, **SOLVER) for _ in range(3)]
-    _, st_w, ss_w = runs[-1]
-    warm_ms = statistics.median(r[1]["total_ms"] for r in runs)
+    vmin_t = 2.0 * sv.h / float(sv.velocity.max())
     out = torch.empty_like(exact)
-    ctx.eik_volumes_to(out.data_ptr())
-    torch.cuda.synchronize()
-    err = float(((out - exact).abs() / exact)[exact >= 2.0 * sv.h / float(sv.velocity.max())].max())
+    variants = []
+    for stride in strides:
+        # the network on every stride-th node (1: all), tau interpolated back to every node
+        pred, infer_ms = surrogate.predict_ceiling(net, ctx, sv.shots, sv.windows, stride=stride)
+        pred, infer_ms = surrogate.predict_ceiling(net, ctx, sv.shots, sv.windows, stride=stride)
+        m = (exact >= vmin_t) & (pred > 0)
+        rel = ((pred - exact) / exact)[m]
+        runs = [ctx.eik_solve_seeded(sv.shots, pred.data_ptr(), 0.02, windows=sv.windows, **SOLVER) for _ in range(3)]
+        _, st_w, ss_w = runs[-1]
+        warm_ms = statistics.median(r[1]["total_ms"] for r in runs)
+        ctx.eik_volumes_to(out.data_ptr())
+        torch.cuda.synchronize()
+        err = float(((out - exact).abs() / exact)[exact >= vmin_t].max())
+        variants.append({
+            "stride": stride, "value": ns / ((warm_ms + infer_ms) / 1000.0),
+            "speedup_vs_plain": plain_ms / (warm_ms + infer_ms),
+            "ms_inference": infer_ms, "ms_per_batch_solve": warm_ms,
+            "inference_frac_of_plain": infer_ms / plain_ms,
+            "activations": st_w["activations"], "inner_iterations": st_w["inner_iterations"],
+            "activations_seeded_launch": ss_w["activations_seeded"], "shots_fallback": ss_w["shots_fallback"],
+            "violations": ss_w["violations"], "stuck": ss_w["stuck"], "max_rel_err_vs_plain": err,
+            "predictor_rel_err": {"median_abs": float(rel.abs().median()),
+                                  "p99_abs": float(rel.abs().float().quantile(0.99)) if rel.numel() < 16_000_000 else None,
+                                  "frac_below_truth_by_2pct": float((rel < -0.02).float().mean())}})
+        del pred
+    best = max(variants, key=lambda v: v["speedup_vs_plain"])
     line = {"metric": "learned warm start vs plain FIM (config 4 surrogate on the config-2 batch)",
-            "value": ns / ((warm_ms + infer_ms) / 1000.0), "unit": UNIT, "higher_is_better": True,
+            "value": best["value"], "unit": UNIT, "higher_is_better": True,
+            "speedup_vs_plain": best["speedup_vs_plain"], "best_stride": best["stride"],
+            "max_rel_err_vs_plain": max(v["max_rel_err_vs_plain"] for v in variants),
+            "shots_fallback": best["shots_fallback"],
             "plain": {"value": ns / (plain_ms / 1000.0), "ms_per_batch": plain_ms,
                       "activations": st_plain["activations"], "inner_iterations": st_plain["inner_iterations"]},
-            "warm": {"ms_per_batch_solve": warm_ms, "ms_inference": infer_ms,
-                     "activations": st_w["activations"], "inner_iterations": st_w["inner_iterations"],
-                     "activations_seeded_launch": ss_w["activations_seeded"], "shots_fallback": ss_w["shots_fallback"],
-                     "violations": ss_w["violations"], "stuck": ss_w["stuck"], "max_rel_err_vs_plain": err},
-            "speedup_vs_plain": plain_ms / (warm_ms + infer_ms),
-            "tolerances_s": SOLVER,
-            "predictor_rel_err": {"median_abs": float(rel.abs().median()), "p99_abs": float(rel.abs().quantile(0.99))
-                                  if rel.numel() < 16_000_000 else None,
-                                  "frac_below_truth_by_2pct": float((rel < -0.02).float().mean())},
+            "warm": variants,
+            "tolerances_s": SOLVER, "inflate": 0.02,
             "training": {k: v for k, v in summ.items() if k != "history"}, "history": summ["history"],
             "data": {"fields": fields, "epochs": epochs, "tile": [64, 64, 64], "h_m": 12.5,
                      "models": "seeded random: 3-6 dipping layers 1500-4500 m/s, 0-12 Gaussian anomalies +-15 %",
@@ -862,7 +876,7 @@ def learned_warm_object(fields, epochs):
             "wall_s": time.perf_counter() - t0}
     net.close()
     ctx.close()
-    del exact, pred, out
+    del exact, out
     torch.cuda.empty_cache()
     return line
 

@@ -429,6 +429,12 @@ int tomo_net_evaluate(tomo_net *net, int n, const tomo_net_sample *samples, floa
  * tomo_eik_volumes and of the ceiling of tomo_eik_solve_seeded; 0 within h of the source.
  * ms (may be NULL): device time. */
 int tomo_net_predict(tomo_net *net, int n, const tomo_net_sample *samples, float h, float *t_pred, float *ms);
+/* The same on a coarse grid: the network sees every stride-th node of each window (the
+ * distance channel normalised by 64 h stride, so large windows stay in the range of the
+ * 64^3 training tiles) at 1/stride^3 of the cost, and tau is interpolated trilinearly back
+ * to every window node before T = tau s_src distance.  stride 1..16; 1 is tomo_net_predict. */
+int tomo_net_predict_strided(tomo_net *net, int n, const tomo_net_sample *samples, float h, int stride, float *t_pred,
+                             float *ms);
 
 /* Training data: fills ctx's model with seeded random tiles (tile x tile nodes laterally,
  * full depth): 3-6 dipping layers of 1500-4500 m/s and 0-12 Gaussian anomalies of up to

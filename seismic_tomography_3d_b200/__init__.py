@@ -166,6 +166,7 @@ def _bind_net(lib):
     lib.tomo_net_train_step.argtypes = [V, I, P(NetSample), F, F, P(D)]
     lib.tomo_net_evaluate.argtypes = [V, I, P(NetSample), F, P(D)]
     lib.tomo_net_predict.argtypes = [V, I, P(NetSample), F, V, P(F)]
+    lib.tomo_net_predict_strided.argtypes = [V, I, P(NetSample), F, I, V, P(F)]
     lib.tomo_random_tiles.argtypes = [V, I, ctypes.c_ulonglong]
     lib.tomo_ctx_slowness_device.argtypes = [V]
     lib.tomo_ctx_slowness_device.restype = V
@@ -526,10 +527,12 @@ class Net:
         self._check(self.lib.tomo_net_evaluate(self.h, len(arr), arr, h, ctypes.byref(loss)))
         return loss.value
 
-    def predict(self, samples, h, out_ptr):
+    def predict(self, samples, h, out_ptr, stride=1):
         """Predicted traveltimes into the device array at out_ptr (back-to-back windows);
-        returns the device time in ms."""
+        stride > 1 runs the network on every stride-th node and interpolates tau back
+        (tomo_net_predict_strided).  Returns the device time in ms."""
         arr = net_samples(samples)
         ms = ctypes.c_float()
-        self._check(self.lib.tomo_net_predict(self.h, len(arr), arr, h, ctypes.c_void_p(out_ptr), ctypes.byref(ms)))
+        self._check(self.lib.tomo_net_predict_strided(self.h, len(arr), arr, h, int(stride), ctypes.c_void_p(out_ptr),
+                                                      ctypes.byref(ms)))
         return ms.value

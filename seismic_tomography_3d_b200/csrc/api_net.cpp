@@ -212,17 +212,20 @@ int refresh_weights(tomo_net *net)
 int pad8(int n) { return (n + 7) / 8 * 8; }
 
 // Jobs of a batch (one padded volume per sample, all of the same padded size).
-int make_jobs(tomo_net *net, int n, const tomo_net_sample *s, float h, Vol &v, std::vector<tomo::net::Job> &jobs)
+// stride k: the network volume holds every k-th window node (ceil(n / k) per axis, padded)
+int make_jobs(tomo_net *net, int n, const tomo_net_sample *s, float h, Vol &v, std::vector<tomo::net::Job> &jobs,
+              int stride = 1)
 {
     int pd = 0, ph = 0, pw = 0;
+    auto ck = [stride](int m) { return (m + stride - 1) / stride; };
     for (int i = 0; i < n; i++) {
         const tomo_window &w = s[i].window;
         if (!s[i].slow || w.x0 < 0 || w.y0 < 0 || w.x1 > s[i].model_nx || w.y1 > s[i].model_ny || w.x1 - w.x0 < 2 ||
             w.y1 - w.y0 < 2 || s[i].nz < 2)
             return fail(net, TOMO_ERR_INVALID_ARG, "sample " + std::to_string(i) + ": bad model or window");
-        pd = std::max(pd, pad8(w.y1 - w.y0));
-        ph = std::max(ph, pad8(w.x1 - w.x0));
-        pw = std::max(pw, pad8(s[i].nz));
+        pd = std::max(pd, pad8(ck(w.y1 - w.y0)));
+        ph = std::max(ph, pad8(ck(w.x1 - w.x0)));
+        pw = std::max(pw, pad8(ck(s[i].nz)));
     }
     v = Vol{n, pd, ph, pw};
     jobs.resize((size_t)n);
@@ -249,6 +252,7 @@ int make_jobs(tomo_net *net, int n, const tomo_net_sample *s, float h, Vol &v, s
         j.out_off = (long long)i * pd * ph * pw;
         j.nat_off = nat;
         j.T = s[i].T;
+        j.stride = stride;
         nat += (long long)j.nz * j.wnx * j.wny;
     }
     NK(net->jobs.ensure((size_t)n));
@@ -461,10 +465,17 @@ int tomo_net_evaluate(tomo_net *net, int n, const tomo_net_sample *samples, floa
 
 int tomo_net_predict(tomo_net *net, int n, const tomo_net_sample *samples, float h, float *t_pred, float *ms)
 {
-    if (!net || n < 1 || !samples || !(h > 0) || !t_pred) return TOMO_ERR_INVALID_ARG;
+    return tomo_net_predict_strided(net, n, samples, h, 1, t_pred, ms);
+}
+
+int tomo_net_predict_strided(tomo_net *net, int n, const tomo_net_sample *samples, float h, int stride, float *t_pred,
+                             float *ms)
+{
+    if (!net || n < 1 || !samples || !(h > 0) || !t_pred || stride < 1 || stride > 16) return TOMO_ERR_INVALID_ARG;
     NK(cudaSetDevice(net->device));
     NK(cudaEventRecord(net->ev[0], net->stream));
     long long nat = 0;
+    auto ck = [stride](int m) { return (m + stride - 1) / stride; };
     for (int i0 = 0; i0 < n;) {
         // as many samples per pass as fit in one window's worth of activations x 8
         int cnt = 1;
@@ -472,16 +483,22 @@ int tomo_net_predict(tomo_net *net, int n, const tomo_net_sample *samples, float
         std::vector<tomo::net::Job> jobs;
         {
             const tomo_window &w = samples[i0].window;
-            const long long one = (long long)pad8(w.y1 - w.y0) * pad8(w.x1 - w.x0) * pad8(samples[i0].nz);
+            const long long one =
+                (long long)pad8(ck(w.y1 - w.y0)) * pad8(ck(w.x1 - w.x0)) * pad8(ck(samples[i0].nz));
             cnt = (int)std::max(1LL, std::min<long long>(n - i0, (8LL << 20) / std::max(one, 1LL)));
         }
-        int rc = make_jobs(net, cnt, samples + i0, h, v, jobs);
+        int rc = make_jobs(net, cnt, samples + i0, h, v, jobs, stride);
         if (rc != TOMO_OK) return rc;
         const long long per = (long long)v.D * v.H * v.W;
         NK(tomo::net::features(net->jobs.ptr, cnt, h, net->act[X].ptr, per, net->stream));
         rc = forward(net, v, false);
         if (rc != TOMO_OK) return rc;
-        NK(tomo::net::tau_to_time(net->jobs.ptr, cnt, h, net->tau.ptr, t_pred + nat, per, net->stream));
+        long long max_nat = 0;
+        for (const auto &j : jobs) max_nat = std::max(max_nat, (long long)j.nz * j.wnx * j.wny);
+        if (stride == 1)
+            NK(tomo::net::tau_to_time(net->jobs.ptr, cnt, h, net->tau.ptr, t_pred + nat, per, net->stream));
+        else
+            NK(tomo::net::tau_to_time_strided(net->jobs.ptr, cnt, h, net->tau.ptr, t_pred + nat, max_nat, net->stream));
         for (const auto &j : jobs) nat += (long long)j.nz * j.wnx * j.wny;
         i0 += cnt;
     }

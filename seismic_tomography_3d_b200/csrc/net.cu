@@ -385,10 +385,11 @@ __device__ __forceinline__ JobGeo job_geo(const Job &j, long long i, float h)
     const int w = (int)(i % j.pw);
     const long long r = i / j.pw;
     const int hh = (int)(r % j.ph), d = (int)(r / j.ph);
-    q.inside = d < j.wny && hh < j.wnx && w < j.nz;
-    q.y = min(d, j.wny - 1);
-    q.x = min(hh, j.wnx - 1);
-    q.z = min(w, j.nz - 1);
+    const int k = j.stride;  // network voxel (d, hh, w) samples window node (k d, k hh, k w)
+    q.inside = d * k < j.wny && hh * k < j.wnx && w * k < j.nz;
+    q.y = min(d * k, j.wny - 1);
+    q.x = min(hh * k, j.wnx - 1);
+    q.z = min(w * k, j.nz - 1);
     const float ex = q.x * h - j.sx, ey = q.y * h - j.sy, ez = q.z * h - j.sz;
     q.dist = sqrtf(ex * ex + ey * ey + ez * ez);
     const long long mstride = (long long)j.nz * j.model_nx;
@@ -409,7 +410,7 @@ __global__ void k_features(const Job *jobs, float h, bf16 *x16)
 #pragma unroll
         for (int k = 0; k < 16; k++) f[k] = __float2bfloat16_rn(0.f);
         f[0] = __float2bfloat16_rn(q.s / q.s_src - 1.0f);
-        f[1] = __float2bfloat16_rn(q.dist / (64.0f * h));
+        f[1] = __float2bfloat16_rn(q.dist / (64.0f * h * (float)j.stride));
         uint4 *dst = reinterpret_cast<uint4 *>(x16 + (j.out_off + i) * 16);
         dst[0] = reinterpret_cast<const uint4 *>(f)[0];
         dst[1] = reinterpret_cast<const uint4 *>(f)[1];
@@ -440,6 +441,52 @@ __global__ void k_tau_to_time(const Job *jobs, float h, const float *tau, float 
         if (!q.inside) continue;
         const float t = q.dist >= h ? tau[j.out_off + i] * q.s_src * q.dist : 0.f;
         t_out[j.nat_off + q.z + (long long)j.nz * (q.x + (long long)j.wnx * q.y)] = t;
+    }
+}
+
+// Strided prediction: tau at every window node, trilinear between the sampled nodes (node
+// c of an axis sits at min(c k, n - 1)), then T = tau s_src distance as k_tau_to_time.
+__device__ __forceinline__ void axis_weight(int x, int k, int n, int &c0, int &c1, float &t)
+{
+    const int nc = (n + k - 1) / k;
+    c0 = min(x / k, nc - 1);
+    c1 = min(c0 + 1, nc - 1);
+    const int p0 = c0 * k, p1 = min(c1 * k, n - 1);
+    t = p1 > p0 ? (float)(x - p0) / (float)(p1 - p0) : 0.f;
+}
+
+__global__ void k_tau_to_time_strided(const Job *jobs, float h, const float *tau, float *t_out)
+{
+    const Job j = jobs[blockIdx.y];
+    const int k = j.stride;
+    const long long n = (long long)j.nz * j.wnx * j.wny;
+    const int sz = min((int)(j.sz / h), j.nz - 1), sx = min((int)(j.sx / h), j.wnx - 1),
+              sy = min((int)(j.sy / h), j.wny - 1);
+    const float s_src =
+        __ldg(j.slow + sz + (long long)j.nz * (j.wx0 + sx) + (long long)j.nz * j.model_nx * (j.wy0 + sy));
+    const float *tj = tau + j.out_off;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int z = (int)(i % j.nz);
+        const long long r = i / j.nz;
+        const int x = (int)(r % j.wnx), y = (int)(r / j.wnx);
+        const float ex = x * h - j.sx, ey = y * h - j.sy, ez = z * h - j.sz;
+        const float dist = sqrtf(ex * ex + ey * ey + ez * ez);
+        float t = 0.f;
+        if (dist >= h) {
+            int z0, z1, x0, x1, y0, y1;
+            float tz, tx, ty;
+            axis_weight(z, k, j.nz, z0, z1, tz);
+            axis_weight(x, k, j.wnx, x0, x1, tx);
+            axis_weight(y, k, j.wny, y0, y1, ty);
+            auto T = [&](int a, int b, int c) { return tj[a + (long long)j.pw * (b + (long long)j.ph * c)]; };
+            const float c00 = T(z0, x0, y0) * (1.f - tz) + T(z1, x0, y0) * tz;
+            const float c01 = T(z0, x0, y1) * (1.f - tz) + T(z1, x0, y1) * tz;
+            const float c10 = T(z0, x1, y0) * (1.f - tz) + T(z1, x1, y0) * tz;
+            const float c11 = T(z0, x1, y1) * (1.f - tz) + T(z1, x1, y1) * tz;
+            const float c0 = c00 * (1.f - tx) + c10 * tx, c1 = c01 * (1.f - tx) + c11 * tx;
+            t = (c0 * (1.f - ty) + c1 * ty) * s_src * dist;
+        }
+        t_out[j.nat_off + i] = t;
     }
 }
 
@@ -626,6 +673,15 @@ cudaError_t tau_to_time(const Job *jobs, int njobs, float h, const float *tau, f
 {
     if (njobs < 1 || njobs > 65535) return cudaErrorInvalidValue;
     k_tau_to_time<<<dim3((unsigned)grid1(max_vox, 256) / 8 + 1, (unsigned)njobs), 256, 0, st>>>(jobs, h, tau, t_out);
+    return cudaGetLastError();
+}
+
+cudaError_t tau_to_time_strided(const Job *jobs, int njobs, float h, const float *tau, float *t_out, long long max_nat,
+                                cudaStream_t st)
+{
+    if (njobs < 1 || njobs > 65535) return cudaErrorInvalidValue;
+    k_tau_to_time_strided<<<dim3((unsigned)grid1(max_nat, 256) / 8 + 1, (unsigned)njobs), 256, 0, st>>>(jobs, h, tau,
+                                                                                                        t_out);
     return cudaGetLastError();
 }
 

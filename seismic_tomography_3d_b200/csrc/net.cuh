@@ -75,16 +75,20 @@ struct Job {
     long long out_off;   // voxel offset of the padded volume in the batch tensors
     long long nat_off;   // offset of the window volume in back-to-back natural outputs
     const float *T;      // the window's traveltimes (natural layout) for training targets
+    int stride;          // the network volume samples every stride-th window node (1: all)
 };
-// Input features: channel 0 = s / s_src - 1, channel 1 = distance / (64 h), channels
-// 2..15 = 0.  Padding voxels repeat the nearest window voxel.
+// Input features: channel 0 = s / s_src - 1, channel 1 = distance / (64 h stride),
+// channels 2..15 = 0.  Padding voxels repeat the nearest window voxel.
 cudaError_t features(const Job *jobs, int njobs, float h, bf16 *x16, long long max_vox, cudaStream_t st);
 // tau = T / (s_src * distance) inside the window at distance >= h, else 0 (not in the loss)
 cudaError_t tau_target(const Job *jobs, int njobs, float h, float *tau, long long max_vox, cudaStream_t st);
 // predicted traveltime tau * s_src * distance into the back-to-back natural layout (0 at
-// distance < h: no ceiling there)
+// distance < h: no ceiling there); jobs with stride > 1 interpolate tau trilinearly between
+// the sampled nodes first (max_nat: the largest window volume)
 cudaError_t tau_to_time(const Job *jobs, int njobs, float h, const float *tau, float *t_out, long long max_vox,
                         cudaStream_t st);
+cudaError_t tau_to_time_strided(const Job *jobs, int njobs, float h, const float *tau, float *t_out,
+                                long long max_nat, cudaStream_t st);
 
 // Seeded random layered models (training data): one 64^3-like tile per entry of `tiles`,
 // written as slowness into the natural-layout model of size nz x nx x ny.

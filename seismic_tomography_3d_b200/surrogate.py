@@ -125,9 +125,10 @@ def train(net: Net, ds: Dataset, epochs=3, batch=8, lr=1e-3, val_frac=0.02, seed
             "history": hist}
 
 
-def predict_ceiling(net: Net, ctx: Context, shots, windows):
+def predict_ceiling(net: Net, ctx: Context, shots, windows, stride=1):
     """Predicted traveltimes of every shot's window (back to back, z fastest) on the device,
-    from the context's current model.  Returns (tensor, device ms)."""
+    from the context's current model; stride > 1: the network on every stride-th node, tau
+    interpolated back.  Returns (tensor, device ms)."""
     import torch
 
     g = ctx.grid
@@ -139,5 +140,5 @@ def predict_ceiling(net: Net, ctx: Context, shots, windows):
     sp = ctx.slowness_device()
     samples = [dict(slow=sp, model_nx=g.nx, model_ny=g.ny, nz=g.nz, window=tuple(int(v) for v in windows[k]),
                     source=tuple(float(v) for v in shots[k]), T=0) for k in range(n)]
-    ms = net.predict(samples, g.dx, out.data_ptr())
+    ms = net.predict(samples, g.dx, out.data_ptr(), stride=stride)
     return out, ms

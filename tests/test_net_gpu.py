@@ -98,6 +98,35 @@ def test_gradients_match_oracle(tomo, shape):
     net.close()
 
 
+def test_strided_prediction_equals_prediction_on_the_subsampled_model(tomo):
+    """tomo_net_predict_strided with stride 2 on a model feeds the network exactly the
+    features the plain prediction gets on that model subsampled by 2 at spacing 2h (same
+    slowness samples, same distances, distance channel / (64 h stride)), so at the sampled
+    nodes both predictions agree; between them the strided one interpolates tau."""
+    import torch
+
+    nx, ny, nz, h, k = 33, 29, 17, 20.0, 2
+    sv = wl.small(6, nx, ny, nz, h=h, nshots=1)
+    slow = (1.0 / sv.velocity).astype(np.float32)
+    src = (8 * h, 12 * h, 2 * h)  # on a node of both grids
+    net = tomo.Net(seed=3)
+    fine_d = _dev(slow)
+    coarse = np.ascontiguousarray(slow[::k, ::k, ::k])
+    coarse_d = _dev(coarse)
+    cy, cx, cz = coarse.shape
+    out_f = torch.zeros(nx * ny * nz, dtype=torch.float32, device="cuda")
+    out_c = torch.zeros(cx * cy * cz, dtype=torch.float32, device="cuda")
+    net.predict([dict(slow=fine_d.data_ptr(), model_nx=nx, model_ny=ny, nz=nz, window=(0, nx, 0, ny), source=src,
+                      T=0)], h, out_f.data_ptr(), stride=k)
+    net.predict([dict(slow=coarse_d.data_ptr(), model_nx=cx, model_ny=cy, nz=cz, window=(0, cx, 0, cy), source=src,
+                      T=0)], k * h, out_c.data_ptr())
+    tf = out_f.cpu().numpy().reshape(ny, nx, nz)
+    tc = out_c.cpu().numpy().reshape(cy, cx, cz)
+    np.testing.assert_allclose(tf[::k, ::k, ::k], tc, rtol=1e-6, atol=0)
+    assert np.all(np.isfinite(tf)) and (tf > 0).mean() > 0.99
+    net.close()
+
+
 def _tiles(tomo, ctx, tile, nz, h, seed):
     """Random tiles as the model, one surface source per tile; returns net samples."""
     import torch
