@@ -46,6 +46,11 @@ sys.path.insert(0, ROOT)
 METRIC = "shot solves/s on 201x201x101, learned-warm vs plain FIM, at 1e-4 rel err"
 UNIT = "shots/s"
 BYTES_PER_NODE_ACT = 12  # slowness read + traveltime read + traveltime write (float32)
+# DRAM bytes (read + write) per brick activation of the headline solve, from one ncu capture
+# of a 16-shot launch of this workload each (dram__bytes_read.sum + dram__bytes_write.sum
+# over the launch's activations; profiles/k_fim_solve_config2.md, k_fim_solve8_config2.md):
+# roofline.traffic is this figure times the timed launch's own activation count.
+DRAM_BYTES_PER_ACTIVATION = {"k_fim_solve": 351.6, "k_fim_solve8": 2787.5}
 # Solver tolerances of the timed runs (seismic_tomography_3d_b200.workloads): the metric is
 # quoted at 1e-4 relative traveltime error, so the face-change and in-brick tolerances are
 # loosened until the error against the FP64 oracle (checked in the cpu_baseline leg,
@@ -546,13 +551,7 @@ def run_ours(args):
     # (one capture of a 16-shot launch of the same workload), scaled to this launch's
     # activations
     kernel = "k_fim_solve8" if stats[0]["nodes_per_brick"] == 512 else "k_fim_solve"
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", f"{kernel}_config2.md")
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            for ln in f:
-                if ln.startswith("dram_bytes_per_activation:"):
-                    traffic = float(ln.split(":")[1]) * act
+    traffic = DRAM_BYTES_PER_ACTIVATION[kernel] * act
 
     # ---- the timed setting against the fully converged field of the same solver ---------
     accuracy_conv = solver_accuracy(ctx, sv, SOLVER_RUN)
