@@ -50,9 +50,11 @@ typedef struct {
     float x, y, z;
 } tomo_point;
 
-/* Lateral solve window of one shot: nodes [x0,x1) x [y0,y1), full depth.  x0, y0 must be
- * multiples of 4; x1 (y1) must be a multiple of 4 or equal nx (ny).  Each windowed solve
- * equals the reference solve on the model cropped to that window. */
+/* Lateral solve window of one shot: nodes [x0,x1) x [y0,y1), full depth, inside the model
+ * and at least 2 x 2 nodes.  Each windowed solve equals the reference solve on the model
+ * cropped to that window.  Windows whose x0, y0 are multiples of 4 and whose x1 (y1) is a
+ * multiple of 4 or nx (ny) read the shared brick-major model in place; any other window
+ * gets its own brick-major slowness copy in device scratch (window nodes x 4 bytes). */
 typedef struct {
     int x0, x1, y0, y1;
 } tomo_window;

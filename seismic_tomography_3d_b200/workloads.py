@@ -118,6 +118,13 @@ def brick_window(rng, n, center, frac_lo=0.6, frac_hi=1.0):
     return a, b
 
 
+def crop_window(rng, n, center, frac_lo=0.6, frac_hi=1.0):
+    """A window [a, b) of about frac*n nodes around `center`, at any origin."""
+    width = max(2, int(round(rng.uniform(frac_lo, frac_hi) * n)))
+    a = int(np.clip(center - width // 2, 0, max(n - width, 0)))
+    return a, min(a + width, n)
+
+
 def regular_receivers(n_side, lo, hi):
     c = np.linspace(lo, hi, n_side, dtype=np.float64)
     yy, xx = np.meshgrid(c, c, indexing="ij")
@@ -139,12 +146,19 @@ def config2_model(seed=2, nx=201, ny=201, nz=101, h=12.5):
     return v.astype(np.float32), rng
 
 
-def config2(seed=2, nx=201, ny=201, nz=101, h=12.5, n_side=8) -> Survey:
+def config2(seed=2, nx=201, ny=201, nz=101, h=12.5, n_side=8, aligned=True) -> Survey:
+    """aligned=False: each window is the seeded crop itself, at any origin (the solver then
+    builds a slowness copy per window); aligned=True rounds the same crops out to bricks."""
     v, rng = config2_model(seed, nx, ny, nz, h)
     shots = jittered_shots(rng, nx, ny, h, n_side)
     wins = []
     for sx, sy, _ in shots:
         ix, iy = int(round(sx / h)), int(round(sy / h))
+        if not aligned:
+            x0, x1 = crop_window(rng, nx, ix)
+            y0, y1 = crop_window(rng, ny, iy)
+            wins.append((x0, x1, y0, y1))
+            continue
         x0, x1 = brick_window(rng, nx, ix)
         y0, y1 = brick_window(rng, ny, iy)
         # the window must contain its shot

@@ -97,6 +97,48 @@ def test_batched_windows_match_cropped_oracle(tomo, oracle_mod):
             assert rel_err(T, Tref, sv.h, sv.velocity.max()) < REL_TOL
 
 
+def _any_windows(rng, sv, n):
+    """Windows of any origin and end (not brick-aligned) around each shot."""
+    wins = []
+    for sx, sy, _ in sv.shots[:n]:
+        ix, iy = int(round(sx / sv.h)), int(round(sy / sv.h))
+        x0 = int(rng.integers(max(0, ix - 9), ix + 1))
+        y0 = int(rng.integers(max(0, iy - 9), iy + 1))
+        x1 = int(rng.integers(ix + 1, min(sv.nx, ix + 10) + 1))
+        y1 = int(rng.integers(iy + 1, min(sv.ny, iy + 10) + 1))
+        wins.append((x0, max(x1, x0 + 2), y0, max(y1, y0 + 2)))
+    return np.asarray(wins, np.int32)
+
+
+@pytest.mark.parametrize("brick", sorted(BRICKS))
+def test_unaligned_windows_match_cropped_oracle(tomo, oracle_mod, brick):
+    """Windows of any origin and end: each gets its own brick-major slowness copy (the
+    cropped model padded by edge replication, as the reference pads a model), so each
+    windowed solve equals the oracle on the cropped model; the receivers follow the
+    window's offset."""
+    nx, ny, nz = 37, 30, 14
+    sv = wl.small(23, nx, ny, nz, nshots=6, nrec=30)
+    wins = _any_windows(np.random.default_rng(23), sv, 6)
+    assert np.any(wins[:, 0] % 4) and np.any(wins[:, 1] % 4)
+    with tomo.Context(nx, ny, nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        t_recv, _ = ctx.eik_solve(sv.shots, windows=wins, receivers=sv.receivers, brick=BRICKS[brick])
+        for i in range(len(sv.shots)):
+            assert ctx.eik_window(i) == tuple(wins[i])
+            T = ctx.eik_volume(i)
+            Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, sv.shots[i], wins[i])
+            assert T.shape == Tref.shape
+            assert rel_err(T, Tref, sv.h, sv.velocity.max()) < REL_TOL
+            # receivers inside the window: sampled from the window's own field
+            x0, x1, y0, y1 = (int(a) for a in wins[i])
+            rx = sv.receivers[:, 0] - np.float32(x0) * np.float32(sv.h)
+            ry = sv.receivers[:, 1] - np.float32(y0) * np.float32(sv.h)
+            inside = (rx >= 0) & (ry >= 0) & (rx <= (x1 - x0 - 1) * sv.h) & (ry <= (y1 - y0 - 1) * sv.h)
+            ref = oracle_mod.first_arrival(T, sv.h, rx[inside], ry[inside], sv.receivers[inside, 2])
+            np.testing.assert_array_equal(t_recv[i][inside], ref)
+            assert np.all(t_recv[i][~inside] >= 1e5)
+
+
 def test_batch_equals_single_solves(tomo):
     nx, ny, nz = 29, 26, 13
     sv = wl.small(5, nx, ny, nz, nshots=5)
@@ -175,7 +217,10 @@ def test_errors_are_status_codes(tomo):
             ctx.eik_solve([[500.0, 5.0, 0.0]])  # outside
         assert e.value.status == -1
         with pytest.raises(tomo.TomoError) as e:
-            ctx.eik_solve([[5.0, 5.0, 0.0]], windows=[[1, 12, 0, 12]])  # unaligned window
+            ctx.eik_solve([[5.0, 5.0, 0.0]], windows=[[0, 13, 0, 12]])  # window beyond the model
+        assert e.value.status == -1
+        with pytest.raises(tomo.TomoError) as e:
+            ctx.eik_solve([[5.0, 5.0, 0.0]], windows=[[1, 12, 0, 12]])  # shot outside its window
         assert e.value.status == -1
         with pytest.raises(tomo.TomoError) as e:
             ctx.eik_solve([[50.0, 50.0, 0.0]], max_rounds=2, schedule=1)  # round cap

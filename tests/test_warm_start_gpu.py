@@ -172,3 +172,38 @@ def test_smooth_upper_bound_is_accepted(big_case):
     ss = _seeded_equals_plain(ctx, sv, shots, plain, exact * 1.02 * (1.0 - 2e-4 * ramp))
     assert ss["stuck"] == 0 and ss["violations"] == 0
     assert ss["shots_fallback"] == 0
+
+
+def test_unaligned_windows_warm_start(tomo):
+    """The warm-started solve and its check read the own slowness copies of windows that
+    are not brick-aligned: an upper bound gives the plain result with no fallback, a low
+    ceiling falls back."""
+    import torch
+
+    sv = wl.small(61, 40, 36, 20, nshots=3)
+    wins = np.array([[1, 23, 3, 30], [5, 40, 0, 17], [2, 39, 7, 36]], np.int32)
+    for i, (x0, x1, y0, y1) in enumerate(wins):  # shots inside their windows
+        sv.shots[i, 0] = np.float32((x0 + 1 + i) * sv.h)
+        sv.shots[i, 1] = np.float32((y0 + 2) * sv.h)
+    with tomo.Context(sv.nx, sv.ny, sv.nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(sv.shots, windows=wins)
+        plain = [ctx.eik_volume(i) for i in range(3)]
+        sizes = ctx.volume_sizes(3, wins)
+        dev = torch.empty(sum(sizes), dtype=torch.float32, device="cuda")
+        ctx.eik_volumes_to(dev.data_ptr())
+        torch.cuda.synchronize()
+        _, _, ss = ctx.eik_solve_seeded(sv.shots, dev.data_ptr(), 0.02, windows=wins)
+        assert ss["shots_fallback"] == 0 and ss["stuck"] == 0
+        check_equal(ctx, dataclasses_replace(sv, wins), plain)
+        low = dev * 0.9
+        torch.cuda.synchronize()
+        _, _, ss = ctx.eik_solve_seeded(sv.shots, low.data_ptr(), 0.02, windows=wins)
+        assert ss["shots_fallback"] == 3
+        check_equal(ctx, dataclasses_replace(sv, wins), plain)
+
+
+def dataclasses_replace(sv, wins):
+    import dataclasses
+
+    return dataclasses.replace(sv, windows=wins)
