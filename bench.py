@@ -636,8 +636,8 @@ def unaligned_windows_object(ctx, sv, solver, stream, steps, barrier, dist, worl
     from seismic_tomography_3d_b200 import workloads as wl
 
     win = wl.config2(seed=2 + 1000 * rank, aligned=False).windows[: len(sv.shots)]
-    out = {"windows": "seeded 60-100 % crops at any origin (%d of %d windows off the brick grid)"
-                      % (int(np.any(win % 4 != 0, axis=1).sum()), len(win))}
+    off_grid = int(np.any(win % 4 != 0, axis=1).sum())
+    out = {"windows": f"seeded 60-100 % crops at any origin ({off_grid} of {len(win)} windows off the brick grid)"}
     for name, kw in (("jw", solver), ("ngb", {"op": 1})):
         ctx.eik_solve(sv.shots, windows=win, receivers=sv.receivers, want_recv=False, **kw)
         barrier()

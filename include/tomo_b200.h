@@ -51,10 +51,10 @@ typedef struct {
 } tomo_point;
 
 /* Lateral solve window of one shot: nodes [x0,x1) x [y0,y1), full depth, inside the model
- * and at least 2 x 2 nodes.  Each windowed solve equals the reference solve on the model
- * cropped to that window.  Windows whose x0, y0 are multiples of 4 and whose x1 (y1) is a
- * multiple of 4 or nx (ny) read the shared brick-major model in place; any other window
- * gets its own brick-major slowness copy in device scratch (window nodes x 4 bytes). */
+ * and at least 2 x 2 nodes, at any origin.  Each windowed solve equals the reference solve
+ * on the model cropped to that window.  Windows whose x0, y0 are multiples of 4 and whose
+ * x1 (y1) is a multiple of 4 or nx (ny) read whole bricks of the device model; any other
+ * window reads its slowness node by node from the same model (no copy). */
 typedef struct {
     int x0, x1, y0, y1;
 } tomo_window;

@@ -331,7 +331,6 @@ int tomo_ctx_destroy(tomo_ctx *ctx)
     ctx->T.release();
     ctx->qflag.release();
     ctx->qflag8.release();
-    ctx->Swin.release();
     ctx->lists.release();
     ctx->ctrl.release();
     ctx->stats.release();
@@ -460,7 +459,6 @@ struct Batch {
     long long v_total = 0;            // all window volumes back to back (floats)
     unsigned long long q_total = 0;   // bricks
     unsigned long long q_total8 = 0;  // 8^3 groups
-    long long s_total = 0;            // own slowness copies of windows not aligned to bricks
     unsigned local_bits = 1;
 };
 
@@ -476,8 +474,9 @@ int make_batch(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_wi
         if (w.x0 < 0 || w.y0 < 0 || w.x1 > g.nx || w.y1 > g.ny || w.x1 - w.x0 < 2 || w.y1 - w.y0 < 2)
             return fail(ctx, TOMO_ERR_INVALID_ARG,
                         "window " + std::to_string(s) + ": must lie inside the model, at least 2 x 2 nodes");
-        // A brick-aligned window is a view of the shared brick-major model; any other window
-        // gets its own copy, padded by edge replication like the cropped model.
+        // A brick-aligned window's bricks are bricks of the shared brick-major model; any other
+        // window gathers its slowness node by node from the model, its padding replicating the
+        // window's edge like the cropped model (node_S).
         const bool aligned = w.x0 % tomo::kBrick == 0 && w.y0 % tomo::kBrick == 0 &&
                              (w.x1 % tomo::kBrick == 0 || w.x1 == g.nx) && (w.y1 % tomo::kBrick == 0 || w.y1 == g.ny);
         ShotDesc &d = bt.sd[(size_t)s];
@@ -508,8 +507,7 @@ int make_batch(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_wi
         tomo::set_brick8(d);
         d.qbase8 = bt.q_total8;
         bt.q_total8 += (unsigned long long)d.gbz8 * d.gbx8 * d.gby8;
-        d.s_off = aligned ? -1 : bt.s_total;
-        if (!aligned) bt.s_total += nb * tomo::kBrickNodes;
+        d.s_gather = aligned ? 0 : 1;
         bt.t_total += nb * tomo::kBrickNodes;
         bt.q_total += (unsigned long long)nb;
         bt.v_total += (long long)g.nz * d.wnx * d.wny;
@@ -536,7 +534,6 @@ int upload_batch(tomo_ctx *ctx, const Batch &bt, int nrec, const tomo_point *rec
     CK(ctx->T.ensure((size_t)bt.t_total));
     CK(ctx->qflag.ensure((size_t)bt.q_total));
     CK(ctx->qflag8.ensure((size_t)bt.q_total8));
-    if (bt.s_total > 0) CK(ctx->Swin.ensure((size_t)bt.s_total));
     CK(ctx->lists.ensure((size_t)bt.q_total * 3));
     CK(ctx->shots_d.ensure((size_t)nshots));
     if (nrec > 0) {
@@ -560,7 +557,6 @@ tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, in
     const tomo_grid &g = ctx->g;
     tomo::FimLaunch p{};
     p.S = ctx->S.ptr;
-    p.Swin = bt.s_total > 0 ? ctx->Swin.ptr : nullptr;
     p.T = ctx->T.ptr;
     p.shots = ctx->shots_d.ptr;
     p.nshots = (int)bt.sd.size();
@@ -627,19 +623,16 @@ int enqueue_fim(tomo_ctx *ctx, const tomo::FimLaunch &p, size_t t_total, size_t 
                 cudaEvent_t ev_solve)
 {
     int grid = 0;
-    if (p.Swin)  // own slowness copies of the windows not aligned to bricks, from the current model
-        CK(tomo::fim_brick_windows(ctx->slow.ptr, p.shots, p.nshots, ctx->g.nz, ctx->g.nx, const_cast<float *>(p.Swin),
-                                   ctx->stream));
     if (c.brick8) {
         CK(tomo::fim_init(p.T, t_total, p.qflag, (size_t)p.list_cap, p.ctrl, p.stats, ctx->stream));
-        CK(tomo::fim_seed8(p.shots, p.nshots, p.S, p.Swin, p.gbx, p.gbz, p.T, p.qflag, p.lists, p.local_bits, p.ctrl,
+        CK(tomo::fim_seed8(p.shots, p.nshots, p.S, p.gbx, p.gbz, p.T, p.qflag, p.lists, p.local_bits, p.ctrl,
                            ctx->stream));
         if (ev_solve) CK(cudaEventRecord(ev_solve, ctx->stream));
         CK(tomo::fim_solve8(p, c.occupancy, c.ieee_sqrt, &grid, ctx->stream));
         return TOMO_OK;
     }
     CK(tomo::fim_init(p.T, t_total, p.qflag, q_total, p.ctrl, p.stats, ctx->stream));
-    CK(tomo::fim_seed(p.shots, p.nshots, p.S, p.Swin, p.gbx, p.gbz, p.T, p.qflag, p.lists, p.local_bits, p.ctrl,
+    CK(tomo::fim_seed(p.shots, p.nshots, p.S, p.gbx, p.gbz, p.T, p.qflag, p.lists, p.local_bits, p.ctrl,
                       ctx->stream, c.async ? 3 * (size_t)p.list_cap : 0));
     CK(band_reset(ctx, p));
     if (ev_solve) CK(cudaEventRecord(ev_solve, ctx->stream));
@@ -822,11 +815,7 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
     CK(tomo::fim_init(ctx->T.ptr, (size_t)bt.t_total, ctx->qflag.ptr, (size_t)bt.q_total, ctx->ctrl.ptr,
                       ctx->stats.ptr, ctx->stream));
     CK(tomo::fim_ceiling(ctx->T.ptr, ctx->shots_d.ptr, nshots, ctx->g.nz, ceiling, 1.0f + inflate, ctx->stream));
-    const float *swin = bt.s_total > 0 ? ctx->Swin.ptr : nullptr;
-    if (swin)
-        CK(tomo::fim_brick_windows(ctx->slow.ptr, ctx->shots_d.ptr, nshots, ctx->g.nz, ctx->g.nx, ctx->Swin.ptr,
-                                   ctx->stream));
-    CK(tomo::fim_seed(ctx->shots_d.ptr, nshots, ctx->S.ptr, swin, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
+    CK(tomo::fim_seed(ctx->shots_d.ptr, nshots, ctx->S.ptr, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
                       ctx->lists.ptr, bt.local_bits, ctx->ctrl.ptr, ctx->stream, cfg.async ? 3 * (size_t)bt.q_total : 0));
     CK(cudaEventRecord(ev[3], ctx->stream));
     tomo::FimLaunch p = fim_params(ctx, bt, cfg, 0);
@@ -835,7 +824,7 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
     CK(cudaEventRecord(ev[4], ctx->stream));
     // 2. check: a node below what its neighbours give came from a ceiling below the truth
     CK(cudaMemsetAsync(ctx->viol.ptr, 0, (size_t)nshots * 3 * sizeof(unsigned long long), ctx->stream));
-    CK(tomo::fim_verify(ctx->T.ptr, ctx->S.ptr, swin, ctx->shots_d.ptr, nshots, ctx->gbx, ctx->gbz, ctx->g.dx,
+    CK(tomo::fim_verify(ctx->T.ptr, ctx->S.ptr, ctx->shots_d.ptr, nshots, ctx->gbx, ctx->gbz, ctx->g.dx,
                         kVerifyRelTol, ceiling, 1.0f + inflate, ctx->g.nz, cfg.ieee_sqrt, ctx->viol.ptr,
                         ctx->stream));
     CK(cudaEventRecord(ev[5], ctx->stream));
@@ -869,7 +858,7 @@ int tomo_eik_solve_seeded(tomo_ctx *ctx, int nshots, const tomo_point *shots, co
                            ctx->stream));
         CK(tomo::fim_reset_shots(ctx->T.ptr, ctx->qflag.ptr, ctx->shots_redo.ptr, nredo, ctx->stream));
         CK(tomo::fim_init(nullptr, 0, nullptr, 0, ctx->ctrl.ptr, ctx->stats.ptr, ctx->stream));
-        CK(tomo::fim_seed(ctx->shots_redo.ptr, nredo, ctx->S.ptr, swin, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
+        CK(tomo::fim_seed(ctx->shots_redo.ptr, nredo, ctx->S.ptr, ctx->gbx, ctx->gbz, ctx->T.ptr, ctx->qflag.ptr,
                           ctx->lists.ptr, bt.local_bits, ctx->ctrl.ptr, ctx->stream, cfg.async ? 3 * (size_t)bt.q_total : 0));
         tomo::FimLaunch p2 = p;
         p2.shots = ctx->shots_redo.ptr;

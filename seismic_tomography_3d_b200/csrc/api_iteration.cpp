@@ -181,8 +181,7 @@ extern "C" int tomo_iteration(tomo_ctx *ctx, int nshots, const tomo_point *shots
                           (const void *)ctx->ray_iota.ptr, (const void *)ctx->ray_order.ptr,
                           (const void *)ctx->order_temp.ptr, (const void *)ctx->t_recv.ptr, (const void *)ctx->T.ptr,
                           (const void *)ctx->qflag.ptr, (const void *)ctx->lists.ptr, (const void *)ctx->S.ptr,
-                          (const void *)ctx->shots_d.ptr, (const void *)ctx->rec.ptr, (const void *)ctx->qflag8.ptr,
-                          (const void *)plan.p.Swin})
+                          (const void *)ctx->shots_d.ptr, (const void *)ctx->rec.ptr, (const void *)ctx->qflag8.ptr})
         push(key_a, p);
     push(key_a, plan.brick8);
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));

@@ -66,7 +66,6 @@ struct tomo_ctx {
     tomo::DevBuf<float> T;
     tomo::DevBuf<unsigned> qflag, lists, ctrl;
     tomo::DevBuf<unsigned> qflag8;  // queue flags of the 8^3 groups (TOMO_BRICK_8 solves)
-    tomo::DevBuf<float> Swin;       // brick-major slowness of windows not aligned to bricks
     tomo::DevBuf<unsigned> fim_keys, band_min, band_park, band_pcnt;  // time-band ordering (per brick keys,
                                                                       // per-shot minima, parking lists, counts)
     tomo::DevBuf<unsigned> tune_word;            // autotuner scratch (largest slowness)

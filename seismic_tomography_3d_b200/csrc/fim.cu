@@ -106,13 +106,23 @@ __device__ __forceinline__ float brick_T(const float *T, const ShotDesc &d, int 
     return __ldcg(T + d.t_off + b * kBrickNodes + (z & 3) + 4 * (x & 3) + 16 * (y & 3));
 }
 
-// Slowness of local brick b (coordinates bz, bx, by) of shot d, 64 nodes brick-major: the
-// window's own copy when its origin is not brick-aligned, else the model's brick.
-__device__ __forceinline__ const float *brick_S(const float *S, const float *Swin, int gbx, int gbz, const ShotDesc &d,
-                                                long long b, int bz, int bx, int by)
+// Slowness of node `node` (z + 4x + 16y) of the shot's local brick (bz, bx, by), from the
+// shared brick-major model.  A brick-aligned window's brick is a model brick.  Any other
+// window maps the node into the model, its padding nodes (x >= wnx, y >= wny) taking the
+// window's last node: the cropped model padded by edge replication, as the model's own
+// padding is (k_brick_model).
+__device__ __forceinline__ float node_S(const float *S, int gbx, int gbz, const ShotDesc &d, int bz, int bx, int by,
+                                        int node)
 {
-    if (d.s_off >= 0) return Swin + d.s_off + b * kBrickNodes;
-    return S + (bz + (long long)gbz * ((bx + (d.wx0 >> 2)) + (long long)gbx * (by + (d.wy0 >> 2)))) * kBrickNodes;
+    if (!d.s_gather)
+        return __ldg(S + (bz + (long long)gbz * ((bx + (d.wx0 >> 2)) + (long long)gbx * (by + (d.wy0 >> 2)))) *
+                             kBrickNodes +
+                     node);
+    const int z = 4 * bz + (node & 3);
+    const int x = min(4 * bx + ((node >> 2) & 3), d.wnx - 1) + d.wx0;
+    const int y = min(4 * by + (node >> 4), d.wny - 1) + d.wy0;
+    return __ldg(S + ((z >> 2) + (long long)gbz * ((x >> 2) + (long long)gbx * (y >> 2))) * kBrickNodes + (z & 3) +
+                 4 * (x & 3) + 16 * (y & 3));
 }
 
 // Receiver sampling (Block_FIM::write_first_arrival, block_FIM.cpp:228-262): trilinear
@@ -226,13 +236,12 @@ __device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, Br
     L.b = item & ((1u << p.local_bits) - 1u);
     const ShotDesc &d = p.shots[L.s];
     brick_coords(d, L.b, L.bz, L.bx, L.by);
-    const float *Sb = brick_S(p.S, p.Swin, p.gbx, p.gbz, d, L.b, L.bz, L.bx, L.by);
     const float *Tb = p.T + d.t_off + (long long)L.b * kBrickNodes;
     // own nodes: (z, x, y) and (z, x, y + 1) with z = lane & 3, x = (lane >> 2) & 3,
     // y = 2 (lane >> 4)
     const int n0 = lane_node(lane);
-    L.s0 = __ldg(Sb + n0);
-    L.s1 = __ldg(Sb + n0 + 16);
+    L.s0 = node_S(p.S, p.gbx, p.gbz, d, L.bz, L.bx, L.by, n0);
+    L.s1 = node_S(p.S, p.gbx, p.gbz, d, L.bz, L.bx, L.by, n0 + 16);
     L.i0 = __ldcg(Tb + n0);
     L.i1 = __ldcg(Tb + n0 + 16);
     const int ti0 = tile_idx(lane & 3, (lane >> 2) & 3, 2 * (lane >> 4));
@@ -880,9 +889,8 @@ __global__ void __launch_bounds__(256) __maxnreg__(fim_regs(MINB)) k_fim_solve8(
             float *Tb = p.T + d.t_off + b * kBrickNodes;
             float s0 = 0.f, s1 = 0.f, i0 = kInf, i1 = kInf;
             if (present) {
-                const float *Sb = brick_S(p.S, p.Swin, p.gbx, p.gbz, d, b, bz, bx, by);
-                s0 = __ldg(Sb + n0);
-                s1 = __ldg(Sb + n0 + 16);
+                s0 = node_S(p.S, p.gbx, p.gbz, d, bz, bx, by, n0);
+                s1 = node_S(p.S, p.gbx, p.gbz, d, bz, bx, by, n0 + 16);
                 i0 = __ldcg(Tb + n0);
                 i1 = __ldcg(Tb + n0 + 16);
             }
@@ -1031,7 +1039,7 @@ __global__ void __launch_bounds__(256) __maxnreg__(fim_regs(MINB)) k_fim_solve8(
     sample_receivers(p.T, p.shots, p.nshots, p.rx, p.ry, p.rz, p.nrec, p.dx, p.dy, p.dz, p.nz, p.t_recv);
 }
 
-__global__ void k_fim_seed8(const ShotDesc *shots, int nshots, const float *S, const float *Swin, int gbx, int gbz,
+__global__ void k_fim_seed8(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz,
                             float *T, unsigned *qflag8, unsigned *lists, unsigned local_bits, unsigned *ctrl)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1039,8 +1047,8 @@ __global__ void k_fim_seed8(const ShotDesc *shots, int nshots, const float *S, c
         const ShotDesc d = shots[s];
         const int bz = d.src_brick % d.nbz, t = d.src_brick / d.nbz;
         const int bx = t % d.nbx, by = t / d.nbx;
-        const float *Sb = brick_S(S, Swin, gbx, gbz, d, d.src_brick, bz, bx, by);
-        T[d.t_off + (long long)d.src_brick * kBrickNodes + d.src_node] = __fmul_rn(Sb[d.src_node], d.src_dist);
+        const float sl = node_S(S, gbx, gbz, d, bz, bx, by, d.src_node);
+        T[d.t_off + (long long)d.src_brick * kBrickNodes + d.src_node] = __fmul_rn(sl, d.src_dist);
         qflag8[d.qbase8 + d.src_brick8] = 1u;
         lists[s] = ((unsigned)s << local_bits) | (unsigned)d.src_brick8;
     }
@@ -1114,7 +1122,7 @@ __global__ void k_fim_init(float4 *T4, size_t n4, unsigned *qflag, size_t nq, un
     if (t < 4) stats[t] = 0ull;
 }
 
-__global__ void k_fim_seed(const ShotDesc *shots, int nshots, const float *S, const float *Swin, int gbx, int gbz,
+__global__ void k_fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz,
                            float *T, unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, int async)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1124,8 +1132,8 @@ __global__ void k_fim_seed(const ShotDesc *shots, int nshots, const float *S, co
         // brick-major slowness at the window's brick.
         const int bz = d.src_brick % d.nbz, t = d.src_brick / d.nbz;
         const int bx = t % d.nbx, by = t / d.nbx;
-        const float *Sb = brick_S(S, Swin, gbx, gbz, d, d.src_brick, bz, bx, by);
-        T[d.t_off + (long long)d.src_brick * kBrickNodes + d.src_node] = __fmul_rn(Sb[d.src_node], d.src_dist);
+        const float sl = node_S(S, gbx, gbz, d, bz, bx, by, d.src_node);
+        T[d.t_off + (long long)d.src_brick * kBrickNodes + d.src_node] = __fmul_rn(sl, d.src_dist);
         qflag[d.qbase + d.src_brick] = 1u;
         lists[s] = ((unsigned)s << local_bits) | (unsigned)d.src_brick;
     }
@@ -1189,7 +1197,7 @@ __global__ void k_fim_ceiling(float *T, const ShotDesc *shots, int nz, const flo
 //    This holds for smooth deficits of any size, which a per-node test cannot see.
 //  * deficit: t is below the update of its final neighbours by more than rel_tol.
 template <bool kFastSqrt>
-__global__ void k_fim_verify(const float *T, const float *S, const float *Swin, const ShotDesc *shots, int gbx, int gbz,
+__global__ void k_fim_verify(const float *T, const float *S, const ShotDesc *shots, int gbx, int gbz,
                              float h, float rel_tol, const float *ceiling, float scale, int nz, unsigned long long *viol)
 {
     const int s = blockIdx.y;
@@ -1215,8 +1223,7 @@ __global__ void k_fim_verify(const float *T, const float *S, const float *Swin, 
         const float xm = x > 0 ? brick_T(T, d, x - 1, y, z) : kInf, xp = x < ex - 1 ? brick_T(T, d, x + 1, y, z) : kInf;
         const float ym = y > 0 ? brick_T(T, d, x, y - 1, z) : kInf, yp = y < ey - 1 ? brick_T(T, d, x, y + 1, z) : kInf;
         const float zm = z > 0 ? brick_T(T, d, x, y, z - 1) : kInf, zp = z < ez - 1 ? brick_T(T, d, x, y, z + 1) : kInf;
-        const long long bl = i / kBrickNodes;
-        const float sl = __ldg(brick_S(S, Swin, gbx, gbz, d, bl, z >> 2, x >> 2, y >> 2) + (i % kBrickNodes));
+        const float sl = node_S(S, gbx, gbz, d, z >> 2, x >> 2, y >> 2, (int)(i % kBrickNodes));
         const float g = godunov_jw<kFastSqrt>(fminf(xm, xp), fminf(ym, yp), fminf(zm, zp), node_const(h, sl));
         if (g < kInf && t < g - rel_tol * g) {
             cnt++;
@@ -1315,7 +1322,7 @@ cudaError_t fim_init(float *T, size_t t_count, unsigned *qflag, size_t q_count, 
     return cudaGetLastError();
 }
 
-cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, const float *Swin, int gbx, int gbz, float *T,
+cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
                      unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st,
                      size_t ring_cap)
 {
@@ -1323,7 +1330,7 @@ cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, const fl
         const cudaError_t e = cudaMemsetAsync(lists, 0xff, ring_cap * sizeof(unsigned), st);
         if (e != cudaSuccess) return e;
     }
-    k_fim_seed<<<(nshots + 127) / 128, 128, 0, st>>>(shots, nshots, S, Swin, gbx, gbz, T, qflag, lists, local_bits,
+    k_fim_seed<<<(nshots + 127) / 128, 128, 0, st>>>(shots, nshots, S, gbx, gbz, T, qflag, lists, local_bits,
                                                      ctrl, ring_cap ? 1 : 0);
     return cudaGetLastError();
 }
@@ -1415,10 +1422,10 @@ cudaError_t fim_solve8(const FimLaunch &p, int occupancy, bool ieee_sqrt, int *g
     return ieee_sqrt ? solve8_occ<false>(p, occupancy, grid_out, st) : solve8_occ<true>(p, occupancy, grid_out, st);
 }
 
-cudaError_t fim_seed8(const ShotDesc *shots, int nshots, const float *S, const float *Swin, int gbx, int gbz, float *T,
+cudaError_t fim_seed8(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
                       unsigned *qflag8, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st)
 {
-    k_fim_seed8<<<(nshots + 127) / 128, 128, 0, st>>>(shots, nshots, S, Swin, gbx, gbz, T, qflag8, lists, local_bits,
+    k_fim_seed8<<<(nshots + 127) / 128, 128, 0, st>>>(shots, nshots, S, gbx, gbz, T, qflag8, lists, local_bits,
                                                       ctrl);
     return cudaGetLastError();
 }
@@ -1439,39 +1446,17 @@ cudaError_t fim_ceiling(float *T, const ShotDesc *shots, int nshots, int nz, con
     return cudaGetLastError();
 }
 
-cudaError_t fim_verify(const float *T, const float *S, const float *Swin, const ShotDesc *shots, int nshots, int gbx,
+cudaError_t fim_verify(const float *T, const float *S, const ShotDesc *shots, int nshots, int gbx,
                        int gbz, float h, float rel_tol, const float *ceiling, float scale, int nz, bool ieee_sqrt,
                        unsigned long long *viol, cudaStream_t st)
 {
     if (nshots < 1 || nshots > 65535) return cudaErrorInvalidValue;
     if (ieee_sqrt)
-        k_fim_verify<false><<<per_shot_grid(nshots), 256, 0, st>>>(T, S, Swin, shots, gbx, gbz, h, rel_tol, ceiling,
+        k_fim_verify<false><<<per_shot_grid(nshots), 256, 0, st>>>(T, S, shots, gbx, gbz, h, rel_tol, ceiling,
                                                                    scale, nz, viol);
     else
-        k_fim_verify<true><<<per_shot_grid(nshots), 256, 0, st>>>(T, S, Swin, shots, gbx, gbz, h, rel_tol, ceiling,
+        k_fim_verify<true><<<per_shot_grid(nshots), 256, 0, st>>>(T, S, shots, gbx, gbz, h, rel_tol, ceiling,
                                                                   scale, nz, viol);
-    return cudaGetLastError();
-}
-
-// Grid: x strides over one shot's pool nodes, y = shot; shots with s_off < 0 do nothing.
-__global__ void k_brick_windows(const float *slow, const ShotDesc *shots, int nz, int model_nx, float *Swin)
-{
-    const ShotDesc d = shots[blockIdx.y];
-    if (d.s_off < 0) return;
-    const long long n = (long long)d.nbx * d.nby * d.nbz * kBrickNodes;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        int z, x, y;
-        pool_node(d, i, z, x, y);
-        const int zc = min(z, nz - 1), xc = min(x, d.wnx - 1) + d.wx0, yc = min(y, d.wny - 1) + d.wy0;
-        Swin[d.s_off + i] = __ldg(slow + zc + (long long)nz * (xc + (long long)model_nx * yc));
-    }
-}
-
-cudaError_t fim_brick_windows(const float *slow, const ShotDesc *shots, int nshots, int nz, int model_nx, float *Swin,
-                              cudaStream_t st)
-{
-    if (nshots < 1 || nshots > 65535) return cudaErrorInvalidValue;
-    k_brick_windows<<<per_shot_grid(nshots), 256, 0, st>>>(slow, shots, nz, model_nx, Swin);
     return cudaGetLastError();
 }
 

@@ -12,7 +12,7 @@ constexpr int kBrickNodes = kBrick * kBrick * kBrick;
 
 // Per-shot descriptor of a batched solve (device array, one per shot).
 struct ShotDesc {
-    int wx0, wy0;        // window origin (nodes, multiples of kBrick)
+    int wx0, wy0;        // window origin (nodes)
     int nbx, nby, nbz;   // window brick grid
     int wnx, wny;        // window extent (nodes, unpadded)
     int src_brick;       // local brick id holding the source node
@@ -22,9 +22,8 @@ struct ShotDesc {
     unsigned long long qbase;  // offset of the shot's bricks in the queue-flag array
     long long v_off;     // offset of the shot's window volume (nz*wnx*wny, z fastest) in
                          // arrays that hold all shots' volumes back to back
-    long long s_off;     // -1: the window is brick-aligned and reads the shared brick-major
-                         // model; else offset of its own brick-major slowness copy (the
-                         // cropped model padded by edge replication) in FimLaunch::Swin
+    int s_gather;        // 0: the window is brick-aligned, its bricks are model bricks; 1:
+                         // slowness is gathered node by node from the model (node_S)
     // Brick index -> coordinates without integer division: b / nbz and (b / nbz) / nbx as
     // (n * m) >> sh, exact for every n below 2^local_bits (set by set_brick_division).
     unsigned long long divz_m, divx_m;
@@ -74,7 +73,6 @@ inline void set_brick8(ShotDesc &d)
 
 struct FimLaunch {
     const float *S;       // slowness, brick-major over the padded model
-    const float *Swin;    // brick-major slowness of the windows that are not brick-aligned
     float *T;             // traveltime pool (brick-major per shot)
     const ShotDesc *shots;
     int nshots;
@@ -117,21 +115,16 @@ cudaError_t fim_init(float *T, size_t t_count, unsigned *qflag, size_t q_count, 
                      unsigned long long *stats, cudaStream_t st);
 // ring_cap > 0: the asynchronous schedule; lists holds a ring of ring_cap = 3 x list_cap
 // items (the whole list buffer).
-cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, const float *Swin, int gbx, int gbz, float *T,
+cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
                      unsigned *qflag, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st,
                      size_t ring_cap = 0);
-// The own brick-major slowness copy of every shot with s_off >= 0: its window of the
-// natural-layout model slow (nz x model_nx x ...), padded to whole bricks by edge
-// replication (Block_FIM::expand_model on the cropped model, block_FIM.cpp:8-57).
-cudaError_t fim_brick_windows(const float *slow, const ShotDesc *shots, int nshots, int nz, int model_nx, float *Swin,
-                              cudaStream_t st);
 // async: the asynchronous schedule (seeded with ring_cap = list_cap), else rounds.
 cudaError_t fim_solve(const FimLaunch &p, int block_warps, int occupancy, bool ieee_sqrt, int *grid_out,
                       cudaStream_t st, bool async = false);
 // 8^3 bricks, rounds schedule: work items are (shot, 8^3 group); p.qflag / p.list_cap are
 // the group queue flags and count; seeded by fim_seed8.  One CTA of 8 warps per group.
 cudaError_t fim_solve8(const FimLaunch &p, int occupancy, bool ieee_sqrt, int *grid_out, cudaStream_t st);
-cudaError_t fim_seed8(const ShotDesc *shots, int nshots, const float *S, const float *Swin, int gbx, int gbz, float *T,
+cudaError_t fim_seed8(const ShotDesc *shots, int nshots, const float *S, int gbx, int gbz, float *T,
                       unsigned *qflag8, unsigned *lists, unsigned local_bits, unsigned *ctrl, cudaStream_t st);
 cudaError_t fim_unbrick(const float *T, const ShotDesc *shots, int shot, int nz, float *out,
                         cudaStream_t st);
@@ -150,7 +143,7 @@ cudaError_t fim_ceiling(float *T, const ShotDesc *shots, int nshots, int nz, con
 // counts the nodes that still hold their ceiling value (ceiling x scale, as fim_ceiling
 // stored it): nodes the solve never lowered.  Either count flags a ceiling below the
 // true time; the second catches smooth deficits of any size.
-cudaError_t fim_verify(const float *T, const float *S, const float *Swin, const ShotDesc *shots, int nshots, int gbx,
+cudaError_t fim_verify(const float *T, const float *S, const ShotDesc *shots, int nshots, int gbx,
                        int gbz, float h, float rel_tol, const float *ceiling, float scale, int nz, bool ieee_sqrt,
                        unsigned long long *viol, cudaStream_t st);
 // Resets the pool regions (T = INF, queue flags 0) of the listed shots only.

@@ -142,7 +142,7 @@ extern "C" int tomo_eik_solve_static(const float *slowness, int nx, int ny, int 
     d.src_node = (sidz & 3) + 4 * (sidx & 3) + 16 * (sidy & 3);
     d.t_off = 0;
     d.qbase = 0;
-    d.s_off = -1;  // the whole grid: the brick-major copy in the array
+    d.s_gather = 0;  // the whole grid: its bricks are the array's model bricks
     const long long nbricks = (long long)d.nbx * d.nby * d.nbz;
     unsigned local_bits = 1;
     while ((1ll << local_bits) < nbricks) local_bits++;
@@ -161,7 +161,7 @@ extern "C" int tomo_eik_solve_static(const float *slowness, int nx, int ny, int 
     CKS(fim_brick_model(slowness, S, nx, ny, nz, pad4(nx), pad4(ny), pad4(nz), st));
     // everything the solve reads is re-initialised: traveltimes, queue flags, control words
     CKS(fim_init(T, (size_t)nbricks * kBrickNodes, qflag, (size_t)nbricks, ctrl, stats, st));
-    CKS(fim_seed(desc, 1, S, nullptr, d.nbx, d.nbz, T, qflag, lists, local_bits, ctrl, st));
+    CKS(fim_seed(desc, 1, S, d.nbx, d.nbz, T, qflag, lists, local_bits, ctrl, st));
     FimLaunch p{};
     p.S = S;
     p.T = T;
