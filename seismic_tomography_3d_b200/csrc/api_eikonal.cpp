@@ -459,6 +459,7 @@ struct Batch {
     long long v_total = 0;            // all window volumes back to back (floats)
     unsigned long long q_total = 0;   // bricks
     unsigned long long q_total8 = 0;  // 8^3 groups
+    bool gather = false;              // some window reads its slowness node by node
     unsigned local_bits = 1;
 };
 
@@ -508,6 +509,7 @@ int make_batch(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tomo_wi
         d.qbase8 = bt.q_total8;
         bt.q_total8 += (unsigned long long)d.gbz8 * d.gbx8 * d.gby8;
         d.s_gather = aligned ? 0 : 1;
+        bt.gather = bt.gather || !aligned;
         bt.t_total += nb * tomo::kBrickNodes;
         bt.q_total += (unsigned long long)nb;
         bt.v_total += (long long)g.nz * d.wnx * d.wny;
@@ -560,6 +562,7 @@ tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, in
     p.T = ctx->T.ptr;
     p.shots = ctx->shots_d.ptr;
     p.nshots = (int)bt.sd.size();
+    p.gather = bt.gather ? 1 : 0;
     p.qflag = c.brick8 ? ctx->qflag8.ptr : ctx->qflag.ptr;
     p.lists = ctx->lists.ptr;
     p.list_cap = (unsigned)(c.brick8 ? bt.q_total8 : bt.q_total);

@@ -11,9 +11,13 @@
 // sums computed identically by every block.
 //
 // A' has very uneven rows: a model cell is crossed by anything from no ray to thousands
-// (config 3: median 3 non-zeros, maximum 3,206).  Rows longer than kLongRow are listed
-// once per call (cgls_long_rows, in row order) and each is summed by a whole block; the
-// 32-lane groups take the rest, so the longest row no longer sets the length of A's.
+// (config 3: median 3 non-zeros, maximum 3,206; config 5: 778 on average).  Rows longer
+// than long_row_limit -- 8 x the mean row length, at least kLongRow -- are listed once per
+// call (cgls_long_rows, in row order) and each is summed by a whole block; the 32-lane
+// groups take the rest, so the longest row no longer sets the length of A's.  A fixed
+// limit of kLongRow sent nearly every config-5 row to a block, one row at a time per block:
+// 2.26 ms per iteration there against 1.83 ms with the relative limit and the unrolled
+// gathers (config 3: 0.111 -> 0.094 ms).
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
 
@@ -56,12 +60,19 @@ __device__ __forceinline__ double grid_sum(const double *partials, int nb, doubl
     return v;
 }
 
+// Rows of A' longer than this are summed by whole blocks (t_ptr[M] = the non-zero count).
+__device__ __forceinline__ int long_row_limit(const int *t_ptr, int M)
+{
+    const long long mean8 = 8ll * t_ptr[M] / (M > 0 ? M : 1);
+    return mean8 > kLongRow ? (int)mean8 : kLongRow;
+}
+
 // y = M x for a CSR matrix with `G` lanes per row: FP32 matrix values, FP64 vectors and
-// row sums.  Returns this thread's share of y'y.  kSkipLong: rows longer than kLongRow
-// are left to spmv_long.
+// row sums.  Returns this thread's share of y'y.  kSkipLong: rows longer than long_row
+// are left to spmv_long.  The gathers are unrolled 4 deep (same summation order).
 template <int G, bool kSkipLong = false>
 __device__ __forceinline__ double spmv(const int *ptr, const int *idx, const float *val, const double *x, double *y,
-                                       int nrows)
+                                       int nrows, int long_row = 0)
 {
     const int lane = threadIdx.x & 31;
     const int sub = lane % G;
@@ -75,9 +86,11 @@ __device__ __forceinline__ double spmv(const int *ptr, const int *idx, const flo
         bool mine = row < nrows;
         if (mine) {
             const int b = __ldg(ptr + row), e = __ldg(ptr + row + 1);
-            mine = !kSkipLong || e - b <= kLongRow;
-            if (mine)
+            mine = !kSkipLong || e - b <= long_row;
+            if (mine) {
+#pragma unroll 4
                 for (int k = b + sub; k < e; k += G) acc += (double)__ldg(val + k) * __ldcg(x + __ldg(idx + k));
+            }
         }
         for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o, G);
         if (mine && sub == 0) {
@@ -114,7 +127,7 @@ __device__ __forceinline__ double spmv_long(const int *ptr, const int *idx, cons
 __device__ __forceinline__ double spmv_t(const CglsLaunch &p, const double *x, double *y, double *sh)
 {
     const double l = spmv_long(p.t_ptr, p.t_idx, p.t_val, x, y, p.long_rows, p.n_long, sh);
-    return l + spmv<32, true>(p.t_ptr, p.t_idx, p.t_val, x, y, p.M);
+    return l + spmv<32, true>(p.t_ptr, p.t_idx, p.t_val, x, y, p.M, long_row_limit(p.t_ptr, p.M));
 }
 
 }  // namespace
@@ -198,7 +211,8 @@ cudaError_t cgls_grid(int *grid)
 namespace {
 struct IsLongRow {
     const int *ptr;
-    __host__ __device__ bool operator()(int r) const { return ptr[r + 1] - ptr[r] > kLongRow; }
+    int M;
+    __device__ bool operator()(int r) const { return ptr[r + 1] - ptr[r] > long_row_limit(ptr, M); }
 };
 }  // namespace
 
@@ -206,7 +220,7 @@ cudaError_t cgls_long_rows(const int *t_ptr, int M, int *rows, int *n_long, void
                            cudaStream_t st)
 {
     return cub::DeviceSelect::If(temp, *temp_bytes, thrust::counting_iterator<int>(0), rows, n_long, M,
-                                 IsLongRow{t_ptr}, st);
+                                 IsLongRow{t_ptr, M}, st);
 }
 
 cudaError_t cgls_run(const CglsLaunch &p, int grid, cudaStream_t st)

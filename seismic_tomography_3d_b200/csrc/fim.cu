@@ -111,18 +111,36 @@ __device__ __forceinline__ float brick_T(const float *T, const ShotDesc &d, int 
 // window maps the node into the model, its padding nodes (x >= wnx, y >= wny) taking the
 // window's last node: the cropped model padded by edge replication, as the model's own
 // padding is (k_brick_model).
-__device__ __forceinline__ float node_S(const float *S, int gbx, int gbz, const ShotDesc &d, int bz, int bx, int by,
-                                        int node)
+__device__ __forceinline__ const float *model_brick_S(const float *S, int gbx, int gbz, const ShotDesc &d, int bz,
+                                                      int bx, int by)
 {
-    if (!d.s_gather)
-        return __ldg(S + (bz + (long long)gbz * ((bx + (d.wx0 >> 2)) + (long long)gbx * (by + (d.wy0 >> 2)))) *
-                             kBrickNodes +
-                     node);
+    return S + (bz + (long long)gbz * ((bx + (d.wx0 >> 2)) + (long long)gbx * (by + (d.wy0 >> 2)))) * kBrickNodes;
+}
+
+__device__ __forceinline__ float gather_S(const float *S, int gbx, int gbz, const ShotDesc &d, int bz, int bx, int by,
+                                          int node)
+{
     const int z = 4 * bz + (node & 3);
     const int x = min(4 * bx + ((node >> 2) & 3), d.wnx - 1) + d.wx0;
     const int y = min(4 * by + (node >> 4), d.wny - 1) + d.wy0;
     return __ldg(S + ((z >> 2) + (long long)gbz * ((x >> 2) + (long long)gbx * (y >> 2))) * kBrickNodes + (z & 3) +
                  4 * (x & 3) + 16 * (y & 3));
+}
+
+__device__ __forceinline__ float node_S(const float *S, int gbx, int gbz, const ShotDesc &d, int bz, int bx, int by,
+                                        int node)
+{
+    if (!d.s_gather) return __ldg(model_brick_S(S, gbx, gbz, d, bz, bx, by) + node);
+    return gather_S(S, gbx, gbz, d, bz, bx, by, node);
+}
+
+// The relaxation kernel's two nodes (node, node + 16) of a gathered window, out of line so
+// that the brick-aligned path keeps its registers and instruction stream.
+__device__ __forceinline__ void gather_S2(const float *S, int gbx, int gbz, const ShotDesc &d, int bz, int bx, int by,
+                                       int node, float &s0, float &s1)
+{
+    s0 = gather_S(S, gbx, gbz, d, bz, bx, by, node);
+    s1 = gather_S(S, gbx, gbz, d, bz, bx, by, node + 16);
 }
 
 // Receiver sampling (Block_FIM::write_first_arrival, block_FIM.cpp:228-262): trilinear
@@ -228,7 +246,10 @@ __device__ __forceinline__ long long halo_slot(const ShotDesc &d, unsigned b, in
 }
 
 // Loads work item `item` into L and into the warp's tile: the lane's two nodes and its three
-// face-halo cells.  The caller synchronises the warp before the tile is read.
+// face-halo cells.  The caller synchronises the warp before the tile is read.  kGather: some
+// shot of the batch gathers its slowness by node (a separate instance, so that batches of
+// brick-aligned windows keep the plain load path).
+template <bool kGather>
 __device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, BrickLoad &L, float *tile)
 {
     const int lane = threadIdx.x & 31;
@@ -240,8 +261,13 @@ __device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, Br
     // own nodes: (z, x, y) and (z, x, y + 1) with z = lane & 3, x = (lane >> 2) & 3,
     // y = 2 (lane >> 4)
     const int n0 = lane_node(lane);
-    L.s0 = node_S(p.S, p.gbx, p.gbz, d, L.bz, L.bx, L.by, n0);
-    L.s1 = node_S(p.S, p.gbx, p.gbz, d, L.bz, L.bx, L.by, n0 + 16);
+    if (!kGather || !d.s_gather) {
+        const float *Sb = model_brick_S(p.S, p.gbx, p.gbz, d, L.bz, L.bx, L.by);
+        L.s0 = __ldg(Sb + n0);
+        L.s1 = __ldg(Sb + n0 + 16);
+    } else {
+        gather_S2(p.S, p.gbx, p.gbz, d, L.bz, L.bx, L.by, n0, L.s0, L.s1);
+    }
     L.i0 = __ldcg(Tb + n0);
     L.i1 = __ldcg(Tb + n0 + 16);
     const int ti0 = tile_idx(lane & 3, (lane >> 2) & 3, 2 * (lane >> 4));
@@ -592,7 +618,7 @@ constexpr int fim_regs(int minb) { return minb <= 1 ? 255 : (65536 / (minb * 256
 // Up to 16 warps per CTA: 2 CTAs x 16 warps measured 1 % faster than 4 x 8 on the config-2
 // batch (half as many CTAs arrive at each round barrier).  kBand: time-band ordering
 // (FimLaunch::band > 0), a separate instance so that the plain kernel keeps its registers.
-template <int MINB, bool kFastSqrt, bool kBand>
+template <int MINB, bool kFastSqrt, bool kBand, bool kGather>
 __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_solve(FimLaunch p)
 {
     extern __shared__ float smem[];
@@ -676,7 +702,7 @@ __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_solve(F
                 tb = __ldcg(p.band_min + (size_t)((round + 2u) % 3u) * p.nshots + s);
             }
             BrickLoad A;
-            load_brick(p, item, A, tile);
+            load_brick<kGather>(p, item, A, tile);
             unsigned next = 0;
             bool defer = false;
             if (kBand && kb != kNoKey) {
@@ -762,7 +788,7 @@ __global__ void __launch_bounds__(256, MINB) k_fim_async(FimLaunch p)
         item = __shfl_sync(kFull, item, 0);
         __threadfence();  // the previous owner's stores of neighbouring bricks are visible
         BrickLoad A;
-        load_brick(p, item, A, tile);
+        load_brick<true>(p, item, A, tile);
         unsigned unused = 0, unused_next = 0;
         relax_brick<kFastSqrt, true>(p, A, 0u, tile, ws, nullptr, nullptr, unused, nullptr, unused_next);
     }
@@ -1341,9 +1367,11 @@ template <int MINB, bool kFastSqrt>
 static cudaError_t launch_solve(const FimLaunch &p, int block_warps, bool async, int *grid_out, cudaStream_t st)
 {
     const bool band = !async && p.band > 0.f;
-    const void *fn = async  ? (const void *)k_fim_async<MINB, kFastSqrt>
-                     : band ? (const void *)k_fim_solve<MINB, kFastSqrt, true>
-                            : (const void *)k_fim_solve<MINB, kFastSqrt, false>;
+    const void *fn = async          ? (const void *)k_fim_async<MINB, kFastSqrt>
+                     : p.gather     ? (band ? (const void *)k_fim_solve<MINB, kFastSqrt, true, true>
+                                            : (const void *)k_fim_solve<MINB, kFastSqrt, false, true>)
+                     : band         ? (const void *)k_fim_solve<MINB, kFastSqrt, true, false>
+                                    : (const void *)k_fim_solve<MINB, kFastSqrt, false, false>;
     if (async && block_warps > 8) block_warps = 8;  // the asynchronous kernel's CTAs hold 8 warps at most
     const int threads = 32 * block_warps;
     // per warp: its tile, its push buffer and (time band) the pushes' keys

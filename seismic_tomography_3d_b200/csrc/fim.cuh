@@ -83,6 +83,7 @@ struct FimLaunch {
     unsigned long long *stats;  // [0] activations, [1] inner iterations, [2] async activation
                                 // count, [3] activations that lowered no node
     int gbx, gbz;         // global brick grid (x, z) for S addressing
+    int gather;           // some shot has ShotDesc::s_gather set (selects the gathering kernel)
     float h;              // grid spacing of the update (dx, as the reference)
     int max_inner, max_rounds;
     float change_tol;     // face drops <= this do not re-queue the neighbour
