@@ -134,10 +134,9 @@ __device__ __forceinline__ float node_S(const float *S, int gbx, int gbz, const 
     return gather_S(S, gbx, gbz, d, bz, bx, by, node);
 }
 
-// The relaxation kernel's two nodes (node, node + 16) of a gathered window, out of line so
-// that the brick-aligned path keeps its registers and instruction stream.
+// Slowness of a relaxation lane's two nodes (node, node + 16) in a gathered window.
 __device__ __forceinline__ void gather_S2(const float *S, int gbx, int gbz, const ShotDesc &d, int bz, int bx, int by,
-                                       int node, float &s0, float &s1)
+                                          int node, float &s0, float &s1)
 {
     s0 = gather_S(S, gbx, gbz, d, bz, bx, by, node);
     s1 = gather_S(S, gbx, gbz, d, bz, bx, by, node + 16);

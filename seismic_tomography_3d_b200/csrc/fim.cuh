@@ -73,6 +73,9 @@ inline void set_brick8(ShotDesc &d)
 
 struct FimLaunch {
     const float *S;       // slowness, brick-major over the padded model
+    const void *spare;    // unused.  Without this slot (and with `gather` beside gbx, gbz)
+                          // the config-2 batch ran 3 % slower, same inputs, in alternating
+                          // runs: the generated code of the parameter loads changes
     float *T;             // traveltime pool (brick-major per shot)
     const ShotDesc *shots;
     int nshots;
@@ -83,7 +86,6 @@ struct FimLaunch {
     unsigned long long *stats;  // [0] activations, [1] inner iterations, [2] async activation
                                 // count, [3] activations that lowered no node
     int gbx, gbz;         // global brick grid (x, z) for S addressing
-    int gather;           // some shot has ShotDesc::s_gather set (selects the gathering kernel)
     float h;              // grid spacing of the update (dx, as the reference)
     int max_inner, max_rounds;
     float change_tol;     // face drops <= this do not re-queue the neighbour
@@ -107,6 +109,7 @@ struct FimLaunch {
     float *t_recv;        // nshots*nrec
     float dx, dy, dz;
     int nz;
+    int gather;           // some shot has ShotDesc::s_gather set (selects the gathering kernel)
 };
 
 // Host-callable launchers (fim.cu).
