@@ -220,6 +220,27 @@ def test_sparse_cgls_gpu_long_columns(tomo, oracle_mod):
     np.testing.assert_array_equal(x, x2)  # fixed-order reductions: deterministic
 
 
+def test_sparse_cgls_gpu_dense_columns(tomo, oracle_mod):
+    """Every column crossed by hundreds of rays (as in the large inversion, 778 non-zeros per
+    row of A' on average): rows of A' up to 8x the mean length stay on the 32-lane path,
+    longer ones go to whole blocks; both paths against the FP64 oracle, deterministic."""
+    rng = np.random.default_rng(13)
+    N, M = 4000, 120
+    jA = np.concatenate([rng.integers(0, M, 90000),              # ~750 per column
+                         np.full(9000, 7), np.full(7000, 61)])   # two columns far above 8x
+    iA = rng.integers(0, N, jA.size).astype(np.int32)
+    jA = jA.astype(np.int32)
+    vA = rng.uniform(0.1, 2.0, jA.size).astype(np.float32)
+    B = rng.standard_normal(N).astype(np.float32)
+    counts = np.bincount(jA, minlength=M)
+    limit = max(256, 8 * jA.size // M)
+    assert ((counts > 256) & (counts <= limit)).sum() > 100 and (counts > limit).sum() == 2
+    x = tomo.sparse_cgls_gpu(iA, jA, vA, B, N, M, 15)
+    x64, _ = oracle_mod.cgls_f64(N, M, iA, jA, vA, B, 15)
+    assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-5
+    np.testing.assert_array_equal(x, tomo.sparse_cgls_gpu(iA, jA, vA, B, N, M, 15))
+
+
 def test_full_iteration_recovered_model(tomo, oracle_mod, small_survey):
     """Device iteration vs the oracle pipeline on the device traveltimes: recovered
     velocity models agree within 0.5 % RMS; in practice ~1e-7."""
