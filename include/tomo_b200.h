@@ -166,6 +166,17 @@ int tomo_set_velocity(tomo_ctx *ctx, const float *velocity);
 int tomo_set_slowness(tomo_ctx *ctx, const float *slowness);
 /* Copies the current slowness (after model updates) to the host. */
 int tomo_get_slowness(tomo_ctx *ctx, float *slowness_out);
+/* Staged velocity upload, for callers that solve one model after another.
+ * tomo_stage_velocity starts copying the next velocity model (m/s, host, nz*nx*ny) into
+ * device staging memory on the context's own copy stream and returns without waiting, so
+ * the copy overlaps the work already queued on the context (a solve of the current model).
+ * tomo_commit_velocity then makes the staged model the context's model (slowness = 1/v,
+ * as tomo_set_velocity) once its copy has landed, without blocking the host.  The host
+ * buffer must stay valid and unchanged until a blocking call on the context (a solve) has
+ * returned after the commit; the copy overlaps only from page-locked host memory.
+ * tomo_commit_velocity without a staged model returns TOMO_ERR_STATE. */
+int tomo_stage_velocity(tomo_ctx *ctx, const float *velocity);
+int tomo_commit_velocity(tomo_ctx *ctx);
 
 /* ------------------------------------------------------------ eikonal solve --------- */
 /* Solves nshots first-arrival traveltime fields in ONE persistent launch.

@@ -104,6 +104,8 @@ def load_library(path: str = LIB_PATH):
     lib.tomo_set_velocity.argtypes = [V, V]
     lib.tomo_set_slowness.argtypes = [V, V]
     lib.tomo_get_slowness.argtypes = [V, V]
+    lib.tomo_stage_velocity.argtypes = [V, V]
+    lib.tomo_commit_velocity.argtypes = [V]
     lib.tomo_eik_solve.argtypes = [V, I, P(Point), P(Window), I, P(Point), V, P(EikOpts), P(EikStats)]
     lib.tomo_eik_volume.argtypes = [V, I, V]
     lib.tomo_eik_window.argtypes = [V, I, P(Window)]
@@ -283,6 +285,25 @@ class Context:
         v = _f32(v)
         assert v.shape == self.shape, (v.shape, self.shape)
         self._check(self.lib.tomo_set_velocity(self.h, v.ctypes.data))
+
+    def stage_velocity(self, v):
+        """Starts copying the next velocity model to the device (tomo_stage_velocity); the
+        array is kept alive here until the next stage call.  Page-locked memory (a pinned
+        torch tensor's data) overlaps the copy with queued work."""
+        if isinstance(v, np.ndarray):
+            v = _f32(v)
+            assert v.shape == self.shape, (v.shape, self.shape)
+            self._staged_host = v
+            ptr = v.ctypes.data
+        else:  # a (pinned) float32 torch tensor of the model's shape
+            assert tuple(v.shape) == self.shape and str(v.dtype) == "torch.float32" and v.is_contiguous()
+            self._staged_host = v
+            ptr = v.data_ptr()
+        self._check(self.lib.tomo_stage_velocity(self.h, ptr))
+
+    def commit_velocity(self):
+        """The staged velocity becomes the model (tomo_commit_velocity)."""
+        self._check(self.lib.tomo_commit_velocity(self.h))
 
     def set_slowness(self, s):
         s = _f32(s)

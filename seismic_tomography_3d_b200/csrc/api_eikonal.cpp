@@ -323,9 +323,11 @@ int tomo_ctx_destroy(tomo_ctx *ctx)
     if (!ctx) return TOMO_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     tomo_release_iteration(ctx);
     tomo_release_tomography(ctx);
     ctx->slow.release();
+    ctx->vel_stage.release();
     ctx->S.release();
     ctx->scratch_v.release();
     ctx->T.release();
@@ -345,6 +347,9 @@ int tomo_ctx_destroy(tomo_ctx *ctx)
     for (auto &ev : ctx->ev)
         if (ev) cudaEventDestroy(ev);
     if (ctx->pinned_ctrl) cudaFreeHost(ctx->pinned_ctrl);
+    if (ctx->ev_staged) cudaEventDestroy(ctx->ev_staged);
+    if (ctx->ev_stage_free) cudaEventDestroy(ctx->ev_stage_free);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return TOMO_OK;
@@ -368,6 +373,46 @@ int tomo_set_slowness(tomo_ctx *ctx, const float *slowness)
     if (!slowness) return fail(ctx, TOMO_ERR_INVALID_ARG, "slowness is NULL");
     CK(cudaSetDevice(ctx->device));
     return upload_model(ctx, slowness, false);
+}
+
+int tomo_stage_velocity(tomo_ctx *ctx, const float *velocity)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (!velocity) return fail(ctx, TOMO_ERR_INVALID_ARG, "velocity is NULL");
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->ev_staged, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->ev_stage_free, cudaEventDisableTiming));
+    }
+    const size_t n = (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz;
+    CK(ctx->vel_stage.ensure(n));
+    // the staging buffer is rewritten only after the last commit's conversion has read it
+    if (ctx->stage_read) CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_stage_free, 0));
+    CK(cudaMemcpyAsync(ctx->vel_stage.ptr, velocity, n * sizeof(float), cudaMemcpyHostToDevice, ctx->copy_stream));
+    CK(cudaEventRecord(ctx->ev_staged, ctx->copy_stream));
+    ctx->staged = true;
+    return TOMO_OK;
+}
+
+int tomo_commit_velocity(tomo_ctx *ctx)
+{
+    if (!ctx) return TOMO_ERR_INVALID_ARG;
+    if (!ctx->staged) return fail(ctx, TOMO_ERR_STATE, "no staged velocity (tomo_stage_velocity)");
+    CK(cudaSetDevice(ctx->device));
+    const size_t n = (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz;
+    CK(ctx->slow.ensure(n));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_staged, 0));
+    CK(tomo::velocity_to_slowness(ctx->vel_stage.ptr, ctx->slow.ptr, n, ctx->stream));
+    CK(cudaEventRecord(ctx->ev_stage_free, ctx->stream));
+    ctx->stage_read = true;
+    ctx->staged = false;
+    int rc = tomo::model_buffers(ctx);
+    if (rc != TOMO_OK) return rc;
+    rc = tomo::rebrick_model(ctx);
+    if (rc != TOMO_OK) return rc;
+    ctx->have_model = true;
+    return TOMO_OK;
 }
 
 int tomo_get_slowness(tomo_ctx *ctx, float *out)

@@ -58,6 +58,12 @@ struct tomo_ctx {
     // padded model (multiple of the brick edge) and its brick grid
     int nxx = 0, nyy = 0, nzz = 0, gbx = 0, gby = 0, gbz = 0;
     tomo::DevBuf<float> slow;      // natural layout, nz*nx*ny (the model state)
+    // staged velocity uploads (tomo_stage_velocity / tomo_commit_velocity)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_staged = nullptr;      // the staged copy has landed
+    cudaEvent_t ev_stage_free = nullptr;  // the last commit has read the staging buffer
+    tomo::DevBuf<float> vel_stage;
+    bool staged = false, stage_read = false;
     tomo::DevBuf<float> S;         // brick-major padded slowness
     tomo::DevBuf<float> scratch_v; // staging for uploads / unbrick
     bool have_model = false;

@@ -344,3 +344,36 @@ def test_time_band_values(tomo):
         for bad in (float("nan"), float("inf"), -float("inf")):
             with pytest.raises(tomo.TomoError):
                 ctx.eik_solve(sv.shots, time_band=bad)
+
+
+def test_staged_velocity_upload(tomo):
+    """tomo_stage_velocity / tomo_commit_velocity: the next model is copied while the current
+    one is solved; each solve sees the model committed before it, as with tomo_set_velocity."""
+    nx, ny, nz = 37, 30, 14
+    sv = wl.small(41, nx, ny, nz, nshots=3, nrec=20)
+    v1 = sv.velocity
+    v2 = (sv.velocity * np.float32(1.1)).astype(np.float32)
+    with tomo.Context(nx, ny, nz, sv.h) as ctx:
+        with pytest.raises(tomo.TomoError):
+            ctx.commit_velocity()  # nothing staged
+        ctx.set_velocity(v1)
+        r1, _ = ctx.eik_solve(sv.shots, receivers=sv.receivers)
+        s1 = ctx.get_slowness()
+        ctx.set_velocity(v2)
+        r2, _ = ctx.eik_solve(sv.shots, receivers=sv.receivers)
+        s2 = ctx.get_slowness()
+        ctx.stage_velocity(v1)
+        ctx.commit_velocity()
+        ctx.stage_velocity(v2)  # copied while the next solve runs
+        q1, _ = ctx.eik_solve(sv.shots, receivers=sv.receivers)
+        np.testing.assert_array_equal(ctx.get_slowness(), s1)
+        ctx.commit_velocity()
+        q2, _ = ctx.eik_solve(sv.shots, receivers=sv.receivers)
+        np.testing.assert_array_equal(ctx.get_slowness(), s2)
+        with pytest.raises(tomo.TomoError):
+            ctx.commit_velocity()  # the staged model was used
+    np.testing.assert_allclose(q1, r1, rtol=1e-5)
+    np.testing.assert_allclose(q2, r2, rtol=1e-5)
+    m = r1 > 0
+    assert np.min(r1[m] / r2[m]) > 1.09  # the models differ: times scale by 1 / 1.1
+    assert np.max(np.abs(r2[m] * 1.1 - r1[m]) / r1[m]) < 1e-4
