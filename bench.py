@@ -649,7 +649,7 @@ def run_ours(args):
 
 def unaligned_windows_object(ctx, sv, solver, stream, steps, barrier, dist, world, rank):
     """The same shots on the seeded crops themselves (any origin, not rounded out to bricks):
-    each window then gets its own brick-major slowness copy, built inside every solve."""
+    those windows read their slowness node by node from the shared model."""
     import torch
 
     from seismic_tomography_3d_b200 import workloads as wl

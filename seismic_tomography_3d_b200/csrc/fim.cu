@@ -11,8 +11,9 @@
 //  * A brick re-queues a neighbour only when a value on the shared face dropped, and
 //    itself when its in-brick iteration cap was hit.  Updates are monotone (min), so this
 //    chaotic relaxation converges to the same fixed point as Block_FIM's schedule.
-//  * Slowness is read from one brick-major copy of the model shared by all shots; each
-//    shot's window is a brick-aligned sub-grid of it.
+//  * Slowness is read from one brick-major copy of the model shared by all shots: whole
+//    bricks for a brick-aligned window, node by node (edge replicated into the padding)
+//    for any other window.
 //  * Optionally (time band), pushes carry the pushing brick's new time, and a brick far
 //    ahead of its shot's front waits on a parking list: rounds then follow traveltime
 //    rather than brick-graph distance, which removes the re-activation cascades of smooth

@@ -148,7 +148,8 @@ def config2_model(seed=2, nx=201, ny=201, nz=101, h=12.5):
 
 def config2(seed=2, nx=201, ny=201, nz=101, h=12.5, n_side=8, aligned=True) -> Survey:
     """aligned=False: each window is the seeded crop itself, at any origin (the solver then
-    builds a slowness copy per window); aligned=True rounds the same crops out to bricks."""
+    gathers those windows' slowness node by node); aligned=True rounds the same crops out
+    to bricks."""
     v, rng = config2_model(seed, nx, ny, nz, h)
     shots = jittered_shots(rng, nx, ny, h, n_side)
     wins = []

@@ -112,10 +112,10 @@ def _any_windows(rng, sv, n):
 
 @pytest.mark.parametrize("brick", sorted(BRICKS))
 def test_unaligned_windows_match_cropped_oracle(tomo, oracle_mod, brick):
-    """Windows of any origin and end: each gets its own brick-major slowness copy (the
-    cropped model padded by edge replication, as the reference pads a model), so each
-    windowed solve equals the oracle on the cropped model; the receivers follow the
-    window's offset."""
+    """Windows of any origin and end: each reads its slowness node by node from the shared
+    model, its padding replicating the window's edge (the cropped model padded as the
+    reference pads a model), so each windowed solve equals the oracle on the cropped model;
+    the receivers follow the window's offset."""
     nx, ny, nz = 37, 30, 14
     sv = wl.small(23, nx, ny, nz, nshots=6, nrec=30)
     wins = _any_windows(np.random.default_rng(23), sv, 6)
@@ -137,6 +137,27 @@ def test_unaligned_windows_match_cropped_oracle(tomo, oracle_mod, brick):
             ref = oracle_mod.first_arrival(T, sv.h, rx[inside], ry[inside], sv.receivers[inside, 2])
             np.testing.assert_array_equal(t_recv[i][inside], ref)
             assert np.all(t_recv[i][~inside] >= 1e5)
+
+
+@pytest.mark.parametrize("brick", sorted(BRICKS))
+def test_unaligned_window_edge_cases(tomo, oracle_mod, brick):
+    """Unaligned origins against the model's far edges (37 x 30 is not a multiple of 4, so
+    the model's own padding and the window's meet), a 2-node-wide window, and a window whose
+    padding is all replicated edge, in one batch with an aligned one."""
+    nx, ny, nz = 37, 30, 14
+    sv = wl.small(31, nx, ny, nz, nshots=1)
+    wins = np.array([[33, 37, 0, 30], [1, 3, 27, 30], [5, 37, 2, 29], [9, 15, 6, 7 + 2], [0, 36, 0, 28]],
+                    np.int32)
+    shots = np.array([[(w[0] + (w[1] - w[0]) // 2) * sv.h, (w[2] + (w[3] - w[2]) // 2) * sv.h, 2 * sv.h]
+                      for w in wins], np.float32)
+    with tomo.Context(nx, ny, nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(shots, windows=wins, brick=BRICKS[brick])
+        for i in range(len(wins)):
+            T = ctx.eik_volume(i)
+            Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, shots[i], wins[i])
+            assert T.shape == Tref.shape
+            assert rel_err(T, Tref, sv.h, sv.velocity.max()) < REL_TOL, i
 
 
 def test_batch_equals_single_solves(tomo):

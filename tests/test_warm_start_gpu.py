@@ -175,9 +175,9 @@ def test_smooth_upper_bound_is_accepted(big_case):
 
 
 def test_unaligned_windows_warm_start(tomo):
-    """The warm-started solve and its check read the own slowness copies of windows that
-    are not brick-aligned: an upper bound gives the plain result with no fallback, a low
-    ceiling falls back."""
+    """The warm-started solve and its check gather the slowness of windows that are not
+    brick-aligned node by node: an upper bound gives the plain result with no fallback, a
+    low ceiling falls back."""
     import torch
 
     sv = wl.small(61, 40, 36, 20, nshots=3)
