@@ -30,6 +30,7 @@ scaling, no data-path collective); time = max over ranks.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -519,36 +520,42 @@ def run_ours(args):
 
     # ---- e2e: host buffers through the C ABI ---------------------------------------------
     nrec = len(sv.receivers)
-    t_out = np.empty((ns, nrec), np.float32)
+    t_pinned = torch.empty((ns, nrec), dtype=torch.float32).pin_memory()
+    t_out = t_pinned.numpy()  # receiver times land in page-locked host memory
     lib = ctx.lib
     # Every step uploads its velocity model from pinned host memory and reads its receiver
     # times back.  The upload of step k + 1 is staged (tomo_stage_velocity) before step k's
     # solve, so the copy runs during that solve; step 0's upload is not overlapped.
+    # The end-to-end loops run more steps than the resident one (host-side jitter of the
+    # calling process shows up in them), with Python's garbage collector paused.
+    e2e_steps = max(3 * args.steps, 30)
+    gc.disable()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     ctx.stage_velocity(vel_pinned)
-    for k in range(args.steps):
+    for k in range(e2e_steps):
         ctx.commit_velocity()
-        if k + 1 < args.steps:
+        if k + 1 < e2e_steps:
             ctx.stage_velocity(vel_pinned)
-        t_out, _ = ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=True, **SOLVER_RUN)
+        ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=True, out=t_out, **SOLVER_RUN)
     e1.record(stream)
     barrier()
-    e2e_ms = e0.elapsed_time(e1) / args.steps
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
     e2e_ms = max_over_ranks(e2e_ms, dist, 'cuda')
     e2e_value = world * ns / (e2e_ms / 1000.0)
     # the same steps with the blocking upload (tomo_set_velocity) before each solve
     barrier()
     s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         tomo_rc = lib.tomo_set_velocity(ctx.h, vel_pinned.data_ptr())
         assert tomo_rc == 0
-        ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=True, **SOLVER_RUN)
+        ctx.eik_solve(sv.shots, windows=sv.windows, receivers=sv.receivers, want_recv=True, out=t_out, **SOLVER_RUN)
     s1.record(stream)
     barrier()
-    serial_ms = max_over_ranks(s0.elapsed_time(s1) / args.steps, dist, 'cuda')
+    gc.enable()
+    serial_ms = max_over_ranks(s0.elapsed_time(s1) / e2e_steps, dist, 'cuda')
     # fields of the timed setting (the last e2e solve) for the oracle check of the CPU leg
     cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
     acc_idx = sample_shots(sv) if cpu_leg else []
@@ -601,7 +608,9 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": int(sv.velocity.nbytes),
                     "d2h_bytes_per_step": int(t_out.nbytes) if t_out is not None else 0,
-                    "upload": "pinned host velocity per step, staged during the previous step's solve",
+                    "steps": e2e_steps,
+                    "upload": "pinned host velocity per step, staged during the previous step's solve; "
+                              "receiver times into pinned host memory",
                     "serial_upload": {"value": world * ns / (serial_ms / 1000.0), "unit": UNIT,
                                       "ms_per_step": serial_ms}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -318,9 +318,11 @@ class Context:
     # -- eikonal ------------------------------------------------------------------------
     def eik_solve(self, shots, windows=None, receivers=None, want_recv=True, max_inner=0, max_rounds=0,
                   block_warps=0, op=0, occupancy=0, change_tol=0.0, inner_tol=0.0, ieee_sqrt=0,
-                  sweep_groups=0, schedule=0, time_band=0.0, spin_limit=0, brick=0):
+                  sweep_groups=0, schedule=0, time_band=0.0, spin_limit=0, brick=0, out=None):
         """Batched solve.  shots (n,3) metres; windows (n,4) [x0,x1,y0,y1] nodes or None;
-        receivers (m,3).  Returns (t_recv (n,m) float32 or None, stats dict)."""
+        receivers (m,3).  Returns (t_recv (n,m) float32 or None, stats dict).  out: a
+        C-contiguous float32 (n,m) array to receive t_recv (e.g. a view of page-locked memory,
+        which the device copies into directly)."""
         sp, ns, _s = _points(shots)
         wp = _w = None
         if windows is not None:
@@ -329,7 +331,12 @@ class Context:
         rp = _r = None
         if receivers is not None and len(receivers):
             rp, nr, _r = _points(receivers)
-        out = np.empty((ns, nr), np.float32) if (want_recv and nr) else None
+        if want_recv and nr and out is not None:
+            assert out.shape == (ns, nr) and out.dtype == np.float32 and out.flags["C_CONTIGUOUS"]
+        elif want_recv and nr:
+            out = np.empty((ns, nr), np.float32)
+        else:
+            out = None
         opts = EikOpts(op, max_inner, max_rounds, brick, block_warps, occupancy, change_tol, inner_tol, ieee_sqrt,
                        sweep_groups, schedule, time_band, spin_limit)
         st = EikStats()
