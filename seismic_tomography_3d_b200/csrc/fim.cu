@@ -270,17 +270,21 @@ __device__ __forceinline__ void load_brick(const FimLaunch &p, unsigned item, Br
     }
     L.i0 = __ldcg(Tb + n0);
     L.i1 = __ldcg(Tb + n0 + 16);
+    // Missing neighbours (grid edge) are INF; the reference's "halo = self" at the edge
+    // cannot lower a node either.  All loads go out before the first shared-memory store.
+    float hv[3];
+    int ht[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        int node;
+        const long long nb = halo_slot(d, L.b, L.bz, L.bx, L.by, lane, q, node, ht[q]);
+        hv[q] = nb >= 0 ? __ldcg(p.T + d.t_off + nb * kBrickNodes + node) : kInf;
+    }
     const int ti0 = tile_idx(lane & 3, (lane >> 2) & 3, 2 * (lane >> 4));
     tile[ti0] = L.i0;
     tile[ti0 + kTileY] = L.i1;
-    // Missing neighbours (grid edge) are INF; the reference's "halo = self" at the edge
-    // cannot lower a node either.
 #pragma unroll
-    for (int q = 0; q < 3; q++) {
-        int node, ti;
-        const long long nb = halo_slot(d, L.b, L.bz, L.bx, L.by, lane, q, node, ti);
-        tile[ti] = nb >= 0 ? __ldcg(p.T + d.t_off + nb * kBrickNodes + node) : kInf;
-    }
+    for (int q = 0; q < 3; q++) tile[ht[q]] = hv[q];
 }
 
 // ---------------------------------------------------------------------------------------
