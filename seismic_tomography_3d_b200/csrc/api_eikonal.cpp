@@ -136,6 +136,7 @@ int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point 
     if (ngroups > nshots) ngroups = nshots;
     if (tiled) ngroups = 1;
     std::vector<int> tab;
+    std::vector<unsigned> shot_tiles;  // per shot and sweep: the sweep's tile count
     int tab_base[16] = {}, tab_nd[16] = {};
     long long nflags = 0;
     if (tiled) {
@@ -147,6 +148,7 @@ int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point 
         }
         // per sweep: first tile of (tile diagonal d, shot s), d-major, and the tile count
         std::vector<int> A((size_t)nshots), B((size_t)nshots), C((size_t)nshots);
+        shot_tiles.assign((size_t)nshots * 16, 0u);
         for (int q = 0; q < 16; q++) {
             int nd = 0;
             for (int s = 0; s < nshots; s++) {
@@ -155,6 +157,7 @@ int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point 
                 B[(size_t)s] = cdiv(tomo::fsm_sweep_range(q, tomo::fsm_sign_x(q), f.wnx + 2, f.sidx).L, tomo::kFsmTX);
                 C[(size_t)s] = cdiv(tomo::fsm_sweep_range(q, tomo::fsm_sign_y(q), f.wny + 2, f.sidy).L, tomo::kFsmTY);
                 nd = std::max(nd, A[(size_t)s] + B[(size_t)s] + C[(size_t)s] - 2);
+                shot_tiles[(size_t)s * 16 + q] = (unsigned)(A[(size_t)s] * B[(size_t)s] * C[(size_t)s]);
             }
             tab_base[q] = (int)tab.size();
             tab_nd[q] = nd;
@@ -167,18 +170,21 @@ int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point 
             if (run >= (1ll << 31)) return fail(ctx, TOMO_ERR_CAPACITY, "too many sweep tiles for one NGB batch");
             tab.push_back((int)run);
         }
-        CK(ctx->fsm_tab.ensure(tab.size()));
+        CK(ctx->fsm_tab.ensure(tab.size() + shot_tiles.size()));
         CK(ctx->fsm_flags.ensure((size_t)nflags));
         CK(cudaMemcpyAsync(ctx->fsm_tab.ptr, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice,
                            ctx->stream));
+        CK(cudaMemcpyAsync(ctx->fsm_tab.ptr + tab.size(), shot_tiles.data(), shot_tiles.size() * sizeof(unsigned),
+                           cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemsetAsync(ctx->fsm_flags.ptr, 0, (size_t)nflags * sizeof(unsigned), ctx->stream));
     }
     CK(ctx->fsm_T.ensure((size_t)total));
     CK(ctx->fsm_shots.ensure((size_t)nshots));
-    CK(ctx->fsm_bar.ensure((size_t)2 * ngroups + 16));
+    CK(ctx->fsm_bar.ensure((size_t)2 * ngroups + 16 + 16 * (size_t)nshots));
     CK(cudaMemcpyAsync(ctx->fsm_shots.ptr, fs.data(), fs.size() * sizeof(tomo::FsmShot), cudaMemcpyHostToDevice,
                        ctx->stream));
-    CK(cudaMemsetAsync(ctx->fsm_bar.ptr, 0, (2 * ngroups + 16) * sizeof(unsigned), ctx->stream));
+    CK(cudaMemsetAsync(ctx->fsm_bar.ptr, 0, (2 * ngroups + 16 + 16 * (size_t)nshots) * sizeof(unsigned),
+                       ctx->stream));
     CK(cudaMemsetAsync(ctx->ctrl.ptr, 0, tomo::kCtrlWords * sizeof(unsigned), ctx->stream));
     CK(cudaMemsetAsync(ctx->stats.ptr, 0, 2 * sizeof(unsigned long long), ctx->stream));
     tomo::FsmLaunch p{};
@@ -212,6 +218,9 @@ int launch_ngb(tomo_ctx *ctx, const std::vector<ShotDesc> &sd, const tomo_point 
         std::memcpy(p.tab_nd, tab_nd, sizeof(tab_nd));
         p.flags = ctx->fsm_flags.ptr;
         p.cursors = ctx->fsm_bar.ptr + 2;
+        p.shot_done = ctx->fsm_bar.ptr + 2 * ngroups + 16;
+        p.shot_tiles = reinterpret_cast<const unsigned *>(ctx->fsm_tab.ptr + tab.size());
+        p.sweep_barrier = nshots == 1 ? 1 : 0;  // 64 shots: 55.4 ms with the counts, 58.3 with barriers
     }
     CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     int grid = 0;

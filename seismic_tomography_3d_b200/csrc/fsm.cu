@@ -302,8 +302,13 @@ cudaError_t fsm_solve(const FsmLaunch &p, int *grid_out, cudaStream_t st)
 // plane (the nodes of a plane are independent), after waiting for its upwind tiles' flags;
 // every tile it waits on was handed out before its own and every CTA is resident, so the
 // waits end.  Each node sees exactly the values it sees in the sequential loop, and the
-// update is the same function, so the result is the plane schedule's bit for bit -- with
-// one grid barrier per sweep instead of one per diagonal plane.  Every source must lie off
+// update is the same function, so the result is the plane schedule's bit for bit -- with no
+// grid barrier between sweeps of a batch: a shot's tile of sweep q + 1 also waits until all
+// of that shot's sweep-q tiles are finished (a per-shot count), since those read its nodes
+// in sweep q's order; shots are independent, so one shot's next sweep overlaps another's
+// drain.  The sweep-q tiles were all handed out before any sweep-(q + 1) tile, so this
+// wait ends too.  A single shot keeps a grid barrier between sweeps (sweep_barrier).
+// Every source must lie off
 // the far faces of its window (halo index sid <= n - 3), so that no read leaves the grid
 // (the reference's flattened reads would otherwise cross a column edge).
 // -------------------------------------------------------------------------------------
@@ -457,10 +462,26 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
                 }
                 r -= ahi - alo + 1;
             }
-            // wait for the upwind tiles of this sweep (lanes 0-6: one each)
+            // wait for the upwind tiles of this sweep (lanes 0-6: one each) and, lane 7, for
+            // the end of the shot's previous sweep, whose tiles read this tile's nodes in their
+            // own order (a per-shot count of finished tiles instead of a grid barrier, so that
+            // shots that finish a sweep early start the next one while others drain theirs)
             const int fa = cdiv(nzz - 1, kFsmTZ), fb = cdiv(nxx - 1, kFsmTX);
             unsigned *flags = p.flags + sh.flag_off;
             bool gave_up = false;
+            if (lane == 7 && q > 0 && !p.sweep_barrier) {
+                const unsigned need = __ldg(p.shot_tiles + (size_t)si * 16 + (q - 1));
+                const unsigned *cnt = p.shot_done + (size_t)si * 16 + (q - 1);
+                unsigned long long spins = 0;
+                while (ld_acquire(cnt) < need) {
+                    if (++spins > p.spin_limit || ld_volatile(p.err) != 0u) {
+                        atomicCAS(p.err, 0u, (unsigned)kDevBarrierTimeout);
+                        gave_up = true;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
             if (lane < 7) {
                 const int dc = (lane + 1) & 1, da = ((lane + 1) >> 1) & 1, db = (lane + 1) >> 2;
                 if (tc >= dc && ta >= da && tb >= db) {
@@ -529,10 +550,16 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
             }
             __threadfence();
             __syncwarp();
-            if (lane == 0) st_release(flags + tc + fa * (ta + fb * tb), (unsigned)(q + 1));
+            if (lane == 0) {
+                st_release(flags + tc + fa * (ta + fb * tb), (unsigned)(q + 1));
+                if (!p.sweep_barrier) atomicAdd(p.shot_done + (size_t)si * 16 + q, 1u);
+            }
         }
-        if (!group_barrier(p.bar, gridDim.x, p.err, p.spin_limit)) return;
+        // one shot: nothing to overlap a sweep's drain with, and a barrier is cheaper than
+        // the per-tile counts
+        if (p.sweep_barrier && q < 15 && !group_barrier(p.bar, gridDim.x, p.err, p.spin_limit)) return;
     }
+    if (!group_barrier(p.bar, gridDim.x, p.err, p.spin_limit)) return;
 
     // reduce_model (accurate_FSM.cpp:62-72) into the brick-major pool of the shot
     for (int m = 0; m < p.nshots; m++) {

@@ -92,6 +92,9 @@ struct FsmLaunch {
     int tab_base[16], tab_nd[16];
     unsigned *flags;          // per tile: last sweep (q + 1) that finished it
     unsigned *cursors;        // 16 tile cursors, zeroed before the launch
+    unsigned *shot_done;      // per shot and sweep: tiles finished (16 x nshots, zeroed)
+    const unsigned *shot_tiles;  // per shot and sweep: tiles of the sweep (16 x nshots)
+    int sweep_barrier;        // 1: a grid barrier between sweeps instead of the per-shot counts
 };
 
 cudaError_t fsm_solve(const FsmLaunch &p, int *grid_out, cudaStream_t st);
