@@ -323,7 +323,7 @@ constexpr int kPZ = 19, kPX = 10;
 constexpr int kHN = kPZ * kPX * kHY;
 constexpr int kTileN = kFsmTZ * kFsmTX * kFsmTY;
 constexpr int kNPlanes = kFsmTZ + kFsmTX + kFsmTY - 2;
-static_assert(kFsmTZ <= 16 && kFsmTX <= 8 && kFsmTY <= 8, "plane table packs (c, a, b) in 4 + 3 + 3 bits");
+static_assert(kFsmTZ <= 32 && kFsmTX <= 8 && kFsmTY <= 8, "plane table packs (c, a, b) in 5 + 3 + 3 bits");
 static_assert(kPZ >= kHZ && kPX >= kHX, "padded strides");
 
 // The update on a tile staged in shared memory.  sget clamps every index into the window,
@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
         for (int b = 0; b < kFsmTY; b++)
             for (int a = 0; a < kFsmTX; a++) {
                 const int c = w - a - b;
-                if (c >= 0 && c < kFsmTZ) plane[m++] = (unsigned short)(c | (a << 4) | (b << 7));
+                if (c >= 0 && c < kFsmTZ) plane[m++] = (unsigned short)(c | (a << 5) | (b << 8));
             }
         if (w == kNPlanes - 1) pstart[kNPlanes] = m;
     }
@@ -526,8 +526,8 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
             for (int w = 0; w < kNPlanes; w++) {
                 for (int m = pstart[w] + lane; m < pstart[w + 1]; m += 32) {
                     const unsigned e = plane[m];
-                    const int lc = tc * kFsmTZ + (int)(e & 15u), la = ta * kFsmTX + (int)((e >> 4) & 7u),
-                              lb = tb * kFsmTY + (int)(e >> 7);
+                    const int lc = tc * kFsmTZ + (int)(e & 31u), la = ta * kFsmTX + (int)((e >> 5) & 7u),
+                              lb = tb * kFsmTY + (int)(e >> 8);
                     if (lc < rz.L && la < rx.L && lb < ry.L) {
                         const int i = rz.i0 + rz.di * lc, j = rx.i0 + rx.di * la, k = ry.i0 + ry.di * lb;
                         const int tn = (i - tz) + kPZ * ((j - tx) + kPX * (k - ty));
