@@ -106,3 +106,20 @@ def test_unaligned_windows_bit_exact(tomo, oracle_mod):
             sy = float(np.float32(sv.shots[i][1]) - np.float32(y0) * np.float32(h))
             T_ref, _ = oracle_mod.fsm_ngb(np.ascontiguousarray(s[y0:y1, x0:x1, :]), h, (sx, sy, float(sv.shots[i][2])), 0)
             np.testing.assert_array_equal(ctx.eik_volume(i), T_ref)
+
+
+def test_ngb_wait_limit_returns_timeout(tomo):
+    """The tile schedule's bounded waits -- grid barriers, upwind-tile flags and the per-shot
+    sweep counts of a batch: with a limit of one poll they give up, the call returns
+    TOMO_ERR_TIMEOUT, and the context then solves the batch to the same bits as before."""
+    sv = wl.small(45, 24, 20, 12, nshots=3)  # every source off the far faces: tile schedule
+    with tomo.Context(sv.nx, sv.ny, sv.nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(sv.shots, op=1)
+        ref = [ctx.eik_volume(i) for i in range(len(sv.shots))]
+        with pytest.raises(tomo.TomoError) as e:
+            ctx.eik_solve(sv.shots, op=1, spin_limit=1)
+        assert e.value.status == -5  # TOMO_ERR_TIMEOUT
+        ctx.eik_solve(sv.shots, op=1)
+        for i in range(len(sv.shots)):
+            np.testing.assert_array_equal(ctx.eik_volume(i), ref[i])
