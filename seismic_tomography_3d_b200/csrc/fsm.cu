@@ -10,7 +10,8 @@
 // is compiled with -fmad=false; division and square root are IEEE) the result is the
 // reference's, bit for bit.  All shots of a batch sweep together in one cooperative launch;
 // blocks form `ngroups` independent groups (shots g, g+ngroups, ...), each with its own
-// bounded barrier between planes.
+// bounded barrier between planes.  The default schedule (k_fsm_tiled, below) orders the
+// same updates tile by tile instead of plane by plane.
 #include "common.cuh"
 #include "fsm.cuh"
 
