@@ -49,9 +49,10 @@ UNIT = "shots/s"
 BYTES_PER_NODE_ACT = 12  # slowness read + traveltime read + traveltime write (float32)
 # DRAM bytes (read + write) per brick activation of the headline solve, from one ncu capture
 # of a 16-shot launch of this workload each (dram__bytes_read.sum + dram__bytes_write.sum
-# over the launch's activations; profiles/k_fim_solve_config2.md, k_fim_solve8_config2.md):
+# over the launch's activations; profiles/k_fim_solve_config2.md, k_fim_solve8_config2.md,
+# k_fim_pair_config2.md):
 # roofline.traffic is this figure times the timed launch's own activation count.
-DRAM_BYTES_PER_ACTIVATION = {"k_fim_solve": 351.6, "k_fim_solve8": 2787.5}
+DRAM_BYTES_PER_ACTIVATION = {"k_fim_solve": 351.6, "k_fim_solve8": 2787.5, "k_fim_pair": 353.5}
 # Solver tolerances of the timed runs (seismic_tomography_3d_b200.workloads): the metric is
 # quoted at 1e-4 relative traveltime error, so the face-change and in-brick tolerances are
 # loosened until the error against the FP64 oracle (checked in the cpu_baseline leg,
@@ -488,6 +489,8 @@ def run_ours(args):
     tuned = None
     if args.brick:  # a fixed brick shape (profiling), default launch shape
         SOLVER_RUN.update(brick=args.brick)
+    elif args.schedule == 3:  # two bricks per warp, its best config-2 shape (profiling)
+        SOLVER_RUN.update(schedule=3, block_warps=8, occupancy=3)
     elif not args.no_autotune:
         shape, tst = ctx.eik_autotune(sv.shots, windows=sv.windows, repeats=2)
         tuned = dict(shape, trials=tst["trials"], best_ms=tst["best_ms"], default_ms=tst["default_ms"])
@@ -573,8 +576,10 @@ def run_ours(args):
     # DRAM bytes per brick activation from the committed ncu summary of the kernel that ran
     # (one capture of a 16-shot launch of the same workload), scaled to this launch's
     # activations
-    kernel = "k_fim_solve8" if stats[0]["nodes_per_brick"] == 512 else "k_fim_solve"
-    traffic = DRAM_BYTES_PER_ACTIVATION[kernel] * act
+    kernel = "k_fim_solve8" if stats[0]["nodes_per_brick"] == 512 else \
+        "k_fim_pair" if (tuned and tuned.get("schedule") == 3) or args.schedule == 3 else "k_fim_solve"
+    per_act = DRAM_BYTES_PER_ACTIVATION.get(kernel)
+    traffic = per_act * act if per_act else None
 
     # ---- the timed setting against the fully converged field of the same solver ---------
     accuracy_conv = solver_accuracy(ctx, sv, SOLVER_RUN)
@@ -1073,6 +1078,9 @@ def main():
                     help="headline solve with the built-in default shape instead of the autotuned one")
     ap.add_argument("--brick", type=int, default=0, choices=[0, 1, 2],
                     help="headline solve with this brick shape (1: 4x4x4, 2: 8x8x8), untuned (profiling)")
+    ap.add_argument("--schedule", type=int, default=0, choices=[0, 3],
+                    help="3: headline solve with two bricks per warp at 8 warps x 3 CTAs per SM, untuned "
+                         "(profiling)")
     args = ap.parse_args()
     if args.warm_start:
         return run_warm_start(args)

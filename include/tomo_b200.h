@@ -130,6 +130,10 @@ typedef struct {
 #define TOMO_SCHED_DEFAULT 0
 #define TOMO_SCHED_ROUNDS  1
 #define TOMO_SCHED_ASYNC   2
+/* PAIR: the ROUNDS schedule with two 4x4x4 bricks per warp (16 lanes each, a y-column of 4
+ *   nodes per lane), sharing the item fetch and queueing.  Brick-aligned windows, no time
+ *   band; other batches run ROUNDS. */
+#define TOMO_SCHED_PAIR    3
 
 typedef struct {
     long long rounds;            /* outer rounds of the persistent solve                  */
@@ -254,8 +258,10 @@ typedef struct {
 
 /* Autotuner of the JW solve (no counterpart in the reference, whose launch shape is fixed).
  * Solves this batch (no receivers) with every launch shape -- 4x4x4 bricks: warps per CTA
- * {16, 8, 4} x CTAs per SM {3, 4, 5, 6} x in-brick iteration cap {8, 16, 32}; 8x8x8 bricks:
- * CTAs of 8 warps per SM {2, 3, 4, 5} x cap {16, 32} -- `repeats` times each (0: 2), then,
+ * {16, 8, 4} x CTAs per SM {3, 4, 5, 6} x in-brick iteration cap {8, 16, 32}; two 4x4x4
+ * bricks per warp (TOMO_SCHED_PAIR): warps {8, 4, 16} x CTAs per SM {3, 4} at the chosen
+ * cap; 8x8x8 bricks: CTAs of 8 warps per SM {2, 3, 4, 5} x cap {16, 32} -- `repeats` times
+ * each (0: 2), then,
  * at the fastest 4x4x4 shape, the time band at 3, 6, 9 and 12 times the slowest brick
  * crossing (4 dx s_max; none is the shape's own time) and, if a band wins, the warps x
  * CTAs-per-SM shapes again with it.

@@ -378,7 +378,7 @@ class Context:
         best, st = EikOpts(), TuneStats()
         self._check(self.lib.tomo_eik_autotune(self.h, ns, sp, wp, repeats, ctypes.byref(best), ctypes.byref(st)))
         shape = {"brick": best.brick, "block_warps": best.block_warps, "occupancy": best.occupancy,
-                 "max_inner": best.max_inner, "time_band": best.time_band}
+                 "max_inner": best.max_inner, "time_band": best.time_band, "schedule": best.schedule}
         return shape, {f: getattr(st, f) for f, _ in st._fields_}
 
     def volume_sizes(self, nshots, windows=None):

@@ -453,6 +453,7 @@ struct SolveCfg {
     float change_tol, inner_tol;
     bool ieee_sqrt;
     bool async;  // asynchronous schedule, else rounds (default)
+    bool pair;   // rounds with two bricks per warp (brick-aligned, unbanded, 4^3 batches)
     float time_band;  // rounds schedule: time-band ordering (s), 0 = off
     unsigned long long spin_limit;  // polls of a device-side wait before it gives up
     bool brick8;      // 8^3 bricks (one CTA per 2 x 2 x 2 group of storage bricks)
@@ -483,6 +484,10 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     // Rounds by default: the asynchronous schedule relaxes bricks before their upwind
     // neighbours have settled and measured 2.5x slower on config 2 (1.8x the activations).
     c.async = opts && opts->schedule == TOMO_SCHED_ASYNC;
+    // Two bricks per warp when asked for, or when the autotuner chose it and the call leaves
+    // the schedule to the default.
+    c.pair = (opts && opts->schedule == TOMO_SCHED_PAIR) ||
+             ((!opts || opts->schedule == TOMO_SCHED_DEFAULT) && ctx->tuned_schedule == TOMO_SCHED_PAIR);
     // Time-band ordering: off by default.  It pays where slow paths reach bricks long
     // before the first arrival does (2.3x on the config-5 starting model at 0.2 s) and
     // costs where they do not (the windowed config-2 batch).  0: the autotuned band, if
@@ -617,6 +622,7 @@ tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, in
     p.shots = ctx->shots_d.ptr;
     p.nshots = (int)bt.sd.size();
     p.gather = bt.gather ? 1 : 0;
+    p.pair = c.pair && !bt.gather && !c.brick8 && c.time_band <= 0.f ? 1 : 0;
     p.qflag = c.brick8 ? ctx->qflag8.ptr : ctx->qflag.ptr;
     p.lists = ctx->lists.ptr;
     p.list_cap = (unsigned)(c.brick8 ? bt.q_total8 : bt.q_total);
@@ -793,7 +799,7 @@ int tomo_eik_solve(tomo_ctx *ctx, int nshots, const tomo_point *shots, const tom
         return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown brick shape (TOMO_BRICK_4 or TOMO_BRICK_8)");
     if (opts && opts->brick == TOMO_BRICK_8 && opts->schedule == TOMO_SCHED_ASYNC)
         return fail(ctx, TOMO_ERR_INVALID_ARG, "8x8x8 bricks run the rounds schedule only");
-    if (opts && (opts->schedule < TOMO_SCHED_DEFAULT || opts->schedule > TOMO_SCHED_ASYNC))
+    if (opts && (opts->schedule < TOMO_SCHED_DEFAULT || opts->schedule > TOMO_SCHED_PAIR))
         return fail(ctx, TOMO_ERR_INVALID_ARG, "unknown work schedule");
     if (opts && !(std::fabs(opts->time_band) < 1e30f))
         return fail(ctx, TOMO_ERR_INVALID_ARG, "time_band must be finite");
@@ -972,6 +978,7 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
     // untuned defaults while timing (an earlier tuning must not leak into the trials)
     ctx->tuned_block_warps = ctx->tuned_occupancy = ctx->tuned_max_inner = 0;
     ctx->tuned_brick = 0;
+    ctx->tuned_schedule = 0;
     ctx->tuned_time_band = 0.f;
     const int warps[] = {kDefaultBlockWarps, 8, 4};
     const int occs[] = {4, 5, 6, 3};
@@ -1007,6 +1014,37 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
                 }
                 ++trials;
             }
+    // Two bricks per warp (TOMO_SCHED_PAIR): warps per CTA {8, 4, 16} x CTAs per SM {3, 4}
+    // (register budgets 80/64), at the chosen in-brick cap.  Config 2: 8 x 3, 5.02 ms against
+    // 5.27 for the one-brick kernel's best shape.
+    bool pair_best = false;
+    int pw = 0, po = 0;
+    {
+        tomo_eik_opts op{};
+        op.op = TOMO_OP_JW;
+        op.brick = TOMO_BRICK_4;
+        op.schedule = TOMO_SCHED_PAIR;
+        op.max_inner = bi;
+        for (int w : {8, 4, 16})
+            for (int oc : {3, 4}) {
+                op.block_warps = w;
+                op.occupancy = oc;
+                float ms = 0.f;
+                for (int r = 0; r < repeats + 1; r++) {
+                    rc = tomo_eik_solve(ctx, nshots, shots, windows, 0, nullptr, nullptr, &op, &st);
+                    if (rc != TOMO_OK) return rc;
+                    if (r == 0) continue;
+                    ms = (r == 1) ? st.solve_ms : std::min(ms, st.solve_ms);
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    pair_best = true;
+                    pw = w;
+                    po = oc;
+                }
+                ++trials;
+            }
+    }
     // 8^3 bricks: one CTA of 8 warps per brick, CTAs per SM {2, 3, 4, 5} (register
     // budgets 128/80/64/48), in-brick cap {16, 32}.
     int bbrick = TOMO_BRICK_4, bo8 = 0, bi8 = 0;
@@ -1063,6 +1101,7 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
             if (ms < best_ms) {
                 best_ms = ms;
                 bb = o.time_band;
+                pair_best = false;  // a banded solve runs the one-brick kernel
             }
             ++trials;
         }
@@ -1097,8 +1136,14 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
         bo = bo8;
         bi = bi8;
         bb = 0.f;
+        pair_best = false;
+    }
+    if (pair_best) {
+        bw = pw;
+        bo = po;
     }
     ctx->tuned_brick = bbrick;
+    ctx->tuned_schedule = pair_best ? TOMO_SCHED_PAIR : 0;
     ctx->tuned_block_warps = bw;
     ctx->tuned_occupancy = bo;
     ctx->tuned_max_inner = bi;
@@ -1111,6 +1156,7 @@ int tomo_eik_autotune(tomo_ctx *ctx, int nshots, const tomo_point *shots, const 
         best->occupancy = bo;
         best->max_inner = bi;
         best->time_band = bb;
+        best->schedule = pair_best ? TOMO_SCHED_PAIR : TOMO_SCHED_DEFAULT;
     }
     if (stats) {
         stats->trials = trials;

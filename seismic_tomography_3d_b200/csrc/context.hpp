@@ -94,6 +94,7 @@ struct tomo_ctx {
     // launch shape chosen by tomo_eik_autotune (0: not tuned)
     int tuned_block_warps = 0, tuned_occupancy = 0, tuned_max_inner = 0;
     int tuned_brick = 0;          // 0: none chosen (4^3); TOMO_BRICK_4 / TOMO_BRICK_8
+    int tuned_schedule = 0;       // 0: none chosen (rounds); TOMO_SCHED_PAIR
     float tuned_time_band = 0.f;  // 0: none chosen (off)
 
     cudaEvent_t ev[8] = {};

@@ -298,10 +298,12 @@ def test_autotune_picks_a_shape_and_keeps_results(tomo):
         ctx.eik_solve(sv.shots, windows=sv.windows)
         ref = [ctx.eik_volume(i) for i in range(len(sv.shots))]
         shape, st = ctx.eik_autotune(sv.shots, windows=sv.windows, repeats=1)
-        # 36 + 8 launch shapes (4^3, 8^3), 4 time bands, and the 12 warps x occupancy shapes
-        # again if a band won
-        assert st["trials"] in (48, 60)
+        # 36 + 6 + 8 launch shapes (4^3, two 4^3 bricks per warp, 8^3), 4 time bands, and the
+        # 12 warps x occupancy shapes again if a band won
+        assert st["trials"] in (54, 66)
         assert shape["brick"] in (1, 2)
+        assert shape["schedule"] in (0, 3)
+        assert shape["schedule"] == 0 or (shape["brick"] == 1 and shape["time_band"] == 0.0)
         assert shape["block_warps"] in (4, 8, 16) and shape["occupancy"] in (2, 3, 4, 5, 6)
         assert shape["max_inner"] in (8, 16, 32)
         assert shape["time_band"] >= 0.0
@@ -398,3 +400,19 @@ def test_staged_velocity_upload(tomo):
     m = r1 > 0
     assert np.min(r1[m] / r2[m]) > 1.09  # the models differ: times scale by 1 / 1.1
     assert np.max(np.abs(r2[m] * 1.1 - r1[m]) / r1[m]) < 1e-4
+
+
+@pytest.mark.parametrize("dims", [(13, 11, 9), (33, 29, 18)])
+def test_pair_schedule_matches_oracle(tomo, oracle_mod, dims):
+    """TOMO_SCHED_PAIR (two bricks per warp, a y-column of four nodes per lane) at the
+    launch shapes the autotuner tries, single shots and a windowed batch (odd brick counts
+    leave the last warp with one brick), against the oracle on the cropped windows."""
+    nx, ny, nz = dims
+    sv = wl.small(sum(dims) + 7, nx, ny, nz, nshots=5, windows=True)
+    with tomo.Context(nx, ny, nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        for bw, occ in ((8, 3), (4, 3), (16, 4)):
+            ctx.eik_solve(sv.shots, windows=sv.windows, schedule=3, block_warps=bw, occupancy=occ)
+            for i in range(len(sv.shots)):
+                Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, sv.shots[i], sv.windows[i])
+                assert rel_err(ctx.eik_volume(i), Tref, sv.h, sv.velocity.max()) < REL_TOL, (bw, occ, i)
