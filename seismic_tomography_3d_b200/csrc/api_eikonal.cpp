@@ -453,7 +453,7 @@ struct SolveCfg {
     float change_tol, inner_tol;
     bool ieee_sqrt;
     bool async;  // asynchronous schedule, else rounds (default)
-    bool pair;   // rounds with two bricks per warp (brick-aligned, unbanded, 4^3 batches)
+    bool pair;   // rounds with two bricks per warp (unbanded 4^3 batches)
     float time_band;  // rounds schedule: time-band ordering (s), 0 = off
     unsigned long long spin_limit;  // polls of a device-side wait before it gives up
     bool brick8;      // 8^3 bricks (one CTA per 2 x 2 x 2 group of storage bricks)
@@ -622,7 +622,7 @@ tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, in
     p.shots = ctx->shots_d.ptr;
     p.nshots = (int)bt.sd.size();
     p.gather = bt.gather ? 1 : 0;
-    p.pair = c.pair && !bt.gather && !c.brick8 && c.time_band <= 0.f ? 1 : 0;
+    p.pair = c.pair && !c.brick8 && c.time_band <= 0.f ? 1 : 0;
     p.qflag = c.brick8 ? ctx->qflag8.ptr : ctx->qflag.ptr;
     p.lists = ctx->lists.ptr;
     p.list_cap = (unsigned)(c.brick8 ? bt.q_total8 : bt.q_total);

@@ -752,7 +752,7 @@ __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_solve(F
 // column holds two red and two black nodes (colour z + x + y): R0, R1 at y = p, p + 2 and
 // K0, K1 at y = 1 - p, 3 - p with p = (z + x) & 1; its y-neighbours are the column's other
 // colour (registers) or the y halo, its x and z neighbours are other lanes' nodes (tile).
-// Brick-aligned windows, no time band.
+// No time band.  kGather: some window of the batch reads its slowness node by node.
 // ---------------------------------------------------------------------------------------
 struct PairNodes {
     float r0, r1, k0, k1;  // current values
@@ -769,7 +769,7 @@ __device__ __forceinline__ float pair_update(float cur, float a, float b, float 
     return fminf(cur, godunov_jw<kFastSqrt, false>(a, b, g, k));
 }
 
-template <int MINB, bool kFastSqrt>
+template <int MINB, bool kFastSqrt, bool kGather>
 __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_pair(FimLaunch p)
 {
     extern __shared__ float smem[];
@@ -816,13 +816,20 @@ __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_pair(Fi
             float *Tb = p.T;
             if (valid) {
                 brick_coords(d, b, bz, bx, by);
-                const float *Sb = model_brick_S(p.S, p.gbx, p.gbz, d, bz, bx, by);
                 Tb = p.T + d.t_off + (long long)b * kBrickNodes;
                 const int n0 = z + 4 * x;
-                hs0 = p.h * __ldg(Sb + n0);
-                hs1 = p.h * __ldg(Sb + n0 + 16);
-                hs2 = p.h * __ldg(Sb + n0 + 32);
-                hs3 = p.h * __ldg(Sb + n0 + 48);
+                if (!kGather || !d.s_gather) {
+                    const float *Sb = model_brick_S(p.S, p.gbx, p.gbz, d, bz, bx, by);
+                    hs0 = p.h * __ldg(Sb + n0);
+                    hs1 = p.h * __ldg(Sb + n0 + 16);
+                    hs2 = p.h * __ldg(Sb + n0 + 32);
+                    hs3 = p.h * __ldg(Sb + n0 + 48);
+                } else {
+                    hs0 = p.h * gather_S(p.S, p.gbx, p.gbz, d, bz, bx, by, n0);
+                    hs1 = p.h * gather_S(p.S, p.gbx, p.gbz, d, bz, bx, by, n0 + 16);
+                    hs2 = p.h * gather_S(p.S, p.gbx, p.gbz, d, bz, bx, by, n0 + 32);
+                    hs3 = p.h * gather_S(p.S, p.gbx, p.gbz, d, bz, bx, by, n0 + 48);
+                }
                 t0 = __ldcg(Tb + n0);
                 t1 = __ldcg(Tb + n0 + 16);
                 t2 = __ldcg(Tb + n0 + 32);
@@ -1634,7 +1641,8 @@ cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx,
 template <int MINB, bool kFastSqrt>
 static cudaError_t launch_pair(const FimLaunch &p, int block_warps, int *grid_out, cudaStream_t st)
 {
-    const void *fn = (const void *)k_fim_pair<MINB, kFastSqrt>;
+    const void *fn = p.gather ? (const void *)k_fim_pair<MINB, kFastSqrt, true>
+                              : (const void *)k_fim_pair<MINB, kFastSqrt, false>;
     const int threads = 32 * block_warps;
     const size_t smem = (size_t)block_warps * (2 * kTileNodes * sizeof(float) + kPushCap * sizeof(unsigned));
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1658,7 +1666,7 @@ template <int MINB, bool kFastSqrt>
 static cudaError_t launch_solve(const FimLaunch &p, int block_warps, bool async, int *grid_out, cudaStream_t st)
 {
     const bool band = !async && p.band > 0.f;
-    if (!async && !band && !p.gather && p.pair) return launch_pair<MINB, kFastSqrt>(p, block_warps, grid_out, st);
+    if (!async && !band && p.pair) return launch_pair<MINB, kFastSqrt>(p, block_warps, grid_out, st);
     const void *fn = async          ? (const void *)k_fim_async<MINB, kFastSqrt>
                      : p.gather     ? (band ? (const void *)k_fim_solve<MINB, kFastSqrt, true, true>
                                             : (const void *)k_fim_solve<MINB, kFastSqrt, false, true>)

@@ -110,7 +110,7 @@ struct FimLaunch {
     float dx, dy, dz;
     int nz;
     int gather;           // some shot has ShotDesc::s_gather set (selects the gathering kernel)
-    int pair;             // rounds schedule, two bricks per warp (k_fim_pair)
+    int pair;             // rounds schedule, two bricks per warp (k_fim_pair; gathering too)
 };
 
 // Host-callable launchers (fim.cu).

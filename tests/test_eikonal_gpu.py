@@ -416,3 +416,16 @@ def test_pair_schedule_matches_oracle(tomo, oracle_mod, dims):
             for i in range(len(sv.shots)):
                 Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, sv.shots[i], sv.windows[i])
                 assert rel_err(ctx.eik_volume(i), Tref, sv.h, sv.velocity.max()) < REL_TOL, (bw, occ, i)
+
+
+def test_pair_schedule_unaligned_windows(tomo, oracle_mod):
+    """Two bricks per warp on windows of any origin (slowness gathered node by node)."""
+    nx, ny, nz = 37, 30, 14
+    sv = wl.small(23, nx, ny, nz, nshots=6, nrec=30)
+    wins = _any_windows(np.random.default_rng(23), sv, 6)
+    with tomo.Context(nx, ny, nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(sv.shots, windows=wins, schedule=3, block_warps=8, occupancy=3)
+        for i in range(len(sv.shots)):
+            Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, sv.shots[i], wins[i])
+            assert rel_err(ctx.eik_volume(i), Tref, sv.h, sv.velocity.max()) < REL_TOL, i
