@@ -131,8 +131,9 @@ typedef struct {
 #define TOMO_SCHED_ROUNDS  1
 #define TOMO_SCHED_ASYNC   2
 /* PAIR: the ROUNDS schedule with two 4x4x4 bricks per warp (16 lanes each, a y-column of 4
- *   nodes per lane), sharing the item fetch and queueing.  Without time band; banded
- *   solves run ROUNDS. */
+ *   nodes per lane), sharing the item fetch and queueing.  DEFAULT runs it for banded
+ *   solves (time_band > 0) and when the autotuner chose it; ROUNDS keeps one brick per
+ *   warp. */
 #define TOMO_SCHED_PAIR    3
 
 typedef struct {

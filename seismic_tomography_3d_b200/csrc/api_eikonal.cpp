@@ -453,7 +453,7 @@ struct SolveCfg {
     float change_tol, inner_tol;
     bool ieee_sqrt;
     bool async;  // asynchronous schedule, else rounds (default)
-    bool pair;   // rounds with two bricks per warp (unbanded 4^3 batches)
+    bool pair;   // rounds with two bricks per warp (4^3 bricks)
     float time_band;  // rounds schedule: time-band ordering (s), 0 = off
     unsigned long long spin_limit;  // polls of a device-side wait before it gives up
     bool brick8;      // 8^3 bricks (one CTA per 2 x 2 x 2 group of storage bricks)
@@ -484,10 +484,6 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     // Rounds by default: the asynchronous schedule relaxes bricks before their upwind
     // neighbours have settled and measured 2.5x slower on config 2 (1.8x the activations).
     c.async = opts && opts->schedule == TOMO_SCHED_ASYNC;
-    // Two bricks per warp when asked for, or when the autotuner chose it and the call leaves
-    // the schedule to the default.
-    c.pair = (opts && opts->schedule == TOMO_SCHED_PAIR) ||
-             ((!opts || opts->schedule == TOMO_SCHED_DEFAULT) && ctx->tuned_schedule == TOMO_SCHED_PAIR);
     // Time-band ordering: off by default.  It pays where slow paths reach bricks long
     // before the first arrival does (2.3x on the config-5 starting model at 0.2 s) and
     // costs where they do not (the windowed config-2 batch).  0: the autotuned band, if
@@ -495,6 +491,12 @@ SolveCfg solve_cfg(const tomo_ctx *ctx, const tomo_eik_opts *opts)
     const float band = opts ? opts->time_band : 0.f;
     c.time_band = band > 0.f ? band : (band < 0.f ? 0.f : ctx->tuned_time_band);
     if (c.async) c.time_band = 0.f;
+    // Two bricks per warp when asked for, or, with the schedule left to the default, when the
+    // autotuner chose it or the solve is banded (time band at 8 warps x 3 CTAs per SM: config
+    // 5 starting model 305 vs 435 ms, config 3 9.0 vs 9.8 ms).
+    const bool sched_default = !opts || opts->schedule == TOMO_SCHED_DEFAULT;
+    c.pair = (opts && opts->schedule == TOMO_SCHED_PAIR) ||
+             (sched_default && (ctx->tuned_schedule == TOMO_SCHED_PAIR || c.time_band > 0.f));
     c.spin_limit = (opts && opts->spin_limit > 0) ? opts->spin_limit : kSpinLimit;
     // Brick shape: 4^3 unless asked for (or tuned to) 8^3.  The 8^3 kernel runs the rounds
     // schedule without the time band.
@@ -622,7 +624,7 @@ tomo::FimLaunch fim_params(tomo_ctx *ctx, const Batch &bt, const SolveCfg &c, in
     p.shots = ctx->shots_d.ptr;
     p.nshots = (int)bt.sd.size();
     p.gather = bt.gather ? 1 : 0;
-    p.pair = c.pair && !c.brick8 && c.time_band <= 0.f ? 1 : 0;
+    p.pair = c.pair && !c.brick8 ? 1 : 0;
     p.qflag = c.brick8 ? ctx->qflag8.ptr : ctx->qflag.ptr;
     p.lists = ctx->lists.ptr;
     p.list_cap = (unsigned)(c.brick8 ? bt.q_total8 : bt.q_total);

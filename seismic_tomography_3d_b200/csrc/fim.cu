@@ -752,7 +752,8 @@ __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_solve(F
 // column holds two red and two black nodes (colour z + x + y): R0, R1 at y = p, p + 2 and
 // K0, K1 at y = 1 - p, 3 - p with p = (z + x) & 1; its y-neighbours are the column's other
 // colour (registers) or the y halo, its x and z neighbours are other lanes' nodes (tile).
-// No time band.  kGather: some window of the batch reads its slowness node by node.
+// kBand: the time band of k_fim_solve, per half (put-offs parked, pushes carry keys).
+// kGather: some window of the batch reads its slowness node by node.
 // ---------------------------------------------------------------------------------------
 struct PairNodes {
     float r0, r1, k0, k1;  // current values
@@ -1008,6 +1009,319 @@ __global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_pair(Fi
         atomicAdd(p.stats + 1, ws.inner);
         atomicAdd(p.stats + 3, ws.idle);
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kRounds] = round;
+    if (!ok || p.nrec == 0) return;
+
+    sample_receivers(p.T, p.shots, p.nshots, p.rx, p.ry, p.rz, p.nrec, p.dx, p.dy, p.dz, p.nz, p.t_recv);
+}
+
+// The time-band instance of k_fim_pair (configs 3 and 5), a separate function so that the
+// unbanded one keeps its registers (folding the band code into it cost it a 12-byte spill
+// and 1.6 % on the config-2 batch).
+template <int MINB, bool kFastSqrt, bool kGather>
+__global__ void __launch_bounds__(512) __maxnreg__(fim_regs(MINB)) k_fim_pair_band(FimLaunch p)
+{
+    constexpr bool kBand = true;
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int half = lane >> 4, hl = lane & 15;
+    float *tile = smem + (2 * warp + half) * kTileNodes;
+    unsigned *pbuf = reinterpret_cast<unsigned *>(smem + 2 * nw * kTileNodes) + warp * kPushCap;
+    // time band: the pushes' keys one push-buffer array above, then the parked items
+    unsigned *pkey = kBand ? reinterpret_cast<unsigned *>(smem + 2 * nw * kTileNodes) + (nw + warp) * kPushCap
+                           : nullptr;
+    unsigned *kbuf = kBand ? reinterpret_cast<unsigned *>(smem + 2 * nw * kTileNodes) + 2 * nw * kPushCap +
+                                 warp * kParkCap
+                           : nullptr;
+    unsigned pcnt = 0, kcnt = 0;
+    unsigned parked_through = 0;
+    WarpStats ws{0ull, 0ull, 0ull, 0ull};
+    const unsigned nwarps = gridDim.x * nw;
+    const unsigned gwarp = blockIdx.x * nw + warp;
+    const int z = hl & 3, x = hl >> 2, par = (z + x) & 1;
+    // tile indices of the column's nodes and of its y halo
+    const int tr0 = tile_idx(z, x, par), tr1 = tile_idx(z, x, par + 2), tk0 = tile_idx(z, x, 1 - par),
+              tk1 = tile_idx(z, x, 3 - par);
+    const int tylo = tile_idx(z, x, -1), tyhi = tile_idx(z, x, kBrick);
+
+    unsigned round = 0, epoch = 0;
+    bool ok = true;
+    for (;;) {
+        const unsigned cur = round % 3u;
+        const unsigned n = ld_volatile(p.ctrl + kCnt0 + cur);
+        if (kBand) {  // parked items due now, as in k_fim_solve
+            const unsigned K = (unsigned)p.park_rounds;
+            const unsigned from = parked_through, to = n == 0u ? round : (round >= K ? round - K + 1u : 0u);
+            unsigned pending = 0;
+            for (unsigned dd = from; dd < to; dd++) {
+                const unsigned j = park_slot(p, dd);
+                const unsigned np = ld_volatile(p.park_cnt + j);
+                if (np) merge_parks(p, j, np, round);
+                pending += np;
+            }
+            if (to > parked_through) parked_through = to;
+            if (blockIdx.x == 0 && threadIdx.x == 0) p.park_cnt[park_slot(p, round + 1u)] = 0u;
+            if (n == 0u && pending == 0u) break;
+        } else if (n == 0u) {
+            break;
+        }
+        if ((int)round >= p.max_rounds) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(p.ctrl + kErr, 0u, (unsigned)kDevRoundCap);
+            ok = false;
+            break;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            p.ctrl[kCnt0 + (round + 2u) % 3u] = 0u;
+            p.ctrl[kCur0 + (round + 2u) % 3u] = 0u;
+        }
+        const unsigned *list = p.lists + (size_t)cur * p.list_cap;
+        unsigned *cursor = p.ctrl + kCur0 + cur;
+        if (kBand && blockIdx.x == 0) {  // per-shot minima for round + 1 (read in round - 1)
+            unsigned *reset = p.band_min + (size_t)((round + 1u) % 3u) * p.nshots;
+            for (int j = threadIdx.x; j < p.nshots; j += blockDim.x) reset[j] = kNoKey;
+        }
+        for (unsigned i = 2u * gwarp; i < n;) {
+            // ---- load: this half's item (none when i + half >= n) ----
+            const bool valid = i + (unsigned)half < n;
+            const unsigned item = valid ? __ldcg(list + i + half) : 0u;
+            const unsigned s = item >> p.local_bits, b = item & ((1u << p.local_bits) - 1u);
+            const ShotDesc &d = p.shots[s];
+            unsigned kb = kNoKey, tb = kNoKey;
+            if (kBand && valid) {  // key and threshold loads go out with the brick's
+                kb = __ldcg(p.keys + d.qbase + b);
+                tb = __ldcg(p.band_min + (size_t)((round + 2u) % 3u) * p.nshots + s);
+            }
+            int bz = 0, bx = 0, by = 0;
+            float hs0 = 0.f, hs1 = 0.f, hs2 = 0.f, hs3 = 0.f;  // h s at y = 0..3
+            float t0 = kInf, t1 = kInf, t2 = kInf, t3 = kInf;
+            float *Tb = p.T;
+            if (valid) {
+                brick_coords(d, b, bz, bx, by);
+                Tb = p.T + d.t_off + (long long)b * kBrickNodes;
+                const int n0 = z + 4 * x;
+                if (!kGather || !d.s_gather) {
+                    const float *Sb = model_brick_S(p.S, p.gbx, p.gbz, d, bz, bx, by);
+                    hs0 = p.h * __ldg(Sb + n0);
+                    hs1 = p.h * __ldg(Sb + n0 + 16);
+                    hs2 = p.h * __ldg(Sb + n0 + 32);
+                    hs3 = p.h * __ldg(Sb + n0 + 48);
+                } else {
+                    hs0 = p.h * gather_S(p.S, p.gbx, p.gbz, d, bz, bx, by, n0);
+                    hs1 = p.h * gather_S(p.S, p.gbx, p.gbz, d, bz, bx, by, n0 + 16);
+                    hs2 = p.h * gather_S(p.S, p.gbx, p.gbz, d, bz, bx, by, n0 + 32);
+                    hs3 = p.h * gather_S(p.S, p.gbx, p.gbz, d, bz, bx, by, n0 + 48);
+                }
+                t0 = __ldcg(Tb + n0);
+                t1 = __ldcg(Tb + n0 + 16);
+                t2 = __ldcg(Tb + n0 + 32);
+                t3 = __ldcg(Tb + n0 + 48);
+                // face halo: slot q = 2 axis + upper, one face node per lane (u, v) = (hl & 3, hl >> 2)
+                const int u = hl & 3, v = hl >> 2;
+                float hv[6];
+#pragma unroll
+                for (int q = 0; q < 6; q++) {
+                    const int axis = q >> 1;
+                    const bool up = q & 1;
+                    long long nb = -1;
+                    int node;
+                    if (axis == 0) {
+                        node = (up ? 0 : 3) + 4 * u + 16 * v;
+                        if (up ? bz < d.nbz - 1 : bz > 0) nb = (long long)b + (up ? 1 : -1);
+                    } else if (axis == 1) {
+                        node = u + (up ? 0 : 12) + 16 * v;
+                        if (up ? bx < d.nbx - 1 : bx > 0) nb = (long long)b + (up ? d.nbz : -d.nbz);
+                    } else {
+                        node = u + 4 * v + (up ? 0 : 48);
+                        const long long sy = (long long)d.nbz * d.nbx;
+                        if (up ? by < d.nby - 1 : by > 0) nb = (long long)b + (up ? sy : -sy);
+                    }
+                    hv[q] = nb >= 0 ? __ldcg(p.T + d.t_off + nb * kBrickNodes + node) : kInf;
+                }
+                tile[tile_idx(z, x, 0)] = t0;
+                tile[tile_idx(z, x, 1)] = t1;
+                tile[tile_idx(z, x, 2)] = t2;
+                tile[tile_idx(z, x, 3)] = t3;
+#pragma unroll
+                for (int q = 0; q < 6; q++) {  // the halo cells' tile places
+                    const int axis = q >> 1, e = (q & 1) ? kBrick : -1;
+                    tile[axis == 0 ? tile_idx(e, u, v) : axis == 1 ? tile_idx(u, e, v) : tile_idx(u, v, e)] = hv[q];
+                }
+            }
+            __syncwarp();
+            // time band: a brick too far ahead of its shot's front is put off (parked)
+            bool defer = false;
+            if (kBand && valid && kb != kNoKey) {
+                if (hl == 0) atomicMin(p.band_min + (size_t)(round % 3u) * p.nshots + s, kb);
+                defer = tb != kNoKey && __uint_as_float(kb) > __uint_as_float(tb) + p.band;
+                if (!defer && hl == 0) p.keys[d.qbase + b] = kNoKey;  // consumed here
+            }
+            const bool relax = valid && !defer;
+            if (kBand) {
+                const unsigned pm = __ballot_sync(kFull, defer && hl == 0);
+                if (defer && hl == 0) kbuf[kcnt + __popc(pm & ((1u << lane) - 1u))] = item;
+                kcnt += __popc(pm);
+                ws.deferred += __popc(pm);
+                if (kcnt > kParkCap - 2u) flush_parks(p, kbuf, kcnt, round);
+            }
+            // the column's colours (par = 0: R at y = 0, 2; K at 1, 3)
+            PairNodes c;
+            c.r0 = par ? t1 : t0;
+            c.r1 = par ? t3 : t2;
+            c.k0 = par ? t0 : t1;
+            c.k1 = par ? t2 : t3;
+            const float hr0 = par ? hs1 : hs0, hr1 = par ? hs3 : hs2, hk0 = par ? hs0 : hs1, hk1 = par ? hs2 : hs3;
+            const float ylo = relax ? tile[tylo] : kInf, yhi = relax ? tile[tyhi] : kInf;
+            // ---- red-black relaxation, each half until its own brick converges ----
+            bool active = relax, more = relax;
+            int it = 0, my_it = 0;
+            for (; it < p.max_inner; ++it) {
+                bool ch = false;
+                if (active) {
+                    const float a0 = fminf(tile[tr0 - kTileX], tile[tr0 + kTileX]);
+                    const float g0 = fminf(tile[tr0 - 1], tile[tr0 + 1]);
+                    const float b0 = fminf(par ? c.k0 : ylo, par ? c.k1 : c.k0);
+                    const float a1 = fminf(tile[tr1 - kTileX], tile[tr1 + kTileX]);
+                    const float g1 = fminf(tile[tr1 - 1], tile[tr1 + 1]);
+                    const float b1 = fminf(par ? c.k1 : c.k0, par ? yhi : c.k1);
+                    const float n0 = pair_update<kFastSqrt>(c.r0, a0, b0, g0, hr0);
+                    const float n1 = pair_update<kFastSqrt>(c.r1, a1, b1, g1, hr1);
+                    tile[tr0] = n0;
+                    tile[tr1] = n1;
+                    ch = (n0 < c.r0 - p.inner_tol) | (n1 < c.r1 - p.inner_tol);
+                    c.r0 = n0;
+                    c.r1 = n1;
+                }
+                __syncwarp();
+                unsigned m = __ballot_sync(kFull, ch) >> (16 * half);
+                if (active && it > 0 && (m & 0xffffu) == 0u) {
+                    active = false;
+                    more = false;
+                    my_it = it + 1;
+                }
+                if (!__any_sync(kFull, active)) {
+                    ++it;
+                    break;
+                }
+                ch = false;
+                if (active) {
+                    const float a0 = fminf(tile[tk0 - kTileX], tile[tk0 + kTileX]);
+                    const float g0 = fminf(tile[tk0 - 1], tile[tk0 + 1]);
+                    const float b0 = fminf(par ? ylo : c.r0, par ? c.r0 : c.r1);
+                    const float a1 = fminf(tile[tk1 - kTileX], tile[tk1 + kTileX]);
+                    const float g1 = fminf(tile[tk1 - 1], tile[tk1 + 1]);
+                    const float b1 = fminf(par ? c.r0 : c.r1, par ? c.r1 : yhi);
+                    const float n0 = pair_update<kFastSqrt>(c.k0, a0, b0, g0, hk0);
+                    const float n1 = pair_update<kFastSqrt>(c.k1, a1, b1, g1, hk1);
+                    tile[tk0] = n0;
+                    tile[tk1] = n1;
+                    ch = (n0 < c.k0 - p.inner_tol) | (n1 < c.k1 - p.inner_tol);
+                    c.k0 = n0;
+                    c.k1 = n1;
+                }
+                __syncwarp();
+                m = __ballot_sync(kFull, ch) >> (16 * half);
+                if (active && (m & 0xffffu) == 0u) {
+                    active = false;
+                    more = false;
+                    my_it = it + 1;
+                }
+                if (!__any_sync(kFull, active)) {
+                    ++it;
+                    break;
+                }
+            }
+            if (active) my_it = it;  // the cap was hit: `more` stays set
+            // next pair of items: the cursor atomic overlaps the epilogue
+            unsigned nx = 0;
+            if (lane == 0) nx = atomicAdd(cursor, 2u);
+            // ---- epilogue per half: values at y = 0..3 against those at load time ----
+            const float v0 = par ? c.k0 : c.r0, v1 = par ? c.r0 : c.k0, v2 = par ? c.k1 : c.r1, v3 = par ? c.r1 : c.k1;
+            const bool drop = relax && ((v0 < t0) | (v1 < t1) | (v2 < t2) | (v3 < t3));
+            const unsigned dm = (__ballot_sync(kFull, drop) >> (16 * half)) & 0xffffu;
+            if (dm && relax) {
+                const int n0 = z + 4 * x;
+                __stcg(Tb + n0, v0);
+                __stcg(Tb + n0 + 16, v1);
+                __stcg(Tb + n0 + 32, v2);
+                __stcg(Tb + n0 + 48, v3);
+            }
+            const bool d0 = relax && v0 < t0 - p.change_tol, d1 = relax && v1 < t1 - p.change_tol,
+                       d2 = relax && v2 < t2 - p.change_tol, d3 = relax && v3 < t3 - p.change_tol;
+            // time band: key of the half's pushes, the smallest new time among its dropped nodes
+            unsigned key = kNoKey;
+            if (kBand) {
+                const unsigned kl = __float_as_uint(
+                    fminf(fminf(d0 ? v0 : kInf, d1 ? v1 : kInf), fminf(d2 ? v2 : kInf, d3 ? v3 : kInf)));
+                const unsigned k0 = __reduce_min_sync(kFull, half == 0 ? kl : 0xffffffffu);
+                const unsigned k1 = __reduce_min_sync(kFull, half == 1 ? kl : 0xffffffffu);
+                key = half ? k1 : k0;
+                if (key == __float_as_uint(kInf)) key = kNoKey;
+            }
+            unsigned fl = 0;  // faces: 1 z-, 2 z+, 4 x-, 8 x+, 16 y-, 32 y+
+            const int t00 = tile_idx(z, x, 0);
+            if (z == 0 && ((d0 && v0 < tile[t00 - 1]) || (d1 && v1 < tile[t00 + kTileY - 1]) ||
+                           (d2 && v2 < tile[t00 + 2 * kTileY - 1]) || (d3 && v3 < tile[t00 + 3 * kTileY - 1])))
+                fl |= 1u;
+            if (z == 3 && ((d0 && v0 < tile[t00 + 1]) || (d1 && v1 < tile[t00 + kTileY + 1]) ||
+                           (d2 && v2 < tile[t00 + 2 * kTileY + 1]) || (d3 && v3 < tile[t00 + 3 * kTileY + 1])))
+                fl |= 2u;
+            if (x == 0 && ((d0 && v0 < tile[t00 - kTileX]) || (d1 && v1 < tile[t00 + kTileY - kTileX]) ||
+                           (d2 && v2 < tile[t00 + 2 * kTileY - kTileX]) ||
+                           (d3 && v3 < tile[t00 + 3 * kTileY - kTileX])))
+                fl |= 4u;
+            if (x == 3 && ((d0 && v0 < tile[t00 + kTileX]) || (d1 && v1 < tile[t00 + kTileY + kTileX]) ||
+                           (d2 && v2 < tile[t00 + 2 * kTileY + kTileX]) ||
+                           (d3 && v3 < tile[t00 + 3 * kTileY + kTileX])))
+                fl |= 8u;
+            if (d0 && v0 < ylo) fl |= 16u;
+            if (d3 && v3 < yhi) fl |= 32u;
+            const unsigned f0 = __reduce_or_sync(kFull, half == 0 ? fl : 0u);
+            const unsigned f1 = __reduce_or_sync(kFull, half == 1 ? fl : 0u);
+            const unsigned face = half ? f1 : f0;
+            bool want = false;
+            int tgt = (int)b;
+            if (relax && hl < 6) {
+                const int axis = hl >> 1;
+                const bool up = hl & 1;
+                const int cc = axis == 0 ? bz : (axis == 1 ? bx : by);
+                const int nmax = axis == 0 ? d.nbz : (axis == 1 ? d.nbx : d.nby);
+                const int stride = axis == 0 ? 1 : (axis == 1 ? d.nbz : d.nbz * d.nbx);
+                want = ((face >> hl) & 1u) && (up ? cc < nmax - 1 : cc > 0);
+                tgt += up ? stride : -stride;
+            } else if (relax && hl == 6) {
+                want = more;
+            }
+            const unsigned wm = __ballot_sync(kFull, want);
+            if (want) {
+                const unsigned slot = pcnt + __popc(wm & ((1u << lane) - 1u));
+                pbuf[slot] = (s << p.local_bits) | (unsigned)tgt;
+                if (kBand) pkey[slot] = key;
+            }
+            pcnt += __popc(wm);
+            if (pcnt > kPushCap - 14u) flush_pushes<kBand>(p, pbuf, pkey, pcnt, round);
+            // stats (lane 0 keeps the warp's): both halves' activations and iterations
+            // (without a band every valid half relaxes: half 0 always, half 1 when i + 1 < n)
+            const bool r0 = kBand ? __shfl_sync(kFull, relax, 0) : true;
+            const bool r1 = kBand ? __shfl_sync(kFull, relax, 16) : i + 1u < n;
+            const int it_h0 = __shfl_sync(kFull, my_it, 0), it_h1 = __shfl_sync(kFull, my_it, 16);
+            ws.act += (r0 ? 1ull : 0ull) + (r1 ? 1ull : 0ull);
+            ws.inner += (unsigned long long)((r0 ? it_h0 : 0) + (r1 ? it_h1 : 0));
+            if (r0 && !__shfl_sync(kFull, dm != 0u, 0)) ws.idle += 1;
+            if (r1 && !__shfl_sync(kFull, dm != 0u, 16)) ws.idle += 1;
+            __syncwarp();  // the tile is rewritten by the next item
+            i = 2u * nwarps + __shfl_sync(kFull, nx, 0);
+        }
+        if (pcnt) flush_pushes<kBand>(p, pbuf, pkey, pcnt, round);
+        if (kBand && kcnt) flush_parks(p, kbuf, kcnt, round);
+        if (!grid_sync(p.ctrl, epoch, p.spin_limit)) { ok = false; break; }
+        ++round;
+    }
+    if (lane == 0 && ws.act) {
+        atomicAdd(p.stats + 0, ws.act);
+        atomicAdd(p.stats + 1, ws.inner);
+        atomicAdd(p.stats + 3, ws.idle);
+    }
+    if (lane == 0 && ws.deferred) atomicAdd(p.stats + 2, ws.deferred);
     if (blockIdx.x == 0 && threadIdx.x == 0) p.ctrl[kRounds] = round;
     if (!ok || p.nrec == 0) return;
 
@@ -1641,10 +1955,15 @@ cudaError_t fim_seed(const ShotDesc *shots, int nshots, const float *S, int gbx,
 template <int MINB, bool kFastSqrt>
 static cudaError_t launch_pair(const FimLaunch &p, int block_warps, int *grid_out, cudaStream_t st)
 {
-    const void *fn = p.gather ? (const void *)k_fim_pair<MINB, kFastSqrt, true>
-                              : (const void *)k_fim_pair<MINB, kFastSqrt, false>;
+    const bool band = p.band > 0.f;
+    const void *fn = band ? (p.gather ? (const void *)k_fim_pair_band<MINB, kFastSqrt, true>
+                                      : (const void *)k_fim_pair_band<MINB, kFastSqrt, false>)
+                          : (p.gather ? (const void *)k_fim_pair<MINB, kFastSqrt, true>
+                                      : (const void *)k_fim_pair<MINB, kFastSqrt, false>);
     const int threads = 32 * block_warps;
-    const size_t smem = (size_t)block_warps * (2 * kTileNodes * sizeof(float) + kPushCap * sizeof(unsigned));
+    // per warp: two tiles, the push buffer, and (time band) the pushes' keys and parked items
+    const size_t smem = (size_t)block_warps * (2 * kTileNodes * sizeof(float) + kPushCap * sizeof(unsigned) +
+                                               (band ? (kPushCap + kParkCap) * sizeof(unsigned) : 0));
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, nsm = 0, per_sm = 0;
@@ -1666,7 +1985,7 @@ template <int MINB, bool kFastSqrt>
 static cudaError_t launch_solve(const FimLaunch &p, int block_warps, bool async, int *grid_out, cudaStream_t st)
 {
     const bool band = !async && p.band > 0.f;
-    if (!async && !band && p.pair) return launch_pair<MINB, kFastSqrt>(p, block_warps, grid_out, st);
+    if (!async && p.pair) return launch_pair<MINB, kFastSqrt>(p, block_warps, grid_out, st);
     const void *fn = async          ? (const void *)k_fim_async<MINB, kFastSqrt>
                      : p.gather     ? (band ? (const void *)k_fim_solve<MINB, kFastSqrt, true, true>
                                             : (const void *)k_fim_solve<MINB, kFastSqrt, false, true>)

@@ -110,7 +110,7 @@ struct FimLaunch {
     float dx, dy, dz;
     int nz;
     int gather;           // some shot has ShotDesc::s_gather set (selects the gathering kernel)
-    int pair;             // rounds schedule, two bricks per warp (k_fim_pair; gathering too)
+    int pair;             // rounds schedule, two bricks per warp (k_fim_pair, k_fim_pair_band)
 };
 
 // Host-callable launchers (fim.cu).
