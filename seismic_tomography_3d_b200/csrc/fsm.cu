@@ -74,12 +74,17 @@ __device__ __forceinline__ float tget(const ShotGrid &g, long long idx)
 }
 
 // Slowness of halo-grid node (i, j, k): the window cropped and replicated by one node.
-__device__ __forceinline__ float sget(const FsmLaunch &p, const ShotGrid &g, int i, int j, int k)
+__device__ __forceinline__ const float *sptr(const FsmLaunch &p, const ShotGrid &g, int i, int j, int k)
 {
     const int z = min(max(i - 1, 0), p.nz - 1);
     const int x = g.s->wx0 + min(max(j - 1, 0), g.s->wnx - 1);
     const int y = g.s->wy0 + min(max(k - 1, 0), g.s->wny - 1);
-    return __ldg(p.slow + z + (long long)x * p.nz + (long long)y * p.nx * p.nz);
+    return p.slow + z + (long long)x * p.nz + (long long)y * p.nx * p.nz;
+}
+
+__device__ __forceinline__ float sget(const FsmLaunch &p, const ShotGrid &g, int i, int j, int k)
+{
+    return __ldg(sptr(p, g, i, j, k));
 }
 
 // Traveltimes and slowness of one shot's halo grid as the sweep reads them, from global
@@ -315,6 +320,11 @@ cudaError_t fsm_solve(const FsmLaunch &p, int *grid_out, cudaStream_t st)
 // -------------------------------------------------------------------------------------
 namespace {
 
+// Unroll depth of the tile staging loop.  Config-2 batch (64 shots), ms per NGB solve with the
+// slowness by cp.async and the octant-specialised plane loop: 4 -> 52.1, 5 -> 49.3, 6 -> 48.6,
+// 7 -> 49.1, 8 -> 55.6 (128 registers); 6 with node indices by division instead of the
+// incremental ones: 49.7.
+constexpr int kStageUnroll = 6;
 constexpr int kHZ = kFsmTZ + 1, kHX = kFsmTX + 1, kHY = kFsmTY + 1;  // a tile + one layer per axis
 // Strides of the staged arrays (z, then x; words): padded from 17 x 9 so that the lanes of a
 // diagonal-plane pass, which differ by (+-19 -+ 1) a + (+-190 -+ 1) b words, fall in
@@ -358,6 +368,46 @@ __device__ __forceinline__ float ngb_update_tile(const FsmLaunch &p, const float
     v.r3 = smin(C(0, cx, cy), C(1, cx, cy));
     v.r0 = C(cz, cx, cy);
     return ngb_core(p, v);
+}
+
+// Asynchronous 4-byte copy global -> shared (cp.async, through L1).  Only for the slowness,
+// which nothing writes while a solve runs, so an L1 line can never be stale; the
+// traveltimes, written by other SMs between tiles, are read through L2 (__ldcg).
+__device__ __forceinline__ void cp_async4(float *dst, const float *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+
+// Waits for this thread's cp.async copies; a warp barrier after it shows them to the warp.
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// One tile of a sweep of octant Q (sweep q with q & 7 == Q), diagonal plane by diagonal
+// plane.  With the octant's steps compile-time constants every staged read is a shared-
+// memory load at a constant offset from the node, and the reads of the 2 x 2 x 2 cell cube
+// that several minima share are loaded once.
+//   t0: the tile's node (0, 0, 0) in Ts; dts: Ts word of a node minus the Ss word of its
+//   cell (i-1, j-1, k-1); nc, na, nb: the sweep's nodes left on each axis from the tile's
+//   first node.
+template <int Q>
+__device__ __forceinline__ void relax_tile(const FsmLaunch &p, float *Ts, const float *Ss,
+                                           const unsigned short *plane, const int *pstart, int lane, int t0, int dts,
+                                           int nc, int na, int nb)
+{
+    constexpr int sz = (Q & 1) ? -1 : 1, sy = (Q & 2) ? -1 : 1, sx = (Q & 4) ? -1 : 1;
+    constexpr int oz = sz, ox = sx * kPZ, oy = sy * kPZ * kPX;  // one step along the sweep
+    constexpr int cz = sz == 1 ? 0 : 1, cx = sx == 1 ? 0 : 1, cy = sy == 1 ? 0 : 1;
+    for (int w = 0; w < kNPlanes; w++) {
+        for (int m = pstart[w] + lane; m < pstart[w + 1]; m += 32) {
+            const unsigned e = plane[m];
+            const int c = (int)(e & 31u), a = (int)((e >> 5) & 7u), b = (int)(e >> 8);
+            if (c < nc && a < na && b < nb) {
+                const int tn = t0 + oz * c + ox * a + oy * b;
+                Ts[tn] = ngb_update_tile(p, Ts, tn, oz, ox, oy, Ss, tn - dts, cz, cx, cy);
+            }
+        }
+        __syncwarp();
+    }
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
@@ -436,7 +486,9 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
             if (lane == 0) item = ld_volatile(p.err) != 0u ? total : (int)atomicAdd(p.cursors + q, 1u);
             item = __shfl_sync(kFull, item, 0);
             if (item >= total) break;
-            // (diagonal, shot): the last table entry <= item (tab[lo] <= item < tab[hi])
+            // (diagonal, shot): the last table entry <= item (tab[lo] <= item < tab[hi]).  A
+            // warp-wide search (32 probes per step, 2-3 dependent loads instead of 12) measured
+            // 3 % slower on the config-2 batch: these loads are broadcasts that hit L1.
             int lo = 0, hi = nd * S;
             while (hi - lo > 1) {
                 const int mid = (lo + hi) >> 1;
@@ -508,35 +560,43 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
             const int tz = rz.di > 0 ? gz - 1 : gz, tx = rx.di > 0 ? gx - 1 : gx, ty = ry.di > 0 ? gy - 1 : gy;
             const float *T = p.T + sh.t_off;
             ShotGrid g{&sh, p.T + sh.t_off, 0, nxx, nyy, nzz};
-            // unrolled so that several iterations' loads are in flight before their shared-
-            // memory stores wait on them (config-2 batch: 58.3 ms against 62.0 rolled, 60.2
-            // unrolled 8)
-#pragma unroll 4
+            // The slowness goes by cp.async, so all its copies are in flight at once and hold
+            // no registers; the traveltime loop is unrolled so that several loads are in
+            // flight before their shared-memory stores wait on them.  Staged node m = lane +
+            // 32 it is (ci, cj, ck), advanced by 32 nodes per iteration without divisions.
+            static_assert(32 / kHZ + 1 <= kHX, "one carry into cj and one into ck per step");
+            int ci = lane % kHZ, cj = (lane / kHZ) % kHX, ck = lane / (kHZ * kHX);
+#pragma unroll kStageUnroll
             for (int m = lane; m < kHZ * kHX * kHY; m += 32) {
-                const int ci = m % kHZ, cj = (m / kHZ) % kHX, ck = m / (kHZ * kHX);
                 const int i = tz + ci, j = tx + cj, k = ty + ck;
+                cp_async4(Ss + ci + kPZ * (cj + kPX * ck), sptr(p, g, gz - 1 + ci, gx - 1 + cj, gy - 1 + ck));
                 Ts[ci + kPZ * (cj + kPX * ck)] = (i >= 0 && i < nzz && j >= 0 && j < nxx && k >= 0 && k < nyy)
                                                      ? __ldcg(T + i + (long long)j * nzz + (long long)k * nxx * nzz)
                                                      : 1e6f;
-                Ss[ci + kPZ * (cj + kPX * ck)] = sget(p, g, gz - 1 + ci, gx - 1 + cj, gy - 1 + ck);
+                ci += 32 % kHZ;
+                cj += 32 / kHZ;
+                if (ci >= kHZ) { ci -= kHZ; ++cj; }
+                if (cj >= kHX) { cj -= kHX; ++ck; }
             }
+            cp_async_wait_all();
             __syncwarp();
-            // one step against the sweep, per axis, in the tile's words
-            const int oz = sgz, ox = sgx * kPZ, oy = sgy * kPZ * kPX;
-            const int cz = sgz == 1 ? 0 : 1, cx = sgx == 1 ? 0 : 1, cy = sgy == 1 ? 0 : 1;
-            for (int w = 0; w < kNPlanes; w++) {
-                for (int m = pstart[w] + lane; m < pstart[w + 1]; m += 32) {
-                    const unsigned e = plane[m];
-                    const int lc = tc * kFsmTZ + (int)(e & 31u), la = ta * kFsmTX + (int)((e >> 5) & 7u),
-                              lb = tb * kFsmTY + (int)(e >> 8);
-                    if (lc < rz.L && la < rx.L && lb < ry.L) {
-                        const int i = rz.i0 + rz.di * lc, j = rx.i0 + rx.di * la, k = ry.i0 + ry.di * lb;
-                        const int tn = (i - tz) + kPZ * ((j - tx) + kPX * (k - ty));
-                        const int sn = (i - gz) + kPZ * ((j - gx) + kPX * (k - gy));  // cell (i-1, j-1, k-1)
-                        Ts[tn] = ngb_update_tile(p, Ts, tn, oz, ox, oy, Ss, sn, cz, cx, cy);
-                    }
-                }
-                __syncwarp();
+            // the tile's first node (c, a, b) = (0, 0, 0) in the traveltime tile, the offset of
+            // a node's cell (i-1, j-1, k-1) in the slowness tile from it, and the nodes left on
+            // each axis; the plane loop is specialised on the sweep's octant
+            const int i0 = rz.i0 + rz.di * tc * kFsmTZ, j0 = rx.i0 + rx.di * ta * kFsmTX,
+                      k0 = ry.i0 + ry.di * tb * kFsmTY;
+            const int t0 = (i0 - tz) + kPZ * ((j0 - tx) + kPX * (k0 - ty));
+            const int dts = (gz - tz) + kPZ * ((gx - tx) + kPX * (gy - ty));
+            const int nc = rz.L - tc * kFsmTZ, na = rx.L - ta * kFsmTX, nb = ry.L - tb * kFsmTY;
+            switch (q & 7) {
+            case 0: relax_tile<0>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 1: relax_tile<1>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 2: relax_tile<2>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 3: relax_tile<3>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 4: relax_tile<4>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 5: relax_tile<5>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 6: relax_tile<6>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            default: relax_tile<7>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
             }
             // the tile's nodes back to global memory, then its flag
             float *Tw = p.T + sh.t_off;
