@@ -194,5 +194,5 @@ def test_config3_iteration_vs_oracle_pipeline(tomo, oracle_mod, config3):
     xrel = float(np.linalg.norm(x_dev - x_or) / np.linalg.norm(x_or))
     print(f"config 3 iteration vs oracle pipeline: model RMS {rms_model:.3e}, update rel L2 {upd:.3e}, "
           f"CGLS x rel L2 {xrel:.3e}; update RMS {np.sqrt(np.mean((dv_or / start) ** 2)):.3e}")
-    assert rms_model < 5e-3  # the north star's bound on recovered models
+    assert rms_model < 5e-3  # recovered models within 0.5 % RMS
     assert upd < 0.1

@@ -9,7 +9,7 @@
     ReLU mask flipped by rounding moves a bias gradient by several per cent);
   * training on solver-generated fields lowers the loss;
   * the trained network's prediction, used as the ceiling of tomo_eik_solve_seeded, leaves
-    the solution unchanged (the plain solve judges it) -- and the test reports what it saves.
+    the solution unchanged (the plain solve checks it) -- and the test reports what it saves.
 """
 import numpy as np
 import pytest

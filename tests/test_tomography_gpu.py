@@ -243,7 +243,7 @@ def test_sparse_cgls_gpu_dense_columns(tomo, oracle_mod):
 
 def test_full_iteration_recovered_model(tomo, oracle_mod, small_survey):
     """Device iteration vs the oracle pipeline on the device traveltimes: recovered
-    velocity models agree within 0.5 % RMS; in practice ~1e-7."""
+    velocity models agree within 0.5 % RMS (the bound on recovered models); in practice ~1e-7."""
     sv = small_survey
     with tomo.Context(sv["nx"], sv["ny"], sv["nz"], sv["h"]) as c0:
         c0.set_velocity(sv["true_v"])

@@ -148,8 +148,8 @@ def test_smooth_deficit_over_config2_window_is_caught(big_case, deficit):
     relative amount that grows smoothly from 0 at the source to `deficit` at the far corner,
     i.e. only ~deficit / 300 between neighbouring nodes along a path -- under the 5e-7
     per-node deficit bar.  Every such node kept its ceiling, so the shots fall back and the
-    result is the plain field (tomo_eik_solve_seeded, the judge the INF seed of
-    block_FIM.cpp:295-369 is replaced under)."""
+    result is the plain field (tomo_eik_solve_seeded, the check under which the INF seed
+    of block_FIM.cpp:295-369 is replaced)."""
     sv, shots, ctx, plain, exact, ramp = big_case
     ss = _seeded_equals_plain(ctx, sv, shots, plain, exact * (1.0 - deficit * ramp))
     assert ss["stuck"] > 0
