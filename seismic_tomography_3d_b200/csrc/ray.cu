@@ -72,10 +72,12 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
             st = kRayOutside;  // receiver outside this shot's window
             L = p.max_steps;   // skip the march
         }
+        // grid node of the current position (least_squares.cpp:215-217 less the halo offset):
+        // the stall test of one step and the gradient stencil of the next use the same one
+        int iz = trunc_div(zi, p.dz), ix = trunc_div(xi, p.dx), iy = trunc_div(yi, p.dy);
         int cap = p.max_steps;
         if (p.smin && L == 0) {
-            const float t0 = t_exp(p.T, d, p.nz, trunc_div(zi, p.dz) + 1, trunc_div(xi, p.dx) + 1,
-                                   trunc_div(yi, p.dy) + 1);
+            const float t0 = t_exp(p.T, d, p.nz, iz + 1, ix + 1, iy + 1);
             const float smin = *p.smin;
             if (smin > 0.0f) {
                 const float c = t0 * (p.length_factor / (smin * rayStep)) + 256.0f;
@@ -84,7 +86,7 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
         }
         const float two_dz = fmul(2.0f, p.dz), two_dx = fmul(2.0f, p.dx), two_dy = fmul(2.0f, p.dy);
         while (L < cap) {
-            const int i = trunc_div(zi, p.dz) + 1, j = trunc_div(xi, p.dx) + 1, k = trunc_div(yi, p.dy) + 1;
+            const int i = iz + 1, j = ix + 1, k = iy + 1;
             const float dTz = fdiv(fsub(t_exp(p.T, d, p.nz, i + 1, j, k), t_exp(p.T, d, p.nz, i - 1, j, k)), two_dz);
             const float dTx = fdiv(fsub(t_exp(p.T, d, p.nz, i, j + 1, k), t_exp(p.T, d, p.nz, i, j - 1, k)), two_dx);
             const float dTy = fdiv(fsub(t_exp(p.T, d, p.nz, i, j, k + 1), t_exp(p.T, d, p.nz, i, j, k - 1)), two_dy);
@@ -96,6 +98,9 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
                 st = kRayNonFinite;
                 break;
             }
+            iz = trunc_div(zi, p.dz);
+            ix = trunc_div(xi, p.dx);
+            iy = trunc_div(yi, p.dy);
             const int im = trunc_div(zi, p.dzt), jm = trunc_div(fadd(xi, ox), p.dxt), km = trunc_div(fadd(yi, oy), p.dyt);
             if (im < 0 || im >= p.nzt || jm < 0 || jm >= p.nxt || km < 0 || km >= p.nyt) {
                 st = kRayOutside;
@@ -132,7 +137,7 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
                 st = kRayOk;
                 break;
             }
-            if (trunc_div(zi, p.dz) == snz && trunc_div(xi, p.dx) == snx && trunc_div(yi, p.dy) == sny) {
+            if (iz == snz && ix == snx && iy == sny) {
                 st = kRayStalled;
                 break;
             }
