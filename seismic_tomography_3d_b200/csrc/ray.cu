@@ -37,6 +37,36 @@ __device__ __forceinline__ float t_exp(const float *T, const ShotDesc &d, int nz
 
 __device__ __forceinline__ int trunc_div(float a, float b) { return (int)fdiv(a, b); }
 
+// A window-local node's offset in its shot's brick-major field is a sum of one part per
+// axis (t_node's brick index times 64 plus the node in the brick, split by axis).
+__device__ __forceinline__ int zpart(int z) { return ((z >> 2) << 6) + (z & 3); }
+__device__ __forceinline__ int xpart(const ShotDesc &d, int x) { return (((x >> 2) * d.nbz) << 6) + 4 * (x & 3); }
+__device__ __forceinline__ long long ypart(const ShotDesc &d, int y)
+{
+    return (((long long)(y >> 2) * d.nbz * d.nbx) << 6) + 16 * (y & 3);
+}
+
+// The six axis neighbours of expanded node (i, j, k), each read as t_exp reads it (clamped
+// per axis), from nine per-axis parts instead of six full index computations.
+__device__ __forceinline__ void t_stencil(const float *T, const ShotDesc &d, int nz, int i, int j, int k, float &zm,
+                                          float &zp, float &xm, float &xp, float &ym, float &yp)
+{
+    const float *Tb = T + d.t_off;
+    const int z0 = i - 1, x0 = j - 1, y0 = k - 1;
+    const int Zc = zpart(min(max(z0, 0), nz - 1)), Zm = zpart(min(max(z0 - 1, 0), nz - 1)),
+              Zp = zpart(min(max(z0 + 1, 0), nz - 1));
+    const int Xc = xpart(d, min(max(x0, 0), d.wnx - 1)), Xm = xpart(d, min(max(x0 - 1, 0), d.wnx - 1)),
+              Xp = xpart(d, min(max(x0 + 1, 0), d.wnx - 1));
+    const long long Yc = ypart(d, min(max(y0, 0), d.wny - 1)), Ym = ypart(d, min(max(y0 - 1, 0), d.wny - 1)),
+                    Yp = ypart(d, min(max(y0 + 1, 0), d.wny - 1));
+    zm = __ldg(Tb + Yc + (Zm + Xc));
+    zp = __ldg(Tb + Yc + (Zp + Xc));
+    xm = __ldg(Tb + Yc + (Zc + Xm));
+    xp = __ldg(Tb + Yc + (Zc + Xp));
+    ym = __ldg(Tb + Ym + (Zc + Xc));
+    yp = __ldg(Tb + Yp + (Zc + Xc));
+}
+
 }  // namespace
 
 __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
@@ -87,9 +117,11 @@ __global__ void __launch_bounds__(128) k_ray_march(RayLaunch p)
         const float two_dz = fmul(2.0f, p.dz), two_dx = fmul(2.0f, p.dx), two_dy = fmul(2.0f, p.dy);
         while (L < cap) {
             const int i = iz + 1, j = ix + 1, k = iy + 1;
-            const float dTz = fdiv(fsub(t_exp(p.T, d, p.nz, i + 1, j, k), t_exp(p.T, d, p.nz, i - 1, j, k)), two_dz);
-            const float dTx = fdiv(fsub(t_exp(p.T, d, p.nz, i, j + 1, k), t_exp(p.T, d, p.nz, i, j - 1, k)), two_dx);
-            const float dTy = fdiv(fsub(t_exp(p.T, d, p.nz, i, j, k + 1), t_exp(p.T, d, p.nz, i, j, k - 1)), two_dy);
+            float tzm, tzp, txm, txp, tym, typ;
+            t_stencil(p.T, d, p.nz, i, j, k, tzm, tzp, txm, txp, tym, typ);
+            const float dTz = fdiv(fsub(tzp, tzm), two_dz);
+            const float dTx = fdiv(fsub(txp, txm), two_dx);
+            const float dTy = fdiv(fsub(typ, tym), two_dy);
             const float norm = __fsqrt_rn(fadd(fadd(fmul(dTx, dTx), fmul(dTy, dTy)), fmul(dTz, dTz)));
             zi = fsub(zi, fdiv(fmul(rayStep, dTz), norm));
             xi = fsub(xi, fdiv(fmul(rayStep, dTx), norm));
