@@ -113,6 +113,11 @@ struct NgbIn {
 
 // Accurate_FSM::inner_sweep (accurate_FSM.cpp:159-265) from the minima on: the same
 // operations in the same order (this file is compiled with -fmad=false).
+// kBranchFree: every candidate is computed and kept only where the reference's test holds
+// (a NaN from a negative discriminant is dropped with it) -- the same values, without the
+// branches.  It pays where the warps wait on the wavefront (one shot) and costs where they
+// issue (batches, whose branches skip candidates no lane needs).
+template <bool kBranchFree = false>
 __device__ __forceinline__ float ngb_core(const FsmLaunch &p, const NgbIn &v)
 {
     const float tv = v.tv, te = v.te, tn = v.tn, tev = v.tev, ten = v.ten, tnv = v.tnv, tnve = v.tnve;
@@ -122,6 +127,41 @@ __device__ __forceinline__ float ngb_core(const FsmLaunch &p, const NgbIn &v)
     const float t1D3 = tn + p.dy * v.m3;
     const float t1D = smin(t1D1, smin(t1D2, t1D3));
 
+    if (kBranchFree) {
+        float Sref = v.r1;
+        float ta = tev + te - tv;
+        float tb = tev - te + tv;
+        float cand = ((tb * dz2i + ta * dx2i) +
+                      sqrtf(4.0f * Sref * Sref * (dz2i + dx2i) - dz2i * dx2i * (ta - tb) * (ta - tb))) /
+                     (dz2i + dx2i);
+        const float c2D1 = ((tv < te + p.dx * Sref) && (te < tv + p.dz * Sref)) ? cand : 1e6f;
+        Sref = v.r2;
+        ta = tv - tn + tnv;
+        tb = tn - tv + tnv;
+        cand = ((ta * dz2i + tb * dy2i) +
+                sqrtf(4.0f * Sref * Sref * (dz2i + dy2i) - dz2i * dy2i * (ta - tb) * (ta - tb))) /
+               (dz2i + dy2i);
+        const float c2D2 = ((tv < tn + p.dy * Sref) && (tn < tv + p.dz * Sref)) ? cand : 1e6f;
+        Sref = v.r3;
+        ta = te - tn + ten;
+        tb = tn - te + ten;
+        cand = ((ta * dx2i + tb * dy2i) +
+                sqrtf(4.0f * Sref * Sref * (dx2i + dy2i) - dx2i * dy2i * (ta - tb) * (ta - tb))) /
+               (dx2i + dy2i);
+        const float c2D3 = ((te < tn + p.dy * Sref) && (tn < te + p.dx * Sref)) ? cand : 1e6f;
+        const float c2D = smin(c2D1, smin(c2D2, c2D3));
+        Sref = v.r0;
+        ta = te - 0.5f * tn + 0.5f * ten - 0.5f * tv + 0.5f * tev - tnv + tnve;
+        tb = tv - 0.5f * tn + 0.5f * tnv - 0.5f * te + 0.5f * tev - ten + tnve;
+        const float tc = tn - 0.5f * te + 0.5f * ten - 0.5f * tv + 0.5f * tnv - tev + tnve;
+        const float t2 = 9.0f * Sref * Sref * p.dsum;
+        const float t3 =
+            p.dz2dx2 * (ta - tb) * (ta - tb) + p.dz2dy2 * (tb - tc) * (tb - tc) + p.dx2dy2 * (ta - tc) * (ta - tc);
+        const float t1 = tb * dz2i + ta * dx2i + tc * dy2i;
+        cand = (t1 + sqrtf(t2 - t3)) / p.dsum;
+        const float c3D = (smin(t1D, c2D) > smax(tv, smax(te, tn)) && t2 >= t3) ? cand : 1e6f;
+        return smin(v.self, smin(t1D, smin(c2D, c3D)));
+    }
     float t2D1 = 1e6f, t2D2 = 1e6f, t2D3 = 1e6f, ta, tb, tc, Sref;
     Sref = v.r1;
     if ((tv < te + p.dx * Sref) && (te < tv + p.dz * Sref)) {
@@ -346,6 +386,7 @@ static_assert(kPZ >= kHZ && kPX >= kHX, "padded strides");
 //   Tt + tb: the node in the traveltime tile; oz, ox, oy: word offsets of one step against
 //   the sweep along z, x, y;  St + sb: cell (i-1, j-1, k-1) in the slowness tile;
 //   cz, cx, cy: 1 - sgnv of each axis (the cube index of i1, j1, k1).
+template <bool kBranchFree>
 __device__ __forceinline__ float ngb_update_tile(const FsmLaunch &p, const float *Tt, int tb, int oz, int ox, int oy,
                                                  const float *St, int sb, int cz, int cx, int cy)
 {
@@ -367,7 +408,7 @@ __device__ __forceinline__ float ngb_update_tile(const FsmLaunch &p, const float
     v.r2 = smin(C(cz, 0, cy), C(cz, 1, cy));
     v.r3 = smin(C(0, cx, cy), C(1, cx, cy));
     v.r0 = C(cz, cx, cy);
-    return ngb_core(p, v);
+    return ngb_core<kBranchFree>(p, v);
 }
 
 // Asynchronous 4-byte copy global -> shared (cp.async, through L1).  Only for the slowness,
@@ -389,7 +430,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //   t0: the tile's node (0, 0, 0) in Ts; dts: Ts word of a node minus the Ss word of its
 //   cell (i-1, j-1, k-1); nc, na, nb: the sweep's nodes left on each axis from the tile's
 //   first node.
-template <int Q>
+template <int Q, bool kBranchFree>
 __device__ __forceinline__ void relax_tile(const FsmLaunch &p, float *Ts, const float *Ss,
                                            const unsigned short *plane, const int *pstart, int lane, int t0, int dts,
                                            int nc, int na, int nb)
@@ -403,7 +444,7 @@ __device__ __forceinline__ void relax_tile(const FsmLaunch &p, float *Ts, const 
             const int c = (int)(e & 31u), a = (int)((e >> 5) & 7u), b = (int)(e >> 8);
             if (c < nc && a < na && b < nb) {
                 const int tn = t0 + oz * c + ox * a + oy * b;
-                Ts[tn] = ngb_update_tile(p, Ts, tn, oz, ox, oy, Ss, tn - dts, cz, cx, cy);
+                Ts[tn] = ngb_update_tile<kBranchFree>(p, Ts, tn, oz, ox, oy, Ss, tn - dts, cz, cx, cy);
             }
         }
         __syncwarp();
@@ -432,6 +473,7 @@ __device__ __forceinline__ int tile_lo(const FsmRange &r, int l0, int T)
 
 }  // namespace
 
+template <bool kBranchFree>
 __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
 {
     extern __shared__ float smem[];
@@ -589,14 +631,14 @@ __global__ void __launch_bounds__(256, 2) k_fsm_tiled(FsmLaunch p)
             const int dts = (gz - tz) + kPZ * ((gx - tx) + kPX * (gy - ty));
             const int nc = rz.L - tc * kFsmTZ, na = rx.L - ta * kFsmTX, nb = ry.L - tb * kFsmTY;
             switch (q & 7) {
-            case 0: relax_tile<0>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
-            case 1: relax_tile<1>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
-            case 2: relax_tile<2>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
-            case 3: relax_tile<3>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
-            case 4: relax_tile<4>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
-            case 5: relax_tile<5>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
-            case 6: relax_tile<6>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
-            default: relax_tile<7>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 0: relax_tile<0, kBranchFree>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 1: relax_tile<1, kBranchFree>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 2: relax_tile<2, kBranchFree>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 3: relax_tile<3, kBranchFree>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 4: relax_tile<4, kBranchFree>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 5: relax_tile<5, kBranchFree>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            case 6: relax_tile<6, kBranchFree>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
+            default: relax_tile<7, kBranchFree>(p, Ts, Ss, plane, pstart, lane, t0, dts, nc, na, nb); break;
             }
             // the tile's nodes back to global memory, then its flag
             float *Tw = p.T + sh.t_off;
@@ -648,21 +690,24 @@ cudaError_t fsm_solve_tiled(const FsmLaunch &p, int *grid_out, cudaStream_t st)
     constexpr int threads = 256;
     const size_t smem = (size_t)(threads / 32) * 2 * kHN * sizeof(float) + kTileN * sizeof(unsigned short) +
                         (kNPlanes + 1) * sizeof(int);
-    cudaError_t e = cudaFuncSetAttribute(k_fsm_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // one shot: the branch-free operator (bound by the wavefront's waits); batches: the
+    // branching one (config 1 11.4 vs 11.9 ms; config-2 batch 52.3 vs 48.6 ms)
+    const void *fn = p.nshots == 1 ? (const void *)k_fsm_tiled<true> : (const void *)k_fsm_tiled<false>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, nsm = 0, per_sm = 0;
     e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fsm_tiled, threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int grid = nsm * per_sm;
     if (grid_out) *grid_out = grid;
     FsmLaunch pp = p;
     void *args[] = {&pp};
-    return cudaLaunchCooperativeKernel((const void *)k_fsm_tiled, dim3(grid), dim3(threads), args, smem, st);
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, smem, st);
 }
 
 }  // namespace tomo
