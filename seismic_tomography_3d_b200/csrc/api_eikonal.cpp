@@ -598,8 +598,14 @@ int upload_batch(tomo_ctx *ctx, const Batch &bt, int nrec, const tomo_point *rec
     CK(ctx->qflag.ensure((size_t)bt.q_total));
     CK(ctx->qflag8.ensure((size_t)bt.q_total8));
     CK(ctx->lists.ensure((size_t)bt.q_total * 3));
+    // Receivers and shot descriptors equal to what the device buffers already hold (the same
+    // survey solved again, as in every iteration of an inversion) are not uploaded again: a
+    // copy from pageable memory also waits for the stream's earlier work.  A buffer that is
+    // (re)allocated here holds nothing yet.
+    if (ctx->shots_d.cap < (size_t)nshots) ctx->sd_up.clear();
     CK(ctx->shots_d.ensure((size_t)nshots));
     if (nrec > 0) {
+        if (ctx->rec.cap < (size_t)nrec * 3) ctx->rec_up.clear();
         CK(ctx->rec.ensure((size_t)nrec * 3));
         CK(ctx->t_recv.ensure((size_t)nshots * nrec));
         std::vector<float> rh((size_t)nrec * 3);
@@ -608,10 +614,19 @@ int upload_batch(tomo_ctx *ctx, const Batch &bt, int nrec, const tomo_point *rec
             rh[(size_t)nrec + r] = receivers[r].y;
             rh[(size_t)2 * nrec + r] = receivers[r].z;
         }
-        CK(cudaMemcpyAsync(ctx->rec.ptr, rh.data(), rh.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        if (rh != ctx->rec_up) {
+            ctx->rec_up.clear();
+            CK(cudaMemcpyAsync(ctx->rec.ptr, rh.data(), rh.size() * sizeof(float), cudaMemcpyHostToDevice,
+                               ctx->stream));
+            ctx->rec_up = std::move(rh);
+        }
     }
-    CK(cudaMemcpyAsync(ctx->shots_d.ptr, bt.sd.data(), bt.sd.size() * sizeof(ShotDesc), cudaMemcpyHostToDevice,
-                       ctx->stream));
+    const size_t sd_bytes = bt.sd.size() * sizeof(ShotDesc);
+    if (ctx->sd_up.size() != bt.sd.size() || std::memcmp(ctx->sd_up.data(), bt.sd.data(), sd_bytes) != 0) {
+        ctx->sd_up.clear();
+        CK(cudaMemcpyAsync(ctx->shots_d.ptr, bt.sd.data(), sd_bytes, cudaMemcpyHostToDevice, ctx->stream));
+        ctx->sd_up = bt.sd;
+    }
     return TOMO_OK;
 }
 

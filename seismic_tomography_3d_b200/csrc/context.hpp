@@ -89,6 +89,10 @@ struct tomo_ctx {
     tomo::DevBuf<float> rec;       // 3*nrec: x | y | z
     tomo::DevBuf<float> t_recv;    // nshots*nrec
     std::vector<tomo_point> rec_h;
+    // what `rec` and `shots_d` hold on the device (as last uploaded), so that a batch with
+    // the same receivers or descriptors as the previous call is not uploaded again
+    std::vector<float> rec_up;
+    std::vector<tomo::ShotDesc> sd_up;
     int nshots = 0, nrec = 0;
     bool have_solve = false;
     // launch shape chosen by tomo_eik_autotune (0: not tuned)
