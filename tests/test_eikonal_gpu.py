@@ -429,3 +429,26 @@ def test_pair_schedule_unaligned_windows(tomo, oracle_mod):
         for i in range(len(sv.shots)):
             Tref = solve_oracle(oracle_mod, sv.velocity, sv.h, sv.shots[i], wins[i])
             assert rel_err(ctx.eik_volume(i), Tref, sv.h, sv.velocity.max()) < REL_TOL, i
+
+
+def test_repeated_batches_change_receivers_and_shots(tomo):
+    """A context keeps the receivers and shot descriptors of the last batch on the device and
+    uploads a batch's only when they differ: after solves with other receivers, other shots
+    and other windows (same counts), each result equals the same solve in a fresh context."""
+    nx, ny, nz, h = 29, 27, 14, 25.0
+    sv_a = wl.small(61, nx, ny, nz, h=h, nshots=4, windows=True, nrec=20)
+    sv_b = wl.small(62, nx, ny, nz, h=h, nshots=4, windows=True, nrec=20)
+    rec_a = sv_a.receivers
+    rec_b = rec_a.copy()
+    rec_b[:, 0] = np.minimum(rec_b[:, 0] + np.float32(h / 3), np.float32((nx - 1) * h))
+    steps = [(sv_a.shots, sv_a.windows, rec_a), (sv_a.shots, sv_a.windows, rec_b),
+             (sv_b.shots, sv_b.windows, rec_b), (sv_b.shots, None, rec_b), (sv_a.shots, sv_a.windows, rec_a)]
+    kw = dict(change_tol=-1.0, inner_tol=0.0)  # converged fields: no schedule-level rounding
+    with tomo.Context(nx, ny, nz, h) as ctx:
+        ctx.set_velocity(sv_a.velocity)
+        for shots, wins, rec in steps:
+            t, _ = ctx.eik_solve(shots, windows=wins, receivers=rec, **kw)
+            with tomo.Context(nx, ny, nz, h) as fresh:
+                fresh.set_velocity(sv_a.velocity)
+                t_ref, _ = fresh.eik_solve(shots, windows=wins, receivers=rec, **kw)
+            np.testing.assert_allclose(t, t_ref, rtol=1e-5, atol=0)
