@@ -14,6 +14,10 @@
   banded tolerances, rays, Tikhonov, CGLS with the reference's 10 iterations, model update
   with smoothing) against the oracle pipeline run from its own FP64 fields
   (least_squares.cpp:163-570): recovered models within 0.5 % RMS.
+* Config 5 (401 x 401 x 201, 256 shots x 10,000 receivers): all shots solved and
+  ray-traced in one context; the first and the last shot's fields against the FP64
+  oracle and their Jacobian rows bit for bit against the oracle's ray tracer.  The
+  oracle pipeline over all 256 shots (hours on the host) is left to config 3.
 
 The oracle runs on the host's cores in threads (its C routines release the GIL).
 """
@@ -196,3 +200,53 @@ def test_config3_iteration_vs_oracle_pipeline(tomo, oracle_mod, config3):
           f"CGLS x rel L2 {xrel:.3e}; update RMS {np.sqrt(np.mean((dv_or / start) ** 2)):.3e}")
     assert rms_model < 5e-3  # recovered models within 0.5 % RMS
     assert upd < 0.1
+
+
+def test_config5_first_and_last_shot_vs_oracle(tomo, oracle_mod):
+    """Config 5 (401 x 401 x 201 at 10 m, 256 full-window shots x 10,000 receivers, 50 m
+    cells) solved and ray-traced in one context, as the inversion does: all 256 shots at the
+    banded timed tolerances on the layered true model, then the whole Jacobian.  The first
+    and the last shot are checked against the oracle.  The last shot's field starts
+    8.5 G nodes into the traveltime pool, past 32-bit offsets.
+      * fields: the FP64 fixed point of the Block_FIM operator on the whole grid
+        (cuda_kernel.cu:217-248), <= 1e-4 relative on nodes with T >= 2h/v_max;
+      * rays: status and every row of G bit for bit against the oracle's ray tracer on the
+        device's own field (least_squares.cpp:192-280), with one explicit step cap on both
+        sides (the device's default cap follows each ray's traveltime instead)."""
+    sv, _, inv = wl.config5_inversion()
+    nrec, ns = len(sv.receivers), len(sv.shots)
+    d = inv["d_tomo"]
+    nt = _n_tomo(sv, d)
+    cap = 20000
+    picks = (0, ns - 1)
+    with tomo.Context(sv.nx, sv.ny, sv.nz, sv.h) as ctx:
+        ctx.set_velocity(sv.velocity)
+        ctx.eik_solve(sv.shots, receivers=sv.receivers, want_recv=False, **wl.TIMED_TOLERANCES_BANDED)
+        jst = ctx.build_jacobian(d, inv["tk_order"], inv["tk_param"], max_ray_steps=cap)
+        rp, cols, vals = ctx.jacobian()
+        status = ctx.ray_status()
+        vols = [ctx.eik_volume(i) for i in picks]
+    assert jst["rays"] == ns * nrec
+    vmax = float(sv.velocity.max())
+    s = (np.float32(1.0) / sv.velocity).astype(np.float32)
+
+    def check(k):
+        i = picks[k]
+        T = vols[k]
+        Tref, _ = oracle_mod.fim_jw(s, sv.h, tuple(map(float, sv.shots[i])))
+        m = Tref >= 2.0 * sv.h / vmax
+        err = float(np.max(np.abs(T[m] - Tref[m]) / Tref[m]))
+        rt = oracle_mod.raytrace(T, sv.h, sv.shots[i], *sv.receivers.T, d, nt, cap)
+        return err, rt
+
+    with cf.ThreadPoolExecutor(len(picks)) as ex:
+        res = list(ex.map(check, range(len(picks))))
+    for (err, rt), i in zip(res, picks):
+        lo, hi = i * nrec, (i + 1) * nrec
+        print(f"config 5 shot {i}: field max rel err {err:.2e} vs FP64 oracle; "
+              f"{int(rp[hi] - rp[lo])} ray non-zeros")
+        assert err <= REL_TOL, (i, err)
+        np.testing.assert_array_equal(status[lo:hi], rt["status"])
+        np.testing.assert_array_equal(np.diff(rp[lo:hi + 1]), np.diff(rt["row_ptr"]))
+        np.testing.assert_array_equal(cols[rp[lo]:rp[hi]], rt["cols"])
+        np.testing.assert_array_equal(vals[rp[lo]:rp[hi]], rt["vals"])
