@@ -45,6 +45,9 @@ constexpr size_t kOffC = kOffL + 3 * 4 * kStaticBricks;       // control words
 constexpr size_t kOffStats = kOffC + 256;                     // activation counters
 constexpr size_t kOffDesc = kOffStats + 256;                  // the shot descriptor
 constexpr size_t kStaticBytes = kOffDesc + 256;
+static_assert(kCtrlWords * sizeof(unsigned) <= 256, "control words overflow their slot");
+static_assert(4 * sizeof(unsigned long long) <= 256, "activation counters overflow their slot");
+static_assert(sizeof(ShotDesc) <= 256, "shot descriptor overflows its slot");
 
 static __device__ __align__(256) unsigned char g_eik_scratch[kStaticBytes];
 
