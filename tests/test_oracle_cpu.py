@@ -188,3 +188,37 @@ def test_gaussian_identity_and_sum(oracle_mod):
     c = np.ones((9, 9, 9), np.float32)
     out = oracle_mod.gaussian(c, 5, 2.0)
     assert np.allclose(out, 1.0, atol=1e-6)
+
+
+def test_linear_gradient_analytic_bounds(oracle_mod):
+    """v(z) = v0 + g z (the config-1 gradient) against its analytic first arrival
+    T = acosh(1 + g^2 r^2 / (2 v_src v)) / g, on nodes with T >= 2h/v_max: the FP64 JW
+    oracle (cuda_kernel.cu:217-248) and, where built, the reference's own Accurate_FSM
+    (accurate_FSM.cpp:577-650) and Podvin-Lecomte (classic.cpp:184-1842).  Sanity bounds
+    about 1.5x the measured errors (JW mean 5.9 %, FSM 0.9 %, P-L 2.4 %), not parity: the
+    first-order JW scheme is the least accurate of the three and errs most next to the
+    point source."""
+    nx, ny, nz, h, v0, g = 41, 41, 21, 25.0, 1500.0, 0.6
+    z = np.arange(nz) * h
+    v = np.ascontiguousarray(np.broadcast_to((v0 + g * z)[None, None, :], (ny, nx, nz)), np.float32)
+    src = (500.0, 500.0, 0.0)
+    Y, X, Z = np.meshgrid(np.arange(ny) * h, np.arange(nx) * h, z, indexing="ij")
+    r2 = (X - src[0]) ** 2 + (Y - src[1]) ** 2 + (Z - src[2]) ** 2
+    Ta = np.arccosh(1.0 + g * g * r2 / (2.0 * (v0 + g * src[2]) * (v0 + g * Z))) / g
+    m = Ta >= 2.0 * h / float(v.max())
+    far = Ta >= 0.5 * Ta.max()
+
+    def rel(T, mask):
+        return (T[mask] - Ta[mask]) / Ta[mask]
+
+    T, _ = oracle_mod.fim_jw((np.float32(1.0) / v).astype(np.float32), h, src)
+    e = rel(T, m)
+    assert np.mean(np.abs(e)) < 0.08 and e.max() < 0.4 and e.min() > -0.01
+    assert np.mean(np.abs(rel(T, far))) < 0.07
+    if not oracle_mod.have_ref():
+        pytest.skip("oracle/_ref (the reference's own solvers) not built")
+    shot = np.array([src], np.float32)
+    for kind, mean_b, max_b in ((oracle_mod.REF_FSM, 0.012, 0.05), (oracle_mod.REF_CLASSIC, 0.035, 0.1)):
+        Tr, _ = oracle_mod.ref_solve(kind, v, h, shot)
+        e = rel(Tr[0], m)
+        assert np.mean(np.abs(e)) < mean_b and e.max() < max_b and e.min() > -1e-3, (kind, e.min(), e.max())
