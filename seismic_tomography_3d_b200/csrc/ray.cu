@@ -267,12 +267,15 @@ __global__ void __launch_bounds__(32 * kSortWarps) k_ray_sort(RayLaunch p)
 // Values of the run-length entries: the reference accumulates rayStep once per step by
 // repeated FP32 addition, starting from rayStep; the first (smallest) cell gets one extra
 // step and the source cell gets the final distance to the source (:243-276).
+// One warp per ray, a lane per run: each run's chain of additions is its own, so the values
+// are those of a serial pass, and the run reads and row writes are contiguous.
 __global__ void __launch_bounds__(128) k_ray_emit(RayLaunch p, const int *row_ptr, int *cols, float *vals)
 {
     const long long nrays = (long long)p.nshots * p.nrec;
     const float rayStep = fmul(0.2f, p.dz);
-    for (long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x; ray < nrays;
-         ray += (long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long ray = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; ray < nrays; ray += nwarps) {
         const int s = (int)(ray / p.nrec);
         const float sxg = p.spos[s], syg = p.spos[p.nshots + s], sz = p.spos[2 * p.nshots + s];
         const int sId = trunc_div(sz, p.dzt) + trunc_div(sxg, p.dxt) * p.nzt + trunc_div(syg, p.dyt) * p.nxt * p.nzt;
@@ -280,7 +283,7 @@ __global__ void __launch_bounds__(128) k_ray_emit(RayLaunch p, const int *row_pt
         const int n = p.nuniq[ray];
         const int base = row_ptr[ray];
         const float fd = p.final_dist[ray];
-        for (int k = 0; k < n; k++) {
+        for (int k = lane; k < n; k += 32) {
             const uint2 e = runs[k];
             float v = rayStep;
             const unsigned adds = (k == 0) ? e.y : e.y - 1u;
@@ -317,14 +320,19 @@ __global__ void k_tk_rows(int n_data_rows, const long long *sizes, int n_model, 
     }
 }
 
+// One warp per row, lanes over its entries (contiguous stores).
 __global__ void k_transpose_prepare(const int *row_ptr, const int *cols, int nrows, int *keys, int *pos, int *rows_of)
 {
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x)
-        for (int k = row_ptr[r]; k < row_ptr[r + 1]; k++) {
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; r < nrows; r += nwarps) {
+        const int e = row_ptr[r + 1];
+        for (int k = row_ptr[r] + lane; k < e; k += 32) {
             keys[k] = cols[k];
             pos[k] = k;
-            rows_of[k] = r;
+            rows_of[k] = (int)r;
         }
+    }
 }
 
 // Sort padding: entries [nnz, cap) get the key ncols (after every column) and their own
@@ -381,7 +389,7 @@ cudaError_t ray_sort(const RayLaunch &p, cudaStream_t st)
 
 cudaError_t ray_emit(const RayLaunch &p, const int *row_ptr, int *cols, float *vals, cudaStream_t st)
 {
-    k_ray_emit<<<grid_for((long long)p.nshots * p.nrec, 128), 128, 0, st>>>(p, row_ptr, cols, vals);
+    k_ray_emit<<<grid_for(32LL * p.nshots * p.nrec, 128), 128, 0, st>>>(p, row_ptr, cols, vals);
     return cudaGetLastError();
 }
 
@@ -409,7 +417,7 @@ cudaError_t csr_transpose_prepare(const int *row_ptr, const int *cols, int nrows
                                   int *rows_of, cudaStream_t st)
 {
     (void)nnz;
-    k_transpose_prepare<<<grid_for(nrows, 256), 256, 0, st>>>(row_ptr, cols, nrows, keys, pos, rows_of);
+    k_transpose_prepare<<<grid_for(32LL * nrows, 256), 256, 0, st>>>(row_ptr, cols, nrows, keys, pos, rows_of);
     return cudaGetLastError();
 }
 
