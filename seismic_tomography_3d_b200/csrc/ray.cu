@@ -248,18 +248,23 @@ __global__ void __launch_bounds__(32 * kSortWarps) k_ray_sort(RayLaunch p)
                 }
                 __syncwarp();
             }
+        // Merge equal cells, 32 sorted entries at a time: an entry that starts a new cell sums
+        // the step counts of the equal entries after it (integers: the order does not matter)
+        // and goes to the slot that the cells before it leave.
         int w = 0;
-        if (lane == 0) {
-            for (int a = 0; a < n; a++) {
-                const uint2 e = buf[a];
-                if (w > 0 && buf[w - 1].x == e.x) buf[w - 1].y += e.y;
-                else buf[w++] = e;
+        for (int b = 0; b < n; b += 32) {
+            const int i = b + lane;
+            const uint2 e = i < n ? buf[i] : make_uint2(0xffffffffu, 0u);
+            const bool head = i < n && (i == 0 || buf[i - 1].x != e.x);
+            const unsigned hm = __ballot_sync(0xffffffffu, head);
+            if (head) {
+                unsigned y = e.y;
+                for (int j = i + 1; j < n && buf[j].x == e.x; ++j) y += buf[j].y;
+                runs[w + __popc(hm & ((1u << lane) - 1u))] = make_uint2(e.x, y);
             }
-            p.nuniq[ray] = w;
+            w += __popc(hm);
         }
-        w = __shfl_sync(0xffffffffu, w, 0);
-        __syncwarp();
-        for (int i = lane; i < w; i += 32) runs[i] = buf[i];
+        if (lane == 0) p.nuniq[ray] = w;
         __syncwarp();
     }
 }
